@@ -1,0 +1,1117 @@
+// Host runtime and C ABI of the B200 HIT_Solver backend (see include/hitb200.h).
+//
+// A plan owns one device arena holding every scratch buffer of its solve,
+// the per-solve descriptor (SolveDev) and the CTA work lists of each kernel.
+// Launch sequences mirror the reference's loop body; every scalar the
+// reference pulls to the host (dt, Lax-Friedrichs speeds, sensor rms, Mach,
+// forcing power) stays in the device scalar block.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/hitb200.h"
+#include "common.cuh"
+#include "kernels_reduce.cuh"
+#include "kernels_stencil.cuh"
+
+using namespace hitb200;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int cuda_fail(cudaError_t e, const char* what) {
+  g_last_error = std::string(what) + ": " + cudaGetErrorString(e);
+  return e == cudaErrorMemoryAllocation ? HITB200_ERR_OOM : HITB200_ERR_CUDA;
+}
+#define HB_CUDA(call)                                  \
+  do {                                                 \
+    cudaError_t e_ = (call);                           \
+    if (e_ != cudaSuccess) return cuda_fail(e_, #call); \
+  } while (0)
+#define HB_LAUNCHED(name)                                    \
+  do {                                                       \
+    cudaError_t e_ = cudaGetLastError();                     \
+    if (e_ != cudaSuccess) return cuda_fail(e_, name);       \
+  } while (0)
+
+int invalid(const std::string& msg) {
+  g_last_error = msg;
+  return HITB200_ERR_INVALID;
+}
+
+bool is_none(double v) { return std::isnan(v); }
+
+// numpy.fft.fftfreq integer bins of an n-point transform.
+int fft_bin(int j, int n) {
+  const int half = (n - 1) / 2 + 1;
+  return j < half ? j : j - n;
+}
+// 2 pi fftfreq(n, d)[j] evaluated the way numpy does (bin * (1 / (n d))).
+double wavenumber(int m, int n, double d) { return 2.0 * M_PI * ((double)m * (1.0 / ((double)n * d))); }
+
+struct Arena {
+  size_t off = 0;
+  size_t take(size_t bytes) {
+    const size_t o = off;
+    off += (bytes + 255) & ~(size_t)255;
+    return o;
+  }
+};
+
+struct ModeTables {
+  std::vector<int2> drag, force;
+  std::vector<double2> kvec;
+  std::vector<int> partner;
+};
+
+ModeTables build_modes(const hitb200_desc& d) {
+  ModeTables t;
+  const double dx = (d.x_max - d.x_min) / d.nx, dy = (d.y_max - d.y_min) / d.ny;
+  for (int jy = 0; jy < d.ny; ++jy)
+    for (int jx = 0; jx < d.nx; ++jx) {
+      const int mx = fft_bin(jx, d.nx), my = fft_bin(jy, d.ny);
+      const double kx = wavenumber(mx, d.nx, dx), ky = wavenumber(my, d.ny, dy);
+      const double k2 = kx * kx + ky * ky;
+      const double mag = std::sqrt(k2);
+      if (d.periodic && d.drag_coefficient > 0.0 && d.drag_kmax > 0.0 && mag >= 0.0 && k2 > 0.0 &&
+          mag <= d.drag_kmax)
+        t.drag.push_back(make_int2(mx, my));
+      if (d.periodic && d.forcing_on && mag >= d.forcing_kmin && mag <= d.forcing_kmax && mag > 0.0) {
+        t.force.push_back(make_int2(mx, my));
+        t.kvec.push_back(make_double2(kx, ky));
+      }
+    }
+  t.partner.assign(kMaxForce, 0);
+  for (size_t i = 0; i < t.force.size(); ++i) {
+    const int px = fft_bin(((-t.force[i].x) % d.nx + d.nx) % d.nx, d.nx);
+    const int py = fft_bin(((-t.force[i].y) % d.ny + d.ny) % d.ny, d.ny);
+    int p = (int)i;
+    for (size_t k = 0; k < t.force.size(); ++k)
+      if (t.force[k].x == px && t.force[k].y == py) p = (int)k;
+    t.partner[i] = p;
+  }
+  return t;
+}
+
+int lines_per_cta(int n, int nlines, int elem) {
+  // Largest R in {8, 4, 2, 1} that fits the warp task budget and ~100 KB of
+  // shared memory, preferring at least 2 CTAs per SM worth of lines.
+  const int tpl = (n + kNodesPerTask - 1) / kNodesPerTask;
+  int best = 1;
+  for (int R : {8, 4, 2, 1}) {
+    if (R * tpl > kMaxTasks * (kStencilThreads / 32)) continue;
+    const size_t b = elem == 4 ? SweepLayout<float>(n, R).bytes() : SweepLayout<double>(n, R).bytes();
+    if (b > 110 * 1024) continue;
+    if ((nlines + R - 1) / R < 2 * 148 && R > 1) continue;
+    best = R;
+    break;
+  }
+  return best;
+}
+
+int mch_for(int n) {
+  const int m = (n + 31) / 32;
+  return m <= 4 ? 4 : m <= 8 ? 8 : m <= 16 ? 16 : 32;
+}
+
+}  // namespace
+
+struct hitb200_plan {
+  hitb200_desc desc{};
+  SolveDev hs{};            // host copy of the device descriptor
+  SolveDev* d_solve = nullptr;
+  unsigned char* arena = nullptr;
+  size_t arena_bytes = 0;
+  Work* d_tiles = nullptr;
+  Work* d_xlines = nullptr;
+  Work* d_ylines = nullptr;
+  int* d_partner = nullptr;
+  int n_tiles = 0, n_x = 0, n_y = 0, Rx = 1, Ry = 1;
+  int elem = 8;
+  size_t smem_x = 0, smem_y = 0, smem_sensor = 0;
+  // graph replay of hitb200_step
+  cudaGraphExec_t graph = nullptr;
+  cudaStream_t graph_stream = nullptr;
+  const double* graph_q = nullptr;
+  bool in_batch = false;
+};
+
+struct hitb200_batch {
+  std::vector<hitb200_plan*> plans;
+  SolveDev* d_solves = nullptr;
+  Work *d_tiles = nullptr, *d_xlines = nullptr, *d_ylines = nullptr;
+  int* d_partner = nullptr;
+  int n_tiles = 0, n_x = 0, n_y = 0, elem = 8, mch_x = 4, mch_y = 4;
+  size_t smem_x = 0, smem_y = 0, smem_sensor = 0;
+  int any_outflow = 0, any_forcing = 0, any_hv = 0, any_noise_upload = 0;
+  cudaGraphExec_t graph = nullptr;
+  cudaStream_t graph_stream = nullptr;
+};
+
+namespace {
+
+// ---- launch helpers shared by plans and batches ----------------------------------
+struct LaunchSet {
+  const SolveDev* solves;
+  int nsolves;
+  const Work *tiles, *xl, *yl;
+  const int* partner;
+  int n_tiles, n_x, n_y, elem, mch_x, mch_y;
+  size_t smem_x, smem_y, smem_sensor;
+  cudaStream_t st;
+};
+
+template <typename T, int AXIS, int MCH>
+void set_sweep_attr(size_t bytes) {
+  static size_t done = 0;
+  if (bytes > done) {
+    cudaFuncSetAttribute(sweep_kernel<T, AXIS, MCH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)bytes);
+    done = bytes;
+  }
+}
+
+template <typename T>
+void set_sensor_attr(size_t bytes) {
+  static size_t done = 0;
+  if (bytes > done) {
+    cudaFuncSetAttribute(sensor_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    done = bytes;
+  }
+}
+
+template <typename T, int AXIS>
+void launch_sweep_t(const LaunchSet& L, int stage, int mode, const Bind& b) {
+  const int mch = AXIS == 0 ? L.mch_x : L.mch_y;
+  const int nb = AXIS == 0 ? L.n_x : L.n_y;
+  const size_t sm = AXIS == 0 ? L.smem_x : L.smem_y;
+  const Work* w = AXIS == 0 ? L.xl : L.yl;
+#define HB_SWEEP(M)                                                                   \
+  case M:                                                                             \
+    set_sweep_attr<T, AXIS, M>(sm);                                                   \
+    sweep_kernel<T, AXIS, M><<<nb, kStencilThreads, sm, L.st>>>(L.solves, w, stage, mode, b); \
+    break;
+  switch (mch) {
+    HB_SWEEP(4)
+    HB_SWEEP(8)
+    HB_SWEEP(16)
+    HB_SWEEP(32)
+  }
+#undef HB_SWEEP
+}
+
+void launch_sweep(const LaunchSet& L, int axis, int stage, int mode, const Bind& b) {
+  if (L.elem == 4)
+    axis == 0 ? launch_sweep_t<float, 0>(L, stage, mode, b) : launch_sweep_t<float, 1>(L, stage, mode, b);
+  else
+    axis == 0 ? launch_sweep_t<double, 0>(L, stage, mode, b) : launch_sweep_t<double, 1>(L, stage, mode, b);
+}
+
+template <typename T>
+void launch_sensor_t(const LaunchSet& L, int sel, int enf, int visc, const Bind& b, uint8_t* mo) {
+  sensor_kernel<T><<<L.n_tiles, kStencilThreads, L.smem_sensor, L.st>>>(L.solves, L.tiles, sel, enf,
+                                                                          visc, b, mo);
+}
+void launch_sensor(const LaunchSet& L, int sel, int enf, int visc, const Bind& b, uint8_t* mo) {
+  if (L.elem == 4) launch_sensor_t<float>(L, sel, enf, visc, b, mo);
+  else launch_sensor_t<double>(L, sel, enf, visc, b, mo);
+}
+void launch_hv(const LaunchSet& L, const Bind& b) {
+  if (L.elem == 4) hv_kernel<float><<<L.n_tiles, kStencilThreads, 0, L.st>>>(L.solves, L.tiles, b);
+  else hv_kernel<double><<<L.n_tiles, kStencilThreads, 0, L.st>>>(L.solves, L.tiles, b);
+}
+void launch_prepass(const LaunchSet& L, int buf, int mode, int enf, const Bind& b) {
+  prepass_kernel<<<L.n_tiles, kRedThreads, 0, L.st>>>(L.solves, L.tiles, buf, mode, enf, b);
+}
+
+// The reference's loop body (OOP/hit2d.py:828-879; riemann_config3.py:728-740).
+int launch_step_sequence(const LaunchSet& L, int any_forcing, int noise_upload, int any_outflow,
+                         int any_hv) {
+  Bind nb{};
+  launch_prepass(L, 0, PRE_STEP, 1, nb);
+  if (any_forcing) {
+    if (noise_upload)
+      noise_dft_kernel<<<L.n_tiles, kRedThreads, 0, L.st>>>(L.solves, L.tiles, nb);
+    else
+      noise_rng_kernel<<<L.nsolves, 128, 0, L.st>>>(L.solves, L.nsolves, L.partner);
+    force_synth_kernel<<<L.n_tiles, kRedThreads, 0, L.st>>>(L.solves, L.tiles, nb);
+  }
+  for (int stage = 0; stage < 3; ++stage) {
+    if (stage > 0) launch_prepass(L, stage, PRE_STAGE, 1, nb);
+    launch_sensor(L, stage, 1, 1, nb, nullptr);
+    launch_sweep(L, 0, stage, SW_STAGE, nb);
+    launch_sweep(L, 1, stage, SW_STAGE, nb);
+    if (any_outflow) guard_kernel<<<L.nsolves, 256, 0, L.st>>>(L.solves, L.nsolves, stage == 2 ? 3 : stage + 1, nb);
+  }
+  if (any_hv) {
+    launch_prepass(L, 1, PRE_SENSOR, 0, nb);
+    launch_sensor(L, 3, 0, 0, nb, nullptr);
+    launch_hv(L, nb);
+    if (any_outflow) guard_kernel<<<L.nsolves, 256, 0, L.st>>>(L.solves, L.nsolves, 0, nb);
+  }
+  HB_LAUNCHED("step kernels");
+  return HITB200_OK;
+}
+
+LaunchSet plan_launch_set(hitb200_plan* p, cudaStream_t st) {
+  LaunchSet L;
+  L.solves = p->d_solve;
+  L.nsolves = 1;
+  L.tiles = p->d_tiles;
+  L.xl = p->d_xlines;
+  L.yl = p->d_ylines;
+  L.partner = p->d_partner;
+  L.n_tiles = p->n_tiles;
+  L.n_x = p->n_x;
+  L.n_y = p->n_y;
+  L.elem = p->elem;
+  L.mch_x = mch_for(p->desc.nx);
+  L.mch_y = mch_for(p->desc.ny);
+  L.smem_x = p->smem_x;
+  L.smem_y = p->smem_y;
+  L.smem_sensor = p->smem_sensor;
+  L.st = st;
+  return L;
+}
+
+// Shared-memory opt-in of every kernel a launch set may use; called at plan /
+// batch creation so that no attribute call happens during graph capture.
+void prime_attributes(int elem, int mch_x, int mch_y, size_t smem_x, size_t smem_y,
+                      size_t smem_sensor) {
+  auto sweep = [&](auto tag, int axis, int mch, size_t bytes) {
+    using T = decltype(tag);
+#define HB_ATTR(M)                                                    \
+  if (mch == M) {                                                     \
+    if (axis == 0) set_sweep_attr<T, 0, M>(bytes);                    \
+    else set_sweep_attr<T, 1, M>(bytes);                              \
+  }
+    HB_ATTR(4) HB_ATTR(8) HB_ATTR(16) HB_ATTR(32)
+#undef HB_ATTR
+  };
+  if (elem == 4) {
+    sweep(float{}, 0, mch_x, smem_x);
+    sweep(float{}, 1, mch_y, smem_y);
+    set_sensor_attr<float>(smem_sensor);
+  } else {
+    sweep(double{}, 0, mch_x, smem_x);
+    sweep(double{}, 1, mch_y, smem_y);
+    set_sensor_attr<double>(smem_sensor);
+  }
+}
+
+int validate_desc(const hitb200_desc* d) {
+  if (!d) return invalid("descriptor is NULL");
+  if (d->nx <= 0 || d->ny <= 0) return invalid("nx and ny must be positive");
+  if (d->nx > kMaxLine || d->ny > kMaxLine)
+    return (g_last_error = "grid lines longer than 1024 nodes are not supported", HITB200_ERR_UNSUPPORTED);
+  if (!(d->x_max > d->x_min) || !(d->y_max > d->y_min)) return invalid("domain extent must be positive");
+  if (d->precision != 0 && d->precision != 1) return invalid("precision must be 0 (fp64) or 1 (fp32 bulk)");
+  if (d->scheme != 0 && d->scheme != 1) return invalid("scheme must be 'hybrid' or 'weno'");
+  if (d->sensor_width < 0 || d->sensor_width > kMaxWidth)
+    return (g_last_error = "sensor width must be in [0, 8]", HITB200_ERR_UNSUPPORTED);
+  if (d->hv_interval < 0) return invalid("hyperviscosity_interval must be >= 0");
+  if (!d->periodic && (d->guard_cells < 0)) return invalid("guard_cells must be >= 0");
+  if (!d->periodic && d->guard_cells > 0 && (d->nx <= 2 * d->guard_cells || d->ny <= 2 * d->guard_cells))
+    return invalid("state is too small for the requested guard cells");
+  if (d->forcing_on) {
+    if (!d->periodic) return invalid("forcing needs a periodic grid");
+    if (d->forcing_kmin < 0.0 || d->forcing_kmax <= 0.0 || d->forcing_kmin > d->forcing_kmax)
+      return invalid("forcing shell must satisfy 0 <= k_min <= k_max");
+    if (d->forcing_correlation_time <= 0.0) return invalid("forcing correlation time must be positive");
+    if (!(d->alpha_memory >= 0.0 && d->alpha_memory < 1.0)) return invalid("alpha_memory must be in [0, 1)");
+  }
+  if (d->mach_control && !is_none(d->target_power)) {
+    if (d->mach_target <= 0.0) return invalid("Mach control requires a positive target Mach number");
+    if (!(d->mach_memory >= 0.0 && d->mach_memory < 1.0)) return invalid("mach_control_memory must be in [0, 1)");
+    if (d->mach_exponent <= 0.0) return invalid("mach_control_exponent must be positive");
+  }
+  return HITB200_OK;
+}
+
+}  // namespace
+
+// =================================================================================
+extern "C" {
+
+const char* hitb200_version(void) { return "hitb200 sm_100a 1.0"; }
+
+size_t hitb200_desc_size(void) { return sizeof(hitb200_desc); }
+
+const char* hitb200_status_string(int status) {
+  switch (status) {
+    case HITB200_OK: return "ok";
+    case HITB200_ERR_NONFINITE: return "state contains NaN or Inf values";
+    case HITB200_ERR_NONPOSITIVE: return "state contains non-positive density or pressure";
+    default: return g_last_error.empty() ? "error" : g_last_error.c_str();
+  }
+}
+
+int hitb200_desc_init(hitb200_desc* d) {
+  if (!d) return invalid("descriptor is NULL");
+  std::memset(d, 0, sizeof(*d));
+  const double nan = std::nan("");
+  d->nx = d->ny = 128;
+  d->x_min = d->y_min = 0.0;
+  d->x_max = d->y_max = 2.0 * M_PI;
+  d->periodic = 1;
+  d->precision = 0;
+  d->scheme = 0;
+  d->gamma = 1.4;
+  d->sensor_width = 4;
+  d->boundary_guard = 0;
+  d->compression_threshold = 2.5;
+  d->jump_threshold = 0.04;
+  d->shear_threshold = nan;
+  d->viscosity = 1.0e-3;
+  d->prandtl = 0.72;
+  d->gas_constant = 1.0;
+  d->hv_mn = 0.002;
+  d->hv_weight[0] = 0.25;
+  d->hv_weight[1] = 1.0;
+  d->hv_weight[2] = 1.0;
+  d->hv_weight[3] = 0.25;
+  d->hv_interval = 5;
+  d->guard_cells = 0;
+  d->drag_coefficient = 0.0;
+  d->drag_kmax = 2.0;
+  d->cooling_time = nan;
+  d->cooling_target_pressure = nan;
+  d->forcing_on = 1;
+  d->forcing_kmin = 0.0;
+  d->forcing_kmax = 3.0;
+  d->forcing_correlation_time = 1.0;
+  d->forcing_rms = 1.0;
+  d->target_power = 1.0e-3;
+  d->min_power = 1.0e-6;
+  d->max_rescale = 20.0;
+  d->alpha_memory = 0.2;
+  d->mach_control = 0;
+  d->mach_target = 0.1;
+  d->mach_memory = 0.995;
+  d->mach_exponent = 2.0;
+  d->mach_min_power = nan;
+  d->mach_max_power = nan;
+  d->cfl = 0.05;
+  d->tfinal = 1.0;
+  d->fixed_dt = 0;
+  d->noise_mode = 0;
+  d->seed = 1234;
+  return HITB200_OK;
+}
+
+size_t hitb200_plan_device_bytes(const hitb200_desc* d) {
+  if (validate_desc(d) != HITB200_OK) return 0;
+  const size_t N = (size_t)d->nx * d->ny;
+  const int elem = d->precision == 1 ? 4 : 8;
+  const int ntx = (d->nx + kTileX - 1) / kTileX, nty = (d->ny + kTileY - 1) / kTileY;
+  const size_t ntile = (size_t)ntx * nty;
+  ModeTables mt = build_modes(*d);
+  Arena a;
+  a.take(sizeof(SolveDev));
+  a.take(2 * 4 * N * sizeof(double));                        // q1, q2
+  a.take(4 * N * elem);                                      // rx
+  if (d->viscosity > 0.0) a.take(3 * N * elem);              // vis
+  a.take(N);                                                 // mask
+  if (d->forcing_on) a.take(2 * N * sizeof(double));         // fx, fy
+  if (d->forcing_on && d->noise_mode == 0) a.take(N * sizeof(double));
+  a.take((d->nx + d->ny) * sizeof(double2));
+  a.take((mt.drag.size() + mt.force.size() + 1) * sizeof(int2));
+  a.take((mt.force.size() + 1) * sizeof(double2));
+  a.take(kMaxForce * sizeof(int));
+  a.take(SCAL_SIZE * sizeof(double));
+  a.take(ntile * (R_FIXED + 4 * mt.drag.size()) * sizeof(double));
+  a.take(ntile * (2 * mt.force.size() + 1) * sizeof(double));
+  a.take(ntile * 4 * sizeof(double));
+  a.take(ntile * NDIAG * sizeof(double));
+  a.take(8 * sizeof(unsigned) + sizeof(int) + NDIAG * sizeof(double));
+  a.take(ntile * sizeof(Work));
+  a.take((size_t)(d->ny + d->nx) * sizeof(Work));
+  return a.off;
+}
+
+int hitb200_plan_create(const hitb200_desc* d, hitb200_plan** out) {
+  if (!out) return invalid("plan pointer is NULL");
+  *out = nullptr;
+  int st = validate_desc(d);
+  if (st != HITB200_OK) return st;
+  ModeTables mt = build_modes(*d);
+  if ((int)mt.drag.size() > kMaxDrag)
+    return (g_last_error = "drag band holds more than 32 modes", HITB200_ERR_UNSUPPORTED);
+  if ((int)mt.force.size() > kMaxForce)
+    return (g_last_error = "forcing shell holds more than 128 modes", HITB200_ERR_UNSUPPORTED);
+  if (d->forcing_on && mt.force.empty()) return invalid("forcing shell contains no Fourier modes on this grid");
+
+  hitb200_plan* p = new hitb200_plan();
+  p->desc = *d;
+  p->elem = d->precision == 1 ? 4 : 8;
+  const int nx = d->nx, ny = d->ny;
+  const size_t N = (size_t)nx * ny;
+  const int ntx = (nx + kTileX - 1) / kTileX, nty = (ny + kTileY - 1) / kTileY;
+  p->n_tiles = ntx * nty;
+  p->Rx = lines_per_cta(nx, ny, p->elem);
+  p->Ry = lines_per_cta(ny, nx, p->elem);
+  if (p->Ry < 2 && nx >= 2) p->Ry = 2;  // y panels: at least 16-byte row segments
+  p->n_x = (ny + p->Rx - 1) / p->Rx;
+  p->n_y = (nx + p->Ry - 1) / p->Ry;
+  p->smem_x = p->elem == 4 ? SweepLayout<float>(nx, p->Rx).bytes() : SweepLayout<double>(nx, p->Rx).bytes();
+  p->smem_y = p->elem == 4 ? SweepLayout<float>(ny, p->Ry).bytes() : SweepLayout<double>(ny, p->Ry).bytes();
+  p->smem_sensor = sensor_smem_bytes(d->sensor_width, p->elem);
+
+  // ---- arena layout ----
+  Arena a;
+  const size_t o_solve = a.take(sizeof(SolveDev));
+  const size_t o_q1 = a.take(4 * N * sizeof(double));
+  const size_t o_q2 = a.take(4 * N * sizeof(double));
+  const size_t o_rx = a.take(4 * N * p->elem);
+  const size_t o_vis = d->viscosity > 0.0 ? a.take(3 * N * p->elem) : 0;
+  const size_t o_mask = a.take(N);
+  const size_t o_fx = d->forcing_on ? a.take(N * sizeof(double)) : 0;
+  const size_t o_fy = d->forcing_on ? a.take(N * sizeof(double)) : 0;
+  const size_t o_noise = (d->forcing_on && d->noise_mode == 0) ? a.take(N * sizeof(double)) : 0;
+  const size_t o_tw = a.take((nx + ny) * sizeof(double2));
+  const size_t o_modes = a.take((mt.drag.size() + mt.force.size() + 1) * sizeof(int2));
+  const size_t o_kvec = a.take((mt.force.size() + 1) * sizeof(double2));
+  const size_t o_partner = a.take(kMaxForce * sizeof(int));
+  const size_t o_scal = a.take(SCAL_SIZE * sizeof(double));
+  const size_t nred = R_FIXED + 4 * mt.drag.size();
+  const size_t o_ppre = a.take(p->n_tiles * nred * sizeof(double));
+  const size_t o_pnoise = a.take(p->n_tiles * (2 * mt.force.size() + 1) * sizeof(double));
+  const size_t o_psynth = a.take(p->n_tiles * 4 * sizeof(double));
+  const size_t o_pdiag = a.take(p->n_tiles * NDIAG * sizeof(double));
+  const size_t o_cnt = a.take(8 * sizeof(unsigned) + sizeof(int) + NDIAG * sizeof(double));
+  const size_t o_tiles = a.take(p->n_tiles * sizeof(Work));
+  const size_t o_xl = a.take(p->n_x * sizeof(Work));
+  const size_t o_yl = a.take(p->n_y * sizeof(Work));
+  p->arena_bytes = a.off;
+  cudaError_t e = cudaMalloc(&p->arena, a.off);
+  if (e != cudaSuccess) {
+    delete p;
+    return cuda_fail(e, "cudaMalloc(plan arena)");
+  }
+  unsigned char* base = p->arena;
+  SolveDev& s = p->hs;
+  std::memset(&s, 0, sizeof(s));
+  s.nx = nx;
+  s.ny = ny;
+  s.periodic = d->periodic;
+  s.scheme = d->scheme;
+  s.precision = d->precision;
+  s.dx = (d->x_max - d->x_min) / nx;
+  s.dy = (d->y_max - d->y_min) / ny;
+  s.gamma = d->gamma;
+  s.width = d->sensor_width;
+  s.boundary_guard = d->periodic ? 0 : d->boundary_guard;
+  s.comp_thr = d->compression_threshold;
+  s.jump_thr = d->jump_threshold;
+  // periodic: shear on when the threshold is given; outflow: when given and > 0
+  s.shear_on = !is_none(d->shear_threshold) && (d->periodic || d->shear_threshold > 0.0);
+  s.shear_thr = is_none(d->shear_threshold) ? 0.0 : d->shear_threshold;
+  s.mu = d->viscosity;
+  s.gas_r = d->gas_constant;
+  s.kappa = d->viscosity * (d->gamma * d->gas_constant / (d->gamma - 1.0)) / d->prandtl;
+  const double h = std::min(s.dx, s.dy);
+  for (int c = 0; c < 4; ++c) s.hv_coef[c] = d->hv_mn * d->hv_weight[c] * std::pow(h, 4.0);
+  const bool hv_on = d->hv_mn > 0.0 && d->hv_interval > 0 && d->scheme == 0;
+  s.hv_interval = hv_on ? d->hv_interval : 0;
+  s.guard = d->periodic ? 0 : d->guard_cells;
+  s.n_drag = (int)mt.drag.size();
+  s.drag_on = s.n_drag > 0;
+  s.drag_coef = d->drag_coefficient;
+  s.cooling_on = !is_none(d->cooling_time) && d->cooling_time > 0.0 && d->periodic;
+  s.cooling_tau = s.cooling_on ? d->cooling_time : 1.0;
+  s.cooling_pref = is_none(d->cooling_target_pressure) ? 1.0 / d->gamma : d->cooling_target_pressure;
+  s.forcing_on = d->forcing_on;
+  s.n_force = (int)mt.force.size();
+  s.f_tau = d->forcing_correlation_time;
+  s.f_rms = d->forcing_rms;
+  s.f_has_target = !is_none(d->target_power);
+  s.f_target = d->target_power;
+  s.f_min_power = d->min_power;
+  s.f_has_max_rescale = !is_none(d->max_rescale);
+  s.f_max_rescale = d->max_rescale;
+  s.f_alpha_memory = d->alpha_memory;
+  s.mach_control = d->mach_control;
+  s.mach_target = d->mach_target;
+  s.mach_memory = d->mach_memory;
+  s.mach_exponent = d->mach_exponent;
+  s.has_mach_min = !is_none(d->mach_min_power);
+  s.mach_min_power = d->mach_min_power;
+  s.has_mach_max = !is_none(d->mach_max_power);
+  s.mach_max_power = d->mach_max_power;
+  s.cfl = d->cfl;
+  s.tfinal = d->tfinal;
+  s.fixed_dt = d->fixed_dt;
+  s.noise_mode = d->noise_mode;
+  s.seed = d->seed;
+  s.nblk_pre = s.nblk_noise = s.nblk_synth = s.nblk_diag = p->n_tiles;
+  s.nred = (int)nred;
+  s.q = nullptr;
+  s.q1 = reinterpret_cast<double*>(base + o_q1);
+  s.q2 = reinterpret_cast<double*>(base + o_q2);
+  s.rx = base + o_rx;
+  s.vis = d->viscosity > 0.0 ? (void*)(base + o_vis) : nullptr;
+  s.mask = base + o_mask;
+  s.fx = d->forcing_on ? reinterpret_cast<double*>(base + o_fx) : nullptr;
+  s.fy = d->forcing_on ? reinterpret_cast<double*>(base + o_fy) : nullptr;
+  s.noise = o_noise ? reinterpret_cast<double*>(base + o_noise) : nullptr;
+  s.twx = reinterpret_cast<double2*>(base + o_tw);
+  s.twy = s.twx + nx;
+  s.modes = reinterpret_cast<int2*>(base + o_modes);
+  s.kvec = reinterpret_cast<double2*>(base + o_kvec);
+  s.scal = reinterpret_cast<double*>(base + o_scal);
+  s.part_pre = reinterpret_cast<double*>(base + o_ppre);
+  s.part_noise = reinterpret_cast<double*>(base + o_pnoise);
+  s.part_synth = reinterpret_cast<double*>(base + o_psynth);
+  s.part_diag = reinterpret_cast<double*>(base + o_pdiag);
+  s.counters = reinterpret_cast<unsigned*>(base + o_cnt);
+  s.near_count = reinterpret_cast<int*>(s.counters + 8);
+  s.diag_out = reinterpret_cast<double*>(base + o_cnt + 64);
+  p->d_solve = reinterpret_cast<SolveDev*>(base + o_solve);
+  p->d_partner = reinterpret_cast<int*>(base + o_partner);
+  p->d_tiles = reinterpret_cast<Work*>(base + o_tiles);
+  p->d_xlines = reinterpret_cast<Work*>(base + o_xl);
+  p->d_ylines = reinterpret_cast<Work*>(base + o_yl);
+
+  // ---- host-built tables ----
+  std::vector<double2> tw(nx + ny);
+  for (int j = 0; j < nx; ++j) {
+    const double th = 2.0 * M_PI * (double)j / (double)nx;
+    tw[j] = make_double2(std::cos(th), -std::sin(th));
+  }
+  for (int j = 0; j < ny; ++j) {
+    const double th = 2.0 * M_PI * (double)j / (double)ny;
+    tw[nx + j] = make_double2(std::cos(th), -std::sin(th));
+  }
+  std::vector<int2> modes(mt.drag);
+  modes.insert(modes.end(), mt.force.begin(), mt.force.end());
+  modes.push_back(make_int2(0, 0));
+  std::vector<double2> kvec(mt.kvec);
+  kvec.push_back(make_double2(0, 0));
+  std::vector<double> scal(SCAL_SIZE, 0.0);
+  scal[S_ACTIVE] = 1.0;
+  scal[S_MAX_STEPS] = -1.0;
+  scal[S_POWER] = s.f_has_target ? d->target_power : std::nan("");
+  scal[S_POWER_DESIRED] = scal[S_POWER];
+  scal[S_F_ALPHA] = 1.0;
+  scal[S_F_SCALE] = 0.0;
+  scal[S_COMP_LIM] = -INFINITY;
+  scal[S_SHEAR_LIM] = INFINITY;
+  std::vector<Work> tiles;
+  for (int ty = 0; ty < nty; ++ty)
+    for (int tx = 0; tx < ntx; ++tx) tiles.push_back({0, tx * kTileX, ty * kTileY, (int)tiles.size()});
+  std::vector<Work> xl, yl;
+  for (int r = 0; r < ny; r += p->Rx) xl.push_back({0, r, std::min(p->Rx, ny - r), 0});
+  for (int c = 0; c < nx; c += p->Ry) yl.push_back({0, c, std::min(p->Ry, nx - c), 0});
+
+#define HB_PUT(dst, src, bytes)                                                  \
+  do {                                                                           \
+    e = cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice);                     \
+    if (e != cudaSuccess) {                                                      \
+      cudaFree(p->arena);                                                        \
+      delete p;                                                                  \
+      return cuda_fail(e, "cudaMemcpy(plan tables)");                            \
+    }                                                                            \
+  } while (0)
+  HB_PUT(s.twx, tw.data(), tw.size() * sizeof(double2));
+  HB_PUT(s.modes, modes.data(), modes.size() * sizeof(int2));
+  HB_PUT(s.kvec, kvec.data(), kvec.size() * sizeof(double2));
+  HB_PUT(p->d_partner, mt.partner.data(), kMaxForce * sizeof(int));
+  HB_PUT(s.scal, scal.data(), SCAL_SIZE * sizeof(double));
+  HB_PUT(p->d_tiles, tiles.data(), tiles.size() * sizeof(Work));
+  HB_PUT(p->d_xlines, xl.data(), xl.size() * sizeof(Work));
+  HB_PUT(p->d_ylines, yl.data(), yl.size() * sizeof(Work));
+  HB_PUT(p->d_solve, &s, sizeof(SolveDev));
+#undef HB_PUT
+  e = cudaMemset(s.counters, 0, 8 * sizeof(unsigned) + sizeof(int));
+  if (e != cudaSuccess) {
+    cudaFree(p->arena);
+    delete p;
+    return cuda_fail(e, "cudaMemset(counters)");
+  }
+  prime_attributes(p->elem, mch_for(nx), mch_for(ny), p->smem_x, p->smem_y, p->smem_sensor);
+  *out = p;
+  return HITB200_OK;
+}
+
+int hitb200_plan_destroy(hitb200_plan* p) {
+  if (!p) return HITB200_OK;
+  if (p->graph) cudaGraphExecDestroy(p->graph);
+  if (p->arena) cudaFree(p->arena);
+  delete p;
+  return HITB200_OK;
+}
+
+// ---- bind the caller's state pointer into the device descriptor ------------------
+static int bind_state(hitb200_plan* p, double* q, cudaStream_t st) {
+  if (p->hs.q == q) return HITB200_OK;
+  p->hs.q = q;
+  HB_CUDA(cudaMemcpyAsync(&p->d_solve->q, &p->hs.q, sizeof(double*), cudaMemcpyHostToDevice, st));
+  HB_CUDA(cudaStreamSynchronize(st));
+  return HITB200_OK;
+}
+
+int hitb200_enforce(hitb200_plan* p, const double* q, double* out, void* stream) {
+  if (!p || !q || !out) return invalid("NULL argument");
+  const size_t plane = (size_t)p->desc.nx * p->desc.ny;
+  enforce_kernel<<<(int)std::min<size_t>((plane + 255) / 256, 4096), 256, 0, (cudaStream_t)stream>>>(
+      q, out, plane, p->desc.gamma);
+  HB_LAUNCHED("enforce_kernel");
+  return HITB200_OK;
+}
+
+int hitb200_enforce_state(const double* q, double* out, int64_t ncells, double gamma, void* stream) {
+  if (!q || !out) return invalid("NULL argument");
+  if (ncells <= 0) return invalid("ncells must be positive");
+  enforce_kernel<<<(int)std::min<int64_t>((ncells + 255) / 256, 4096), 256, 0, (cudaStream_t)stream>>>(
+      q, out, (size_t)ncells, gamma);
+  HB_LAUNCHED("enforce_kernel");
+  return HITB200_OK;
+}
+
+int hitb200_sensor(hitb200_plan* p, const double* q, uint8_t* mask, int enforce_first, void* stream) {
+  if (!p || !q || !mask) return invalid("NULL argument");
+  LaunchSet L = plan_launch_set(p, (cudaStream_t)stream);
+  Bind b{};
+  b.use = 1;
+  b.qin = q;
+  launch_prepass(L, 0, PRE_SENSOR, enforce_first, b);
+  launch_sensor(L, 0, enforce_first, 0, b, mask);
+  HB_LAUNCHED("sensor");
+  return HITB200_OK;
+}
+
+int hitb200_axis_derivative(hitb200_plan* p, const double* q, const uint8_t* mask, int axis,
+                            double* out, void* stream) {
+  if (!p || !q || !mask || !out) return invalid("NULL argument");
+  if (axis != 0 && axis != 1) return invalid("axis must be 0 (x) or 1 (y)");
+  LaunchSet L = plan_launch_set(p, (cudaStream_t)stream);
+  Bind b{};
+  b.use = 1;
+  b.qin = q;
+  b.mask = mask;
+  b.out = out;
+  launch_prepass(L, 0, PRE_STAGE, 1, b);
+  launch_sweep(L, axis, 0, SW_DERIV, b);
+  HB_LAUNCHED("axis_derivative");
+  return HITB200_OK;
+}
+
+int hitb200_rhs(hitb200_plan* p, const double* q, int terms, const double* fx, const double* fy,
+                double* out, void* stream) {
+  if (!p || !q || !out) return invalid("NULL argument");
+  if ((terms & HITB200_TERM_FORCING) && (!fx || !fy)) return invalid("forcing term needs fx and fy");
+  if ((terms & ~HITB200_TERM_ALL) != 0) return invalid("unknown rhs term bits");
+  if ((terms & HITB200_TERM_VISCOUS) && p->desc.viscosity > 0.0 && !p->hs.vis)
+    return invalid("plan has no viscous buffer");
+  LaunchSet L = plan_launch_set(p, (cudaStream_t)stream);
+  Bind b{};
+  b.use = 1;
+  b.qin = q;
+  b.mask = p->hs.mask;
+  b.out = out;
+  b.fx = fx;
+  b.fy = fy;
+  b.terms = terms;
+  launch_prepass(L, 0, PRE_STAGE, 1, b);
+  launch_sensor(L, 0, 1, (terms & HITB200_TERM_VISCOUS) ? 1 : 0, b, p->hs.mask);
+  launch_sweep(L, 0, 0, SW_RHS, b);
+  launch_sweep(L, 1, 0, SW_RHS, b);
+  HB_LAUNCHED("rhs");
+  return HITB200_OK;
+}
+
+int hitb200_viscous_rhs(hitb200_plan* p, const double* q, double* out, void* stream) {
+  if (!p || !q || !out) return invalid("NULL argument");
+  const size_t plane = (size_t)p->desc.nx * p->desc.ny;
+  if (p->desc.viscosity == 0.0) {
+    HB_CUDA(cudaMemsetAsync(out, 0, 4 * plane * sizeof(double), (cudaStream_t)stream));
+    return HITB200_OK;
+  }
+  LaunchSet L = plan_launch_set(p, (cudaStream_t)stream);
+  Bind b{};
+  b.use = 1;
+  b.qin = q;
+  launch_prepass(L, 0, PRE_SENSOR, 0, b);
+  launch_sensor(L, 0, 0, 1, b, p->hs.mask);
+  const int nb = (int)std::min<size_t>((plane + 255) / 256, 4096);
+  if (p->elem == 4)
+    vis_copy_kernel<float><<<nb, 256, 0, (cudaStream_t)stream>>>((const float*)p->hs.vis, out, plane);
+  else
+    vis_copy_kernel<double><<<nb, 256, 0, (cudaStream_t)stream>>>((const double*)p->hs.vis, out, plane);
+  HB_LAUNCHED("viscous_rhs");
+  return HITB200_OK;
+}
+
+int hitb200_hyperviscosity(hitb200_plan* p, const double* q, const uint8_t* active, double* out,
+                           void* stream) {
+  if (!p || !q || !out) return invalid("NULL argument");
+  if (!active) return invalid("active_mask is required: hyperviscosity may only be applied on compact-FD nodes");
+  if (q == out) return invalid("hyperviscosity output must not alias its input");
+  LaunchSet L = plan_launch_set(p, (cudaStream_t)stream);
+  Bind b{};
+  b.use = 1;
+  b.qin = q;
+  b.qout = out;
+  b.mask = active;
+  b.invert_mask = 0;
+  launch_hv(L, b);
+  HB_LAUNCHED("hyperviscosity");
+  return HITB200_OK;
+}
+
+int hitb200_outflow_guard(hitb200_plan* p, double* q, void* stream) {
+  if (!p || !q) return invalid("NULL argument");
+  Bind b{};
+  b.use = 1;
+  b.qout = q;
+  guard_kernel<<<1, 256, 0, (cudaStream_t)stream>>>(p->d_solve, 1, 0, b);
+  HB_LAUNCHED("guard_kernel");
+  return HITB200_OK;
+}
+
+int hitb200_stable_time_step(hitb200_plan* p, const double* q, double cfl, double remaining,
+                             double* dt_out) {
+  if (!p || !q || !dt_out) return invalid("NULL argument");
+  LaunchSet L = plan_launch_set(p, 0);
+  Bind b{};
+  b.use = 1;
+  b.qin = q;
+  launch_prepass(L, 0, PRE_CHECK, 0, b);
+  HB_LAUNCHED("prepass");
+  double sr = 0.0;
+  HB_CUDA(cudaMemcpy(&sr, p->hs.scal + S_DT, sizeof(double), cudaMemcpyDeviceToHost));
+  double dt = cfl / sr;
+  if (!std::isnan(remaining)) dt = std::min(dt, remaining);
+  *dt_out = dt;
+  return HITB200_OK;
+}
+
+int hitb200_validate(hitb200_plan* p, const double* q) {
+  if (!p || !q) return invalid("NULL argument");
+  LaunchSet L = plan_launch_set(p, 0);
+  Bind b{};
+  b.use = 1;
+  b.qin = q;
+  double zero = 0.0;
+  HB_CUDA(cudaMemcpy(p->hs.scal + S_STATUS, &zero, sizeof(double), cudaMemcpyHostToDevice));
+  launch_prepass(L, 0, PRE_CHECK, 0, b);
+  HB_LAUNCHED("prepass");
+  double stv = 0.0;
+  HB_CUDA(cudaMemcpy(&stv, p->hs.scal + S_STATUS, sizeof(double), cudaMemcpyDeviceToHost));
+  const int bits = (int)stv;
+  if (bits & ST_NONFINITE) return HITB200_ERR_NONFINITE;
+  if (bits & (ST_NONPOS_RHO | ST_NONPOS_P)) return HITB200_ERR_NONPOSITIVE;
+  return HITB200_OK;
+}
+
+int hitb200_forcing_update(hitb200_plan* p, const double* q, const double* noise, double dt,
+                           double target_power, double* fx, double* fy, void* stream) {
+  if (!p || !q || !fx || !fy) return invalid("NULL argument");
+  if (!p->desc.forcing_on) return invalid("plan has no forcing");
+  if (!(dt > 0.0)) return invalid("forcing update requires dt > 0");
+  if (!noise && p->desc.noise_mode == 0) return invalid("noise field required (noise_mode 0)");
+  cudaStream_t st = (cudaStream_t)stream;
+  const double decay = std::exp(-dt / p->desc.forcing_correlation_time);
+  const double vals[3] = {decay, std::sqrt(std::max(1.0 - decay * decay, 0.0)), target_power};
+  HB_CUDA(cudaMemcpyAsync(p->hs.scal + S_F_DECAY, &vals[0], sizeof(double), cudaMemcpyHostToDevice, st));
+  HB_CUDA(cudaMemcpyAsync(p->hs.scal + S_XI_SCALE, &vals[1], sizeof(double), cudaMemcpyHostToDevice, st));
+  HB_CUDA(cudaMemcpyAsync(p->hs.scal + S_POWER, &vals[2], sizeof(double), cudaMemcpyHostToDevice, st));
+  LaunchSet L = plan_launch_set(p, st);
+  Bind b{};
+  b.use = 1;
+  if (noise) {
+    b.qin = noise;
+    noise_dft_kernel<<<L.n_tiles, kRedThreads, 0, st>>>(L.solves, L.tiles, b);
+  } else {
+    noise_rng_kernel<<<1, 128, 0, st>>>(L.solves, 1, L.partner);
+  }
+  Bind b2{};
+  b2.use = 1;
+  b2.qin = q;
+  force_synth_kernel<<<L.n_tiles, kRedThreads, 0, st>>>(L.solves, L.tiles, b2);
+  const size_t plane = (size_t)p->desc.nx * p->desc.ny;
+  const int nb = (int)std::min<size_t>((plane + 255) / 256, 4096);
+  scale_copy_kernel<<<nb, 256, 0, st>>>(p->hs.fx, fx, p->hs.scal, S_F_SCALE, plane);
+  scale_copy_kernel<<<nb, 256, 0, st>>>(p->hs.fy, fy, p->hs.scal, S_F_SCALE, plane);
+  HB_LAUNCHED("forcing_update");
+  HB_CUDA(cudaStreamSynchronize(st));  // host-side scalars above live on this stack frame
+  return HITB200_OK;
+}
+
+int hitb200_step(hitb200_plan* p, double* q, const double* noise, void* stream) {
+  if (!p || !q) return invalid("NULL argument");
+  if (p->in_batch) return invalid("plan belongs to a batch; use hitb200_batch_step");
+  cudaStream_t st = (cudaStream_t)stream;
+  const int upload = p->desc.forcing_on && p->desc.noise_mode == 0;
+  if (upload && !noise) return invalid("noise field required (noise_mode 0)");
+  int r = bind_state(p, q, st);
+  if (r != HITB200_OK) return r;
+  if (upload)
+    HB_CUDA(cudaMemcpyAsync((void*)p->hs.noise, noise, (size_t)p->desc.nx * p->desc.ny * sizeof(double),
+                            cudaMemcpyDeviceToDevice, st));
+  LaunchSet L = plan_launch_set(p, st);
+  return launch_step_sequence(L, p->desc.forcing_on, upload, !p->desc.periodic, p->hs.hv_interval > 0);
+}
+
+int hitb200_run(hitb200_plan* p, double* q, int32_t nsteps, void* stream) {
+  if (!p || !q) return invalid("NULL argument");
+  if (nsteps < 0) return invalid("nsteps must be >= 0");
+  if (p->desc.forcing_on && p->desc.noise_mode == 0)
+    return invalid("hitb200_run needs noise_mode 1 (device noise) when forcing is on");
+  cudaStream_t st = (cudaStream_t)stream;
+  int r = bind_state(p, q, st);
+  if (r != HITB200_OK) return r;
+  if (!p->graph || p->graph_stream != st) {
+    if (p->graph) cudaGraphExecDestroy(p->graph);
+    p->graph = nullptr;
+    cudaStream_t cap;
+    HB_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+    LaunchSet L = plan_launch_set(p, cap);
+    // make every kernel's shared-memory attribute final before capture
+    HB_CUDA(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
+    r = launch_step_sequence(L, p->desc.forcing_on, 0, !p->desc.periodic, p->hs.hv_interval > 0);
+    cudaGraph_t gr;
+    cudaError_t e = cudaStreamEndCapture(cap, &gr);
+    cudaStreamDestroy(cap);
+    if (r != HITB200_OK) return r;
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+    e = cudaGraphInstantiate(&p->graph, gr, 0);
+    cudaGraphDestroy(gr);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGraphInstantiate");
+    p->graph_stream = st;
+  }
+  for (int i = 0; i < nsteps; ++i) HB_CUDA(cudaGraphLaunch(p->graph, st));
+  return HITB200_OK;
+}
+
+int hitb200_set_time(hitb200_plan* p, double time, int64_t step, double dt, int64_t max_steps) {
+  if (!p) return invalid("NULL argument");
+  double v[4] = {dt, time, (double)step, 1.0};
+  double ms = max_steps < 0 ? -1.0 : (double)max_steps;
+  HB_CUDA(cudaMemcpy(p->hs.scal + S_DT, v, 4 * sizeof(double), cudaMemcpyHostToDevice));
+  HB_CUDA(cudaMemcpy(p->hs.scal + S_MAX_STEPS, &ms, sizeof(double), cudaMemcpyHostToDevice));
+  return HITB200_OK;
+}
+
+int hitb200_read_scalars(hitb200_plan* p, double* out, int32_t n) {
+  if (!p || !out) return invalid("NULL argument");
+  if (n < 0 || n > HITB200_S_COUNT) return invalid("n out of range");
+  HB_CUDA(cudaDeviceSynchronize());
+  HB_CUDA(cudaMemcpy(out, p->hs.scal, n * sizeof(double), cudaMemcpyDeviceToHost));
+  int near = 0;
+  HB_CUDA(cudaMemcpy(&near, p->hs.near_count, sizeof(int), cudaMemcpyDeviceToHost));
+  if (n > HITB200_S_NEAR_THRESHOLD) out[HITB200_S_NEAR_THRESHOLD] = near;
+  return HITB200_OK;
+}
+
+int hitb200_copy_scalars_async(hitb200_plan* p, double* dst, int32_t n, void* stream) {
+  if (!p || !dst) return invalid("NULL argument");
+  if (n < 0 || n > HITB200_S_COUNT) return invalid("n out of range");
+  HB_CUDA(cudaMemcpyAsync(dst, p->hs.scal, n * sizeof(double), cudaMemcpyDefault, (cudaStream_t)stream));
+  return HITB200_OK;
+}
+
+int hitb200_diagnostics(hitb200_plan* p, const double* q, double* out, int32_t n) {
+  if (!p || !q || !out) return invalid("NULL argument");
+  LaunchSet L = plan_launch_set(p, 0);
+  Bind b{};
+  b.use = 1;
+  b.qin = q;
+  diag_kernel<<<L.n_tiles, kRedThreads, 0, 0>>>(L.solves, L.tiles, b);
+  HB_LAUNCHED("diag_kernel");
+  double raw[NDIAG];
+  HB_CUDA(cudaMemcpy(raw, p->hs.diag_out, sizeof(raw), cudaMemcpyDeviceToHost));
+  const double N = (double)p->desc.nx * p->desc.ny;
+  const double area = (p->desc.x_max - p->desc.x_min) * (p->desc.y_max - p->desc.y_min);
+  const double mr = raw[D_RHO] / N, mu = raw[D_U] / N, mv = raw[D_V] / N;
+  // fluctuation moments mean(rho (u - <u>)^2) etc. from raw sums
+  const double uu = raw[D_RUU] / N - 2.0 * mu * raw[D_RU] / N + mu * mu * mr;
+  const double vv = raw[D_RVV] / N - 2.0 * mv * raw[D_RV] / N + mv * mv * mr;
+  const double uv = raw[D_RUV] / N - mu * raw[D_RV] / N - mv * raw[D_RU] / N + mu * mv * mr;
+  const double sum = uu + vv, cov = std::sqrt(std::max(uu * vv, 0.0));
+  const double vals[17] = {0.5 * sum,
+                           0.5 * uu,
+                           0.5 * vv,
+                           sum > 0.0 ? std::fabs(uu - vv) / sum : 0.0,
+                           cov > 0.0 ? uv / cov : 0.0,
+                           std::sqrt(raw[D_VEL2] / N),
+                           std::sqrt(raw[D_VEL2] / N) / (raw[D_C] / N),
+                           mr,
+                           raw[D_P] / N,
+                           mr * area,
+                           raw[D_Q1] / N * area,
+                           raw[D_Q2] / N * area,
+                           raw[D_Q3] / N * area,
+                           raw[D_RHOMIN],
+                           raw[D_RHOMAX],
+                           raw[D_PMIN],
+                           raw[D_PMAX]};
+  for (int i = 0; i < n && i < 17; ++i) out[i] = vals[i];
+  return HITB200_OK;
+}
+
+// ---- batched form ---------------------------------------------------------------------
+int hitb200_batch_create(const hitb200_desc* descs, int32_t n, hitb200_batch** out) {
+  if (!descs || !out || n <= 0) return invalid("batch needs at least one descriptor");
+  *out = nullptr;
+  for (int i = 1; i < n; ++i)
+    if (descs[i].precision != descs[0].precision) return invalid("batch members must share precision");
+  hitb200_batch* b = new hitb200_batch();
+  std::vector<SolveDev> hs;
+  std::vector<Work> tiles, xl, yl;
+  std::vector<int> partner;
+  for (int i = 0; i < n; ++i) {
+    hitb200_plan* p = nullptr;
+    int r = hitb200_plan_create(&descs[i], &p);
+    if (r != HITB200_OK) {
+      hitb200_batch_destroy(b);
+      return r;
+    }
+    p->in_batch = true;
+    b->plans.push_back(p);
+    hs.push_back(p->hs);
+    const int ntx = (p->desc.nx + kTileX - 1) / kTileX, nty = (p->desc.ny + kTileY - 1) / kTileY;
+    int k = 0;
+    for (int ty = 0; ty < nty; ++ty)
+      for (int tx = 0; tx < ntx; ++tx) tiles.push_back({i, tx * kTileX, ty * kTileY, k++});
+    for (int r0 = 0; r0 < p->desc.ny; r0 += p->Rx) xl.push_back({i, r0, std::min(p->Rx, p->desc.ny - r0), 0});
+    for (int c0 = 0; c0 < p->desc.nx; c0 += p->Ry) yl.push_back({i, c0, std::min(p->Ry, p->desc.nx - c0), 0});
+    ModeTables mt = build_modes(p->desc);
+    partner.insert(partner.end(), mt.partner.begin(), mt.partner.end());
+    b->elem = p->elem;
+    b->mch_x = std::max(b->mch_x, mch_for(p->desc.nx));
+    b->mch_y = std::max(b->mch_y, mch_for(p->desc.ny));
+    b->smem_x = std::max(b->smem_x, p->smem_x);
+    b->smem_y = std::max(b->smem_y, p->smem_y);
+    b->smem_sensor = std::max(b->smem_sensor, p->smem_sensor);
+    b->any_outflow |= !p->desc.periodic;
+    b->any_forcing |= p->desc.forcing_on;
+    b->any_hv |= p->hs.hv_interval > 0;
+    b->any_noise_upload |= (p->desc.forcing_on && p->desc.noise_mode == 0);
+  }
+  if (b->any_noise_upload) {
+    hitb200_batch_destroy(b);
+    return invalid("batched solves draw forcing noise on the device (noise_mode 1)");
+  }
+  b->n_tiles = (int)tiles.size();
+  b->n_x = (int)xl.size();
+  b->n_y = (int)yl.size();
+  // interleave the sweep work of different solves so that large grids start first
+  cudaError_t e;
+  size_t bytes = hs.size() * sizeof(SolveDev) + (tiles.size() + xl.size() + yl.size()) * sizeof(Work) +
+                 partner.size() * sizeof(int) + 1024;
+  unsigned char* buf = nullptr;
+  e = cudaMalloc(&buf, bytes);
+  if (e != cudaSuccess) {
+    hitb200_batch_destroy(b);
+    return cuda_fail(e, "cudaMalloc(batch tables)");
+  }
+  size_t off = 0;
+  auto put = [&](const void* src, size_t nbytes) -> unsigned char* {
+    unsigned char* d = buf + off;
+    off += (nbytes + 255) & ~(size_t)255;
+    cudaMemcpy(d, src, nbytes, cudaMemcpyHostToDevice);
+    return d;
+  };
+  b->d_solves = reinterpret_cast<SolveDev*>(put(hs.data(), hs.size() * sizeof(SolveDev)));
+  b->d_tiles = reinterpret_cast<Work*>(put(tiles.data(), tiles.size() * sizeof(Work)));
+  b->d_xlines = reinterpret_cast<Work*>(put(xl.data(), xl.size() * sizeof(Work)));
+  b->d_ylines = reinterpret_cast<Work*>(put(yl.data(), yl.size() * sizeof(Work)));
+  b->d_partner = reinterpret_cast<int*>(put(partner.data(), partner.size() * sizeof(int)));
+  prime_attributes(b->elem, b->mch_x, b->mch_y, b->smem_x, b->smem_y, b->smem_sensor);
+  // member plans keep their own descriptors pointing at the batch copy
+  for (int i = 0; i < n; ++i) b->plans[i]->d_solve = b->d_solves + i;
+  *out = b;
+  return HITB200_OK;
+}
+
+int hitb200_batch_destroy(hitb200_batch* b) {
+  if (!b) return HITB200_OK;
+  if (b->graph) cudaGraphExecDestroy(b->graph);
+  if (b->d_solves) cudaFree(b->d_solves);
+  for (hitb200_plan* p : b->plans) {
+    p->d_solve = nullptr;
+    hitb200_plan_destroy(p);
+  }
+  delete b;
+  return HITB200_OK;
+}
+
+hitb200_plan* hitb200_batch_plan(hitb200_batch* b, int32_t i) {
+  if (!b || i < 0 || i >= (int)b->plans.size()) return nullptr;
+  return b->plans[i];
+}
+
+int hitb200_batch_bind(hitb200_batch* b, double* const* q) {
+  if (!b || !q) return invalid("NULL argument");
+  for (size_t i = 0; i < b->plans.size(); ++i) {
+    if (!q[i]) return invalid("NULL state pointer");
+    b->plans[i]->hs.q = q[i];
+    HB_CUDA(cudaMemcpy(&b->d_solves[i].q, &q[i], sizeof(double*), cudaMemcpyHostToDevice));
+  }
+  return HITB200_OK;
+}
+
+static LaunchSet batch_launch_set(hitb200_batch* b, cudaStream_t st) {
+  LaunchSet L;
+  L.solves = b->d_solves;
+  L.nsolves = (int)b->plans.size();
+  L.tiles = b->d_tiles;
+  L.xl = b->d_xlines;
+  L.yl = b->d_ylines;
+  L.partner = b->d_partner;
+  L.n_tiles = b->n_tiles;
+  L.n_x = b->n_x;
+  L.n_y = b->n_y;
+  L.elem = b->elem;
+  L.mch_x = b->mch_x;
+  L.mch_y = b->mch_y;
+  L.smem_x = b->smem_x;
+  L.smem_y = b->smem_y;
+  L.smem_sensor = b->smem_sensor;
+  L.st = st;
+  return L;
+}
+
+int hitb200_batch_step(hitb200_batch* b, void* stream) {
+  if (!b) return invalid("NULL argument");
+  for (hitb200_plan* p : b->plans)
+    if (!p->hs.q) return invalid("batch state not bound");
+  LaunchSet L = batch_launch_set(b, (cudaStream_t)stream);
+  return launch_step_sequence(L, b->any_forcing, 0, b->any_outflow, b->any_hv);
+}
+
+int hitb200_batch_run(hitb200_batch* b, int32_t nsteps, void* stream) {
+  if (!b) return invalid("NULL argument");
+  for (hitb200_plan* p : b->plans)
+    if (!p->hs.q) return invalid("batch state not bound");
+  cudaStream_t st = (cudaStream_t)stream;
+  if (!b->graph || b->graph_stream != st) {
+    if (b->graph) cudaGraphExecDestroy(b->graph);
+    b->graph = nullptr;
+    cudaStream_t cap;
+    HB_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+    LaunchSet L = batch_launch_set(b, cap);
+    HB_CUDA(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
+    int r = launch_step_sequence(L, b->any_forcing, 0, b->any_outflow, b->any_hv);
+    cudaGraph_t gr;
+    cudaError_t e = cudaStreamEndCapture(cap, &gr);
+    cudaStreamDestroy(cap);
+    if (r != HITB200_OK) return r;
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+    e = cudaGraphInstantiate(&b->graph, gr, 0);
+    cudaGraphDestroy(gr);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGraphInstantiate");
+    b->graph_stream = st;
+  }
+  for (int i = 0; i < nsteps; ++i) HB_CUDA(cudaGraphLaunch(b->graph, st));
+  return HITB200_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,794 @@
+// Stencil kernels: shock sensor (+ viscous terms), the x / y line sweeps of
+// the hybrid compact/WENO7 flux derivative with their fused epilogues, the
+// biharmonic hyperviscosity, the outflow guard and the state clean.
+#pragma once
+
+#include "common.cuh"
+#include "kernels_reduce.cuh"
+#include "weno.cuh"
+
+namespace hitb200 {
+
+constexpr unsigned kFull = 0xffffffffu;
+constexpr int kStencilThreads = 256;
+constexpr int kSenTX = 32, kSenTY = 16;
+
+// =============================================================================
+// Shock sensor (OOP/spatial_operator.py:147-176, 263-304;
+// OOP/problems/riemann_config3.py:128-162, 288-326) and viscous terms
+// (OOP/equations.py:232-267) on a 32 x 16 tile with a (width + 1) halo.
+// Raw flags are evaluated on the tile plus a width-wide ring, then dilated
+// separably: a row pass (OR over +-width in x) and a column pass.
+// =============================================================================
+template <typename T>
+__device__ __forceinline__ T jump3(T am, T a, T ap, T eps) {
+  const T right = fabs(ap - a) / (fabs(ap) + fabs(a) + eps);
+  const T left = fabs(a - am) / (fabs(a) + fabs(am) + eps);
+  const T curv = fabs(ap - T(2) * a + am) / (fabs(ap) + T(2) * fabs(a) + fabs(am) + eps);
+  return fmax(fmax(left, right), curv);
+}
+
+__host__ __device__ inline int sensor_halo(int width) { return width + 1 > 2 ? width + 1 : 2; }
+
+__host__ __device__ inline size_t sensor_smem_bytes(int width, int elem) {
+  const int hw = sensor_halo(width);
+  const size_t sx = kSenTX + 2 * hw, sy = kSenTY + 2 * hw;
+  const size_t prim = 5 * sx * sy * (size_t)elem;
+  const size_t raw = (size_t)(kSenTY + 2 * width) * (kSenTX + 2 * width);
+  const size_t row = (size_t)(kSenTY + 2 * width) * kSenTX;
+  return prim + raw + row + 16;
+}
+
+// sel: 0 q, 1 q1, 2 q2, 3 hyperviscosity input (stage-3 output q1, runs only on
+// hyperviscosity steps).  want_visc: also write the viscous terms.
+template <typename T>
+__global__ void __launch_bounds__(kStencilThreads)
+    sensor_kernel(const SolveDev* __restrict__ solves, const Work* __restrict__ work, int sel,
+                  int enf, int want_visc, Bind bind, uint8_t* __restrict__ mask_out) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const Work wk = work[blockIdx.x];
+  const SolveDev& S = solves[wk.solve];
+  const double* sc = S.scal;
+  if (!bind.use) {
+    if (sel == 3 && sc[S_HV_STEP] == 0.0) return;
+    if (sel != 3 && sc[S_ACTIVE] == 0.0) return;
+  }
+  const double* q = bind.use ? bind.qin : (sel == 3 ? S.q1 : stage_in(S, sel));
+  uint8_t* mask = bind.use ? mask_out : S.mask;
+  const int nx = S.nx, ny = S.ny, per = S.periodic;
+  const size_t plane = (size_t)nx * ny;
+  const int W = S.width, HW = sensor_halo(W);
+  const int SX = kSenTX + 2 * HW, SY = kSenTY + 2 * HW;
+  const int x0 = wk.a, y0 = wk.b;
+  const T g = T(S.gamma);
+  T* RHO = reinterpret_cast<T*>(smem);
+  T* U = RHO + SX * SY;
+  T* V = U + SX * SY;
+  T* P = V + SX * SY;
+  T* E = P + SX * SY;
+  uint8_t* RAW = reinterpret_cast<uint8_t*>(E + SX * SY);
+  const int RX = kSenTX + 2 * W, RY = kSenTY + 2 * W;
+  uint8_t* ROW = RAW + RX * RY;
+
+  for (int idx = threadIdx.x; idx < SX * SY; idx += blockDim.x) {
+    const int a = idx / SX, b = idx % SX;
+    const int gj = wrap_or_clamp(y0 - HW + a, ny, per), gi = wrap_or_clamp(x0 - HW + b, nx, per);
+    const size_t o = (size_t)gj * nx + gi;
+    T q0 = T(q[o]), q1 = T(q[o + plane]), q2 = T(q[o + 2 * plane]), q3 = T(q[o + 3 * plane]);
+    if (enf) enforce_node(q0, q1, q2, q3, g);
+    const Prim<T> p = primitives(q0, q1, q2, q3, g);
+    RHO[idx] = p.rho;
+    U[idx] = p.u;
+    V[idx] = p.v;
+    P[idx] = p.p;
+    E[idx] = p.p / (p.rho * (g - T(1)));
+  }
+  __syncthreads();
+
+  const T eps_r = T(sc[S_EPS_RHO]), eps_p = T(sc[S_EPS_P]), eps_e = T(sc[S_EPS_E]);
+  const T thr = T(S.jump_thr);
+  const T comp_lim = T(sc[S_COMP_LIM]), shear_lim = T(sc[S_SHEAR_LIM]);
+  const T tdx = T(2.0 * S.dx), tdy = T(2.0 * S.dy), hx = T(S.dx), hy = T(S.dy);
+  const T tol = T(32) * (sizeof(T) == 4 ? T(FLT_EPSILON) : T(DBL_EPSILON));
+  int near = 0;
+  for (int idx = threadIdx.x; idx < RX * RY; idx += blockDim.x) {
+    const int ar = idx / RX, br = idx % RX;
+    const int gj = y0 - W + ar, gi = x0 - W + br;
+    const bool inside = gj >= 0 && gj < ny && gi >= 0 && gi < nx;
+    if (!per && !inside) {
+      RAW[idx] = 0;
+      continue;
+    }
+    const int a = ar + (HW - W), b = br + (HW - W);
+    const int c = a * SX + b;
+    // sensor velocity gradients: central; first-order one-sided at outflow edges
+    T dudx, dvdx, dudy, dvdy;
+    if (per || (gi > 0 && gi < nx - 1)) {
+      dudx = (U[c + 1] - U[c - 1]) / tdx;
+      dvdx = (V[c + 1] - V[c - 1]) / tdx;
+    } else if (nx == 1) {
+      dudx = dvdx = T(0);
+    } else if (gi == 0) {
+      dudx = (U[c + 1] - U[c]) / hx;
+      dvdx = (V[c + 1] - V[c]) / hx;
+    } else {
+      dudx = (U[c] - U[c - 1]) / hx;
+      dvdx = (V[c] - V[c - 1]) / hx;
+    }
+    if (per || (gj > 0 && gj < ny - 1)) {
+      dudy = (U[c + SX] - U[c - SX]) / tdy;
+      dvdy = (V[c + SX] - V[c - SX]) / tdy;
+    } else if (ny == 1) {
+      dudy = dvdy = T(0);
+    } else if (gj == 0) {
+      dudy = (U[c + SX] - U[c]) / hy;
+      dvdy = (V[c + SX] - V[c]) / hy;
+    } else {
+      dudy = (U[c] - U[c - SX]) / hy;
+      dvdy = (V[c] - V[c - SX]) / hy;
+    }
+    const T div = dudx + dvdy;
+    const T vort = dvdx - dudy;
+    const T jr = fmax(jump3(RHO[c - 1], RHO[c], RHO[c + 1], eps_r),
+                      jump3(RHO[c - SX], RHO[c], RHO[c + SX], eps_r));
+    const T jp = fmax(jump3(P[c - 1], P[c], P[c + 1], eps_p),
+                      jump3(P[c - SX], P[c], P[c + SX], eps_p));
+    const T je = fmax(jump3(E[c - 1], E[c], E[c + 1], eps_e),
+                      jump3(E[c - SX], E[c], E[c + SX], eps_e));
+    bool m = (div < comp_lim) || (fabs(vort) > shear_lim) || (jr > thr) || (jp > thr) || (je > thr);
+    if (!per && S.boundary_guard > 0) {
+      const int bg = S.boundary_guard;
+      if (gj < bg || gj >= ny - bg || gi < bg || gi >= nx - bg) m = true;
+    }
+    RAW[idx] = m ? 1 : 0;
+    // nodes of this tile whose metric sits within roundoff of a threshold
+    if (ar >= W && ar < W + kSenTY && br >= W && br < W + kSenTX && inside) {
+      const T tj = tol * thr;
+      bool nr = fabs(jr - thr) <= tj || fabs(jp - thr) <= tj || fabs(je - thr) <= tj;
+      if (isfinite(comp_lim)) nr = nr || fabs(div - comp_lim) <= tol * fabs(comp_lim);
+      if (isfinite(shear_lim)) nr = nr || fabs(fabs(vort) - shear_lim) <= tol * shear_lim;
+      near += nr ? 1 : 0;
+    }
+  }
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < RY * kSenTX; idx += blockDim.x) {
+    const int ar = idx / kSenTX, bx = idx % kSenTX;
+    uint8_t v = 0;
+    for (int d = 0; d <= 2 * W; ++d) v |= RAW[ar * RX + bx + d];
+    ROW[idx] = v;
+  }
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < kSenTX * kSenTY; idx += blockDim.x) {
+    const int ty = idx / kSenTX, tx = idx % kSenTX;
+    const int gj = y0 + ty, gi = x0 + tx;
+    if (gj >= ny || gi >= nx) continue;
+    uint8_t v = 0;
+    for (int d = 0; d <= 2 * W; ++d) v |= ROW[(ty + d) * kSenTX + tx];
+    mask[(size_t)gj * nx + gi] = v;
+  }
+  near = warp_sum(near);
+  if ((threadIdx.x & 31) == 0 && near > 0) atomicAdd(S.near_count, near);
+
+  if (!want_visc || S.mu == 0.0) return;
+  // viscous stress and heat-flux divergence, central differences (periodic)
+  const T mu = T(S.mu), kap = T(S.kappa), rgas = T(S.gas_r);
+  const T two3 = T(2.0 / 3.0);
+  T* visp = reinterpret_cast<T*>(S.vis);
+  for (int idx = threadIdx.x; idx < kSenTX * kSenTY; idx += blockDim.x) {
+    const int ty = idx / kSenTX, tx = idx % kSenTX;
+    const int gj = y0 + ty, gi = x0 + tx;
+    if (gj >= ny || gi >= nx) continue;
+    const int c = (ty + HW) * SX + tx + HW;
+    auto ddx = [&](const T* f, int o) { return (f[o + 1] - f[o - 1]) / tdx; };
+    auto ddy = [&](const T* f, int o) { return (f[o + SX] - f[o - SX]) / tdy; };
+    auto temp = [&](int o) { return P[o] / (RHO[o] * rgas); };
+    auto txx = [&](int o) {
+      const T ux = ddx(U, o);
+      return T(2) * mu * ux - two3 * mu * (ux + ddy(V, o));
+    };
+    auto tyy = [&](int o) {
+      const T vy = ddy(V, o);
+      return T(2) * mu * vy - two3 * mu * (ddx(U, o) + vy);
+    };
+    auto txy = [&](int o) { return mu * (ddy(U, o) + ddx(V, o)); };
+    auto efx = [&](int o) {
+      const T dtx = (temp(o + 1) - temp(o - 1)) / tdx;
+      return U[o] * txx(o) + V[o] * txy(o) + kap * dtx;
+    };
+    auto efy = [&](int o) {
+      const T dty = (temp(o + SX) - temp(o - SX)) / tdy;
+      return U[o] * txy(o) + V[o] * tyy(o) + kap * dty;
+    };
+    const T r1 = (txx(c + 1) - txx(c - 1)) / tdx + (txy(c + SX) - txy(c - SX)) / tdy;
+    const T r2 = (txy(c + 1) - txy(c - 1)) / tdx + (tyy(c + SX) - tyy(c - SX)) / tdy;
+    const T r3 = (efx(c + 1) - efx(c - 1)) / tdx + (efy(c + SX) - efy(c - SX)) / tdy;
+    const size_t o = (size_t)gj * nx + gi;
+    visp[o] = r1;
+    visp[plane + o] = r2;
+    visp[2 * plane + o] = r3;
+  }
+}
+
+// =============================================================================
+// Line sweeps.  A CTA owns R whole grid lines (rows for x, columns for y) of
+// one solve and runs, in shared memory:
+//   L  stage the enforced state, normal velocity and pressure of every node
+//      of the lines plus a 5-node halo (periodic wrap or clamped edge);
+//   H  per component: the hybrid face flux (6-point compact flux, or the
+//      compactised WENO7 flux on flagged faces) by warps that each own 29
+//      consecutive nodes, exchanging neighbour faces by shuffles, and the
+//      face difference raw_i = (H_{i+1/2} - H_{i-1/2}) / h;
+//   S  the compact tridiagonal solve 3/8 d_{i-1} + d_i + 3/8 d_{i+1} = raw_i,
+//      one warp per (line, component), as two first-order recurrences
+//      (factorisation below) evaluated by a chunked warp scan;
+//   E  the fused epilogue (partial rhs for x; RK stage combine + clean for y).
+//
+// Factorisation: a s^-1 + 1 + a s = (-a/rho)(1 - rho s^-1)(1 - rho s) with
+// rho = (sqrt(1 - 4 a^2) - 1) / (2 a) = (sqrt(7) - 4) / 3 for a = 3/8, so
+// d = (-rho/a) (1 - rho s)^-1 (1 - rho s^-1)^-1 raw: a forward recurrence
+// y_i = raw_i + rho y_{i-1} and a backward one z_i = y_i + rho z_{i+1}.
+// Periodic lines close each recurrence exactly (y_{-1} = y_{n-1} gives
+// y_{-1} = y~_{n-1} / (1 - rho^n)); outflow lines (identity first and last
+// rows, riemann_config3.py:244-264) add the two homogeneous solutions rho^i
+// and rho^(n-1-i) fitted to the end rows.
+// =============================================================================
+constexpr double kRhoSolve = -0.45141622964513645;  // (sqrt(7) - 4) / 3
+constexpr double kSolveScale = 1.2037766123870306;  // -rho / a
+constexpr int kMaxTasks = 16;                        // H-phase tasks per warp
+constexpr int kNodesPerTask = 29;
+
+template <typename T>
+__host__ __device__ inline int pad_index(int i) {
+  return sizeof(T) == 4 ? i + (i >> 5) : i + (i >> 4);
+}
+
+template <typename T>
+struct SweepLayout {
+  int n, LS, LQ, R;
+  __host__ __device__ SweepLayout(int n_, int R_) : n(n_), R(R_) {
+    LS = n + 2 * kHalo;
+    const int lp = pad_index<T>(n - 1) + 1;
+    LQ = (LS > lp ? LS : lp);
+    LQ = (LQ + 3) & ~3;
+  }
+  __host__ __device__ size_t bytes() const {
+    size_t b = (size_t)R * (4 * LQ + 2 * LS) * sizeof(T);
+    b += (size_t)R * (n + 2);
+    return (b + 15) & ~(size_t)15;
+  }
+};
+
+enum SweepMode : int { SW_STAGE = 0, SW_DERIV = 1, SW_RHS = 2 };
+
+// rhs terms of rhs_with_forcing (OOP/hit2d.py:847-867) that a solve carries:
+// 1 inviscid, 2 viscous, 4 forcing, 8 drag, 16 cooling.
+__device__ __forceinline__ int fused_terms(const SolveDev& S) {
+  return 1 | (S.mu > 0.0 ? 2 : 0) | (S.forcing_on ? 4 : 0) | (S.drag_on ? 8 : 0) |
+         (S.cooling_on ? 16 : 0);
+}
+
+constexpr double kB1C1 = 1.0 / 20.0 + (-1.0 / 480.0);
+constexpr double kA1B1C1 = 25.0 / 32.0 + 1.0 / 20.0 + (-1.0 / 480.0);
+
+// Physical flux component c at staged node s (x: AXIS 0, y: AXIS 1).
+template <typename T, int AXIS>
+__device__ __forceinline__ T line_flux(int c, const T* qs, int LQ, const T* un, const T* pp, int s) {
+  const T u = un[s];
+  if (c == 0) return qs[(1 + AXIS) * LQ + s];
+  if (c == 3) return (qs[3 * LQ + s] + pp[s]) * u;
+  const T f = qs[c * LQ + s] * u;
+  return (c == 1 + AXIS) ? f + pp[s] : f;
+}
+
+template <typename T, int AXIS>
+__device__ __forceinline__ T compact_face(int c, const T* qs, int LQ, const T* un, const T* pp,
+                                          int s) {
+  auto F = [&](int k) { return line_flux<T, AXIS>(c, qs, LQ, un, pp, s + k); };
+  return T(-1.0 / 480.0) * (F(3) + F(-2)) + T(kB1C1) * (F(2) + F(-1)) + T(kA1B1C1) * (F(1) + F(0));
+}
+
+template <typename T, int AXIS>
+__device__ __forceinline__ T weno_face(int c, const T* qs, int LQ, const T* un, const T* pp, int s,
+                                       T alpha) {
+  T fp[8], fm[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    const int sk = s - 3 + k;
+    const T F = line_flux<T, AXIS>(c, qs, LQ, un, pp, sk);
+    const T Q = qs[c * LQ + sk];
+    fp[k] = T(0.5) * (F + alpha * Q);
+    fm[k] = T(0.5) * (F - alpha * Q);
+  }
+  return weno7(fp[0], fp[1], fp[2], fp[3], fp[4], fp[5], fp[6]) +
+         weno7(fm[7], fm[6], fm[5], fm[4], fm[3], fm[2], fm[1]);
+}
+
+// Warp-cooperative solve of one line held at line[pad(i)], i in [0, n).
+template <typename T, int MCH>
+__device__ __forceinline__ void line_solve(T* line, int n, int per) {
+  const int lane = threadIdx.x & 31;
+  const int m = (n + 31) >> 5;
+  const int start = lane * m;
+  const int len = max(0, min(m, n - start));
+  const T rho = T(kRhoSolve);
+  T x[MCH];
+  T rfirst = T(0), rlast = T(0);
+#pragma unroll
+  for (int k = 0; k < MCH; ++k) {
+    x[k] = (k < len) ? line[pad_index<T>(start + k)] : T(0);
+    if (k < len && start + k == n - 1) rlast = x[k];
+  }
+  rfirst = x[0];
+  // forward y_i = raw_i + rho y_{i-1}
+  T acc = T(0), M = T(1);
+#pragma unroll
+  for (int k = 0; k < MCH; ++k)
+    if (k < len) {
+      acc = x[k] + rho * acc;
+      x[k] = acc;
+      M *= rho;
+    }
+  T A = acc;
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const T Mo = __shfl_up_sync(kFull, M, off), Ao = __shfl_up_sync(kFull, A, off);
+    if (lane >= off) {
+      A = M * Ao + A;
+      M = M * Mo;
+    }
+  }
+  {
+    T Me = __shfl_up_sync(kFull, M, 1), Ae = __shfl_up_sync(kFull, A, 1);
+    if (lane == 0) {
+      Me = T(1);
+      Ae = T(0);
+    }
+    const T Mt = __shfl_sync(kFull, M, 31), At = __shfl_sync(kFull, A, 31);
+    const T yin = per ? Me * (At / (T(1) - Mt)) + Ae : Ae;
+    T pw = rho;
+#pragma unroll
+    for (int k = 0; k < MCH; ++k)
+      if (k < len) {
+        x[k] += pw * yin;
+        pw *= rho;
+      }
+  }
+  // backward z_i = y_i + rho z_{i+1}
+  acc = T(0);
+  M = T(1);
+#pragma unroll
+  for (int k = MCH - 1; k >= 0; --k)
+    if (k < len) {
+      acc = x[k] + rho * acc;
+      x[k] = acc;
+      M *= rho;
+    }
+  A = acc;
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const T Mo = __shfl_down_sync(kFull, M, off), Ao = __shfl_down_sync(kFull, A, off);
+    if (lane + off < 32) {
+      A = M * Ao + A;
+      M = M * Mo;
+    }
+  }
+  {
+    T Me = __shfl_down_sync(kFull, M, 1), Ae = __shfl_down_sync(kFull, A, 1);
+    if (lane == 31) {
+      Me = T(1);
+      Ae = T(0);
+    }
+    const T Mt = __shfl_sync(kFull, M, 0), At = __shfl_sync(kFull, A, 0);
+    const T zin = per ? Me * (At / (T(1) - Mt)) + Ae : Ae;
+    T pw = rho;
+#pragma unroll
+    for (int k = MCH - 1; k >= 0; --k)
+      if (k < len) {
+        x[k] = T(kSolveScale) * (x[k] + pw * zin);
+        pw *= rho;
+      }
+  }
+  if (!per) {
+    // identity end rows: d = p + A rho^i + B rho^(n-1-i)
+    const int llast = (n - 1) / m;
+    rfirst = __shfl_sync(kFull, rfirst, 0);
+    rlast = __shfl_sync(kFull, rlast, llast);
+    T plast = T(0);
+#pragma unroll
+    for (int k = 0; k < MCH; ++k)
+      if (k < len && start + k == n - 1) plast = x[k];
+    const T pfirst = __shfl_sync(kFull, x[0], 0);
+    plast = __shfl_sync(kFull, plast, llast);
+    if (n == 1) {
+      if (len > 0) x[0] = rfirst;
+    } else {
+      const T e = T(pow(double(kRhoSolve), double(n - 1)));
+      const T r0 = rfirst - pfirst, r1 = rlast - plast;
+      const T den = T(1) - e * e;
+      const T ca = (r0 - e * r1) / den, cb = (r1 - e * r0) / den;
+      if (len > 0) {
+        T pa = T(pow(double(kRhoSolve), double(start)));
+        T pb = T(pow(double(kRhoSolve), double(n - start - len)));
+        T pbk[MCH];
+#pragma unroll
+        for (int k = MCH - 1; k >= 0; --k)
+          if (k < len) {
+            pbk[k] = pb;
+            pb *= rho;
+          }
+#pragma unroll
+        for (int k = 0; k < MCH; ++k)
+          if (k < len) {
+            x[k] += ca * pa + cb * pbk[k];
+            pa *= rho;
+          }
+      }
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < MCH; ++k)
+    if (k < len) line[pad_index<T>(start + k)] = x[k];
+}
+
+// stage: 0, 1, 2 (SSP-RK3 stage); mode: SweepMode.  For AXIS 1 with
+// mode SW_STAGE the epilogue writes the stage state
+//   stage 0: q1 = clean(q + dt L)
+//   stage 1: q2 = clean(3/4 q + 1/4 (q1 + dt L))
+//   stage 2:      clean(1/3 q + 2/3 (q2 + dt L))     (OOP/time_operator.py:21-26)
+template <typename T, int AXIS, int MCH>
+__global__ void __launch_bounds__(kStencilThreads)
+    sweep_kernel(const SolveDev* __restrict__ solves, const Work* __restrict__ work, int stage,
+                 int mode, Bind bind) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const Work wk = work[blockIdx.x];
+  const SolveDev& S = solves[wk.solve];
+  const double* sc = S.scal;
+  if (!bind.use && sc[S_ACTIVE] == 0.0) return;
+  const int nx = S.nx, ny = S.ny, per = S.periodic;
+  const int n = AXIS == 0 ? nx : ny;
+  const size_t plane = (size_t)nx * ny;
+  const int line0 = wk.a, R = wk.b;
+  const SweepLayout<T> L(n, R);
+  const int LS = L.LS, LQ = L.LQ;
+  const T g = T(S.gamma);
+  const double h = AXIS == 0 ? S.dx : S.dy;
+  const double* qin = bind.use ? bind.qin : stage_in(S, stage);
+  const uint8_t* mask = bind.use ? bind.mask : S.mask;
+  const T alpha = T(AXIS == 0 ? sc[S_ALPHA_X] : sc[S_ALPHA_Y]);
+  T* QS = reinterpret_cast<T*>(smem);
+  T* UN = QS + (size_t)R * 4 * LQ;
+  T* PP = UN + (size_t)R * LS;
+  uint8_t* MK = reinterpret_cast<uint8_t*>(PP + (size_t)R * LS);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+
+  // ---- L: stage the lines ----------------------------------------------------
+  for (int idx = threadIdx.x; idx < R * LS; idx += blockDim.x) {
+    int r, p;
+    if (AXIS == 0) {
+      r = idx / LS;
+      p = idx - r * LS;
+    } else {
+      r = idx % R;
+      p = idx / R;
+    }
+    const int gp = wrap_or_clamp(p - kHalo, n, per);
+    const size_t o = AXIS == 0 ? (size_t)(line0 + r) * nx + gp : (size_t)gp * nx + line0 + r;
+    T a0 = T(qin[o]), a1 = T(qin[o + plane]), a2 = T(qin[o + 2 * plane]), a3 = T(qin[o + 3 * plane]);
+    enforce_node(a0, a1, a2, a3, g);
+    const Prim<T> pr = primitives(a0, a1, a2, a3, g);
+    T* qs = QS + (size_t)r * 4 * LQ + p;
+    qs[0] = a0;
+    qs[LQ] = a1;
+    qs[2 * LQ] = a2;
+    qs[3 * LQ] = a3;
+    UN[r * LS + p] = AXIS == 0 ? pr.u : pr.v;
+    PP[r * LS + p] = pr.p;
+  }
+  const int weno_all = S.scheme == 1;
+  for (int idx = threadIdx.x; idx < R * (n + 2); idx += blockDim.x) {
+    int r, p;
+    if (AXIS == 0) {
+      r = idx / (n + 2);
+      p = idx - r * (n + 2);
+    } else {
+      r = idx % R;
+      p = idx / R;
+    }
+    const int gp = wrap_or_clamp(p - 1, n, per);
+    const size_t o = AXIS == 0 ? (size_t)(line0 + r) * nx + gp : (size_t)gp * nx + line0 + r;
+    MK[r * (n + 2) + p] = weno_all ? 1 : mask[o];
+  }
+  __syncthreads();
+
+  // ---- H: face fluxes and their differences, one component at a time ----------
+  const int tpl = (n + kNodesPerTask - 1) / kNodesPerTask;
+  const int ntask = R * tpl;
+  const T inv_h = T(1.0 / h);
+  for (int c = 0; c < 4; ++c) {
+    T rv[kMaxTasks];
+    int ri[kMaxTasks];
+#pragma unroll
+    for (int t = 0; t < kMaxTasks; ++t) {
+      ri[t] = -1;
+      rv[t] = T(0);
+      const int task = warp + t * nwarp;
+      if (task < ntask) {
+        const int r = task / tpl, base = (task - r * tpl) * kNodesPerTask;
+        const int il = base - 2 + lane;  // this lane's face il + 1/2
+        const T* qs = QS + (size_t)r * 4 * LQ;
+        const T* un = UN + r * LS;
+        const T* pp = PP + r * LS;
+        const uint8_t* mk = MK + r * (n + 2);
+        auto flg = [&](int f) -> bool { return f >= -1 && f <= n - 1 && (mk[f + 1] | mk[f + 2]); };
+        const bool f0 = flg(il);
+        const bool need = flg(il - 1) || f0 || flg(il + 1);
+        T wv = T(0);
+        if (need) {
+          const int ie = per ? il : min(max(il, -1), n - 1);
+          wv = weno_face<T, AXIS>(c, qs, LQ, un, pp, ie + kHalo, alpha);
+        }
+        const T wp = __shfl_down_sync(kFull, wv, 1), wm = __shfl_up_sync(kFull, wv, 1);
+        T hf = T(0);
+        if (il >= -1 && il <= n - 1) {
+          if (f0) {
+            hf = T(kCompactA) * wp + wv;
+            hf = hf + T(kCompactA) * wm;
+          } else {
+            hf = compact_face<T, AXIS>(c, qs, LQ, un, pp, il + kHalo);
+          }
+        }
+        const T hm = __shfl_up_sync(kFull, hf, 1);
+        if (lane >= 2 && lane <= 30 && il >= 0 && il < n) {
+          rv[t] = (hf - hm) * inv_h;
+          ri[t] = r * 4 * LQ + c * LQ + pad_index<T>(il);
+        }
+      }
+    }
+    __syncthreads();  // every read of this component's staged values is done
+#pragma unroll
+    for (int t = 0; t < kMaxTasks; ++t)
+      if (ri[t] >= 0) QS[ri[t]] = rv[t];
+  }
+  __syncthreads();
+
+  // ---- S: compact solves ---------------------------------------------------------
+  for (int item = warp; item < 4 * R; item += nwarp) {
+    const int r = item >> 2, c = item & 3;
+    line_solve<T, MCH>(QS + (size_t)r * 4 * LQ + c * LQ, n, per);
+  }
+  __syncthreads();
+
+  // ---- E: epilogue ------------------------------------------------------------------
+  const double fs = sc[S_F_SCALE];
+  const int terms = bind.use ? bind.terms : fused_terms(S);
+  for (int idx = threadIdx.x; idx < R * n; idx += blockDim.x) {
+    int r, p;
+    if (AXIS == 0) {
+      r = idx / n;
+      p = idx - r * n;
+    } else {
+      r = idx % R;
+      p = idx / R;
+    }
+    const int row = AXIS == 0 ? line0 + r : p, col = AXIS == 0 ? p : line0 + r;
+    const size_t o = (size_t)row * nx + col;
+    const T* dl = QS + (size_t)r * 4 * LQ + pad_index<T>(p);
+    T d[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) d[c] = dl[c * LQ];
+    if (mode == SW_DERIV) {
+#pragma unroll
+      for (int c = 0; c < 4; ++c) bind.out[c * plane + o] = double(d[c]);
+      continue;
+    }
+    if (!(terms & 1)) {
+#pragma unroll
+      for (int c = 0; c < 4; ++c) d[c] = T(0);
+    }
+    if (AXIS == 0) {
+      T v[4] = {-d[0], -d[1], -d[2], -d[3]};
+      if ((terms & 2) && S.mu > 0.0) {
+        const T* vis = reinterpret_cast<const T*>(S.vis);
+        v[1] += vis[o];
+        v[2] += vis[plane + o];
+        v[3] += vis[2 * plane + o];
+      }
+      if (terms & (4 | 8)) {
+        const Prim<double> pr = primitives(qin[o], qin[o + plane], qin[o + 2 * plane], qin[o + 3 * plane], S.gamma);
+        if (terms & 4) {
+          const T fxv = bind.use ? T(bind.fx[o]) : T(fs * S.fx[o]);
+          const T fyv = bind.use ? T(bind.fy[o]) : T(fs * S.fy[o]);
+          const T rho = T(pr.rho), u = T(pr.u), vv = T(pr.v);
+          v[1] += rho * fxv;
+          v[2] += rho * fyv;
+          v[3] += rho * (u * fxv + vv * fyv);
+        }
+        if ((terms & 8) && S.drag_on) {
+          T lx = T(0), ly = T(0);
+          for (int md = 0; md < S.n_drag; ++md) {
+            const int2 k = S.modes[md];
+            int ix = (int)(((long long)k.x * col) % nx);
+            if (ix < 0) ix += nx;
+            int iy = (int)(((long long)k.y * row) % ny);
+            if (iy < 0) iy += ny;
+            const double2 ex = S.twx[ix], ey = S.twy[iy];
+            const T er = T(cmul_re(ex, ey)), ei = T(-cmul_im(ex, ey));
+            const double* cf = sc + S_DRAG + 4 * md;
+            lx += T(cf[0]) * er - T(cf[1]) * ei;
+            ly += T(cf[2]) * er - T(cf[3]) * ei;
+          }
+          v[1] += lx;
+          v[2] += ly;
+          v[3] += T(pr.u) * lx + T(pr.v) * ly;
+        }
+      }
+      if (terms & 16) v[3] += T(sc[S_COOL]);
+      T* rx = reinterpret_cast<T*>(S.rx);
+#pragma unroll
+      for (int c = 0; c < 4; ++c) rx[c * plane + o] = v[c];
+    } else {
+      const T* rx = reinterpret_cast<const T*>(S.rx);
+      double rhs[4];
+#pragma unroll
+      for (int c = 0; c < 4; ++c) rhs[c] = double(rx[c * plane + o]) - double(d[c]);
+      if (mode == SW_RHS) {
+#pragma unroll
+        for (int c = 0; c < 4; ++c) bind.out[c * plane + o] = rhs[c];
+        continue;
+      }
+      const double dt = sc[S_DT];
+      const double* q0 = bind.use ? bind.q0 : S.q;
+      double* qo = bind.use ? bind.qout : stage_out(S, stage);
+      double s[4];
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        const double t = qin[c * plane + o] + dt * rhs[c];
+        if (stage == 0) s[c] = t;
+        else if (stage == 1) s[c] = 0.75 * q0[c * plane + o] + 0.25 * t;
+        else s[c] = (1.0 / 3.0) * q0[c * plane + o] + (2.0 / 3.0) * t;
+      }
+      enforce_node(s[0], s[1], s[2], s[3], S.gamma);
+#pragma unroll
+      for (int c = 0; c < 4; ++c) qo[c * plane + o] = s[c];
+    }
+  }
+}
+
+// =============================================================================
+// Biharmonic hyperviscosity q - mn w h^4 active lap(lap q), then enforce
+// (OOP/spatial_operator.py:394-435 periodic; riemann_config3.py:390-416 with
+// an edge-padded Laplacian, applied to the padded Laplacian again).
+// =============================================================================
+template <typename T>
+__global__ void __launch_bounds__(kStencilThreads)
+    hv_kernel(const SolveDev* __restrict__ solves, const Work* __restrict__ work, Bind bind) {
+  constexpr int QX = kSenTX + 4, QY = kSenTY + 4, LX = kSenTX + 2, LY = kSenTY + 2;
+  __shared__ T Qs[4][QY][QX];
+  __shared__ T Ls[4][LY][LX];
+  const Work wk = work[blockIdx.x];
+  const SolveDev& S = solves[wk.solve];
+  if (!bind.use && S.scal[S_HV_STEP] == 0.0) return;
+  const double* q = bind.use ? bind.qin : S.q1;
+  double* out = bind.use ? bind.qout : S.q;
+  const uint8_t* mask = bind.use ? bind.mask : S.mask;
+  const int inv = bind.use ? bind.invert_mask : 1;
+  const int nx = S.nx, ny = S.ny, per = S.periodic;
+  const size_t plane = (size_t)nx * ny;
+  const int x0 = wk.a, y0 = wk.b;
+  for (int idx = threadIdx.x; idx < QX * QY; idx += blockDim.x) {
+    const int a = idx / QX, b = idx % QX;
+    const int gj = wrap_or_clamp(y0 - 2 + a, ny, per), gi = wrap_or_clamp(x0 - 2 + b, nx, per);
+    const size_t o = (size_t)gj * nx + gi;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) Qs[c][a][b] = T(q[c * plane + o]);
+  }
+  __syncthreads();
+  const T dx2 = T(S.dx * S.dx), dy2 = T(S.dy * S.dy);
+  for (int idx = threadIdx.x; idx < LX * LY; idx += blockDim.x) {
+    int a = idx / LX, b = idx % LX;
+    // outflow: the Laplacian is itself edge-padded before the second pass
+    int gj = y0 - 1 + a, gi = x0 - 1 + b;
+    if (!per) {
+      const int cj = gj < 0 ? 0 : (gj >= ny ? ny - 1 : gj);
+      const int ci = gi < 0 ? 0 : (gi >= nx ? nx - 1 : gi);
+      a += cj - gj;
+      b += ci - gi;
+    }
+    const int qa = a + 1, qb = b + 1;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      const T lx = (Qs[c][qa][qb + 1] - T(2) * Qs[c][qa][qb] + Qs[c][qa][qb - 1]) / dx2;
+      const T ly = (Qs[c][qa + 1][qb] - T(2) * Qs[c][qa][qb] + Qs[c][qa - 1][qb]) / dy2;
+      Ls[c][idx / LX][idx % LX] = lx + ly;
+    }
+  }
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < kSenTX * kSenTY; idx += blockDim.x) {
+    const int ty = idx / kSenTX, tx = idx % kSenTX;
+    const int gj = y0 + ty, gi = x0 + tx;
+    if (gj >= ny || gi >= nx) continue;
+    const size_t o = (size_t)gj * nx + gi;
+    const bool active = inv ? (mask[o] == 0) : (mask[o] != 0);
+    const int a = ty + 1, b = tx + 1;
+    double s[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      const T bx = (Ls[c][a][b + 1] - T(2) * Ls[c][a][b] + Ls[c][a][b - 1]) / dx2;
+      const T by = (Ls[c][a + 1][b] - T(2) * Ls[c][a][b] + Ls[c][a - 1][b]) / dy2;
+      const double bih = double(bx + by);
+      s[c] = q[c * plane + o] - (active ? S.hv_coef[c] : 0.0) * bih;
+    }
+    enforce_node(s[0], s[1], s[2], s[3], S.gamma);
+#pragma unroll
+    for (int c = 0; c < 4; ++c) out[c * plane + o] = s[c];
+  }
+}
+
+// Outflow guard: every guard cell takes the value of the nearest interior
+// cell column/row g or n-g-1 (x first, then y: the corner takes (g, g)).
+// sel: 0 q, 1 q1, 2 q2, 3 stage-3 output; one CTA per solve.
+__global__ void guard_kernel(const SolveDev* __restrict__ solves, int nsolves, int sel, Bind bind) {
+  const int s = blockIdx.x;
+  if (s >= nsolves) return;
+  const SolveDev& S = solves[s];
+  if (S.periodic || S.guard <= 0) return;
+  if (!bind.use && S.scal[S_ACTIVE] == 0.0 && sel != 0) return;
+  double* q = bind.use ? bind.qout : (sel == 0 ? S.q : sel == 1 ? S.q1 : sel == 2 ? S.q2 : stage_out(S, 2));
+  const int nx = S.nx, ny = S.ny, gc = S.guard;
+  const size_t plane = (size_t)nx * ny;
+  const int top = 2 * gc * nx;                 // full rows
+  const int side = 2 * gc * (ny - 2 * gc);     // side columns of interior rows
+  for (int t = threadIdx.x; t < top + side; t += blockDim.x) {
+    int j, i;
+    if (t < top) {
+      const int rr = t / nx;
+      i = t % nx;
+      j = rr < gc ? rr : ny - 2 * gc + rr;
+    } else {
+      const int u = t - top, cc = u % (2 * gc);
+      j = gc + u / (2 * gc);
+      i = cc < gc ? cc : nx - 2 * gc + cc;
+    }
+    const int J = j < gc ? gc : (j > ny - gc - 1 ? ny - gc - 1 : j);
+    const int I = i < gc ? gc : (i > nx - gc - 1 ? nx - gc - 1 : i);
+    if (J == j && I == i) continue;
+    const size_t dst = (size_t)j * nx + i, src = (size_t)J * nx + I;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) q[c * plane + dst] = q[c * plane + src];
+  }
+}
+
+__global__ void enforce_kernel(const double* __restrict__ q, double* __restrict__ out, size_t plane,
+                               double gamma) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < plane;
+       i += (size_t)gridDim.x * blockDim.x) {
+    double s0 = q[i], s1 = q[plane + i], s2 = q[2 * plane + i], s3 = q[3 * plane + i];
+    enforce_node(s0, s1, s2, s3, gamma);
+    out[i] = s0;
+    out[plane + i] = s1;
+    out[2 * plane + i] = s2;
+    out[3 * plane + i] = s3;
+  }
+}
+
+// out[c] = scale * a  (forcing accelerations for the API, viscous copy)
+__global__ void scale_copy_kernel(const double* __restrict__ a, double* __restrict__ out,
+                                  const double* __restrict__ scal, int slot, size_t n) {
+  const double s = slot >= 0 ? scal[slot] : 1.0;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    out[i] = s * a[i];
+}
+
+template <typename T>
+__global__ void vis_copy_kernel(const T* __restrict__ vis, double* __restrict__ out, size_t plane) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < plane;
+       i += (size_t)gridDim.x * blockDim.x) {
+    out[i] = 0.0;
+    out[plane + i] = double(vis[i]);
+    out[2 * plane + i] = double(vis[plane + i]);
+    out[3 * plane + i] = double(vis[2 * plane + i]);
+  }
+}
+
+}  // namespace hitb200

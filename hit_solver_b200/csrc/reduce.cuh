@@ -1,0 +1,86 @@
+// Grid reductions of the hot path and the scalar logic that consumes them.
+//
+// Every reducing kernel follows one deterministic pattern: each CTA reduces
+// its tile (warp shuffles, then across warps in shared memory) and writes one
+// row of per-block partials; the last CTA of the solve to finish (atomic
+// ticket) sums the partials in a fixed order and runs the scalar logic in one
+// thread.  Results therefore do not depend on scheduling, and no value ever
+// travels to the host: time step, Lax-Friedrichs speeds, sensor limits,
+// Mach control and forcing scales stay in the solve's scalar block.
+#pragma once
+
+#include "common.cuh"
+
+namespace hitb200 {
+
+constexpr int kRedThreads = 256;
+constexpr int kRedWarps = kRedThreads / 32;
+constexpr int kTileX = 32;   // prepass / noise / synth tile: 32 x 16 cells
+constexpr int kTileY = 16;
+
+enum RedOp : int { OP_SUM = 0, OP_MAX = 1 };
+
+// Reduce `v` over the CTA into sm[warp][slot] (call from all threads).
+template <int OP>
+__device__ __forceinline__ void warp_to_smem(double v, double* sm, int slot, int nslots) {
+  v = OP == OP_SUM ? warp_sum(v) : warp_max(v);
+  if ((threadIdx.x & 31) == 0) sm[(threadIdx.x >> 5) * nslots + slot] = v;
+}
+
+// After __syncthreads: threads t < nslots combine the warps and store row `blk`.
+__device__ __forceinline__ void smem_to_partials(const double* sm, int nslots,
+                                                 const int* ops, double* part, int blk) {
+  for (int t = threadIdx.x; t < nslots; t += blockDim.x) {
+    double acc = sm[t];
+    const int op = ops ? ops[t] : OP_SUM;
+    for (int w = 1; w < kRedWarps; ++w) {
+      double x = sm[w * nslots + t];
+      acc = op == OP_SUM ? acc + x : fmax(acc, x);
+    }
+    part[(size_t)blk * nslots + t] = acc;
+  }
+}
+
+// Ticket: returns true in the last CTA of the solve.  Resets the counter.
+__device__ __forceinline__ bool last_block(unsigned* counter, int nblk) {
+  __shared__ bool is_last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned t = atomicAdd(counter, 1u);
+    is_last = (t == (unsigned)nblk - 1u);
+    if (is_last) *counter = 0u;
+  }
+  __syncthreads();
+  if (is_last) __threadfence();
+  return is_last;
+}
+
+// Final fixed-order reduction of partials[nblk][nslots] into out[nslots].
+__device__ __forceinline__ void finalize_partials(const double* part, int nblk, int nslots,
+                                                  const int* ops, double* out) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int t = warp; t < nslots; t += kRedWarps) {
+    const int op = ops ? ops[t] : OP_SUM;
+    double acc = op == OP_SUM ? 0.0 : -INFINITY;
+    for (int b = lane; b < nblk; b += 32) {
+      double x = __ldcg(part + (size_t)b * nslots + t);
+      acc = op == OP_SUM ? acc + x : fmax(acc, x);
+    }
+    acc = op == OP_SUM ? warp_sum(acc) : warp_max(acc);
+    if (lane == 0) out[t] = acc;
+  }
+  __syncthreads();
+}
+
+__device__ __forceinline__ int red_op(int slot) {
+  switch (slot) {
+    case R_AX: case R_AY: case R_RHO: case R_P: case R_E: case R_SR:
+    case R_NONFINITE: case R_NONPOS_RHO: case R_NONPOS_P:
+      return OP_MAX;
+    default:
+      return OP_SUM;
+  }
+}
+
+}  // namespace hitb200

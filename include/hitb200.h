@@ -1,0 +1,234 @@
+/*
+ * hitb200.h — C ABI of the B200 (sm_100a) backend for the HIT_Solver hot path:
+ * the hybrid compact/WENO7 right-hand side, its shock sensor, the viscous and
+ * source terms, the biharmonic hyperviscosity, the SSP-RK3 step and the
+ * reductions that drive time step, forcing and Mach control.
+ *
+ * Conventions
+ *   - State arrays are device pointers to C-contiguous double[4][ny][nx]
+ *     ordered [rho, rho*u, rho*v, E] (OOP/equations.py:126-130).  Scalar
+ *     fields are double[ny][nx]; masks are uint8_t[ny][nx] (0/1).
+ *   - Every call is stream-ordered on the given cudaStream_t (passed as
+ *     void*; NULL = legacy default stream) and returns an int status
+ *     (HITB200_OK = 0).  Only calls documented as "synchronises" wait for the
+ *     device.
+ *   - The caller owns every array it passes.  A plan owns its scratch, which
+ *     it allocates in hitb200_plan_create and frees in hitb200_plan_destroy.
+ *   - Plans are not thread-safe; distinct plans may be used concurrently.
+ *
+ * Each entry point names the reference interface it replaces (file:line
+ * within the HIT_Solver project).
+ */
+#ifndef HITB200_H
+#define HITB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------- */
+#define HITB200_OK 0
+#define HITB200_ERR_INVALID 1     /* bad argument or descriptor  -> ValueError        */
+#define HITB200_ERR_CUDA 2        /* CUDA runtime failure        -> RuntimeError      */
+#define HITB200_ERR_NONFINITE 3   /* NaN/Inf in the state        -> FloatingPointError */
+#define HITB200_ERR_NONPOSITIVE 4 /* rho <= 0 or p <= 0          -> FloatingPointError */
+#define HITB200_ERR_OOM 5         /* device allocation failed    -> MemoryError       */
+#define HITB200_ERR_UNSUPPORTED 6 /* grid or option outside the supported range        */
+
+/* ---- rhs term selection (bit mask) --------------------------------------- */
+#define HITB200_TERM_INVISCID 1 /* -dF/dx - dG/dy, hybrid scheme  */
+#define HITB200_TERM_VISCOUS 2  /* viscous stress + heat flux     */
+#define HITB200_TERM_FORCING 4  /* rho f source (fx, fy given)    */
+#define HITB200_TERM_DRAG 8     /* low-k momentum drag            */
+#define HITB200_TERM_COOLING 16 /* uniform mean-pressure sink     */
+#define HITB200_TERM_ALL 31
+
+/* ---- solve descriptor ----------------------------------------------------- */
+/* One grid and its physics.  NaN in an optional double means "None" in the
+ * reference's Python API.  hitb200_desc_init fills the reference defaults of
+ * HIT2DConfig (OOP/hit2d.py:36-80). */
+typedef struct hitb200_desc {
+  int32_t nx, ny;
+  double x_min, x_max, y_min, y_max;
+  int32_t periodic;  /* 1: periodic (HIT); 0: outflow with guard cells (Riemann) */
+  int32_t precision; /* 0: FP64 throughout; 1: FP32 stencil/WENO/flux arithmetic, FP64 state */
+  int32_t scheme;    /* 0: hybrid compact/WENO; 1: WENO on every face (Riemann "weno") */
+  double gamma;
+  /* shock sensor (OOP/spatial_operator.py:252-304, riemann_config3.py:278-326) */
+  int32_t sensor_width;
+  int32_t boundary_guard; /* outflow only: band forced to WENO before dilation */
+  double compression_threshold;
+  double jump_threshold;
+  double shear_threshold; /* NaN: shear part off */
+  /* viscous / thermal (OOP/equations.py:211-267); viscosity 0 turns it off */
+  double viscosity, prandtl, gas_constant;
+  /* hyperviscosity (OOP/spatial_operator.py:380-435, riemann_config3.py:381-416) */
+  double hv_mn;
+  double hv_weight[4];
+  int32_t hv_interval; /* steps between applications inside hitb200_step; 0: never */
+  int32_t guard_cells; /* outflow guard (riemann_config3.py:419-429) */
+  /* HIT sources (OOP/hit2d.py:264-426) */
+  double drag_coefficient, drag_kmax; /* coefficient <= 0: off */
+  double cooling_time;                /* <= 0 or NaN: off */
+  double cooling_target_pressure;     /* NaN: 1/gamma */
+  /* OU forcing (OOP/forcing.py:11-130) */
+  int32_t forcing_on;
+  double forcing_kmin, forcing_kmax, forcing_correlation_time, forcing_rms;
+  double target_power; /* NaN: None */
+  double min_power;
+  double max_rescale;  /* NaN: None */
+  double alpha_memory;
+  /* Mach control (OOP/hit2d.py:293-349) */
+  int32_t mach_control;
+  double mach_target, mach_memory, mach_exponent;
+  double mach_min_power, mach_max_power; /* NaN: None */
+  /* time stepping */
+  double cfl, tfinal;
+  int32_t fixed_dt;   /* 1: dt fixed by hitb200_set_time (Riemann); 0: CFL dt each step (HIT) */
+  int32_t noise_mode; /* 0: forcing noise fields uploaded by the caller; 1: device RNG */
+  uint64_t seed;      /* device RNG seed (noise_mode 1) */
+} hitb200_desc;
+
+typedef struct hitb200_plan hitb200_plan;
+
+/* Scalar slots readable with hitb200_read_scalars (doubles). */
+enum hitb200_scalar {
+  HITB200_S_ALPHA_X = 0,  /* Lax-Friedrichs speed of the last RHS, x */
+  HITB200_S_ALPHA_Y = 1,
+  HITB200_S_DIV_RMS = 2,  /* sensor divergence rms of the last RHS */
+  HITB200_S_VORT_RMS = 3,
+  HITB200_S_DT = 4,       /* time step of the current / last step */
+  HITB200_S_TIME = 5,
+  HITB200_S_STEP = 6,
+  HITB200_S_ACTIVE = 7,   /* 1 while time < tfinal (and step < max_steps) */
+  HITB200_S_MACH = 8,     /* Mt of the step's start state */
+  HITB200_S_POWER = 9,    /* adaptive forcing power target */
+  HITB200_S_POWER_DESIRED = 10,
+  HITB200_S_F_ALPHA = 11, /* forcing info (OOP/forcing.py:119-130) */
+  HITB200_S_F_ALPHA_TARGET = 12,
+  HITB200_S_F_POWER_BEFORE = 13,
+  HITB200_S_F_INJECTED = 14,
+  HITB200_S_F_FXX = 15,
+  HITB200_S_F_FYY = 16,
+  HITB200_S_F_FXY = 17,
+  HITB200_S_F_AF = 18,
+  HITB200_S_F_DECAY = 19,
+  HITB200_S_F_SCALE = 20, /* factor applied to the unit-rms forcing shape */
+  HITB200_S_MAX_STEPS = 21,
+  HITB200_S_STATUS = 22,  /* OR of status bits found by the step's reductions */
+  HITB200_S_NEAR_THRESHOLD = 23, /* sensor nodes within roundoff of a threshold */
+  HITB200_S_HV_APPLIED = 24,     /* hyperviscosity applications so far */
+  HITB200_S_COUNT = 32
+};
+
+/* ---- plan ---------------------------------------------------------------- */
+/* Defaults of HIT2DConfig (OOP/hit2d.py:36-80) on a 2*pi periodic square. */
+int hitb200_desc_init(hitb200_desc* desc);
+/* Replaces constructing the sensor/operator/hyperviscosity/forcing objects
+ * (OOP/hit2d.py:773-803, OOP/problems/riemann_config3.py:689-707). */
+int hitb200_plan_create(const hitb200_desc* desc, hitb200_plan** plan);
+int hitb200_plan_destroy(hitb200_plan* plan);
+/* Device bytes a plan of this descriptor allocates (admission control). */
+size_t hitb200_plan_device_bytes(const hitb200_desc* desc);
+const char* hitb200_status_string(int status);
+/* Library build identifier, for logs. */
+const char* hitb200_version(void);
+/* sizeof(hitb200_desc), so that bindings can check their struct layout. */
+size_t hitb200_desc_size(void);
+
+/* ---- operators on caller arrays (stream ordered) --------------------------- */
+/* EulerEquation2D.enforce_physical_state (OOP/equations.py:165-181). */
+int hitb200_enforce(hitb200_plan* plan, const double* q, double* out, void* stream);
+/* The same without a plan: ncells = nx * ny nodes of a [4][ny][nx] state. */
+int hitb200_enforce_state(const double* q, double* out, int64_t ncells, double gamma,
+                          void* stream);
+/* PeriodicEulerShockSensor2D.detect (OOP/spatial_operator.py:263-304) and
+ * NonPeriodicEulerShockSensor2D.detect (riemann_config3.py:288-326).
+ * enforce_first=1 evaluates it on enforce_physical_state(q), as rhs() does. */
+int hitb200_sensor(hitb200_plan* plan, const double* q, uint8_t* mask, int enforce_first,
+                   void* stream);
+/* _axis_derivative (OOP/spatial_operator.py:321-342, riemann_config3.py:344-357)
+ * on enforce_physical_state(q) with a caller mask; axis 0 = x, 1 = y. */
+int hitb200_axis_derivative(hitb200_plan* plan, const double* q, const uint8_t* mask, int axis,
+                            double* out, void* stream);
+/* PeriodicHybridEuler2DOperator.rhs (OOP/spatial_operator.py:344-367) when
+ * terms = HITB200_TERM_INVISCID; rhs_with_forcing (OOP/hit2d.py:847-867) with
+ * all terms; any subset gives the sum of those terms (e.g. HITB200_TERM_DRAG
+ * alone is large_scale_drag_source, OOP/hit2d.py:370-399).  fx, fy (may be
+ * NULL without HITB200_TERM_FORCING) are the step's forcing accelerations. */
+int hitb200_rhs(hitb200_plan* plan, const double* q, int terms, const double* fx,
+                const double* fy, double* out, void* stream);
+/* CompressibleNavierStokes2D.viscous_rhs (OOP/equations.py:232-267). */
+int hitb200_viscous_rhs(hitb200_plan* plan, const double* q, double* out, void* stream);
+/* PeriodicHyperviscosity2D.apply (OOP/spatial_operator.py:407-435) and
+ * LocalHyperviscosity2D.apply (riemann_config3.py:398-416); active == NULL
+ * returns HITB200_ERR_INVALID as the reference raises ValueError. */
+int hitb200_hyperviscosity(hitb200_plan* plan, const double* q, const uint8_t* active,
+                           double* out, void* stream);
+/* apply_outflow_guard, in place (riemann_config3.py:419-429). */
+int hitb200_outflow_guard(hitb200_plan* plan, double* q, void* stream);
+/* stable_time_step (OOP/spatial_operator.py:369-377); synchronises. */
+int hitb200_stable_time_step(hitb200_plan* plan, const double* q, double cfl,
+                             double remaining_time, double* dt_out);
+/* validate_raw_physical_state (riemann_config3.py:442-452); synchronises and
+ * returns HITB200_ERR_NONFINITE / HITB200_ERR_NONPOSITIVE. */
+int hitb200_validate(hitb200_plan* plan, const double* q);
+
+/* ---- forcing ---------------------------------------------------------------- */
+/* IsotropicShellOUForcing2D.update (OOP/forcing.py:70-130) for the state q
+ * (its primitives give rho, u, v).  noise: device double[ny][nx] white noise
+ * (NULL with noise_mode 1 draws it on the device).  Writes fx, fy (the final,
+ * scaled accelerations) and updates the plan's OU potential and alpha; the
+ * info values are then in the scalar slots HITB200_S_F_*. */
+int hitb200_forcing_update(hitb200_plan* plan, const double* q, const double* noise, double dt,
+                           double target_power, double* fx, double* fy, void* stream);
+
+/* ---- time stepping ---------------------------------------------------------- */
+/* One step of the reference's loop body (OOP/hit2d.py:829-879,
+ * riemann_config3.py:729-740): time step from CFL (or the fixed dt), Mach
+ * control, forcing update, SSPRK3.step (OOP/time_operator.py:21-26) with
+ * rhs_with_forcing and the clean filter, then hyperviscosity every
+ * hv_interval steps.  q is advanced in place.  noise: this step's white-noise
+ * field (noise_mode 0 with forcing on) or NULL.  Time, step count and every
+ * control scalar stay on the device. */
+int hitb200_step(hitb200_plan* plan, double* q, const double* noise, void* stream);
+/* nsteps calls of hitb200_step replayed from one captured CUDA graph
+ * (noise_mode 1 or forcing off).  Steps after time reaches tfinal (or
+ * max_steps) are no-ops on the device. */
+int hitb200_run(hitb200_plan* plan, double* q, int32_t nsteps, void* stream);
+/* Set time, step count, dt (used when fixed_dt = 1) and max_steps (< 0: no limit). */
+int hitb200_set_time(hitb200_plan* plan, double time, int64_t step, double dt, int64_t max_steps);
+/* Copy scalar slots [0, n) to host memory; synchronises. */
+int hitb200_read_scalars(hitb200_plan* plan, double* out, int32_t n);
+/* Copy the device scalar slots asynchronously into caller memory
+ * (host-pinned or device), n doubles. */
+int hitb200_copy_scalars_async(hitb200_plan* plan, double* dst, int32_t n, void* stream);
+/* Scalar diagnostics of compute_diagnostics (OOP/hit2d.py:471-548), without
+ * the spectral divergence/vorticity, plus conservation sums and extrema:
+ * out[0..16] = kinetic_energy, Kx, Ky, A_K, C_uv, rms_velocity,
+ * turbulent_mach, mean_density, mean_pressure, mass (mean rho * area),
+ * x-momentum, y-momentum, total energy (integrals over the domain),
+ * raw rho min, rho max, p min, p max.  Synchronises. */
+int hitb200_diagnostics(hitb200_plan* plan, const double* q, double* out, int32_t n);
+
+/* ---- batched form ------------------------------------------------------------- */
+/* Many independent solves (any mix of grid sizes) advanced by one launch per
+ * kernel of the step: the "ensemble" / serving form.  All descriptors must
+ * share precision. */
+typedef struct hitb200_batch hitb200_batch;
+int hitb200_batch_create(const hitb200_desc* descs, int32_t n, hitb200_batch** batch);
+int hitb200_batch_destroy(hitb200_batch* batch);
+/* The member plan of solve i (for per-solve set_time / read_scalars). */
+hitb200_plan* hitb200_batch_plan(hitb200_batch* batch, int32_t i);
+/* Bind the state array of every solve (device pointers, kept until rebound). */
+int hitb200_batch_bind(hitb200_batch* batch, double* const* q);
+int hitb200_batch_step(hitb200_batch* batch, void* stream);
+int hitb200_batch_run(hitb200_batch* batch, int32_t nsteps, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HITB200_H */

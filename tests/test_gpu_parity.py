@@ -1,0 +1,344 @@
+"""GPU parity of the native kernels against the CPU oracle (pinned to the
+reference's golden vectors in tests/test_oracle_golden.py).
+
+Tolerances (relative to the largest magnitude of the compared field):
+  FP64 plain form: 1e-9 for RHS-type fields and states after a step; sensor
+  masks equal exactly.  FP32-bulk form: 2e-4 for RHS-type fields, 1e-6 for
+  states after one step; masks equal outside the dilated footprint of nodes
+  within 1e-4 (relative) of a sensor threshold.
+"""
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import hit_oracle as O
+from tests.gpu_util import dev, host, near_threshold_footprint, periodic_state, rel_err
+
+pytestmark = pytest.mark.gpu
+
+from hit_solver_b200 import _lib, core  # noqa: E402
+from hit_solver_b200.descs import grid_desc, set_sensor  # noqa: E402
+from hit_solver_b200.domain import Domain2D  # noqa: E402
+
+G = 1.4
+TOL64 = 1e-9
+TOL32 = 2e-4
+
+
+def periodic_plan(nx, ny, precision="fp64", width=4, jump=0.04, shear=None, **kw):
+    dom = Domain2D(0.0, 2 * np.pi, 0.0, 2 * np.pi, nx, ny)
+    d = grid_desc(dom, G, True, precision)
+    set_sensor(d, width, 2.5, jump, shear)
+    for k, v in kw.items():
+        setattr(d, k, v)
+    return core.Plan(d), dom
+
+
+def outflow_plan(nx, ny, precision="fp64", scheme=0, shear=None, **kw):
+    dom = Domain2D(0.0, 1.0, 0.0, 1.0, nx, ny)
+    d = grid_desc(dom, G, False, precision)
+    set_sensor(d, 4, 2.5, 0.025, shear, 4)
+    d.scheme = scheme
+    d.guard_cells = 2
+    for k, v in kw.items():
+        setattr(d, k, v)
+    return core.Plan(d), dom
+
+
+PERIODIC_CASES = [(32, 24, False), (40, 36, True), (128, 96, True), (10, 12, True), (37, 29, True)]
+
+
+@pytest.mark.parametrize("nx,ny,blob", PERIODIC_CASES)
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_periodic_sensor(nx, ny, blob, precision):
+    q = periodic_state(nx, ny, blob)
+    plan, dom = periodic_plan(nx, ny, precision)
+    prm = O.SensorParams(4, 2.5, 0.04, None)
+    qs = O.enforce(q, G)
+    want = O.sensor(qs, dom.dx, dom.dy, G, prm, True)
+    got = host(plan.sensor(dev(qs), enforce_first=False))
+    if precision == "fp64":
+        np.testing.assert_array_equal(got, want)
+    else:
+        skip, _ = near_threshold_footprint(qs, dom.dx, dom.dy, G, prm, True, 1e-4)
+        assert np.array_equal(got[~skip], want[~skip])
+    # shear part and another width
+    plan2, _ = periodic_plan(nx, ny, precision, width=3, shear=1.5)
+    prm2 = O.SensorParams(3, 2.5, 0.04, 1.5)
+    want2 = O.sensor(qs, dom.dx, dom.dy, G, prm2, True)
+    got2 = host(plan2.sensor(dev(qs), enforce_first=False))
+    skip2, _ = near_threshold_footprint(qs, dom.dx, dom.dy, G, prm2, True,
+                                        1e-12 if precision == "fp64" else 1e-4)
+    assert np.array_equal(got2[~skip2], want2[~skip2])
+
+
+@pytest.mark.parametrize("nx,ny,blob", PERIODIC_CASES)
+@pytest.mark.parametrize("precision,tol", [("fp64", TOL64), ("fp32", TOL32)])
+def test_periodic_axis_derivatives_and_rhs(nx, ny, blob, precision, tol):
+    q = periodic_state(nx, ny, blob)
+    plan, dom = periodic_plan(nx, ny, precision)
+    prm = O.SensorParams(4, 2.5, 0.04, None)
+    want, parts = O.inviscid_rhs(q, dom.dx, dom.dy, G, prm, True, return_parts=True)
+    mask = dev(parts["mask"].astype(np.uint8))
+    d_x = host(plan.axis_derivative(dev(q), mask, 0))
+    d_y = host(plan.axis_derivative(dev(q), mask, 1))
+    assert rel_err(d_x, parts["d_x"]) < tol
+    assert rel_err(d_y, parts["d_y"]) < tol
+    if precision == "fp64":
+        got = host(plan.rhs(dev(q), _lib.TERM_INVISCID))
+        assert rel_err(got, want) < tol
+
+
+def test_weno_everywhere_and_all_smooth():
+    """Faces flagged everywhere (mask all ones) and nowhere (all zeros)."""
+    q = periodic_state(48, 40, True)
+    plan, dom = periodic_plan(48, 40)
+    qs = O.enforce(q, G)
+    for fill in (0, 1):
+        m = np.full((40, 48), bool(fill))
+        for axis, ax in ((0, -1), (1, -2)):
+            want = O.axis_derivative(qs, m, dom.dx if axis == 0 else dom.dy, G, ax, True)
+            got = host(plan.axis_derivative(dev(q), dev(m.astype(np.uint8)), axis))
+            assert rel_err(got, want) < TOL64
+
+
+@pytest.mark.parametrize("nx,ny", [(64, 48), (37, 29)])
+@pytest.mark.parametrize("precision,tol", [("fp64", TOL64), ("fp32", TOL32)])
+def test_hit_full_rhs_and_sources(nx, ny, precision, tol):
+    q = periodic_state(nx, ny, True)
+    rng = np.random.default_rng(5)
+    fx, fy = 0.3 * rng.standard_normal((ny, nx)), 0.3 * rng.standard_normal((ny, nx))
+    plan, dom = periodic_plan(nx, ny, precision, viscosity=1e-3, drag_coefficient=0.1,
+                              drag_kmax=2.0, cooling_time=5.0)
+    prm = O.HITParams(nx=nx, ny=ny, viscosity=1e-3, large_scale_drag=0.1, cooling_time=5.0)
+    want = O.hit_rhs(q, prm, fx, fy)
+    got = host(plan.rhs(dev(q), _lib.TERM_ALL, dev(fx), dev(fy)))
+    assert rel_err(got, want) < tol
+    # individual source terms (no inviscid part)
+    dx, dy = dom.dx, dom.dy
+    checks = [
+        (_lib.TERM_VISCOUS, O.viscous_rhs(q, dx, dy, G, 1e-3)),
+        (_lib.TERM_DRAG, O.drag_source(q, dx, dy, G, 0.1, 2.0)),
+        (_lib.TERM_COOLING, O.cooling_source(q, G, 5.0)),
+        (_lib.TERM_FORCING, O.forcing_source(q, fx, fy, G)),
+    ]
+    for term, ref in checks:
+        out = host(plan.rhs(dev(q), term, dev(fx), dev(fy)))
+        assert rel_err(out, ref) < (1e-12 if precision == "fp64" else 1e-5), term
+
+
+@pytest.mark.parametrize("name", ["periodic_hit_32x24", "periodic_blob_40x36"])
+def test_golden_periodic_fixtures(name):
+    """Native FP64 results against the reference's own outputs."""
+    from pathlib import Path
+
+    d = np.load(Path(__file__).parent / "golden" / f"{name}.npz")
+    q = d["q"]
+    ny, nx = q.shape[1:]
+    plan, dom = periodic_plan(nx, ny, viscosity=1e-3, drag_coefficient=0.1, drag_kmax=2.0,
+                              cooling_time=5.0)
+    qs = host(plan.enforce(dev(q)))
+    np.testing.assert_array_equal(plan_sensor := host(plan.sensor(dev(qs), False)), d["mask"])
+    assert plan_sensor.dtype == bool
+    assert rel_err(host(plan.rhs(dev(q), _lib.TERM_INVISCID)), d["rhs"]) < TOL64
+    assert rel_err(host(plan.viscous_rhs(dev(q))), d["viscous"]) < 1e-12
+    assert abs(plan.stable_time_step(dev(q), 0.05, 1.0) - float(d["dt"])) < 1e-15
+    hv, _ = periodic_plan(nx, ny, hv_mn=0.002)
+    out = host(hv.hyperviscosity(dev(q), dev((~d["mask"]).astype(np.uint8))))
+    assert rel_err(out, d["hv"]) < 1e-14
+
+
+@pytest.mark.parametrize("nx,ny", [(40, 36), (128, 96)])
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-13), ("fp32", 1e-9)])
+def test_hyperviscosity(nx, ny, precision, tol):
+    q = periodic_state(nx, ny, True)
+    plan, dom = periodic_plan(nx, ny, precision, hv_mn=0.002)
+    m = O.sensor(q, dom.dx, dom.dy, G, O.SensorParams(), True)
+    want = O.hyperviscosity(q, ~m, dom.dx, dom.dy, G, 0.002, (0.25, 1, 1, 0.25), True)
+    got = host(plan.hyperviscosity(dev(q), dev((~m).astype(np.uint8))))
+    assert rel_err(got, want) < tol
+    # nodes outside the active mask are untouched up to the enforce filter
+    np.testing.assert_allclose(got[:, m], O.enforce(q, G)[:, m], rtol=0, atol=1e-15)
+
+
+RIEMANN_CASES = [("c3", 3, 64, 64, 0.5, None), ("c6", 6, 48, 56, 0.5, None),
+                 ("c308", 3, 40, 40, 0.8, 2.0)]
+
+
+def riemann_state(number, nx, ny, split, steps=8):
+    prm = O.RiemannParams(number=number, nx=nx, ny=ny, x_split=split, y_split=split)
+    q0, dt, n = O.riemann_setup(prm)
+    q, _, _, _ = O.riemann_run(prm, max_steps=steps)
+    return q, dt, prm
+
+
+@pytest.mark.parametrize("tag,number,nx,ny,split,shear", RIEMANN_CASES)
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_riemann_sensor_rhs(tag, number, nx, ny, split, shear, precision):
+    q, dt, prm = riemann_state(number, nx, ny, split)
+    plan, dom = outflow_plan(nx, ny, precision, shear=shear)
+    sp = O.SensorParams(4, 2.5, 0.025, shear, 4)
+    qs = O.enforce(q, G)
+    want = O.sensor(qs, dom.dx, dom.dy, G, sp, False)
+    got = host(plan.sensor(dev(qs), False))
+    if precision == "fp64":
+        np.testing.assert_array_equal(got, want)
+    else:
+        skip, _ = near_threshold_footprint(qs, dom.dx, dom.dy, G, sp, False, 1e-4)
+        assert np.array_equal(got[~skip], want[~skip])
+    tol = TOL64 if precision == "fp64" else TOL32
+    want_rhs, parts = O.inviscid_rhs(q, dom.dx, dom.dy, G, sp, False, return_parts=True)
+    m = dev(parts["mask"].astype(np.uint8))
+    assert rel_err(host(plan.axis_derivative(dev(q), m, 0)), parts["d_x"]) < tol
+    assert rel_err(host(plan.axis_derivative(dev(q), m, 1)), parts["d_y"]) < tol
+    if precision == "fp64":
+        assert rel_err(host(plan.rhs(dev(q), _lib.TERM_INVISCID)), want_rhs) < tol
+        wplan, _ = outflow_plan(nx, ny, precision, scheme=1, shear=shear)
+        want_w = O.inviscid_rhs(q, dom.dx, dom.dy, G, sp, False, "weno")
+        assert rel_err(host(wplan.rhs(dev(q), _lib.TERM_INVISCID)), want_w) < tol
+
+
+@pytest.mark.parametrize("tag", ["c3_32", "c6_24x28", "c308_20"])
+def test_golden_riemann_fixtures(tag):
+    from pathlib import Path
+
+    d = np.load(Path(__file__).parent / "golden" / f"riemann_{tag}.npz")
+    q = d["q"]
+    ny, nx = q.shape[1:]
+    sh = float(d["shear"])
+    plan, dom = outflow_plan(nx, ny, shear=None if sh < 0 else sh, hv_mn=float(d["mn"]))
+    qs = host(plan.enforce(dev(q)))
+    np.testing.assert_array_equal(host(plan.sensor(dev(qs), False)), d["mask"])
+    assert rel_err(host(plan.rhs(dev(q), _lib.TERM_INVISCID)), d["rhs"]) < TOL64
+    hv = host(plan.outflow_guard(plan.hyperviscosity(dev(q), dev((~d["mask"]).astype(np.uint8)))))
+    assert rel_err(hv, d["hv"]) < 1e-14
+    dt = plan.stable_time_step(dev(d["q0"]), 0.4, None)
+    n = int(np.ceil(float(d["tfinal"]) / dt))
+    assert n == int(d["n"]) and abs(float(d["tfinal"]) / n - float(d["dt"])) < 1e-17
+
+
+def test_outflow_guard_and_validate():
+    q, _, _ = riemann_state(3, 24, 20, 0.5, steps=2)
+    plan, _ = outflow_plan(24, 20)
+    qq = q.copy()
+    qq[:, 5, 7] += 0.3
+    want = O.outflow_guard(qq, 2)
+    np.testing.assert_array_equal(host(plan.outflow_guard(dev(qq))), want)
+    assert plan.validate(dev(q)) == _lib.OK
+    bad = q.copy()
+    bad[2, 3, 4] = np.nan
+    assert plan.validate(dev(bad)) == _lib.ERR_NONFINITE
+    bad = q.copy()
+    bad[0, 3, 4] = -1.0
+    assert plan.validate(dev(bad)) == _lib.ERR_NONPOSITIVE
+
+
+@pytest.mark.parametrize("nx,ny", [(32, 24), (64, 64)])
+def test_forcing_update_sequence(nx, ny):
+    q = periodic_state(nx, ny, False)
+    dom = Domain2D(0.0, 2 * np.pi, 0.0, 2 * np.pi, nx, ny)
+    d = grid_desc(dom, G, True)
+    d.forcing_on, d.forcing_kmin, d.forcing_kmax, d.forcing_correlation_time = 1, 3.0, 5.0, 0.5
+    plan = core.Plan(d)
+    ref = O.ShellOUForcing(nx, ny, dom.dx, dom.dy, 3.0, 5.0, 0.5, 1.0, 1e-3, 1e-6, 20.0, 0.2, 99)
+    rho, u, v, _ = O.primitives(q, G)
+    rng = np.random.default_rng(99)
+    for k in range(3):
+        noise = rng.standard_normal((ny, nx))
+        dt = 0.004 * (1 + 0.1 * k)
+        fx_w, fy_w, info = ref.update(dt, rho, u, v, noise=noise)
+        fx, fy = plan.forcing_update(dev(q), dev(noise), dt, 1e-3)
+        assert rel_err(host(fx), fx_w) < 1e-11
+        assert rel_err(host(fy), fy_w) < 1e-11
+        s = plan.scalars()
+        assert s[_lib.S_F_ALPHA] == pytest.approx(info["alpha"], rel=1e-10)
+        assert s[_lib.S_F_INJECTED] == pytest.approx(info["injected_power"], rel=1e-9)
+        assert s[_lib.S_F_FXX] == pytest.approx(info["Fxx"], rel=1e-10)
+        assert s[_lib.S_F_AF] == pytest.approx(info["A_F"], rel=1e-8, abs=1e-12)
+        assert s[_lib.S_F_DECAY] == pytest.approx(info["ou_decay"], rel=1e-15)
+
+
+def _hit_solver(nx, ny, precision="fp64", **kw):
+    from hit_solver_b200.hit2d import HIT2DConfig, HITSolver
+
+    cfg = HIT2DConfig(nx=nx, ny=ny, tfinal=kw.pop("tfinal", 1.0), cfl=0.05, target_mach=0.25,
+                      initial_kmin=3, initial_kmax=5, forcing_kmin=3.0, forcing_kmax=5.0,
+                      forcing_correlation_time=0.5, mach_control=True, mach_control_target=0.25,
+                      viscosity=7.5e-4, large_scale_drag=0.1, cooling_time=5.0,
+                      hyperviscosity_mn=0.002, precision=precision, **kw)
+    prm = O.HITParams(nx=nx, ny=ny, tfinal=cfg.tfinal, cfl=0.05, target_mach=0.25,
+                      forcing_correlation_time=0.5, mach_control=True, mach_control_target=0.25,
+                      viscosity=7.5e-4, large_scale_drag=0.1, cooling_time=5.0)
+    return HITSolver(cfg), prm
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-10), ("fp32", 2e-6)])
+def test_hit_fused_steps_match_oracle(precision, tol):
+    """hitb200_step (dt, Mach control, OU forcing with the reference's NumPy
+    noise stream, SSP-RK3, hyperviscosity every 5 steps) against the oracle
+    driver over 6 steps."""
+    solver, prm = _hit_solver(48, 40, precision)
+    want, t_w, steps_w, info_w = O.hit_run(prm, max_steps=6)
+    solver.advance(6)
+    s = solver.scalars()
+    assert int(s[_lib.S_STEP]) == steps_w == 6
+    assert s[_lib.S_TIME] == pytest.approx(t_w, rel=1e-12)
+    assert rel_err(host(solver.q), want) < tol
+    assert s[_lib.S_F_INJECTED] == pytest.approx(info_w["injected_power"], rel=1e-6)
+    assert int(s[_lib.S_HV_APPLIED]) == 1
+
+
+def test_hit_golden_run():
+    """The reference's own run_simulation output (24x24, 5 steps to t=0.02)."""
+    from pathlib import Path
+
+    d = np.load(Path(__file__).parent / "golden" / "hit_run_24.npz")
+    solver, _ = _hit_solver(24, 24, tfinal=0.02)
+    solver.advance(int(d["steps"]) + 2)  # extra steps are no-ops after tfinal
+    s = solver.scalars()
+    assert int(s[_lib.S_STEP]) == int(d["steps"])
+    assert s[_lib.S_TIME] == pytest.approx(float(d["time"]), rel=1e-14)
+    assert rel_err(host(solver.q), d["q"]) < 1e-10
+
+
+@pytest.mark.parametrize("tag,number,nx,ny,split,shear", RIEMANN_CASES)
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-10), ("fp32", 1e-5)])
+def test_riemann_run_matches_oracle(tag, number, nx, ny, split, shear, precision, tol):
+    from hit_solver_b200.problems.riemann import RiemannConfig3, RiemannConfig6, RiemannSolver
+
+    cls = RiemannConfig6 if number == 6 else RiemannConfig3
+    hv_interval = 5 if split == 0.8 else 1
+    cfg = cls(nx=nx, ny=ny, x_split=split, y_split=split, shear_threshold=shear,
+              hyperviscosity_interval=hv_interval, precision=precision)
+    solver = RiemannSolver(cfg)
+    prm = O.RiemannParams(number=number, nx=nx, ny=ny, x_split=split, y_split=split,
+                          tfinal=cfg.tfinal, shear_threshold=shear, hyperviscosity_interval=hv_interval)
+    want, dt, steps, apps = O.riemann_run(prm, max_steps=10)
+    assert solver.dt == pytest.approx(dt, rel=1e-15)
+    solver.advance(10)
+    assert rel_err(host(solver.q), want) < tol
+    assert int(solver.plan.scalars()[_lib.S_HV_APPLIED]) == apps
+
+
+@pytest.mark.parametrize("tag", ["c3_32", "c6_24x28", "c308_20"])
+def test_riemann_golden_runs(tag):
+    """The reference's own run_riemann output to t = 0.02."""
+    from pathlib import Path
+
+    from hit_solver_b200.problems.riemann import (RiemannConfig3, RiemannConfig3Offset08,
+                                                  RiemannConfig6, run_riemann)
+
+    d = np.load(Path(__file__).parent / "golden" / f"riemann_{tag}.npz")
+    ny, nx = d["q"].shape[1:]
+    sh = float(d["shear"])
+    cls = {"c3_32": RiemannConfig3, "c6_24x28": RiemannConfig6, "c308_20": RiemannConfig3Offset08}[tag]
+    cfg = cls(nx=nx, ny=ny, tfinal=0.02, shear_threshold=None if sh < 0 else sh,
+              progress_every=10 ** 6)
+    q, diag = run_riemann(cfg)
+    assert diag.steps == int(d["run_steps"])
+    assert diag.hyperviscosity_applications == int(d["run_hv_apps"])
+    assert rel_err(host(q), d["q_run"]) < 1e-10
+    assert diag.density_max == pytest.approx(float(d["run_density_max"]), rel=1e-10)
+    assert diag.max_abs_vorticity == pytest.approx(float(d["run_max_abs_vorticity"]), rel=1e-8)
+    assert diag.final_sensor_fraction == pytest.approx(float(d["run_sensor_fraction"]), abs=1e-12)
