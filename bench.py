@@ -1,0 +1,460 @@
+#!/usr/bin/env python
+"""Throughput of the HIT_Solver RHS / SSP-RK3 hot path on B200.
+
+Workload (the reference's headline Riemann case): Lax-Liu configuration 3 on
+a 512 x 512 grid, hybrid compact/WENO7 scheme, sensor width 4, jump
+threshold 0.025, no shear term, hyperviscosity mn = 0.001 every step,
+CFL 0.4 (dt fixed from the initial state), outflow guard cells 2.
+One step = one full SSP-RK3 step (three RHS evaluations, clean filters,
+hyperviscosity).  Metric: cell-updates/s (cells x steps / s).
+
+  value       FP32-bulk form (FP32 stencil/WENO/flux arithmetic, FP64 state),
+              one solve, device-timed with CUDA events, L2 flushed before
+              every timed step (the solve's working set would otherwise stay
+              in the 126 MB L2).
+  plain_fp64  the same solve in the plain FP64 form.
+  batched     B independent 512^2 solves (quadrant-state sweep of the split
+              point) advanced by one launch per kernel of the step.
+  e2e         the public API with host buffers: the initial state uploaded
+              from pinned memory, each step's scalar record (time, status)
+              read back, the final state downloaded, all inside the timed
+              region.
+  roofline    the step's dominant kernel: algorithmic bytes per launch /
+              its CUDA-event launch time.
+  cpu_baseline  the CPU oracle (NumPy FP64 restatement of the reference
+              algorithm) on a bounded number of steps of the same workload.
+
+Launch:  python bench.py [--gpus N --steps K --warmup W]; for N > 1 under
+torchrun each rank runs its own replica (the solve does not shard).
+``--impl reference`` times the reference algorithm's CPU implementation
+(the oracle port) on the host cores instead.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+if str(ROOT) not in sys.path:
+    sys.path.insert(0, str(ROOT))
+
+METRIC = "cell-updates/s per RK3 step (Riemann config 3, 512x512, hybrid WENO7/compact)"
+NX = NY = 512
+WORKLOAD = {"workload": "riemann_config3_512x512_hybrid_hv1_cfl0.4", "nx": NX, "ny": NY,
+            "scheme": "hybrid", "sensor_width": 4, "jump_threshold": 0.025, "shear": None,
+            "hyperviscosity_mn": 0.001, "hyperviscosity_interval": 1, "cfl": 0.4,
+            "guard_cells": 2, "precision": "fp32-bulk (fp64 state)"}
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse_args():
+    p = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=200)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", choices=("b200", "reference"), default="b200")
+    p.add_argument("--batch", type=int, default=8, help="solves in the batched measurement")
+    p.add_argument("--cpu-steps", type=int, default=3, help="oracle steps in the cpu_baseline sample")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+# ----------------------------------------------------------------------------------
+# distributed plumbing (replicas only: no data-path collective)
+# ----------------------------------------------------------------------------------
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        backend = "nccl" if args.impl == "b200" else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+    return world, rank, local
+
+
+def dist_max(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def dist_barrier(world: int) -> None:
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def dist_finish(world: int) -> None:
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+# ----------------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ----------------------------------------------------------------------------------
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.path = Path(tempfile.mkstemp(prefix="clocks_", suffix=".csv")[1])
+        self.gpu = gpu_index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.fh,
+                stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.fh.close()
+
+    def summary(self):
+        if self.proc is None or not self.path.exists():
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        rows = []
+        for line in self.path.read_text().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) >= 9:
+                rows.append(f)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None, "reasons": reasons,
+                "samples": len(rows)}
+
+
+def measured_peak():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+        except (KeyError, ValueError):
+            pass
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+def ncu_traffic(kernel: str):
+    """Per-launch DRAM traffic of the dominant kernel from the committed ncu
+    summary (profiles/ncu_traffic.json), scaled to this workload, or None."""
+    p = ROOT / "profiles" / "ncu_traffic.json"
+    if not p.exists():
+        return None
+    try:
+        data = json.loads(p.read_text())
+        entry = data.get(kernel)
+        if entry is None:
+            return None
+        return float(entry["bytes_per_cell"]) * NX * NY
+    except (KeyError, ValueError, TypeError):
+        return None
+
+
+# ----------------------------------------------------------------------------------
+# b200 arm
+# ----------------------------------------------------------------------------------
+def make_solver(precision: str, x_split: float = 0.5):
+    from hit_solver_b200.problems.riemann import RiemannConfig3, RiemannSolver
+
+    cfg = RiemannConfig3(nx=NX, ny=NY, x_split=x_split, y_split=x_split, shear_threshold=None,
+                         precision=precision)
+    solver = RiemannSolver(cfg)
+    # timing runs continue past tfinal: no step limit on the device
+    solver.plan.set_time(0.0, 0, solver.dt, -1)
+    return solver
+
+
+def flush_buffer():
+    import torch
+
+    return torch.empty(320 * 2 ** 20 // 4, dtype=torch.float32, device="cuda")  # 320 MB > L2
+
+
+def timed_steps(advance, steps: int, flush) -> float:
+    """Sum of per-step CUDA-event times with an L2 flush before each step."""
+    import torch
+
+    st = torch.cuda.current_stream()
+    total = 0.0
+    evs = []
+    for _ in range(steps):
+        flush.zero_()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(st)
+        advance()
+        b.record(st)
+        evs.append((a, b))
+    torch.cuda.synchronize()
+    for a, b in evs:
+        total += a.elapsed_time(b)
+    return total / 1e3
+
+
+def profile_steps(profile_fn, nprof: int, flush):
+    """Per-kernel-type mean launch time and algorithmic bytes over nprof
+    uncaptured steps, each after an L2 flush."""
+    per = {}
+    for _ in range(nprof):
+        flush.zero_()
+        for name, ms, by in profile_fn():
+            d = per.setdefault(name, {"ms": 0.0, "bytes": 0.0, "launches": 0})
+            d["ms"] += ms
+            d["bytes"] += by
+            d["launches"] += 1
+    for d in per.values():
+        d["ms_per_launch"] = d["ms"] / d["launches"]
+        d["bytes_per_launch"] = d["bytes"] / d["launches"]
+        d["ms_per_step"] = d["ms"] / nprof
+    return per
+
+
+def run_b200(args, world, rank, local):
+    import numpy as np
+    import torch
+
+    from hit_solver_b200 import _lib
+    from hit_solver_b200.batch import Batch
+    from hit_solver_b200.problems.riemann import riemann_descriptor, RiemannConfig3
+
+    torch.cuda.set_device(local)
+    K, W = args.steps, max(args.warmup, 3)
+    flush = flush_buffer()
+    cells = NX * NY
+
+    # ---- FP32-bulk single solve (value) ----
+    s32 = make_solver("fp32-bulk")
+    s32.advance(W)
+    torch.cuda.synchronize()
+    dist_barrier(world)
+    with ClockSampler(local) as clk:
+        t32 = timed_steps(lambda: s32.advance(1), K, flush)
+        torch.cuda.synchronize()
+    dist_barrier(world)
+    t32 = dist_max(t32, world)
+    launches_per_step = len(s32.plan.step_profile(s32.q))
+
+    # ---- plain FP64 single solve ----
+    s64 = make_solver("fp64")
+    s64.advance(W)
+    t64 = dist_max(timed_steps(lambda: s64.advance(1), K, flush), world)
+
+    # ---- batched: B independent solves, split points swept over [0.3, 0.8] ----
+    B = max(1, args.batch)
+    descs, states, dts = [], [], []
+    for i in range(B):
+        split = 0.3 + 0.5 * i / max(B - 1, 1)
+        cfg = RiemannConfig3(nx=NX, ny=NY, x_split=split, y_split=split, shear_threshold=None,
+                             precision="fp32-bulk")
+        sv = make_solver("fp32-bulk", split)
+        descs.append(riemann_descriptor(cfg))
+        states.append(sv.q.clone())
+        dts.append(sv.dt)
+        del sv
+    batch = Batch(descs)
+    batch.bind(states)
+    for m, dt in zip(batch.members, dts):
+        m.set_time(0.0, 0, dt, -1)
+    batch.run(W)
+    tb = dist_max(timed_steps(lambda: batch.run(1), max(K // 4, 5), flush), world)
+    kb = max(K // 4, 5)
+
+    # ---- roofline of the dominant kernel (FP32-bulk solve) ----
+    per = profile_steps(lambda: s32.plan.step_profile(s32.q), 5, flush)
+    dom_name = max(per, key=lambda k: per[k]["ms_per_step"])
+    dom = per[dom_name]
+    peak, peak_kind = measured_peak()
+    achieved = dom["bytes_per_launch"] / (dom["ms_per_launch"] / 1e3) / 1e9
+
+    # ---- e2e through the public API with host buffers ----
+    q_host = s32.q.detach().cpu().pin_memory()
+    out_host = torch.empty_like(q_host).pin_memory()
+    scal_host = torch.empty((K, _lib.S_COUNT), dtype=torch.float64).pin_memory()
+    e2e_solver = make_solver("fp32-bulk")
+    q_dev = e2e_solver.q
+    e2e_solver.advance(W)
+    torch.cuda.synchronize()
+    st = torch.cuda.current_stream()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(st)
+    q_dev.copy_(q_host, non_blocking=True)
+    for k in range(K):
+        e2e_solver.plan.run(q_dev, 1)
+        e2e_solver.plan.lib.hitb200_copy_scalars_async(e2e_solver.plan.handle,
+                                                       scal_host[k].data_ptr(), _lib.S_COUNT,
+                                                       st.cuda_stream)
+    out_host.copy_(q_dev, non_blocking=True)
+    b.record(st)
+    torch.cuda.synchronize()
+    te2e = dist_max(a.elapsed_time(b) / 1e3, world)
+    state_bytes = 4 * cells * 8
+    if int(scal_host[:, _lib.S_STATUS].max()) & 1:
+        raise FloatingPointError("non-finite state during the e2e run")
+
+    # ---- CPU baseline (oracle port, rank 0 at N = 1) ----
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(args.cpu_steps)
+
+    if rank != 0:
+        return None
+    value = world * cells * K / t32
+    line = {
+        "metric": METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": world,
+        "steps": K, "warmup": W, "ms_per_step": 1e3 * t32 / K, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "fp32 (fp64 state)",
+        "data": "synthetic: the reference's own Riemann config-3 initial state (no dataset)",
+        "config": {**WORKLOAD, "parallelism": f"replicas x{world}" if world > 1 else "single",
+                   "l2": "flushed (320 MB write) before every timed step"},
+        "plain_fp64": {"value": world * cells * K / t64, "ms_per_step": 1e3 * t64 / K,
+                       "dtype": "fp64"},
+        "batched": {"value": world * B * cells * kb / tb, "ms_per_step": 1e3 * tb / kb,
+                    "solves": B, "dtype": "fp32 (fp64 state)",
+                    "speedup_vs_plain_fp64": (B * cells * kb / tb) / (cells * K / t64)},
+        "e2e": {"value": world * cells * K / te2e, "unit": "cell-updates/s",
+                "h2d_bytes_per_step": state_bytes / K,
+                "d2h_bytes_per_step": 8 * _lib.S_COUNT + state_bytes / K},
+        "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": achieved, "peak": peak,
+                     "unit": "GB/s", "frac": achieved / peak,
+                     "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"
+                     if peak_kind == "measured" else "fallback 6.65 TB/s",
+                     "traffic": ncu_traffic(dom_name),
+                     "bytes_per_launch": dom["bytes_per_launch"],
+                     "ms_per_launch": dom["ms_per_launch"],
+                     "kernels": {k: {"ms_per_step": round(v["ms_per_step"], 5),
+                                     "ms_per_launch": round(v["ms_per_launch"], 5),
+                                     "gbs": round(v["bytes_per_launch"] / (v["ms_per_launch"] / 1e3) / 1e9, 1)
+                                     if v["bytes_per_launch"] > 0 else None}
+                                 for k, v in sorted(per.items(), key=lambda kv: -kv[1]["ms_per_step"])}},
+        "gpu_launches": K * launches_per_step,
+        "clocks": clk.summary(),
+    }
+    if cpu is not None:
+        line["cpu_baseline"] = cpu
+    return line
+
+
+def cpu_baseline(steps: int):
+    """The oracle (NumPy FP64 port of the reference algorithm) on `steps` RK3
+    steps of the same 512^2 workload, one process."""
+    import numpy as np
+
+    from oracle import hit_oracle as O
+
+    prm = O.RiemannParams(number=3, nx=NX, ny=NY)
+    q, dt, n = O.riemann_setup(prm)
+    O.riemann_run(prm, max_steps=1, q0=q, dt=dt)  # warm-up
+    t0 = time.perf_counter()
+    O.riemann_run(prm, max_steps=steps, q0=q, dt=dt)
+    el = time.perf_counter() - t0
+    return {"value": NX * NY * steps / el, "unit": "cell-updates/s", "cores": 1, "kind": "port",
+            "sample": f"{steps} RK3 steps of the 512x512 workload, NumPy FP64 oracle, 1 process "
+                      f"({el:.1f} s)"}
+
+
+# ----------------------------------------------------------------------------------
+# reference arm: the reference algorithm's CPU implementation on all host cores
+# ----------------------------------------------------------------------------------
+def _ref_worker(args):
+    steps, seed = args
+    import numpy as np
+
+    from oracle import hit_oracle as O
+
+    prm = O.RiemannParams(number=3, nx=NX, ny=NY)
+    q, dt, n = O.riemann_setup(prm)
+    O.riemann_run(prm, max_steps=1, q0=q, dt=dt)
+    t0 = time.perf_counter()
+    O.riemann_run(prm, max_steps=steps, q0=q, dt=dt)
+    return time.perf_counter() - t0
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return None
+    import multiprocessing as mp
+
+    os.environ.setdefault("OMP_NUM_THREADS", "1")
+    cores = os.cpu_count() or 1
+    procs = max(1, min(cores, 32))  # each process holds ~0.5 GB of NumPy temporaries
+    # bounded sample: each process advances the 512^2 workload a few steps;
+    # ~4 s per step per process, so the run stays within a few minutes
+    steps = max(1, min(args.steps, 8))
+    ctx = mp.get_context("spawn")
+    t0 = time.perf_counter()
+    with ctx.Pool(procs) as pool:
+        times = pool.map(_ref_worker, [(steps, i) for i in range(procs)])
+    wall = time.perf_counter() - t0
+    slowest = max(times)
+    value = procs * NX * NY * steps / slowest
+    return {
+        "metric": METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": world,
+        "steps": steps, "warmup": 1, "ms_per_step": 1e3 * slowest / steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp64",
+        "data": "synthetic: the reference's own Riemann config-3 initial state",
+        "config": {**WORKLOAD, "precision": "fp64", "parallelism": f"{procs} host processes"},
+        "impl": "reference",
+        "cpu_baseline": {"value": value, "unit": "cell-updates/s", "cores": procs, "kind": "port",
+                         "sample": f"{steps} RK3 steps of the 512x512 workload in each of {procs} "
+                                   f"processes (NumPy FP64 oracle; wall {wall:.1f} s)"},
+        "e2e": {"value": value, "unit": "cell-updates/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    args = parse_args()
+    world, rank, local = dist_setup(args)
+    try:
+        if args.impl == "reference":
+            line = run_reference(args, world, rank)
+        else:
+            line = run_b200(args, world, rank, local)
+        if rank == 0 and line is not None:
+            print(json.dumps(line))
+    finally:
+        dist_finish(world)
+
+
+if __name__ == "__main__":
+    main()

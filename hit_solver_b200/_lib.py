@@ -107,6 +107,12 @@ SIGNATURES = [
      [_VP, _DP, _DP, ctypes.c_double, ctypes.c_double, _DP, _DP, _VP]),
     ("hitb200_step", ctypes.c_int, [_VP, _DP, _DP, _VP]),
     ("hitb200_run", ctypes.c_int, [_VP, _DP, ctypes.c_int32, _VP]),
+    ("hitb200_step_profile", ctypes.c_int,
+     [_VP, _DP, _DP, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_double),
+      ctypes.c_int32, ctypes.POINTER(ctypes.c_int32), ctypes.c_char_p, ctypes.c_size_t, _VP]),
+    ("hitb200_batch_step_profile", ctypes.c_int,
+     [_VP, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_double), ctypes.c_int32,
+      ctypes.POINTER(ctypes.c_int32), ctypes.c_char_p, ctypes.c_size_t, _VP]),
     ("hitb200_set_time", ctypes.c_int,
      [_VP, ctypes.c_double, ctypes.c_int64, ctypes.c_double, ctypes.c_int64]),
     ("hitb200_read_scalars", ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_double), ctypes.c_int32]),

@@ -151,6 +151,12 @@ class Plan:
     def run(self, q, nsteps: int) -> None:
         _lib.check(self.lib.hitb200_run(self.handle, q.data_ptr(), int(nsteps), stream_handle()))
 
+    def step_profile(self, q, noise=None):
+        """One uncaptured step with per-launch CUDA events: list of
+        (kernel, ms, algorithmic bytes)."""
+        return profile_call(lambda ms, b, cap, cnt, names, size: self.lib.hitb200_step_profile(
+            self.handle, q.data_ptr(), ptr(noise), ms, b, cap, cnt, names, size, stream_handle()))
+
     def set_time(self, time=0.0, step=0, dt=0.0, max_steps=-1) -> None:
         torch.cuda.current_stream().synchronize()
         _lib.check(self.lib.hitb200_set_time(self.handle, float(time), int(step), float(dt),
@@ -166,6 +172,16 @@ class Plan:
         torch.cuda.current_stream().synchronize()
         _lib.check(self.lib.hitb200_diagnostics(self.handle, q.data_ptr(), buf, 17))
         return list(buf)
+
+
+def profile_call(fn, cap: int = 64):
+    ms = (ctypes.c_float * cap)()
+    by = (ctypes.c_double * cap)()
+    cnt = ctypes.c_int32()
+    names = ctypes.create_string_buffer(4096)
+    _lib.check(fn(ms, by, cap, ctypes.byref(cnt), names, 4096))
+    labels = names.value.decode().split("\n")
+    return [(labels[i], float(ms[i]), float(by[i])) for i in range(min(cnt.value, cap))]
 
 
 def plan_for(desc: _lib.Desc) -> Plan:

@@ -165,7 +165,38 @@ struct LaunchSet {
   int n_tiles, n_x, n_y, elem, mch_x, mch_y;
   size_t smem_x, smem_y, smem_sensor;
   cudaStream_t st;
+  // cells of all solves, and of the solves carrying viscous / forcing terms
+  double cells = 0, cells_visc = 0, cells_force = 0;
 };
+
+// Optional per-launch event recorder for hitb200_step_profile.  bytes are the
+// algorithmic DRAM bytes of the launch: unique inputs read once plus outputs
+// written once, at their stored precision.
+struct Prof {
+  cudaStream_t st;
+  std::vector<cudaEvent_t> ev;
+  std::vector<const char*> names;
+  std::vector<double> bytes;
+  void mark(const char* n, double b) {
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    cudaEventRecord(e, st);
+    ev.push_back(e);
+    names.push_back(n);
+    bytes.push_back(b);
+  }
+  void end() {
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    cudaEventRecord(e, st);
+    ev.push_back(e);
+  }
+  ~Prof() {
+    for (cudaEvent_t e : ev) cudaEventDestroy(e);
+  }
+};
+#define PMARK(name, b) \
+  if (prof) prof->mark(name, b)
 
 template <typename T, int AXIS, int MCH>
 void set_sweep_attr(size_t bytes) {
@@ -232,30 +263,75 @@ void launch_prepass(const LaunchSet& L, int buf, int mode, int enf, const Bind& 
 
 // The reference's loop body (OOP/hit2d.py:828-879; riemann_config3.py:728-740).
 int launch_step_sequence(const LaunchSet& L, int any_forcing, int noise_upload, int any_outflow,
-                         int any_hv) {
+                         int any_hv, Prof* prof = nullptr) {
   Bind nb{};
+  const double N = L.cells, e = L.elem;
+  PMARK("prepass", 32 * N);
   launch_prepass(L, 0, PRE_STEP, 1, nb);
   if (any_forcing) {
-    if (noise_upload)
+    if (noise_upload) {
+      PMARK("noise_dft", 8 * L.cells_force);
       noise_dft_kernel<<<L.n_tiles, kRedThreads, 0, L.st>>>(L.solves, L.tiles, nb);
-    else
+    } else {
+      PMARK("noise_rng", 0.0);
       noise_rng_kernel<<<L.nsolves, 128, 0, L.st>>>(L.solves, L.nsolves, L.partner);
+    }
+    PMARK("force_synth", 48 * L.cells_force);
     force_synth_kernel<<<L.n_tiles, kRedThreads, 0, L.st>>>(L.solves, L.tiles, nb);
   }
   for (int stage = 0; stage < 3; ++stage) {
-    if (stage > 0) launch_prepass(L, stage, PRE_STAGE, 1, nb);
+    if (stage > 0) {
+      PMARK("prepass", 32 * N);
+      launch_prepass(L, stage, PRE_STAGE, 1, nb);
+    }
+    PMARK("sensor", 33 * N + 3 * e * L.cells_visc);
     launch_sensor(L, stage, 1, 1, nb, nullptr);
+    PMARK("sweep_x", 33 * N + 3 * e * L.cells_visc + 16 * L.cells_force + 4 * e * N);
     launch_sweep(L, 0, stage, SW_STAGE, nb);
+    PMARK("sweep_y", (stage == 0 ? 65 : 97) * N + 4 * e * N);
     launch_sweep(L, 1, stage, SW_STAGE, nb);
-    if (any_outflow) guard_kernel<<<L.nsolves, 256, 0, L.st>>>(L.solves, L.nsolves, stage == 2 ? 3 : stage + 1, nb);
+    if (any_outflow) {
+      PMARK("guard", 0.0);
+      guard_kernel<<<L.nsolves, 256, 0, L.st>>>(L.solves, L.nsolves, stage == 2 ? 3 : stage + 1, nb);
+    }
   }
   if (any_hv) {
+    PMARK("hv_prepass", 32 * N);
     launch_prepass(L, 1, PRE_SENSOR, 0, nb);
+    PMARK("hv_sensor", 33 * N);
     launch_sensor(L, 3, 0, 0, nb, nullptr);
+    PMARK("hv", 65 * N);
     launch_hv(L, nb);
-    if (any_outflow) guard_kernel<<<L.nsolves, 256, 0, L.st>>>(L.solves, L.nsolves, 0, nb);
+    if (any_outflow) {
+      PMARK("guard", 0.0);
+      guard_kernel<<<L.nsolves, 256, 0, L.st>>>(L.solves, L.nsolves, 0, nb);
+    }
   }
+  if (prof) prof->end();
   HB_LAUNCHED("step kernels");
+  return HITB200_OK;
+}
+
+int finish_profile(Prof& pr, float* ms, double* bytes, int32_t cap, int32_t* count, char* names,
+                   size_t names_size) {
+  HB_CUDA(cudaStreamSynchronize(pr.st));
+  const int n = (int)pr.names.size();
+  if (count) *count = n;
+  std::string all;
+  for (int i = 0; i < n; ++i) {
+    float t = 0.f;
+    HB_CUDA(cudaEventElapsedTime(&t, pr.ev[i], pr.ev[i + 1]));
+    if (i < cap) {
+      if (ms) ms[i] = t;
+      if (bytes) bytes[i] = pr.bytes[i];
+    }
+    all += pr.names[i];
+    all += '\n';
+  }
+  if (names && names_size > 0) {
+    std::strncpy(names, all.c_str(), names_size - 1);
+    names[names_size - 1] = 0;
+  }
   return HITB200_OK;
 }
 
@@ -277,6 +353,9 @@ LaunchSet plan_launch_set(hitb200_plan* p, cudaStream_t st) {
   L.smem_y = p->smem_y;
   L.smem_sensor = p->smem_sensor;
   L.st = st;
+  L.cells = (double)p->desc.nx * p->desc.ny;
+  L.cells_visc = p->desc.viscosity > 0.0 ? L.cells : 0.0;
+  L.cells_force = p->desc.forcing_on ? L.cells : 0.0;
   return L;
 }
 
@@ -854,7 +933,7 @@ int hitb200_step(hitb200_plan* p, double* q, const double* noise, void* stream) 
   if (r != HITB200_OK) return r;
   if (upload)
     HB_CUDA(cudaMemcpyAsync((void*)p->hs.noise, noise, (size_t)p->desc.nx * p->desc.ny * sizeof(double),
-                            cudaMemcpyDeviceToDevice, st));
+                            cudaMemcpyDefault, st));
   LaunchSet L = plan_launch_set(p, st);
   return launch_step_sequence(L, p->desc.forcing_on, upload, !p->desc.periodic, p->hs.hv_interval > 0);
 }
@@ -1058,6 +1137,41 @@ int hitb200_batch_bind(hitb200_batch* b, double* const* q) {
   return HITB200_OK;
 }
 
+static LaunchSet batch_launch_set(hitb200_batch* b, cudaStream_t st);
+
+int hitb200_step_profile(hitb200_plan* p, double* q, const double* noise, float* ms, double* bytes,
+                         int32_t cap, int32_t* count, char* names, size_t names_size, void* stream) {
+  if (!p || !q) return invalid("NULL argument");
+  if (p->in_batch) return invalid("plan belongs to a batch; use hitb200_batch_step_profile");
+  cudaStream_t st = (cudaStream_t)stream;
+  const int upload = p->desc.forcing_on && p->desc.noise_mode == 0;
+  if (upload && !noise) return invalid("noise field required (noise_mode 0)");
+  int r = bind_state(p, q, st);
+  if (r != HITB200_OK) return r;
+  if (upload)
+    HB_CUDA(cudaMemcpyAsync((void*)p->hs.noise, noise, (size_t)p->desc.nx * p->desc.ny * sizeof(double),
+                            cudaMemcpyDefault, st));
+  Prof pr;
+  pr.st = st;
+  LaunchSet L = plan_launch_set(p, st);
+  r = launch_step_sequence(L, p->desc.forcing_on, upload, !p->desc.periodic, p->hs.hv_interval > 0, &pr);
+  if (r != HITB200_OK) return r;
+  return finish_profile(pr, ms, bytes, cap, count, names, names_size);
+}
+
+int hitb200_batch_step_profile(hitb200_batch* b, float* ms, double* bytes, int32_t cap,
+                               int32_t* count, char* names, size_t names_size, void* stream) {
+  if (!b) return invalid("NULL argument");
+  for (hitb200_plan* p : b->plans)
+    if (!p->hs.q) return invalid("batch state not bound");
+  Prof pr;
+  pr.st = (cudaStream_t)stream;
+  LaunchSet L = batch_launch_set(b, pr.st);
+  int r = launch_step_sequence(L, b->any_forcing, 0, b->any_outflow, b->any_hv, &pr);
+  if (r != HITB200_OK) return r;
+  return finish_profile(pr, ms, bytes, cap, count, names, names_size);
+}
+
 static LaunchSet batch_launch_set(hitb200_batch* b, cudaStream_t st) {
   LaunchSet L;
   L.solves = b->d_solves;
@@ -1076,6 +1190,12 @@ static LaunchSet batch_launch_set(hitb200_batch* b, cudaStream_t st) {
   L.smem_y = b->smem_y;
   L.smem_sensor = b->smem_sensor;
   L.st = st;
+  for (hitb200_plan* p : b->plans) {
+    const double n = (double)p->desc.nx * p->desc.ny;
+    L.cells += n;
+    if (p->desc.viscosity > 0.0) L.cells_visc += n;
+    if (p->desc.forcing_on) L.cells_force += n;
+  }
   return L;
 }
 

@@ -199,6 +199,15 @@ int hitb200_step(hitb200_plan* plan, double* q, const double* noise, void* strea
  * (noise_mode 1 or forcing off).  Steps after time reaches tfinal (or
  * max_steps) are no-ops on the device. */
 int hitb200_run(hitb200_plan* plan, double* q, int32_t nsteps, void* stream);
+/* One hitb200_step run uncaptured with a CUDA event before every kernel
+ * launch; synchronises.  For launch i < cap: ms[i] = its device time and
+ * bytes[i] = its algorithmic DRAM bytes (unique inputs read once plus outputs
+ * written once, at stored precision).  *count = launches in the step; names
+ * receives their labels, one per line.  No reference counterpart: it
+ * instruments the step for roofline measurement. */
+int hitb200_step_profile(hitb200_plan* plan, double* q, const double* noise, float* ms,
+                         double* bytes, int32_t cap, int32_t* count, char* names,
+                         size_t names_size, void* stream);
 /* Set time, step count, dt (used when fixed_dt = 1) and max_steps (< 0: no limit). */
 int hitb200_set_time(hitb200_plan* plan, double time, int64_t step, double dt, int64_t max_steps);
 /* Copy scalar slots [0, n) to host memory; synchronises. */
@@ -227,6 +236,9 @@ hitb200_plan* hitb200_batch_plan(hitb200_batch* batch, int32_t i);
 int hitb200_batch_bind(hitb200_batch* batch, double* const* q);
 int hitb200_batch_step(hitb200_batch* batch, void* stream);
 int hitb200_batch_run(hitb200_batch* batch, int32_t nsteps, void* stream);
+/* hitb200_step_profile for a batch (launches cover all member solves). */
+int hitb200_batch_step_profile(hitb200_batch* batch, float* ms, double* bytes, int32_t cap,
+                               int32_t* count, char* names, size_t names_size, void* stream);
 
 #ifdef __cplusplus
 }

@@ -50,3 +50,19 @@ def periodic_state(nx, ny, blob=True, seed=1234, mach=0.25):
         p = np.where(inside, 1.4, p)
         q = O.enforce(O.conservative(rho, u, v, p, 1.4), 1.4)
     return q
+
+
+def ulp_floor(fn, q, seed=0):
+    """The oracle's own sensitivity to a one-ulp relative perturbation of its
+    input: rel_err(fn(q (1 + 1e-16 xi)), fn(q)).  The reference's WENO
+    smoothness indicators are quadratic forms of raw values whose roundoff
+    (~1e-13 absolute on O(1) data) rivals eps = 1e-10 near constant states, so
+    its nonlinear weights, and hence its fluxes, move at this level; FP64
+    parity is asserted relative to this floor."""
+    rng = np.random.default_rng(seed)
+    qp = q * (1.0 + 1e-16 * rng.standard_normal(q.shape))
+    return rel_err(fn(qp), fn(q))
+
+
+def fp64_tol(fn, q):
+    return max(20.0 * ulp_floor(fn, q), 1e-11)
