@@ -100,12 +100,10 @@ ModeTables build_modes(const hitb200_desc& d) {
 }
 
 int lines_per_cta(int n, int nlines, int elem) {
-  // Largest R in {8, 4, 2, 1} that fits the warp task budget and ~100 KB of
-  // shared memory, preferring at least 2 CTAs per SM worth of lines.
-  const int tpl = (n + kNodesPerTask - 1) / kNodesPerTask;
+  // Largest R in {8, 4, 2, 1} whose shared memory lets two CTAs share an SM
+  // and that still leaves at least two CTAs per SM worth of lines.
   int best = 1;
   for (int R : {8, 4, 2, 1}) {
-    if (R * tpl > kMaxTasks * (kStencilThreads / 32)) continue;
     const size_t b = elem == 4 ? SweepLayout<float>(n, R).bytes() : SweepLayout<double>(n, R).bytes();
     if (b > 110 * 1024) continue;
     if ((nlines + R - 1) / R < 2 * 148 && R > 1) continue;
@@ -113,6 +111,12 @@ int lines_per_cta(int n, int nlines, int elem) {
     break;
   }
   return best;
+}
+
+int guard_blocks_for(const hitb200_desc& d) {
+  if (d.periodic || d.guard_cells <= 0) return 1;
+  const long band = 2L * d.guard_cells * (d.nx + d.ny);
+  return (int)std::max(1L, std::min(64L, (band + 255) / 256));
 }
 
 int mch_for(int n) {
@@ -129,10 +133,11 @@ struct hitb200_plan {
   unsigned char* arena = nullptr;
   size_t arena_bytes = 0;
   Work* d_tiles = nullptr;
+  Work* d_tiles32 = nullptr;
   Work* d_xlines = nullptr;
   Work* d_ylines = nullptr;
   int* d_partner = nullptr;
-  int n_tiles = 0, n_x = 0, n_y = 0, Rx = 1, Ry = 1;
+  int n_tiles = 0, n_tiles32 = 0, n_x = 0, n_y = 0, Rx = 1, Ry = 1;
   int elem = 8;
   size_t smem_x = 0, smem_y = 0, smem_sensor = 0;
   // graph replay of hitb200_step
@@ -145,9 +150,9 @@ struct hitb200_plan {
 struct hitb200_batch {
   std::vector<hitb200_plan*> plans;
   SolveDev* d_solves = nullptr;
-  Work *d_tiles = nullptr, *d_xlines = nullptr, *d_ylines = nullptr;
+  Work *d_tiles = nullptr, *d_tiles32 = nullptr, *d_xlines = nullptr, *d_ylines = nullptr;
   int* d_partner = nullptr;
-  int n_tiles = 0, n_x = 0, n_y = 0, elem = 8, mch_x = 4, mch_y = 4;
+  int n_tiles = 0, n_tiles32 = 0, n_x = 0, n_y = 0, elem = 8, mch_x = 4, mch_y = 4, guard_blocks = 1;
   size_t smem_x = 0, smem_y = 0, smem_sensor = 0;
   int any_outflow = 0, any_forcing = 0, any_hv = 0, any_noise_upload = 0;
   cudaGraphExec_t graph = nullptr;
@@ -160,9 +165,9 @@ namespace {
 struct LaunchSet {
   const SolveDev* solves;
   int nsolves;
-  const Work *tiles, *xl, *yl;
+  const Work *tiles, *tiles32, *xl, *yl;
   const int* partner;
-  int n_tiles, n_x, n_y, elem, mch_x, mch_y;
+  int n_tiles, n_tiles32, n_x, n_y, elem, mch_x, mch_y, guard_blocks;
   size_t smem_x, smem_y, smem_sensor;
   cudaStream_t st;
   // cells of all solves, and of the solves carrying viscous / forcing terms
@@ -246,7 +251,7 @@ void launch_sweep(const LaunchSet& L, int axis, int stage, int mode, const Bind&
 
 template <typename T>
 void launch_sensor_t(const LaunchSet& L, int sel, int enf, int visc, const Bind& b, uint8_t* mo) {
-  sensor_kernel<T><<<L.n_tiles, kStencilThreads, L.smem_sensor, L.st>>>(L.solves, L.tiles, sel, enf,
+  sensor_kernel<T><<<L.n_tiles32, kStencilThreads, L.smem_sensor, L.st>>>(L.solves, L.tiles32, sel, enf,
                                                                           visc, b, mo);
 }
 void launch_sensor(const LaunchSet& L, int sel, int enf, int visc, const Bind& b, uint8_t* mo) {
@@ -292,7 +297,7 @@ int launch_step_sequence(const LaunchSet& L, int any_forcing, int noise_upload, 
     launch_sweep(L, 1, stage, SW_STAGE, nb);
     if (any_outflow) {
       PMARK("guard", 0.0);
-      guard_kernel<<<L.nsolves, 256, 0, L.st>>>(L.solves, L.nsolves, stage == 2 ? 3 : stage + 1, nb);
+      guard_kernel<<<dim3(L.guard_blocks, L.nsolves), 256, 0, L.st>>>(L.solves, L.nsolves, stage == 2 ? 3 : stage + 1, nb);
     }
   }
   if (any_hv) {
@@ -304,7 +309,7 @@ int launch_step_sequence(const LaunchSet& L, int any_forcing, int noise_upload, 
     launch_hv(L, nb);
     if (any_outflow) {
       PMARK("guard", 0.0);
-      guard_kernel<<<L.nsolves, 256, 0, L.st>>>(L.solves, L.nsolves, 0, nb);
+      guard_kernel<<<dim3(L.guard_blocks, L.nsolves), 256, 0, L.st>>>(L.solves, L.nsolves, 0, nb);
     }
   }
   if (prof) prof->end();
@@ -340,6 +345,9 @@ LaunchSet plan_launch_set(hitb200_plan* p, cudaStream_t st) {
   L.solves = p->d_solve;
   L.nsolves = 1;
   L.tiles = p->d_tiles;
+  L.tiles32 = p->d_tiles32;
+  L.n_tiles32 = p->n_tiles32;
+  L.guard_blocks = guard_blocks_for(p->desc);
   L.xl = p->d_xlines;
   L.yl = p->d_ylines;
   L.partner = p->d_partner;
@@ -510,6 +518,7 @@ size_t hitb200_plan_device_bytes(const hitb200_desc* d) {
   a.take(ntile * NDIAG * sizeof(double));
   a.take(8 * sizeof(unsigned) + sizeof(int) + NDIAG * sizeof(double));
   a.take(ntile * sizeof(Work));
+  a.take((size_t)((d->nx + kSenTX - 1) / kSenTX) * ((d->ny + kSenTY - 1) / kSenTY) * sizeof(Work));
   a.take((size_t)(d->ny + d->nx) * sizeof(Work));
   return a.off;
 }
@@ -565,6 +574,9 @@ int hitb200_plan_create(const hitb200_desc* d, hitb200_plan** out) {
   const size_t o_pdiag = a.take(p->n_tiles * NDIAG * sizeof(double));
   const size_t o_cnt = a.take(8 * sizeof(unsigned) + sizeof(int) + NDIAG * sizeof(double));
   const size_t o_tiles = a.take(p->n_tiles * sizeof(Work));
+  const int ntx32 = (nx + kSenTX - 1) / kSenTX, nty32 = (ny + kSenTY - 1) / kSenTY;
+  p->n_tiles32 = ntx32 * nty32;
+  const size_t o_tiles32 = a.take(p->n_tiles32 * sizeof(Work));
   const size_t o_xl = a.take(p->n_x * sizeof(Work));
   const size_t o_yl = a.take(p->n_y * sizeof(Work));
   p->arena_bytes = a.off;
@@ -654,6 +666,7 @@ int hitb200_plan_create(const hitb200_desc* d, hitb200_plan** out) {
   p->d_solve = reinterpret_cast<SolveDev*>(base + o_solve);
   p->d_partner = reinterpret_cast<int*>(base + o_partner);
   p->d_tiles = reinterpret_cast<Work*>(base + o_tiles);
+  p->d_tiles32 = reinterpret_cast<Work*>(base + o_tiles32);
   p->d_xlines = reinterpret_cast<Work*>(base + o_xl);
   p->d_ylines = reinterpret_cast<Work*>(base + o_yl);
 
@@ -684,6 +697,9 @@ int hitb200_plan_create(const hitb200_desc* d, hitb200_plan** out) {
   std::vector<Work> tiles;
   for (int ty = 0; ty < nty; ++ty)
     for (int tx = 0; tx < ntx; ++tx) tiles.push_back({0, tx * kTileX, ty * kTileY, (int)tiles.size()});
+  std::vector<Work> tiles32;
+  for (int ty = 0; ty < nty32; ++ty)
+    for (int tx = 0; tx < ntx32; ++tx) tiles32.push_back({0, tx * kSenTX, ty * kSenTY, (int)tiles32.size()});
   std::vector<Work> xl, yl;
   for (int r = 0; r < ny; r += p->Rx) xl.push_back({0, r, std::min(p->Rx, ny - r), 0});
   for (int c = 0; c < nx; c += p->Ry) yl.push_back({0, c, std::min(p->Ry, nx - c), 0});
@@ -703,6 +719,7 @@ int hitb200_plan_create(const hitb200_desc* d, hitb200_plan** out) {
   HB_PUT(p->d_partner, mt.partner.data(), kMaxForce * sizeof(int));
   HB_PUT(s.scal, scal.data(), SCAL_SIZE * sizeof(double));
   HB_PUT(p->d_tiles, tiles.data(), tiles.size() * sizeof(Work));
+  HB_PUT(p->d_tiles32, tiles32.data(), tiles32.size() * sizeof(Work));
   HB_PUT(p->d_xlines, xl.data(), xl.size() * sizeof(Work));
   HB_PUT(p->d_ylines, yl.data(), yl.size() * sizeof(Work));
   HB_PUT(p->d_solve, &s, sizeof(SolveDev));
@@ -849,7 +866,7 @@ int hitb200_outflow_guard(hitb200_plan* p, double* q, void* stream) {
   Bind b{};
   b.use = 1;
   b.qout = q;
-  guard_kernel<<<1, 256, 0, (cudaStream_t)stream>>>(p->d_solve, 1, 0, b);
+  guard_kernel<<<dim3(guard_blocks_for(p->desc), 1), 256, 0, (cudaStream_t)stream>>>(p->d_solve, 1, 0, b);
   HB_LAUNCHED("guard_kernel");
   return HITB200_OK;
 }
@@ -1043,7 +1060,7 @@ int hitb200_batch_create(const hitb200_desc* descs, int32_t n, hitb200_batch** o
     if (descs[i].precision != descs[0].precision) return invalid("batch members must share precision");
   hitb200_batch* b = new hitb200_batch();
   std::vector<SolveDev> hs;
-  std::vector<Work> tiles, xl, yl;
+  std::vector<Work> tiles, tiles32, xl, yl;
   std::vector<int> partner;
   for (int i = 0; i < n; ++i) {
     hitb200_plan* p = nullptr;
@@ -1059,6 +1076,11 @@ int hitb200_batch_create(const hitb200_desc* descs, int32_t n, hitb200_batch** o
     int k = 0;
     for (int ty = 0; ty < nty; ++ty)
       for (int tx = 0; tx < ntx; ++tx) tiles.push_back({i, tx * kTileX, ty * kTileY, k++});
+    const int ntx32 = (p->desc.nx + kSenTX - 1) / kSenTX, nty32 = (p->desc.ny + kSenTY - 1) / kSenTY;
+    int k32 = 0;
+    for (int ty = 0; ty < nty32; ++ty)
+      for (int tx = 0; tx < ntx32; ++tx) tiles32.push_back({i, tx * kSenTX, ty * kSenTY, k32++});
+    b->guard_blocks = std::max(b->guard_blocks, guard_blocks_for(p->desc));
     for (int r0 = 0; r0 < p->desc.ny; r0 += p->Rx) xl.push_back({i, r0, std::min(p->Rx, p->desc.ny - r0), 0});
     for (int c0 = 0; c0 < p->desc.nx; c0 += p->Ry) yl.push_back({i, c0, std::min(p->Ry, p->desc.nx - c0), 0});
     ModeTables mt = build_modes(p->desc);
@@ -1079,11 +1101,13 @@ int hitb200_batch_create(const hitb200_desc* descs, int32_t n, hitb200_batch** o
     return invalid("batched solves draw forcing noise on the device (noise_mode 1)");
   }
   b->n_tiles = (int)tiles.size();
+  b->n_tiles32 = (int)tiles32.size();
   b->n_x = (int)xl.size();
   b->n_y = (int)yl.size();
   // interleave the sweep work of different solves so that large grids start first
   cudaError_t e;
-  size_t bytes = hs.size() * sizeof(SolveDev) + (tiles.size() + xl.size() + yl.size()) * sizeof(Work) +
+  size_t bytes = hs.size() * sizeof(SolveDev) +
+                 (tiles.size() + tiles32.size() + xl.size() + yl.size()) * sizeof(Work) +
                  partner.size() * sizeof(int) + 1024;
   unsigned char* buf = nullptr;
   e = cudaMalloc(&buf, bytes);
@@ -1100,6 +1124,7 @@ int hitb200_batch_create(const hitb200_desc* descs, int32_t n, hitb200_batch** o
   };
   b->d_solves = reinterpret_cast<SolveDev*>(put(hs.data(), hs.size() * sizeof(SolveDev)));
   b->d_tiles = reinterpret_cast<Work*>(put(tiles.data(), tiles.size() * sizeof(Work)));
+  b->d_tiles32 = reinterpret_cast<Work*>(put(tiles32.data(), tiles32.size() * sizeof(Work)));
   b->d_xlines = reinterpret_cast<Work*>(put(xl.data(), xl.size() * sizeof(Work)));
   b->d_ylines = reinterpret_cast<Work*>(put(yl.data(), yl.size() * sizeof(Work)));
   b->d_partner = reinterpret_cast<int*>(put(partner.data(), partner.size() * sizeof(int)));
@@ -1177,6 +1202,9 @@ static LaunchSet batch_launch_set(hitb200_batch* b, cudaStream_t st) {
   L.solves = b->d_solves;
   L.nsolves = (int)b->plans.size();
   L.tiles = b->d_tiles;
+  L.tiles32 = b->d_tiles32;
+  L.n_tiles32 = b->n_tiles32;
+  L.guard_blocks = b->guard_blocks;
   L.xl = b->d_xlines;
   L.yl = b->d_ylines;
   L.partner = b->d_partner;

@@ -124,12 +124,25 @@ struct Work {
 };
 
 // ---- small device helpers --------------------------------------------------------
-__device__ __forceinline__ int wrap_or_clamp(int i, int n, int periodic) {
+// Periodic wrap / outflow clamp of a node index within one grid length of
+// the domain (larger offsets, only on tiny grids, fall back to a modulo).
+__device__ __forceinline__ int fold_node(int i, int n, int periodic) {
   if (periodic) {
-    i %= n;
-    return i < 0 ? i + n : i;
+    if (i < 0) i += n;
+    else if (i >= n) i -= n;
+    if (i < 0 || i >= n) {
+      i %= n;
+      if (i < 0) i += n;
+    }
+    return i;
   }
   return i < 0 ? 0 : (i >= n ? n - 1 : i);
+}
+
+// (m * j) mod n in [0, n) for a Fourier mode m and grid index j (32-bit: |m| <= n).
+__device__ __forceinline__ int mode_index(int m, int j, int n) {
+  int t = (m * j) % n;
+  return t < 0 ? t + n : t;
 }
 
 template <typename T>

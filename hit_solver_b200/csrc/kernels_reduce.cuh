@@ -117,24 +117,59 @@ __global__ void __launch_bounds__(kRedThreads)
   __shared__ double sm[kRedWarps * (R_FIXED + 4 * kMaxDrag)];
   __shared__ double red[R_FIXED + 4 * kMaxDrag];
   const bool need_grad = (mode != PRE_CHECK);
-  if (need_grad) {
-    for (int idx = threadIdx.x; idx < (kTileY + 2) * (kTileX + 2); idx += blockDim.x) {
-      const int a = idx / (kTileX + 2), b = idx % (kTileX + 2);
-      const int gj = wrap_or_clamp(y0 + a - 1, ny, per), gi = wrap_or_clamp(x0 + b - 1, nx, per);
-      const size_t o = (size_t)gj * nx + gi;
-      double q0 = q[o], q1 = q[o + plane], q2 = q[o + 2 * plane], q3 = q[o + 3 * plane];
-      if (enf) enforce_node(q0, q1, q2, q3, g);
-      const Prim<double> p = primitives(q0, q1, q2, q3, g);
-      su[a][b] = p.u;
-      sv[a][b] = p.v;
-    }
-    __syncthreads();
-  }
+  const int tx = threadIdx.x & 31, ty0 = threadIdx.x >> 5;
 
   double ax = 0, ay = 0, div2 = 0, vort2 = 0, mr = 0, mp = 0, me = 0, ps = 0, sr = 0, vel2 = 0,
          cs = 0, fnf = 0, fnr = 0, fnp = 0;
-  const int tx = threadIdx.x & 31, ty0 = threadIdx.x >> 5;
-  double mom[2][2];  // rho*u, rho*v of this thread's two cells (for the drag transform)
+  // Every node of the tile and its one-node halo is loaded once; tile nodes
+  // also feed the pointwise reductions here.
+  for (int a = ty0; a < kTileY + 2; a += kRedWarps) {
+    const int gy = y0 + a - 1;
+    const int gj = fold_node(gy, ny, per);
+    for (int b = tx; b < kTileX + 2; b += 32) {
+      const int gx = x0 + b - 1;
+      const bool own = a >= 1 && a <= kTileY && b >= 1 && b <= kTileX && gy < ny && gx < nx;
+      if (!need_grad && !own) continue;
+      const int gi = fold_node(gx, nx, per);
+      const size_t o = (size_t)gj * nx + gi;
+      const double q0 = q[o], q1 = q[o + plane], q2 = q[o + 2 * plane], q3 = q[o + 3 * plane];
+      if (need_grad) {
+        double e0 = q0, e1 = q1, e2 = q2, e3 = q3;
+        if (enf) enforce_node(e0, e1, e2, e3, g);
+        const Prim<double> p = primitives(e0, e1, e2, e3, g);
+        su[a][b] = p.u;
+        sv[a][b] = p.v;
+        if (own) {
+          const double c = sqrt(g * p.p / p.rho);
+          ax = fmax(ax, fabs(p.u) + c);
+          ay = fmax(ay, fabs(p.v) + c);
+          mr = fmax(mr, fabs(p.rho));
+          mp = fmax(mp, fabs(p.p));
+          me = fmax(me, fabs(p.p / (p.rho * (g - 1.0))));
+        }
+      }
+      if (!own) continue;
+      // raw state: time step, Mach, cooling, validation
+      const double rho = q0 > kRhoFloor ? q0 : kRhoFloor;
+      const double rinv = 1.0 / rho;
+      const double u = q1 * rinv, v = q2 * rinv;
+      double pr = (g - 1.0) * (q3 - 0.5 * rho * (u * u + v * v));
+      pr = pr > kPFloor ? pr : kPFloor;
+      const double cr = sqrt(g * pr * rinv);
+      ps += pr;
+      sr = fmax(sr, (fabs(u) + cr) / S.dx + (fabs(v) + cr) / S.dy);
+      vel2 += u * u + v * v;
+      cs += cr;
+      const double i0 = 1.0 / q0;
+      const double ur = q1 * i0, vr = q2 * i0;
+      const double praw = (g - 1.0) * (q3 - 0.5 * q0 * (ur * ur + vr * vr));
+      if (!(isfinite(q0) && isfinite(q1) && isfinite(q2) && isfinite(q3)) || !isfinite(praw))
+        fnf = 1.0;
+      if (q0 <= 0.0) fnr = 1.0;
+      if (praw <= 0.0) fnp = 1.0;
+    }
+  }
+  if (need_grad) __syncthreads();
   int cj[2], ci[2];
   bool valid[2];
 #pragma unroll
@@ -144,68 +179,37 @@ __global__ void __launch_bounds__(kRedThreads)
     cj[k] = gj;
     ci[k] = gi;
     valid[k] = (gj < ny && gi < nx);
-    mom[k][0] = mom[k][1] = 0.0;
-    if (!valid[k]) continue;
-    const size_t o = (size_t)gj * nx + gi;
-    const double q0 = q[o], q1 = q[o + plane], q2 = q[o + 2 * plane], q3 = q[o + 3 * plane];
-    mom[k][0] = q1;
-    mom[k][1] = q2;
-    // raw state: time step, Mach, cooling, validation
-    const Prim<double> pr = primitives(q0, q1, q2, q3, g);
-    const double cr = sqrt(g * pr.p / pr.rho);
-    ps += pr.p;
-    sr = fmax(sr, (fabs(pr.u) + cr) / S.dx + (fabs(pr.v) + cr) / S.dy);
-    vel2 += pr.u * pr.u + pr.v * pr.v;
-    cs += cr;
-    {
-      const double ur = q1 / q0, vr = q2 / q0;
-      const double praw = (g - 1.0) * (q3 - 0.5 * q0 * (ur * ur + vr * vr));
-      if (!(isfinite(q0) && isfinite(q1) && isfinite(q2) && isfinite(q3)) || !isfinite(praw))
-        fnf = 1.0;
-      if (q0 <= 0.0) fnr = 1.0;
-      if (praw <= 0.0) fnp = 1.0;
+    if (!valid[k] || !need_grad) continue;
+    // sensor divergence / vorticity: central, one-sided at outflow edges
+    const int a = ty + 1, b = tx + 1;
+    double dudx, dvdx, dudy, dvdy;
+    if (per || (gi > 0 && gi < nx - 1)) {
+      dudx = (su[a][b + 1] - su[a][b - 1]) / (2.0 * S.dx);
+      dvdx = (sv[a][b + 1] - sv[a][b - 1]) / (2.0 * S.dx);
+    } else if (nx == 1) {
+      dudx = dvdx = 0.0;
+    } else if (gi == 0) {
+      dudx = (su[a][b + 1] - su[a][b]) / S.dx;
+      dvdx = (sv[a][b + 1] - sv[a][b]) / S.dx;
+    } else {
+      dudx = (su[a][b] - su[a][b - 1]) / S.dx;
+      dvdx = (sv[a][b] - sv[a][b - 1]) / S.dx;
     }
-    if (need_grad) {
-      double e0 = q0, e1 = q1, e2 = q2, e3 = q3;
-      if (enf) enforce_node(e0, e1, e2, e3, g);
-      const Prim<double> p = primitives(e0, e1, e2, e3, g);
-      const double c = sqrt(g * p.p / p.rho);
-      ax = fmax(ax, fabs(p.u) + c);
-      ay = fmax(ay, fabs(p.v) + c);
-      mr = fmax(mr, fabs(p.rho));
-      mp = fmax(mp, fabs(p.p));
-      me = fmax(me, fabs(p.p / (p.rho * (g - 1.0))));
-      // sensor divergence / vorticity: central, one-sided at outflow edges
-      const int a = ty + 1, b = tx + 1;
-      double dudx, dvdx, dudy, dvdy;
-      if (per || (gi > 0 && gi < nx - 1)) {
-        dudx = (su[a][b + 1] - su[a][b - 1]) / (2.0 * S.dx);
-        dvdx = (sv[a][b + 1] - sv[a][b - 1]) / (2.0 * S.dx);
-      } else if (nx == 1) {
-        dudx = dvdx = 0.0;
-      } else if (gi == 0) {
-        dudx = (su[a][b + 1] - su[a][b]) / S.dx;
-        dvdx = (sv[a][b + 1] - sv[a][b]) / S.dx;
-      } else {
-        dudx = (su[a][b] - su[a][b - 1]) / S.dx;
-        dvdx = (sv[a][b] - sv[a][b - 1]) / S.dx;
-      }
-      if (per || (gj > 0 && gj < ny - 1)) {
-        dudy = (su[a + 1][b] - su[a - 1][b]) / (2.0 * S.dy);
-        dvdy = (sv[a + 1][b] - sv[a - 1][b]) / (2.0 * S.dy);
-      } else if (ny == 1) {
-        dudy = dvdy = 0.0;
-      } else if (gj == 0) {
-        dudy = (su[a + 1][b] - su[a][b]) / S.dy;
-        dvdy = (sv[a + 1][b] - sv[a][b]) / S.dy;
-      } else {
-        dudy = (su[a][b] - su[a - 1][b]) / S.dy;
-        dvdy = (sv[a][b] - sv[a - 1][b]) / S.dy;
-      }
-      const double dv = dudx + dvdy, vo = dvdx - dudy;
-      div2 += dv * dv;
-      vort2 += vo * vo;
+    if (per || (gj > 0 && gj < ny - 1)) {
+      dudy = (su[a + 1][b] - su[a - 1][b]) / (2.0 * S.dy);
+      dvdy = (sv[a + 1][b] - sv[a - 1][b]) / (2.0 * S.dy);
+    } else if (ny == 1) {
+      dudy = dvdy = 0.0;
+    } else if (gj == 0) {
+      dudy = (su[a + 1][b] - su[a][b]) / S.dy;
+      dvdy = (sv[a + 1][b] - sv[a][b]) / S.dy;
+    } else {
+      dudy = (su[a][b] - su[a - 1][b]) / S.dy;
+      dvdy = (sv[a][b] - sv[a - 1][b]) / S.dy;
     }
+    const double dv = dudx + dvdy, vo = dvdx - dudy;
+    div2 += dv * dv;
+    vort2 += vo * vo;
   }
   const int nslots = (mode == PRE_STAGE || mode == PRE_STEP) ? S.nred : R_FIXED;
   warp_to_smem<OP_MAX>(ax, sm, R_AX, nslots);
@@ -230,16 +234,14 @@ __global__ void __launch_bounds__(kRedThreads)
 #pragma unroll
       for (int k = 0; k < 2; ++k) {
         if (!valid[k]) continue;
-        int ix = (int)(((long long)md.x * ci[k]) % nx);
-        if (ix < 0) ix += nx;
-        int iy = (int)(((long long)md.y * cj[k]) % ny);
-        if (iy < 0) iy += ny;
-        const double2 ex = S.twx[ix], ey = S.twy[iy];
+        const size_t o = (size_t)cj[k] * nx + ci[k];
+        const double m0 = q[o + plane], m1 = q[o + 2 * plane];
+        const double2 ex = S.twx[mode_index(md.x, ci[k], nx)], ey = S.twy[mode_index(md.y, cj[k], ny)];
         const double2 e = make_double2(cmul_re(ex, ey), cmul_im(ex, ey));  // e^{-i theta}
-        v[0] += mom[k][0] * e.x;
-        v[1] += mom[k][0] * e.y;
-        v[2] += mom[k][1] * e.x;
-        v[3] += mom[k][1] * e.y;
+        v[0] += m0 * e.x;
+        v[1] += m0 * e.y;
+        v[2] += m1 * e.x;
+        v[3] += m1 * e.y;
       }
 #pragma unroll
       for (int k = 0; k < 4; ++k) warp_to_smem<OP_SUM>(v[k], sm, R_FIXED + 4 * m + k, nslots);
@@ -342,11 +344,7 @@ __global__ void __launch_bounds__(kRedThreads)
 #pragma unroll
     for (int k = 0; k < 2; ++k) {
       if (!valid[k]) continue;
-      int ix = (int)(((long long)md.x * ci[k]) % nx);
-      if (ix < 0) ix += nx;
-      int iy = (int)(((long long)md.y * cj[k]) % ny);
-      if (iy < 0) iy += ny;
-      const double2 ex = S.twx[ix], ey = S.twy[iy];
+      const double2 ex = S.twx[mode_index(md.x, ci[k], nx)], ey = S.twy[mode_index(md.y, cj[k], ny)];
       re += val[k] * cmul_re(ex, ey);
       im += val[k] * cmul_im(ex, ey);
     }
@@ -476,11 +474,7 @@ __global__ void __launch_bounds__(kRedThreads)
     double fx = 0.0, fy = 0.0;
     for (int m = 0; m < nf; ++m) {
       const int2 md = modes[m];
-      int ix = (int)(((long long)md.x * gi) % nx);
-      if (ix < 0) ix += nx;
-      int iy = (int)(((long long)md.y * gj) % ny);
-      if (iy < 0) iy += ny;
-      const double2 ex = S.twx[ix], ey = S.twy[iy];
+      const double2 ex = S.twx[mode_index(md.x, gi, nx)], ey = S.twy[mode_index(md.y, gj, ny)];
       // e^{+i theta} = conj(e^{-i theta})
       const double er = cmul_re(ex, ey), ei = -cmul_im(ex, ey);
       fx += ca[m].x * er - ca[m].y * ei;

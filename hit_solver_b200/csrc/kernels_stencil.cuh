@@ -10,8 +10,11 @@
 namespace hitb200 {
 
 constexpr unsigned kFull = 0xffffffffu;
+
+
 constexpr int kStencilThreads = 256;
-constexpr int kSenTX = 32, kSenTY = 16;
+constexpr int kSenTX = 32, kSenTY = 32;  // sensor tile
+constexpr int kHvTX = 32, kHvTY = 16;    // hyperviscosity tile
 
 // =============================================================================
 // Shock sensor (OOP/spatial_operator.py:147-176, 263-304;
@@ -21,11 +24,40 @@ constexpr int kSenTX = 32, kSenTY = 16;
 // separably: a row pass (OR over +-width in x) and a column pass.
 // =============================================================================
 template <typename T>
-__device__ __forceinline__ T jump3(T am, T a, T ap, T eps) {
-  const T right = fabs(ap - a) / (fabs(ap) + fabs(a) + eps);
-  const T left = fabs(a - am) / (fabs(a) + fabs(am) + eps);
-  const T curv = fabs(ap - T(2) * a + am) / (fabs(ap) + T(2) * fabs(a) + fabs(am) + eps);
-  return fmax(fmax(left, right), curv);
+__device__ __forceinline__ T type_eps() {
+  return sizeof(T) == 4 ? T(FLT_EPSILON) : T(DBL_EPSILON);
+}
+
+// fl(num / den) > thr for den > 0, exactly as the reference's IEEE quotient
+// compares, but decided by a multiplication unless the quotient lies within
+// ~8 ulp of the threshold (then the quotient itself is formed).
+template <typename T>
+__device__ __forceinline__ bool ratio_gt(T num, T den, T thr) {
+  const T e = T(8) * type_eps<T>();
+  const T t = thr * den;
+  if (num > t * (T(1) + e)) return true;
+  if (num < t * (T(1) - e)) return false;
+  return num / den > thr;
+}
+
+// |num / den - thr| within tol * thr (a node "within roundoff" of the threshold)
+template <typename T>
+__device__ __forceinline__ bool ratio_near(T num, T den, T thr, T tol) {
+  const T t = thr * den;
+  return fabs(num - t) <= tol * t;
+}
+
+// The reference's relative jump metric max(left, right, curvature) > thr
+// (OOP/spatial_operator.py:147-166), one axis, neighbours am / ap.
+template <typename T>
+__device__ __forceinline__ bool jump_gt(T am, T a, T ap, T eps, T thr, T tol, bool& near) {
+  const T aa = fabs(a), aap = fabs(ap), aam = fabs(am);
+  const T nr = fabs(ap - a), dr = aap + aa + eps;
+  const T nl = fabs(a - am), dl = aa + aam + eps;
+  const T nc = fabs(ap - T(2) * a + am), dc = aap + T(2) * aa + aam + eps;
+  near = near || ratio_near(nr, dr, thr, tol) || ratio_near(nl, dl, thr, tol) ||
+         ratio_near(nc, dc, thr, tol);
+  return ratio_gt(nr, dr, thr) || ratio_gt(nl, dl, thr) || ratio_gt(nc, dc, thr);
 }
 
 __host__ __device__ inline int sensor_halo(int width) { return width + 1 > 2 ? width + 1 : 2; }
@@ -37,6 +69,14 @@ __host__ __device__ inline size_t sensor_smem_bytes(int width, int elem) {
   const size_t raw = (size_t)(kSenTY + 2 * width) * (kSenTX + 2 * width);
   const size_t row = (size_t)(kSenTY + 2 * width) * kSenTX;
   return prim + raw + row + 16;
+}
+
+// Central difference quotient of the sensor.  FP64 divides by 2h exactly as
+// the reference; FP32 multiplies by the reciprocal.
+template <typename T>
+__device__ __forceinline__ T dq(T a, T b, T h2, T ih2) {
+  if constexpr (sizeof(T) == 8) return (a - b) / h2;
+  else return (a - b) * ih2;
 }
 
 // sel: 0 q, 1 q1, 2 q2, 3 hyperviscosity input (stage-3 output q1, runs only on
@@ -60,6 +100,7 @@ __global__ void __launch_bounds__(kStencilThreads)
   const int W = S.width, HW = sensor_halo(W);
   const int SX = kSenTX + 2 * HW, SY = kSenTY + 2 * HW;
   const int x0 = wk.a, y0 = wk.b;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5, nty = blockDim.x >> 5;
   const T g = T(S.gamma);
   T* RHO = reinterpret_cast<T*>(smem);
   T* U = RHO + SX * SY;
@@ -70,115 +111,109 @@ __global__ void __launch_bounds__(kStencilThreads)
   const int RX = kSenTX + 2 * W, RY = kSenTY + 2 * W;
   uint8_t* ROW = RAW + RX * RY;
 
-  for (int idx = threadIdx.x; idx < SX * SY; idx += blockDim.x) {
-    const int a = idx / SX, b = idx % SX;
-    const int gj = wrap_or_clamp(y0 - HW + a, ny, per), gi = wrap_or_clamp(x0 - HW + b, nx, per);
-    const size_t o = (size_t)gj * nx + gi;
-    T q0 = T(q[o]), q1 = T(q[o + plane]), q2 = T(q[o + 2 * plane]), q3 = T(q[o + 3 * plane]);
-    if (enf) enforce_node(q0, q1, q2, q3, g);
-    const Prim<T> p = primitives(q0, q1, q2, q3, g);
-    RHO[idx] = p.rho;
-    U[idx] = p.u;
-    V[idx] = p.v;
-    P[idx] = p.p;
-    E[idx] = p.p / (p.rho * (g - T(1)));
+  for (int a = ty; a < SY; a += nty) {
+    const int gj = fold_node(y0 - HW + a, ny, per);
+    for (int b = tx; b < SX; b += 32) {
+      const int gi = fold_node(x0 - HW + b, nx, per);
+      const size_t o = (size_t)gj * nx + gi;
+      T q0 = T(q[o]), q1 = T(q[o + plane]), q2 = T(q[o + 2 * plane]), q3 = T(q[o + 3 * plane]);
+      if (enf) enforce_node(q0, q1, q2, q3, g);
+      const Prim<T> p = primitives(q0, q1, q2, q3, g);
+      const int k = a * SX + b;
+      RHO[k] = p.rho;
+      U[k] = p.u;
+      V[k] = p.v;
+      P[k] = p.p;
+      E[k] = p.p / (p.rho * (g - T(1)));
+    }
   }
   __syncthreads();
 
   const T eps_r = T(sc[S_EPS_RHO]), eps_p = T(sc[S_EPS_P]), eps_e = T(sc[S_EPS_E]);
   const T thr = T(S.jump_thr);
   const T comp_lim = T(sc[S_COMP_LIM]), shear_lim = T(sc[S_SHEAR_LIM]);
+  const bool comp_on = isfinite(comp_lim), shear_on = isfinite(shear_lim);
   const T tdx = T(2.0 * S.dx), tdy = T(2.0 * S.dy), hx = T(S.dx), hy = T(S.dy);
-  const T tol = T(32) * (sizeof(T) == 4 ? T(FLT_EPSILON) : T(DBL_EPSILON));
-  int near = 0;
-  for (int idx = threadIdx.x; idx < RX * RY; idx += blockDim.x) {
-    const int ar = idx / RX, br = idx % RX;
-    const int gj = y0 - W + ar, gi = x0 - W + br;
-    const bool inside = gj >= 0 && gj < ny && gi >= 0 && gi < nx;
-    if (!per && !inside) {
-      RAW[idx] = 0;
-      continue;
-    }
-    const int a = ar + (HW - W), b = br + (HW - W);
-    const int c = a * SX + b;
-    // sensor velocity gradients: central; first-order one-sided at outflow edges
-    T dudx, dvdx, dudy, dvdy;
-    if (per || (gi > 0 && gi < nx - 1)) {
-      dudx = (U[c + 1] - U[c - 1]) / tdx;
-      dvdx = (V[c + 1] - V[c - 1]) / tdx;
-    } else if (nx == 1) {
-      dudx = dvdx = T(0);
-    } else if (gi == 0) {
-      dudx = (U[c + 1] - U[c]) / hx;
-      dvdx = (V[c + 1] - V[c]) / hx;
-    } else {
-      dudx = (U[c] - U[c - 1]) / hx;
-      dvdx = (V[c] - V[c - 1]) / hx;
-    }
-    if (per || (gj > 0 && gj < ny - 1)) {
-      dudy = (U[c + SX] - U[c - SX]) / tdy;
-      dvdy = (V[c + SX] - V[c - SX]) / tdy;
-    } else if (ny == 1) {
-      dudy = dvdy = T(0);
-    } else if (gj == 0) {
-      dudy = (U[c + SX] - U[c]) / hy;
-      dvdy = (V[c + SX] - V[c]) / hy;
-    } else {
-      dudy = (U[c] - U[c - SX]) / hy;
-      dvdy = (V[c] - V[c - SX]) / hy;
-    }
-    const T div = dudx + dvdy;
-    const T vort = dvdx - dudy;
-    const T jr = fmax(jump3(RHO[c - 1], RHO[c], RHO[c + 1], eps_r),
-                      jump3(RHO[c - SX], RHO[c], RHO[c + SX], eps_r));
-    const T jp = fmax(jump3(P[c - 1], P[c], P[c + 1], eps_p),
-                      jump3(P[c - SX], P[c], P[c + SX], eps_p));
-    const T je = fmax(jump3(E[c - 1], E[c], E[c + 1], eps_e),
-                      jump3(E[c - SX], E[c], E[c + SX], eps_e));
-    bool m = (div < comp_lim) || (fabs(vort) > shear_lim) || (jr > thr) || (jp > thr) || (je > thr);
-    if (!per && S.boundary_guard > 0) {
-      const int bg = S.boundary_guard;
-      if (gj < bg || gj >= ny - bg || gi < bg || gi >= nx - bg) m = true;
-    }
-    RAW[idx] = m ? 1 : 0;
-    // nodes of this tile whose metric sits within roundoff of a threshold
-    if (ar >= W && ar < W + kSenTY && br >= W && br < W + kSenTX && inside) {
-      const T tj = tol * thr;
-      bool nr = fabs(jr - thr) <= tj || fabs(jp - thr) <= tj || fabs(je - thr) <= tj;
-      if (isfinite(comp_lim)) nr = nr || fabs(div - comp_lim) <= tol * fabs(comp_lim);
-      if (isfinite(shear_lim)) nr = nr || fabs(fabs(vort) - shear_lim) <= tol * shear_lim;
-      near += nr ? 1 : 0;
+  const T itdx = T(1.0 / (2.0 * S.dx)), itdy = T(1.0 / (2.0 * S.dy));
+  const T tol = T(32) * type_eps<T>();
+  int near_count = 0;
+  for (int ar = ty; ar < RY; ar += nty) {
+    const int gj = y0 - W + ar;
+    for (int br = tx; br < RX; br += 32) {
+      const int gi = x0 - W + br;
+      const bool inside = gj >= 0 && gj < ny && gi >= 0 && gi < nx;
+      const int idx = ar * RX + br;
+      if (!per && !inside) {
+        RAW[idx] = 0;
+        continue;
+      }
+      const int c = (ar + HW - W) * SX + br + HW - W;
+      bool near = false;
+      bool m = false;
+      // sensor velocity gradients: central; first-order one-sided at outflow edges
+      T dudx = T(0), dvdx = T(0), dudy = T(0), dvdy = T(0);
+      const bool cx = per || (gi > 0 && gi < nx - 1), cy = per || (gj > 0 && gj < ny - 1);
+      if (comp_on || shear_on) {
+        if (cx) dudx = dq(U[c + 1], U[c - 1], tdx, itdx);
+        else if (nx > 1) dudx = gi == 0 ? (U[c + 1] - U[c]) / hx : (U[c] - U[c - 1]) / hx;
+        if (cy) dvdy = dq(V[c + SX], V[c - SX], tdy, itdy);
+        else if (ny > 1) dvdy = gj == 0 ? (V[c + SX] - V[c]) / hy : (V[c] - V[c - SX]) / hy;
+      }
+      if (comp_on) {
+        const T div = dudx + dvdy;
+        m = div < comp_lim;
+        near = near || fabs(div - comp_lim) <= tol * fabs(comp_lim);
+      }
+      if (shear_on) {
+        if (cx) dvdx = dq(V[c + 1], V[c - 1], tdx, itdx);
+        else if (nx > 1) dvdx = gi == 0 ? (V[c + 1] - V[c]) / hx : (V[c] - V[c - 1]) / hx;
+        if (cy) dudy = dq(U[c + SX], U[c - SX], tdy, itdy);
+        else if (ny > 1) dudy = gj == 0 ? (U[c + SX] - U[c]) / hy : (U[c] - U[c - SX]) / hy;
+        const T av = fabs(dvdx - dudy);
+        m = m || av > shear_lim;
+        near = near || fabs(av - shear_lim) <= tol * shear_lim;
+      }
+      m = jump_gt(RHO[c - 1], RHO[c], RHO[c + 1], eps_r, thr, tol, near) || m;
+      m = jump_gt(RHO[c - SX], RHO[c], RHO[c + SX], eps_r, thr, tol, near) || m;
+      m = jump_gt(P[c - 1], P[c], P[c + 1], eps_p, thr, tol, near) || m;
+      m = jump_gt(P[c - SX], P[c], P[c + SX], eps_p, thr, tol, near) || m;
+      m = jump_gt(E[c - 1], E[c], E[c + 1], eps_e, thr, tol, near) || m;
+      m = jump_gt(E[c - SX], E[c], E[c + SX], eps_e, thr, tol, near) || m;
+      if (!per && S.boundary_guard > 0) {
+        const int bg = S.boundary_guard;
+        if (gj < bg || gj >= ny - bg || gi < bg || gi >= nx - bg) m = true;
+      }
+      RAW[idx] = m ? 1 : 0;
+      // nodes of this tile whose metric sits within roundoff of a threshold
+      if (near && inside && ar >= W && ar < W + kSenTY && br >= W && br < W + kSenTX) ++near_count;
     }
   }
   __syncthreads();
-  for (int idx = threadIdx.x; idx < RY * kSenTX; idx += blockDim.x) {
-    const int ar = idx / kSenTX, bx = idx % kSenTX;
+  for (int ar = ty; ar < RY; ar += nty) {
     uint8_t v = 0;
-    for (int d = 0; d <= 2 * W; ++d) v |= RAW[ar * RX + bx + d];
-    ROW[idx] = v;
+    for (int d = 0; d <= 2 * W; ++d) v |= RAW[ar * RX + tx + d];
+    ROW[ar * kSenTX + tx] = v;
   }
   __syncthreads();
-  for (int idx = threadIdx.x; idx < kSenTX * kSenTY; idx += blockDim.x) {
-    const int ty = idx / kSenTX, tx = idx % kSenTX;
-    const int gj = y0 + ty, gi = x0 + tx;
+  for (int a = ty; a < kSenTY; a += nty) {
+    const int gj = y0 + a, gi = x0 + tx;
     if (gj >= ny || gi >= nx) continue;
     uint8_t v = 0;
-    for (int d = 0; d <= 2 * W; ++d) v |= ROW[(ty + d) * kSenTX + tx];
+    for (int d = 0; d <= 2 * W; ++d) v |= ROW[(a + d) * kSenTX + tx];
     mask[(size_t)gj * nx + gi] = v;
   }
-  near = warp_sum(near);
-  if ((threadIdx.x & 31) == 0 && near > 0) atomicAdd(S.near_count, near);
+  near_count = warp_sum(near_count);
+  if (tx == 0 && near_count > 0) atomicAdd(S.near_count, near_count);
 
   if (!want_visc || S.mu == 0.0) return;
   // viscous stress and heat-flux divergence, central differences (periodic)
   const T mu = T(S.mu), kap = T(S.kappa), rgas = T(S.gas_r);
   const T two3 = T(2.0 / 3.0);
   T* visp = reinterpret_cast<T*>(S.vis);
-  for (int idx = threadIdx.x; idx < kSenTX * kSenTY; idx += blockDim.x) {
-    const int ty = idx / kSenTX, tx = idx % kSenTX;
-    const int gj = y0 + ty, gi = x0 + tx;
+  for (int a = ty; a < kSenTY; a += nty) {
+    const int gj = y0 + a, gi = x0 + tx;
     if (gj >= ny || gi >= nx) continue;
-    const int c = (ty + HW) * SX + tx + HW;
+    const int c = (a + HW) * SX + tx + HW;
     auto ddx = [&](const T* f, int o) { return (f[o + 1] - f[o - 1]) / tdx; };
     auto ddy = [&](const T* f, int o) { return (f[o + SX] - f[o - SX]) / tdy; };
     auto temp = [&](int o) { return P[o] / (RHO[o] * rgas); };
@@ -242,17 +277,23 @@ __host__ __device__ inline int pad_index(int i) {
   return sizeof(T) == 4 ? i + (i >> 5) : i + (i >> 4);
 }
 
+// Shared memory of one sweep CTA holding R lines of n nodes:
+//   FQ [R][8][LS]  flux F_c (c < 4) and enforced state Q_c (c >= 4) of every
+//                  node plus a 5-node halo on each side (LS = n + 10)
+//   RB [R][4][LQ]  face differences raw_i, solved in place into d_i (padded
+//                  index so that the chunked solve reads without bank conflicts)
+//   MK [R][n + 2]  sensor mask of nodes -1 .. n
 template <typename T>
 struct SweepLayout {
   int n, LS, LQ, R;
   __host__ __device__ SweepLayout(int n_, int R_) : n(n_), R(R_) {
     LS = n + 2 * kHalo;
-    const int lp = pad_index<T>(n - 1) + 1;
-    LQ = (LS > lp ? LS : lp);
+    LS = (LS + 1) & ~1;
+    LQ = pad_index<T>(n - 1) + 1;
     LQ = (LQ + 3) & ~3;
   }
   __host__ __device__ size_t bytes() const {
-    size_t b = (size_t)R * (4 * LQ + 2 * LS) * sizeof(T);
+    size_t b = (size_t)R * (8 * LS + 4 * LQ) * sizeof(T);
     b += (size_t)R * (n + 2);
     return (b + 15) & ~(size_t)15;
   }
@@ -270,34 +311,23 @@ __device__ __forceinline__ int fused_terms(const SolveDev& S) {
 constexpr double kB1C1 = 1.0 / 20.0 + (-1.0 / 480.0);
 constexpr double kA1B1C1 = 25.0 / 32.0 + 1.0 / 20.0 + (-1.0 / 480.0);
 
-// Physical flux component c at staged node s (x: AXIS 0, y: AXIS 1).
-template <typename T, int AXIS>
-__device__ __forceinline__ T line_flux(int c, const T* qs, int LQ, const T* un, const T* pp, int s) {
-  const T u = un[s];
-  if (c == 0) return qs[(1 + AXIS) * LQ + s];
-  if (c == 3) return (qs[3 * LQ + s] + pp[s]) * u;
-  const T f = qs[c * LQ + s] * u;
-  return (c == 1 + AXIS) ? f + pp[s] : f;
+// 6-point compact interface flux C_{i+1/2} (OOP/spatial_operator.py:179-189).
+template <typename T>
+__device__ __forceinline__ T compact_face(const T* F, int s) {
+  return T(-1.0 / 480.0) * (F[s + 3] + F[s - 2]) + T(kB1C1) * (F[s + 2] + F[s - 1]) +
+         T(kA1B1C1) * (F[s + 1] + F[s]);
 }
 
-template <typename T, int AXIS>
-__device__ __forceinline__ T compact_face(int c, const T* qs, int LQ, const T* un, const T* pp,
-                                          int s) {
-  auto F = [&](int k) { return line_flux<T, AXIS>(c, qs, LQ, un, pp, s + k); };
-  return T(-1.0 / 480.0) * (F(3) + F(-2)) + T(kB1C1) * (F(2) + F(-1)) + T(kA1B1C1) * (F(1) + F(0));
-}
-
-template <typename T, int AXIS>
-__device__ __forceinline__ T weno_face(int c, const T* qs, int LQ, const T* un, const T* pp, int s,
-                                       T alpha) {
+// WENO7 flux W_{i+1/2} of the Lax-Friedrichs split f+- = (F +- alpha Q) / 2
+// (OOP/spatial_operator.py:192-211).
+template <typename T>
+__device__ __forceinline__ T weno_face(const T* F, const T* Q, int s, T alpha) {
   T fp[8], fm[8];
 #pragma unroll
   for (int k = 0; k < 8; ++k) {
-    const int sk = s - 3 + k;
-    const T F = line_flux<T, AXIS>(c, qs, LQ, un, pp, sk);
-    const T Q = qs[c * LQ + sk];
-    fp[k] = T(0.5) * (F + alpha * Q);
-    fm[k] = T(0.5) * (F - alpha * Q);
+    const T f = F[s - 3 + k], aq = alpha * Q[s - 3 + k];
+    fp[k] = T(0.5) * (f + aq);
+    fm[k] = T(0.5) * (f - aq);
   }
   return weno7(fp[0], fp[1], fp[2], fp[3], fp[4], fp[5], fp[6]) +
          weno7(fm[7], fm[6], fm[5], fm[4], fm[3], fm[2], fm[1]);
@@ -406,7 +436,8 @@ __device__ __forceinline__ void line_solve(T* line, int n, int per) {
       const T r0 = rfirst - pfirst, r1 = rlast - plast;
       const T den = T(1) - e * e;
       const T ca = (r0 - e * r1) / den, cb = (r1 - e * r0) / den;
-      if (len > 0) {
+      // the homogeneous terms are below roundoff beyond ~80 nodes from an end
+      if (len > 0 && (start < 96 || start + len > n - 96)) {
         T pa = T(pow(double(kRhoSolve), double(start)));
         T pb = T(pow(double(kRhoSolve), double(n - start - len)));
         T pbk[MCH];
@@ -435,8 +466,9 @@ __device__ __forceinline__ void line_solve(T* line, int n, int per) {
 //   stage 0: q1 = clean(q + dt L)
 //   stage 1: q2 = clean(3/4 q + 1/4 (q1 + dt L))
 //   stage 2:      clean(1/3 q + 2/3 (q2 + dt L))     (OOP/time_operator.py:21-26)
+// R (lines per CTA) is a power of two.
 template <typename T, int AXIS, int MCH>
-__global__ void __launch_bounds__(kStencilThreads)
+__global__ void __launch_bounds__(kStencilThreads, 2)
     sweep_kernel(const SolveDev* __restrict__ solves, const Work* __restrict__ work, int stage,
                  int mode, Bind bind) {
   extern __shared__ __align__(16) unsigned char smem[];
@@ -448,142 +480,156 @@ __global__ void __launch_bounds__(kStencilThreads)
   const int n = AXIS == 0 ? nx : ny;
   const size_t plane = (size_t)nx * ny;
   const int line0 = wk.a, R = wk.b;
-  const SweepLayout<T> L(n, R);
+  const int rsh = R > 4 ? 3 : (R > 2 ? 2 : (R > 1 ? 1 : 0));  // ceil(log2 R)
+  const SweepLayout<T> L(n, 1 << rsh);
   const int LS = L.LS, LQ = L.LQ;
   const T g = T(S.gamma);
   const double h = AXIS == 0 ? S.dx : S.dy;
   const double* qin = bind.use ? bind.qin : stage_in(S, stage);
   const uint8_t* mask = bind.use ? bind.mask : S.mask;
   const T alpha = T(AXIS == 0 ? sc[S_ALPHA_X] : sc[S_ALPHA_Y]);
-  T* QS = reinterpret_cast<T*>(smem);
-  T* UN = QS + (size_t)R * 4 * LQ;
-  T* PP = UN + (size_t)R * LS;
-  uint8_t* MK = reinterpret_cast<uint8_t*>(PP + (size_t)R * LS);
+  const int RL = 1 << rsh;  // layout lines (>= R: the last CTA may hold fewer)
+  T* FQ = reinterpret_cast<T*>(smem);
+  T* RB = FQ + (size_t)RL * 8 * LS;
+  uint8_t* MK = reinterpret_cast<uint8_t*>(RB + (size_t)RL * 4 * LQ);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
 
-  // ---- L: stage the lines ----------------------------------------------------
-  for (int idx = threadIdx.x; idx < R * LS; idx += blockDim.x) {
+  // ---- L: stage flux and enforced state of the lines ---------------------------
+  // x lines: consecutive threads take consecutive nodes of a row; y lines:
+  // consecutive threads take the R columns of a row, then the next row.
+  const int nl = AXIS == 0 ? R * LS : (LS << rsh);
+  for (int idx = threadIdx.x; idx < nl; idx += blockDim.x) {
     int r, p;
     if (AXIS == 0) {
-      r = idx / LS;
-      p = idx - r * LS;
+      r = 0;
+      p = idx;
+      while (p >= LS) {
+        p -= LS;
+        ++r;
+      }
     } else {
-      r = idx % R;
-      p = idx / R;
+      r = idx & (RL - 1);
+      p = idx >> rsh;
+      if (r >= R) continue;
     }
-    const int gp = wrap_or_clamp(p - kHalo, n, per);
+    const int gp = fold_node(p - kHalo, n, per);
     const size_t o = AXIS == 0 ? (size_t)(line0 + r) * nx + gp : (size_t)gp * nx + line0 + r;
     T a0 = T(qin[o]), a1 = T(qin[o + plane]), a2 = T(qin[o + 2 * plane]), a3 = T(qin[o + 3 * plane]);
-    enforce_node(a0, a1, a2, a3, g);
-    const Prim<T> pr = primitives(a0, a1, a2, a3, g);
-    T* qs = QS + (size_t)r * 4 * LQ + p;
-    qs[0] = a0;
-    qs[LQ] = a1;
-    qs[2 * LQ] = a2;
-    qs[3 * LQ] = a3;
-    UN[r * LS + p] = AXIS == 0 ? pr.u : pr.v;
-    PP[r * LS + p] = pr.p;
+    // enforce_physical_state, then primitive_from_conservative of the result
+    const T rho = a0 > T(kRhoFloor) ? a0 : T(kRhoFloor);
+    const T rinv = T(1) / rho;
+    T u = a1 * rinv, v = a2 * rinv;
+    const T kin = T(0.5) * rho * (u * u + v * v);
+    T pr = (g - T(1)) * (a3 - kin);
+    a1 = rho * u;
+    a2 = rho * v;
+    a3 = pr > T(kPFloor) ? a3 : T(kPFloor) / (g - T(1)) + kin;
+    u = a1 * rinv;
+    v = a2 * rinv;
+    pr = (g - T(1)) * (a3 - T(0.5) * rho * (u * u + v * v));
+    pr = pr > T(kPFloor) ? pr : T(kPFloor);
+    const T un = AXIS == 0 ? u : v;
+    T* f = FQ + (size_t)r * 8 * LS + p;
+    f[0 * LS] = AXIS == 0 ? a1 : a2;
+    f[1 * LS] = a1 * un + (AXIS == 0 ? pr : T(0));
+    f[2 * LS] = a2 * un + (AXIS == 0 ? T(0) : pr);
+    f[3 * LS] = (a3 + pr) * un;
+    f[4 * LS] = rho;
+    f[5 * LS] = a1;
+    f[6 * LS] = a2;
+    f[7 * LS] = a3;
   }
   const int weno_all = S.scheme == 1;
-  for (int idx = threadIdx.x; idx < R * (n + 2); idx += blockDim.x) {
+  const int nm = AXIS == 0 ? R * (n + 2) : ((n + 2) << rsh);
+  for (int idx = threadIdx.x; idx < nm; idx += blockDim.x) {
     int r, p;
     if (AXIS == 0) {
-      r = idx / (n + 2);
-      p = idx - r * (n + 2);
+      r = 0;
+      p = idx;
+      while (p >= n + 2) {
+        p -= n + 2;
+        ++r;
+      }
     } else {
-      r = idx % R;
-      p = idx / R;
+      r = idx & (RL - 1);
+      p = idx >> rsh;
+      if (r >= R) continue;
     }
-    const int gp = wrap_or_clamp(p - 1, n, per);
+    const int gp = fold_node(p - 1, n, per);
     const size_t o = AXIS == 0 ? (size_t)(line0 + r) * nx + gp : (size_t)gp * nx + line0 + r;
     MK[r * (n + 2) + p] = weno_all ? 1 : mask[o];
   }
   __syncthreads();
 
-  // ---- H: face fluxes and their differences, one component at a time ----------
+  // ---- H: face fluxes and their differences --------------------------------------
+  // Warp task = (line, component, 29 consecutive nodes): lanes hold faces
+  // base-2 .. base+29, exchange neighbour faces by shuffles and write
+  // raw_i = (H_{i+1/2} - H_{i-1/2}) / h of nodes base .. base+28.
   const int tpl = (n + kNodesPerTask - 1) / kNodesPerTask;
-  const int ntask = R * tpl;
+  const int ntask = R * 4 * tpl;
   const T inv_h = T(1.0 / h);
-  for (int c = 0; c < 4; ++c) {
-    T rv[kMaxTasks];
-    int ri[kMaxTasks];
-#pragma unroll
-    for (int t = 0; t < kMaxTasks; ++t) {
-      ri[t] = -1;
-      rv[t] = T(0);
-      const int task = warp + t * nwarp;
-      if (task < ntask) {
-        const int r = task / tpl, base = (task - r * tpl) * kNodesPerTask;
-        const int il = base - 2 + lane;  // this lane's face il + 1/2
-        const T* qs = QS + (size_t)r * 4 * LQ;
-        const T* un = UN + r * LS;
-        const T* pp = PP + r * LS;
-        const uint8_t* mk = MK + r * (n + 2);
-        auto flg = [&](int f) -> bool { return f >= -1 && f <= n - 1 && (mk[f + 1] | mk[f + 2]); };
-        const bool f0 = flg(il);
-        const bool need = flg(il - 1) || f0 || flg(il + 1);
-        T wv = T(0);
-        if (need) {
-          const int ie = per ? il : min(max(il, -1), n - 1);
-          wv = weno_face<T, AXIS>(c, qs, LQ, un, pp, ie + kHalo, alpha);
-        }
-        const T wp = __shfl_down_sync(kFull, wv, 1), wm = __shfl_up_sync(kFull, wv, 1);
-        T hf = T(0);
-        if (il >= -1 && il <= n - 1) {
-          if (f0) {
-            hf = T(kCompactA) * wp + wv;
-            hf = hf + T(kCompactA) * wm;
-          } else {
-            hf = compact_face<T, AXIS>(c, qs, LQ, un, pp, il + kHalo);
-          }
-        }
-        const T hm = __shfl_up_sync(kFull, hf, 1);
-        if (lane >= 2 && lane <= 30 && il >= 0 && il < n) {
-          rv[t] = (hf - hm) * inv_h;
-          ri[t] = r * 4 * LQ + c * LQ + pad_index<T>(il);
-        }
+#pragma unroll 1
+  for (int task = warp; task < ntask; task += nwarp) {
+    const int rc = task / tpl, seg = task - rc * tpl;
+    const int r = rc >> 2, c = rc & 3;
+    const int il = seg * kNodesPerTask - 2 + lane;  // this lane's face il + 1/2
+    const T* F = FQ + (size_t)(r * 8 + c) * LS + kHalo;
+    const T* Q = FQ + (size_t)(r * 8 + 4 + c) * LS + kHalo;
+    const uint8_t* mk = MK + r * (n + 2) + 1;  // mk[i] = node i, i in [-1, n]
+    auto flg = [&](int f) -> bool { return f >= -1 && f <= n - 1 && (mk[f] | mk[f + 1]); };
+    const bool f0 = flg(il);
+    const bool need = flg(il - 1) || f0 || flg(il + 1);
+    T wv = T(0);
+    if (need) wv = weno_face<T>(F, Q, per ? il : min(max(il, -1), n - 1), alpha);
+    const T wp = __shfl_down_sync(kFull, wv, 1), wm = __shfl_up_sync(kFull, wv, 1);
+    T hf = T(0);
+    if (il >= -1 && il <= n - 1) {
+      if (f0) {
+        hf = T(kCompactA) * wp + wv;
+        hf = hf + T(kCompactA) * wm;
+      } else {
+        hf = compact_face<T>(F, il);
       }
     }
-    __syncthreads();  // every read of this component's staged values is done
-#pragma unroll
-    for (int t = 0; t < kMaxTasks; ++t)
-      if (ri[t] >= 0) QS[ri[t]] = rv[t];
+    const T hm = __shfl_up_sync(kFull, hf, 1);
+    if (lane >= 2 && lane <= 30 && il >= 0 && il < n)
+      RB[(size_t)(r * 4 + c) * LQ + pad_index<T>(il)] = (hf - hm) * inv_h;
   }
   __syncthreads();
 
-  // ---- S: compact solves ---------------------------------------------------------
-  for (int item = warp; item < 4 * R; item += nwarp) {
-    const int r = item >> 2, c = item & 3;
-    line_solve<T, MCH>(QS + (size_t)r * 4 * LQ + c * LQ, n, per);
-  }
+  // ---- S: compact solves -------------------------------------------------------------
+  for (int item = warp; item < 4 * R; item += nwarp)
+    line_solve<T, MCH>(RB + (size_t)item * LQ, n, per);
   __syncthreads();
 
-  // ---- E: epilogue ------------------------------------------------------------------
+  // ---- E: epilogue ----------------------------------------------------------------------
   const double fs = sc[S_F_SCALE];
   const int terms = bind.use ? bind.terms : fused_terms(S);
-  for (int idx = threadIdx.x; idx < R * n; idx += blockDim.x) {
+  const int ne = AXIS == 0 ? R * n : (n << rsh);
+  for (int idx = threadIdx.x; idx < ne; idx += blockDim.x) {
     int r, p;
     if (AXIS == 0) {
-      r = idx / n;
-      p = idx - r * n;
+      r = 0;
+      p = idx;
+      while (p >= n) {
+        p -= n;
+        ++r;
+      }
     } else {
-      r = idx % R;
-      p = idx / R;
+      r = idx & (RL - 1);
+      p = idx >> rsh;
+      if (r >= R) continue;
     }
     const int row = AXIS == 0 ? line0 + r : p, col = AXIS == 0 ? p : line0 + r;
     const size_t o = (size_t)row * nx + col;
-    const T* dl = QS + (size_t)r * 4 * LQ + pad_index<T>(p);
+    const T* dl = RB + (size_t)r * 4 * LQ + pad_index<T>(p);
     T d[4];
 #pragma unroll
-    for (int c = 0; c < 4; ++c) d[c] = dl[c * LQ];
+    for (int c = 0; c < 4; ++c) d[c] = (terms & 1) ? dl[c * LQ] : T(0);
     if (mode == SW_DERIV) {
 #pragma unroll
-      for (int c = 0; c < 4; ++c) bind.out[c * plane + o] = double(d[c]);
+      for (int c = 0; c < 4; ++c) bind.out[c * plane + o] = double(dl[c * LQ]);
       continue;
-    }
-    if (!(terms & 1)) {
-#pragma unroll
-      for (int c = 0; c < 4; ++c) d[c] = T(0);
     }
     if (AXIS == 0) {
       T v[4] = {-d[0], -d[1], -d[2], -d[3]};
@@ -607,11 +653,7 @@ __global__ void __launch_bounds__(kStencilThreads)
           T lx = T(0), ly = T(0);
           for (int md = 0; md < S.n_drag; ++md) {
             const int2 k = S.modes[md];
-            int ix = (int)(((long long)k.x * col) % nx);
-            if (ix < 0) ix += nx;
-            int iy = (int)(((long long)k.y * row) % ny);
-            if (iy < 0) iy += ny;
-            const double2 ex = S.twx[ix], ey = S.twy[iy];
+            const double2 ex = S.twx[mode_index(k.x, col, nx)], ey = S.twy[mode_index(k.y, row, ny)];
             const T er = T(cmul_re(ex, ey)), ei = T(-cmul_im(ex, ey));
             const double* cf = sc + S_DRAG + 4 * md;
             lx += T(cf[0]) * er - T(cf[1]) * ei;
@@ -639,17 +681,17 @@ __global__ void __launch_bounds__(kStencilThreads)
       const double dt = sc[S_DT];
       const double* q0 = bind.use ? bind.q0 : S.q;
       double* qo = bind.use ? bind.qout : stage_out(S, stage);
-      double s[4];
+      double sv[4];
 #pragma unroll
       for (int c = 0; c < 4; ++c) {
         const double t = qin[c * plane + o] + dt * rhs[c];
-        if (stage == 0) s[c] = t;
-        else if (stage == 1) s[c] = 0.75 * q0[c * plane + o] + 0.25 * t;
-        else s[c] = (1.0 / 3.0) * q0[c * plane + o] + (2.0 / 3.0) * t;
+        if (stage == 0) sv[c] = t;
+        else if (stage == 1) sv[c] = 0.75 * q0[c * plane + o] + 0.25 * t;
+        else sv[c] = (1.0 / 3.0) * q0[c * plane + o] + (2.0 / 3.0) * t;
       }
-      enforce_node(s[0], s[1], s[2], s[3], S.gamma);
+      enforce_node(sv[0], sv[1], sv[2], sv[3], S.gamma);
 #pragma unroll
-      for (int c = 0; c < 4; ++c) qo[c * plane + o] = s[c];
+      for (int c = 0; c < 4; ++c) qo[c * plane + o] = sv[c];
     }
   }
 }
@@ -662,7 +704,7 @@ __global__ void __launch_bounds__(kStencilThreads)
 template <typename T>
 __global__ void __launch_bounds__(kStencilThreads)
     hv_kernel(const SolveDev* __restrict__ solves, const Work* __restrict__ work, Bind bind) {
-  constexpr int QX = kSenTX + 4, QY = kSenTY + 4, LX = kSenTX + 2, LY = kSenTY + 2;
+  constexpr int QX = kHvTX + 4, QY = kHvTY + 4, LX = kHvTX + 2, LY = kHvTY + 2;
   __shared__ T Qs[4][QY][QX];
   __shared__ T Ls[4][LY][LX];
   const Work wk = work[blockIdx.x];
@@ -677,7 +719,7 @@ __global__ void __launch_bounds__(kStencilThreads)
   const int x0 = wk.a, y0 = wk.b;
   for (int idx = threadIdx.x; idx < QX * QY; idx += blockDim.x) {
     const int a = idx / QX, b = idx % QX;
-    const int gj = wrap_or_clamp(y0 - 2 + a, ny, per), gi = wrap_or_clamp(x0 - 2 + b, nx, per);
+    const int gj = fold_node(y0 - 2 + a, ny, per), gi = fold_node(x0 - 2 + b, nx, per);
     const size_t o = (size_t)gj * nx + gi;
 #pragma unroll
     for (int c = 0; c < 4; ++c) Qs[c][a][b] = T(q[c * plane + o]);
@@ -703,8 +745,8 @@ __global__ void __launch_bounds__(kStencilThreads)
     }
   }
   __syncthreads();
-  for (int idx = threadIdx.x; idx < kSenTX * kSenTY; idx += blockDim.x) {
-    const int ty = idx / kSenTX, tx = idx % kSenTX;
+  for (int idx = threadIdx.x; idx < kHvTX * kHvTY; idx += blockDim.x) {
+    const int ty = idx / kHvTX, tx = idx % kHvTX;
     const int gj = y0 + ty, gi = x0 + tx;
     if (gj >= ny || gi >= nx) continue;
     const size_t o = (size_t)gj * nx + gi;
@@ -728,7 +770,7 @@ __global__ void __launch_bounds__(kStencilThreads)
 // cell column/row g or n-g-1 (x first, then y: the corner takes (g, g)).
 // sel: 0 q, 1 q1, 2 q2, 3 stage-3 output; one CTA per solve.
 __global__ void guard_kernel(const SolveDev* __restrict__ solves, int nsolves, int sel, Bind bind) {
-  const int s = blockIdx.x;
+  const int s = blockIdx.y;
   if (s >= nsolves) return;
   const SolveDev& S = solves[s];
   if (S.periodic || S.guard <= 0) return;
@@ -738,7 +780,7 @@ __global__ void guard_kernel(const SolveDev* __restrict__ solves, int nsolves, i
   const size_t plane = (size_t)nx * ny;
   const int top = 2 * gc * nx;                 // full rows
   const int side = 2 * gc * (ny - 2 * gc);     // side columns of interior rows
-  for (int t = threadIdx.x; t < top + side; t += blockDim.x) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < top + side; t += gridDim.x * blockDim.x) {
     int j, i;
     if (t < top) {
       const int rr = t / nx;

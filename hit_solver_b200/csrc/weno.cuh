@@ -36,23 +36,35 @@ HITB200_WENO_IS(weno_is3, 2107.0, 1083920.0 / 2107.0, 203060.0 / 13549.0, -2594.
 #undef HITB200_WENO_IS
 
 // Value at the right face of v3 from v0..v6 (the reference's v1..v7).
+// Nonlinear weights alpha_k = d_k / (eps + IS_k)^2 normalised by their sum.
+// FP64: all four weights are scaled by prod_k (eps + IS_k)^2 so that the face
+// value needs one division (the scaled weights stay within 1e-60 .. 1e40).
+// FP32: that product would underflow, so each weight uses a fast reciprocal
+// (2 ulp), which perturbs the convex combination far below FP32 flux error.
 template <typename T>
 __device__ __forceinline__ T weno7(T v0, T v1, T v2, T v3, T v4, T v5, T v6) {
   const T eps = T(1e-10);
-  T q0 = T(-1.0 / 4.0) * v0 + T(13.0 / 12.0) * v1 - T(23.0 / 12.0) * v2 + T(25.0 / 12.0) * v3;
-  T q1 = T(1.0 / 12.0) * v1 - T(5.0 / 12.0) * v2 + T(13.0 / 12.0) * v3 + T(1.0 / 4.0) * v4;
-  T q2 = T(-1.0 / 12.0) * v2 + T(7.0 / 12.0) * v3 + T(7.0 / 12.0) * v4 - T(1.0 / 12.0) * v5;
-  T q3 = T(1.0 / 4.0) * v3 + T(13.0 / 12.0) * v4 - T(5.0 / 12.0) * v5 + T(1.0 / 12.0) * v6;
-  T is0 = weno_is0<T>(v0, v1, v2, v3) - T(3) * v0 * v0;
-  T is1 = weno_is1<T>(v1, v2, v3, v4);
-  T is2 = weno_is2<T>(v2, v3, v4, v5);
-  T is3 = weno_is3<T>(v3, v4, v5, v6);
-  T e0 = eps + is0, e1 = eps + is1, e2 = eps + is2, e3 = eps + is3;
-  T a0 = T(1.0 / 35.0) / (e0 * e0);
-  T a1 = T(12.0 / 35.0) / (e1 * e1);
-  T a2 = T(18.0 / 35.0) / (e2 * e2);
-  T a3 = T(4.0 / 35.0) / (e3 * e3);
-  return (a0 * q0 + a1 * q1 + a2 * q2 + a3 * q3) / (a0 + a1 + a2 + a3);
+  const T q0 = T(-1.0 / 4.0) * v0 + T(13.0 / 12.0) * v1 - T(23.0 / 12.0) * v2 + T(25.0 / 12.0) * v3;
+  const T q1 = T(1.0 / 12.0) * v1 - T(5.0 / 12.0) * v2 + T(13.0 / 12.0) * v3 + T(1.0 / 4.0) * v4;
+  const T q2 = T(-1.0 / 12.0) * v2 + T(7.0 / 12.0) * v3 + T(7.0 / 12.0) * v4 - T(1.0 / 12.0) * v5;
+  const T q3 = T(1.0 / 4.0) * v3 + T(13.0 / 12.0) * v4 - T(5.0 / 12.0) * v5 + T(1.0 / 12.0) * v6;
+  const T e0 = eps + (weno_is0<T>(v0, v1, v2, v3) - T(3) * v0 * v0);
+  const T e1 = eps + weno_is1<T>(v1, v2, v3, v4);
+  const T e2 = eps + weno_is2<T>(v2, v3, v4, v5);
+  const T e3 = eps + weno_is3<T>(v3, v4, v5, v6);
+  const T s0 = e0 * e0, s1 = e1 * e1, s2 = e2 * e2, s3 = e3 * e3;
+  if constexpr (sizeof(T) == 8) {
+    const T p01 = s0 * s1, p23 = s2 * s3;
+    const T w0 = T(1.0 / 35.0) * s1 * p23;
+    const T w1 = T(12.0 / 35.0) * s0 * p23;
+    const T w2 = T(18.0 / 35.0) * s3 * p01;
+    const T w3 = T(4.0 / 35.0) * s2 * p01;
+    return (w0 * q0 + w1 * q1 + w2 * q2 + w3 * q3) / (w0 + w1 + w2 + w3);
+  } else {
+    const float a0 = __fdividef(1.0f / 35.0f, s0), a1 = __fdividef(12.0f / 35.0f, s1);
+    const float a2 = __fdividef(18.0f / 35.0f, s2), a3 = __fdividef(4.0f / 35.0f, s3);
+    return __fdividef(a0 * q0 + a1 * q1 + a2 * q2 + a3 * q3, a0 + a1 + a2 + a3);
+  }
 }
 
 }  // namespace hitb200
