@@ -217,7 +217,8 @@ template <typename T>
 void set_sensor_attr(size_t bytes) {
   static size_t done = 0;
   if (bytes > done) {
-    cudaFuncSetAttribute(sensor_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    cudaFuncSetAttribute(sensor_kernel<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    cudaFuncSetAttribute(sensor_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
     done = bytes;
   }
 }
@@ -251,8 +252,12 @@ void launch_sweep(const LaunchSet& L, int axis, int stage, int mode, const Bind&
 
 template <typename T>
 void launch_sensor_t(const LaunchSet& L, int sel, int enf, int visc, const Bind& b, uint8_t* mo) {
-  sensor_kernel<T><<<L.n_tiles32, kStencilThreads, L.smem_sensor, L.st>>>(L.solves, L.tiles32, sel, enf,
-                                                                          visc, b, mo);
+  if (b.use)
+    sensor_kernel<T, true><<<L.n_tiles32, kSensorThreads, L.smem_sensor, L.st>>>(
+        L.solves, L.tiles32, sel, enf, visc, b, mo);
+  else
+    sensor_kernel<T, false><<<L.n_tiles32, kSensorThreads, L.smem_sensor, L.st>>>(
+        L.solves, L.tiles32, sel, enf, visc, b, mo);
 }
 void launch_sensor(const LaunchSet& L, int sel, int enf, int visc, const Bind& b, uint8_t* mo) {
   if (L.elem == 4) launch_sensor_t<float>(L, sel, enf, visc, b, mo);
@@ -263,7 +268,7 @@ void launch_hv(const LaunchSet& L, const Bind& b) {
   else hv_kernel<double><<<L.n_tiles, kStencilThreads, 0, L.st>>>(L.solves, L.tiles, b);
 }
 void launch_prepass(const LaunchSet& L, int buf, int mode, int enf, const Bind& b) {
-  prepass_kernel<<<L.n_tiles, kRedThreads, 0, L.st>>>(L.solves, L.tiles, buf, mode, enf, b);
+  prepass_kernel<<<L.n_tiles32, kRedThreads, 0, L.st>>>(L.solves, L.tiles32, buf, mode, enf, b);
 }
 
 // The reference's loop body (OOP/hit2d.py:828-879; riemann_config3.py:728-740).
@@ -276,13 +281,13 @@ int launch_step_sequence(const LaunchSet& L, int any_forcing, int noise_upload, 
   if (any_forcing) {
     if (noise_upload) {
       PMARK("noise_dft", 8 * L.cells_force);
-      noise_dft_kernel<<<L.n_tiles, kRedThreads, 0, L.st>>>(L.solves, L.tiles, nb);
+      noise_dft_kernel<<<L.n_tiles32, kRedThreads, 0, L.st>>>(L.solves, L.tiles32, nb);
     } else {
       PMARK("noise_rng", 0.0);
       noise_rng_kernel<<<L.nsolves, 128, 0, L.st>>>(L.solves, L.nsolves, L.partner);
     }
     PMARK("force_synth", 48 * L.cells_force);
-    force_synth_kernel<<<L.n_tiles, kRedThreads, 0, L.st>>>(L.solves, L.tiles, nb);
+    force_synth_kernel<<<L.n_tiles32, kRedThreads, 0, L.st>>>(L.solves, L.tiles32, nb);
   }
   for (int stage = 0; stage < 3; ++stage) {
     if (stage > 0) {
@@ -496,7 +501,7 @@ size_t hitb200_plan_device_bytes(const hitb200_desc* d) {
   if (validate_desc(d) != HITB200_OK) return 0;
   const size_t N = (size_t)d->nx * d->ny;
   const int elem = d->precision == 1 ? 4 : 8;
-  const int ntx = (d->nx + kTileX - 1) / kTileX, nty = (d->ny + kTileY - 1) / kTileY;
+  const int ntx = (d->nx + kHvTX - 1) / kHvTX, nty = (d->ny + kHvTY - 1) / kHvTY;
   const size_t ntile = (size_t)ntx * nty;
   ModeTables mt = build_modes(*d);
   Arena a;
@@ -540,7 +545,7 @@ int hitb200_plan_create(const hitb200_desc* d, hitb200_plan** out) {
   p->elem = d->precision == 1 ? 4 : 8;
   const int nx = d->nx, ny = d->ny;
   const size_t N = (size_t)nx * ny;
-  const int ntx = (nx + kTileX - 1) / kTileX, nty = (ny + kTileY - 1) / kTileY;
+  const int ntx = (nx + kHvTX - 1) / kHvTX, nty = (ny + kHvTY - 1) / kHvTY;
   p->n_tiles = ntx * nty;
   p->Rx = lines_per_cta(nx, ny, p->elem);
   p->Ry = lines_per_cta(ny, nx, p->elem);
@@ -640,7 +645,7 @@ int hitb200_plan_create(const hitb200_desc* d, hitb200_plan** out) {
   s.fixed_dt = d->fixed_dt;
   s.noise_mode = d->noise_mode;
   s.seed = d->seed;
-  s.nblk_pre = s.nblk_noise = s.nblk_synth = s.nblk_diag = p->n_tiles;
+  s.nblk_pre = s.nblk_noise = s.nblk_synth = s.nblk_diag = p->n_tiles32;
   s.nred = (int)nred;
   s.q = nullptr;
   s.q1 = reinterpret_cast<double*>(base + o_q1);
@@ -696,7 +701,7 @@ int hitb200_plan_create(const hitb200_desc* d, hitb200_plan** out) {
   scal[S_SHEAR_LIM] = INFINITY;
   std::vector<Work> tiles;
   for (int ty = 0; ty < nty; ++ty)
-    for (int tx = 0; tx < ntx; ++tx) tiles.push_back({0, tx * kTileX, ty * kTileY, (int)tiles.size()});
+    for (int tx = 0; tx < ntx; ++tx) tiles.push_back({0, tx * kHvTX, ty * kHvTY, (int)tiles.size()});
   std::vector<Work> tiles32;
   for (int ty = 0; ty < nty32; ++ty)
     for (int tx = 0; tx < ntx32; ++tx) tiles32.push_back({0, tx * kSenTX, ty * kSenTY, (int)tiles32.size()});
@@ -923,14 +928,14 @@ int hitb200_forcing_update(hitb200_plan* p, const double* q, const double* noise
   b.use = 1;
   if (noise) {
     b.qin = noise;
-    noise_dft_kernel<<<L.n_tiles, kRedThreads, 0, st>>>(L.solves, L.tiles, b);
+    noise_dft_kernel<<<L.n_tiles32, kRedThreads, 0, st>>>(L.solves, L.tiles32, b);
   } else {
     noise_rng_kernel<<<1, 128, 0, st>>>(L.solves, 1, L.partner);
   }
   Bind b2{};
   b2.use = 1;
   b2.qin = q;
-  force_synth_kernel<<<L.n_tiles, kRedThreads, 0, st>>>(L.solves, L.tiles, b2);
+  force_synth_kernel<<<L.n_tiles32, kRedThreads, 0, st>>>(L.solves, L.tiles32, b2);
   const size_t plane = (size_t)p->desc.nx * p->desc.ny;
   const int nb = (int)std::min<size_t>((plane + 255) / 256, 4096);
   scale_copy_kernel<<<nb, 256, 0, st>>>(p->hs.fx, fx, p->hs.scal, S_F_SCALE, plane);
@@ -1019,7 +1024,7 @@ int hitb200_diagnostics(hitb200_plan* p, const double* q, double* out, int32_t n
   Bind b{};
   b.use = 1;
   b.qin = q;
-  diag_kernel<<<L.n_tiles, kRedThreads, 0, 0>>>(L.solves, L.tiles, b);
+  diag_kernel<<<L.n_tiles32, kRedThreads, 0, 0>>>(L.solves, L.tiles32, b);
   HB_LAUNCHED("diag_kernel");
   double raw[NDIAG];
   HB_CUDA(cudaMemcpy(raw, p->hs.diag_out, sizeof(raw), cudaMemcpyDeviceToHost));
@@ -1072,10 +1077,10 @@ int hitb200_batch_create(const hitb200_desc* descs, int32_t n, hitb200_batch** o
     p->in_batch = true;
     b->plans.push_back(p);
     hs.push_back(p->hs);
-    const int ntx = (p->desc.nx + kTileX - 1) / kTileX, nty = (p->desc.ny + kTileY - 1) / kTileY;
+    const int ntx = (p->desc.nx + kHvTX - 1) / kHvTX, nty = (p->desc.ny + kHvTY - 1) / kHvTY;
     int k = 0;
     for (int ty = 0; ty < nty; ++ty)
-      for (int tx = 0; tx < ntx; ++tx) tiles.push_back({i, tx * kTileX, ty * kTileY, k++});
+      for (int tx = 0; tx < ntx; ++tx) tiles.push_back({i, tx * kHvTX, ty * kHvTY, k++});
     const int ntx32 = (p->desc.nx + kSenTX - 1) / kSenTX, nty32 = (p->desc.ny + kSenTY - 1) / kSenTY;
     int k32 = 0;
     for (int ty = 0; ty < nty32; ++ty)

@@ -9,6 +9,8 @@
 
 namespace hitb200 {
 
+constexpr unsigned kFullMask = 0xffffffffu;
+
 // Pointers a kernel works on when it is called as an operator on caller
 // arrays (use = 1) instead of on the solve's own stage buffers.
 struct Bind {
@@ -98,7 +100,7 @@ __device__ void step_control(const SolveDev& S, const double* red, double* sc) {
 // RHS needs before its flux pass.
 //   ENF = 1: sensor/LF quantities on enforce_physical_state(q), as
 //   PeriodicHybridEuler2DOperator.rhs does (OOP/spatial_operator.py:345-346).
-__global__ void __launch_bounds__(kRedThreads)
+__global__ void __launch_bounds__(kRedThreads, 2)
     prepass_kernel(const SolveDev* __restrict__ solves, const Work* __restrict__ work, int buf,
                    int mode, int enf, Bind bind) {
   const Work w = work[blockIdx.x];
@@ -110,6 +112,8 @@ __global__ void __launch_bounds__(kRedThreads)
   const int nx = S.nx, ny = S.ny, per = S.periodic;
   const size_t plane = (size_t)nx * ny;
   const double g = S.gamma;
+  const double igm1 = 1.0 / (g - 1.0), idx_ = 1.0 / S.dx, idy_ = 1.0 / S.dy;
+  const double ih2x = 1.0 / (2.0 * S.dx), ih2y = 1.0 / (2.0 * S.dy);
   const int x0 = w.a, y0 = w.b;
 
   __shared__ double su[kTileY + 2][kTileX + 2];
@@ -120,7 +124,8 @@ __global__ void __launch_bounds__(kRedThreads)
   const int tx = threadIdx.x & 31, ty0 = threadIdx.x >> 5;
 
   double ax = 0, ay = 0, div2 = 0, vort2 = 0, mr = 0, mp = 0, me = 0, ps = 0, sr = 0, vel2 = 0,
-         cs = 0, fnf = 0, fnr = 0, fnp = 0;
+         cs = 0;
+  int bad = 0;  // validation flags: 1 non-finite, 2 rho <= 0, 4 p <= 0
   // Every node of the tile and its one-node halo is loaded once; tile nodes
   // also feed the pointwise reductions here.
   for (int a = ty0; a < kTileY + 2; a += kRedWarps) {
@@ -133,48 +138,58 @@ __global__ void __launch_bounds__(kRedThreads)
       const int gi = fold_node(gx, nx, per);
       const size_t o = (size_t)gj * nx + gi;
       const double q0 = q[o], q1 = q[o + plane], q2 = q[o + 2 * plane], q3 = q[o + 3 * plane];
+      // One reciprocal and one square root per node serve the enforced state
+      // (sensor / Lax-Friedrichs quantities) and the raw state (time step,
+      // Mach, cooling); both share the floored density.
+      const double rho = q0 > kRhoFloor ? q0 : kRhoFloor;
+      const double rinv = 1.0 / rho;
+      const double ur = q1 * rinv, vr = q2 * rinv;
+      const double kin = 0.5 * rho * (ur * ur + vr * vr);
+      const double p_raw = (g - 1.0) * (q3 - kin);
+      double ue = ur, ve = vr, pe = p_raw;
+      if (need_grad && enf) {
+        const double e1 = rho * ur, e2 = rho * vr;
+        const double e3 = p_raw > kPFloor ? q3 : kPFloor / (g - 1.0) + kin;
+        ue = e1 * rinv;
+        ve = e2 * rinv;
+        pe = (g - 1.0) * (e3 - 0.5 * rho * (ue * ue + ve * ve));
+      }
+      pe = pe > kPFloor ? pe : kPFloor;
+      const double pr = p_raw > kPFloor ? p_raw : kPFloor;
+      const double cr = sqrt(g * pr * rinv);
       if (need_grad) {
-        double e0 = q0, e1 = q1, e2 = q2, e3 = q3;
-        if (enf) enforce_node(e0, e1, e2, e3, g);
-        const Prim<double> p = primitives(e0, e1, e2, e3, g);
-        su[a][b] = p.u;
-        sv[a][b] = p.v;
+        su[a][b] = ue;
+        sv[a][b] = ve;
         if (own) {
-          const double c = sqrt(g * p.p / p.rho);
-          ax = fmax(ax, fabs(p.u) + c);
-          ay = fmax(ay, fabs(p.v) + c);
-          mr = fmax(mr, fabs(p.rho));
-          mp = fmax(mp, fabs(p.p));
-          me = fmax(me, fabs(p.p / (p.rho * (g - 1.0))));
+          const double c = enf ? sqrt(g * pe * rinv) : cr;
+          ax = fmax(ax, fabs(ue) + c);
+          ay = fmax(ay, fabs(ve) + c);
+          mr = fmax(mr, rho);
+          mp = fmax(mp, pe);
+          me = fmax(me, pe * rinv * igm1);
         }
       }
       if (!own) continue;
       // raw state: time step, Mach, cooling, validation
-      const double rho = q0 > kRhoFloor ? q0 : kRhoFloor;
-      const double rinv = 1.0 / rho;
-      const double u = q1 * rinv, v = q2 * rinv;
-      double pr = (g - 1.0) * (q3 - 0.5 * rho * (u * u + v * v));
-      pr = pr > kPFloor ? pr : kPFloor;
-      const double cr = sqrt(g * pr * rinv);
       ps += pr;
-      sr = fmax(sr, (fabs(u) + cr) / S.dx + (fabs(v) + cr) / S.dy);
-      vel2 += u * u + v * v;
+      sr = fmax(sr, (fabs(ur) + cr) * idx_ + (fabs(vr) + cr) * idy_);
+      vel2 += ur * ur + vr * vr;
       cs += cr;
-      const double i0 = 1.0 / q0;
-      const double ur = q1 * i0, vr = q2 * i0;
-      const double praw = (g - 1.0) * (q3 - 0.5 * q0 * (ur * ur + vr * vr));
-      if (!(isfinite(q0) && isfinite(q1) && isfinite(q2) && isfinite(q3)) || !isfinite(praw))
-        fnf = 1.0;
-      if (q0 <= 0.0) fnr = 1.0;
-      if (praw <= 0.0) fnp = 1.0;
+      // validate_raw_physical_state: p = (g-1)(E - (m_x^2 + m_y^2) / (2 rho)) on
+      // the unfloored density; its sign is that of 2 rho E - |m|^2 when rho > 0
+      const bool fin = isfinite(q0) && isfinite(q1) && isfinite(q2) && isfinite(q3);
+      const double pp = 2.0 * q0 * q3 - (q1 * q1 + q2 * q2);
+      if (!fin || !isfinite(pp)) bad |= 1;
+      if (q0 <= 0.0) bad |= 2;
+      else if (pp <= 0.0) bad |= 4;
     }
   }
   if (need_grad) __syncthreads();
-  int cj[2], ci[2];
-  bool valid[2];
+  int cj[kCellsPerThread], ci[kCellsPerThread];
+  bool valid[kCellsPerThread];
 #pragma unroll
-  for (int k = 0; k < 2; ++k) {
-    const int ty = ty0 + 8 * k;
+  for (int k = 0; k < kCellsPerThread; ++k) {
+    const int ty = ty0 + kRedWarps * k;
     const int gj = y0 + ty, gi = x0 + tx;
     cj[k] = gj;
     ci[k] = gi;
@@ -184,28 +199,28 @@ __global__ void __launch_bounds__(kRedThreads)
     const int a = ty + 1, b = tx + 1;
     double dudx, dvdx, dudy, dvdy;
     if (per || (gi > 0 && gi < nx - 1)) {
-      dudx = (su[a][b + 1] - su[a][b - 1]) / (2.0 * S.dx);
-      dvdx = (sv[a][b + 1] - sv[a][b - 1]) / (2.0 * S.dx);
+      dudx = (su[a][b + 1] - su[a][b - 1]) * ih2x;
+      dvdx = (sv[a][b + 1] - sv[a][b - 1]) * ih2x;
     } else if (nx == 1) {
       dudx = dvdx = 0.0;
     } else if (gi == 0) {
-      dudx = (su[a][b + 1] - su[a][b]) / S.dx;
-      dvdx = (sv[a][b + 1] - sv[a][b]) / S.dx;
+      dudx = (su[a][b + 1] - su[a][b]) * idx_;
+      dvdx = (sv[a][b + 1] - sv[a][b]) * idx_;
     } else {
-      dudx = (su[a][b] - su[a][b - 1]) / S.dx;
-      dvdx = (sv[a][b] - sv[a][b - 1]) / S.dx;
+      dudx = (su[a][b] - su[a][b - 1]) * idx_;
+      dvdx = (sv[a][b] - sv[a][b - 1]) * idx_;
     }
     if (per || (gj > 0 && gj < ny - 1)) {
-      dudy = (su[a + 1][b] - su[a - 1][b]) / (2.0 * S.dy);
-      dvdy = (sv[a + 1][b] - sv[a - 1][b]) / (2.0 * S.dy);
+      dudy = (su[a + 1][b] - su[a - 1][b]) * ih2y;
+      dvdy = (sv[a + 1][b] - sv[a - 1][b]) * ih2y;
     } else if (ny == 1) {
       dudy = dvdy = 0.0;
     } else if (gj == 0) {
-      dudy = (su[a + 1][b] - su[a][b]) / S.dy;
-      dvdy = (sv[a + 1][b] - sv[a][b]) / S.dy;
+      dudy = (su[a + 1][b] - su[a][b]) * idy_;
+      dvdy = (sv[a + 1][b] - sv[a][b]) * idy_;
     } else {
-      dudy = (su[a][b] - su[a - 1][b]) / S.dy;
-      dvdy = (sv[a][b] - sv[a - 1][b]) / S.dy;
+      dudy = (su[a][b] - su[a - 1][b]) * idy_;
+      dvdy = (sv[a][b] - sv[a - 1][b]) * idy_;
     }
     const double dv = dudx + dvdy, vo = dvdx - dudy;
     div2 += dv * dv;
@@ -223,16 +238,19 @@ __global__ void __launch_bounds__(kRedThreads)
   warp_to_smem<OP_MAX>(sr, sm, R_SR, nslots);
   warp_to_smem<OP_SUM>(vel2, sm, R_VEL2, nslots);
   warp_to_smem<OP_SUM>(cs, sm, R_CSUM, nslots);
-  warp_to_smem<OP_MAX>(fnf, sm, R_NONFINITE, nslots);
-  warp_to_smem<OP_MAX>(fnr, sm, R_NONPOS_RHO, nslots);
-  warp_to_smem<OP_MAX>(fnp, sm, R_NONPOS_P, nslots);
+  bad = __reduce_or_sync(kFullMask, bad);
+  if ((threadIdx.x & 31) == 0) {
+    sm[(threadIdx.x >> 5) * nslots + R_NONFINITE] = (bad & 1) ? 1.0 : 0.0;
+    sm[(threadIdx.x >> 5) * nslots + R_NONPOS_RHO] = (bad & 2) ? 1.0 : 0.0;
+    sm[(threadIdx.x >> 5) * nslots + R_NONPOS_P] = (bad & 4) ? 1.0 : 0.0;
+  }
   if (nslots > R_FIXED) {
     // low-k momentum transform of the drag band filter (OOP/hit2d.py:352-399)
     for (int m = 0; m < S.n_drag; ++m) {
       const int2 md = S.modes[m];
       double v[4] = {0, 0, 0, 0};
 #pragma unroll
-      for (int k = 0; k < 2; ++k) {
+      for (int k = 0; k < kCellsPerThread; ++k) {
         if (!valid[k]) continue;
         const size_t o = (size_t)cj[k] * nx + ci[k];
         const double m0 = q[o + plane], m1 = q[o + 2 * plane];
@@ -265,6 +283,7 @@ __global__ void __launch_bounds__(kRedThreads)
     for (int t = warp; t < nslots; t += kRedWarps) {
       const int op = pre_op(t);
       double acc = op == OP_SUM ? 0.0 : -INFINITY;
+#pragma unroll 8
       for (int b = lane; b < S.nblk_pre; b += 32) {
         const double x = __ldcg(S.part_pre + (size_t)b * nslots + t);
         acc = op == OP_SUM ? acc + x : fmax(acc, x);
@@ -327,12 +346,12 @@ __global__ void __launch_bounds__(kRedThreads)
   __shared__ double sm[kRedWarps * 2 * kMaxForce];
   __shared__ double red[2 * kMaxForce];
   const int tx = threadIdx.x & 31, ty0 = threadIdx.x >> 5;
-  double val[2];
-  int cj[2], ci[2];
-  bool valid[2];
+  double val[kCellsPerThread];
+  int cj[kCellsPerThread], ci[kCellsPerThread];
+  bool valid[kCellsPerThread];
 #pragma unroll
-  for (int k = 0; k < 2; ++k) {
-    cj[k] = w.b + ty0 + 8 * k;
+  for (int k = 0; k < kCellsPerThread; ++k) {
+    cj[k] = w.b + ty0 + kRedWarps * k;
     ci[k] = w.a + tx;
     valid[k] = cj[k] < ny && ci[k] < nx;
     val[k] = valid[k] ? xi[(size_t)cj[k] * nx + ci[k]] : 0.0;
@@ -342,7 +361,7 @@ __global__ void __launch_bounds__(kRedThreads)
     const int2 md = modes[m];
     double re = 0.0, im = 0.0;
 #pragma unroll
-    for (int k = 0; k < 2; ++k) {
+    for (int k = 0; k < kCellsPerThread; ++k) {
       if (!valid[k]) continue;
       const double2 ex = S.twx[mode_index(md.x, ci[k], nx)], ey = S.twy[mode_index(md.y, cj[k], ny)];
       re += val[k] * cmul_re(ex, ey);
@@ -362,6 +381,7 @@ __global__ void __launch_bounds__(kRedThreads)
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int t = warp; t < nslots; t += kRedWarps) {
       double acc = 0.0;
+#pragma unroll 8
       for (int b = lane; b < S.nblk_noise; b += 32)
         acc += __ldcg(S.part_noise + (size_t)b * nslots + t);
       acc = warp_sum(acc);
@@ -468,8 +488,8 @@ __global__ void __launch_bounds__(kRedThreads)
   const int tx = threadIdx.x & 31, ty0 = threadIdx.x >> 5;
   double sxx = 0, syy = 0, sxy = 0, spow = 0;
 #pragma unroll
-  for (int k = 0; k < 2; ++k) {
-    const int gj = w.b + ty0 + 8 * k, gi = w.a + tx;
+  for (int k = 0; k < kCellsPerThread; ++k) {
+    const int gj = w.b + ty0 + kRedWarps * k, gi = w.a + tx;
     if (gj >= ny || gi >= nx) continue;
     double fx = 0.0, fy = 0.0;
     for (int m = 0; m < nf; ++m) {
@@ -564,8 +584,8 @@ __global__ void __launch_bounds__(kRedThreads)
   acc[D_RHOMAX] = acc[D_PMAX] = -INFINITY;
   const int tx = threadIdx.x & 31, ty0 = threadIdx.x >> 5;
 #pragma unroll
-  for (int k = 0; k < 2; ++k) {
-    const int gj = w.b + ty0 + 8 * k, gi = w.a + tx;
+  for (int k = 0; k < kCellsPerThread; ++k) {
+    const int gj = w.b + ty0 + kRedWarps * k, gi = w.a + tx;
     if (gj >= ny || gi >= nx) continue;
     const size_t o = (size_t)gj * nx + gi;
     const double q0 = q[o], q1 = q[o + plane], q2 = q[o + 2 * plane], q3 = q[o + 3 * plane];

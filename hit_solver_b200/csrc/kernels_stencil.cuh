@@ -14,6 +14,7 @@ constexpr unsigned kFull = 0xffffffffu;
 
 constexpr int kStencilThreads = 256;
 constexpr int kSenTX = 32, kSenTY = 32;  // sensor tile
+constexpr int kSensorThreads = 512;
 constexpr int kHvTX = 32, kHvTY = 16;    // hyperviscosity tile
 
 // =============================================================================
@@ -28,16 +29,21 @@ __device__ __forceinline__ T type_eps() {
   return sizeof(T) == 4 ? T(FLT_EPSILON) : T(DBL_EPSILON);
 }
 
+// Exact quotient test, out of line: reached only within ~8 ulp of a threshold.
+template <typename T>
+__device__ __noinline__ bool quotient_gt(T num, T den, T thr) {
+  return num / den > thr;
+}
+
 // fl(num / den) > thr for den > 0, exactly as the reference's IEEE quotient
 // compares, but decided by a multiplication unless the quotient lies within
 // ~8 ulp of the threshold (then the quotient itself is formed).
 template <typename T>
 __device__ __forceinline__ bool ratio_gt(T num, T den, T thr) {
-  const T e = T(8) * type_eps<T>();
   const T t = thr * den;
-  if (num > t * (T(1) + e)) return true;
-  if (num < t * (T(1) - e)) return false;
-  return num / den > thr;
+  const T d = num - t;
+  if (fabs(d) > T(8) * type_eps<T>() * t) return d > T(0);
+  return quotient_gt(num, den, thr);
 }
 
 // |num / den - thr| within tol * thr (a node "within roundoff" of the threshold)
@@ -47,17 +53,22 @@ __device__ __forceinline__ bool ratio_near(T num, T den, T thr, T tol) {
   return fabs(num - t) <= tol * t;
 }
 
-// The reference's relative jump metric max(left, right, curvature) > thr
-// (OOP/spatial_operator.py:147-166), one axis, neighbours am / ap.
-template <typename T>
-__device__ __forceinline__ bool jump_gt(T am, T a, T ap, T eps, T thr, T tol, bool& near) {
-  const T aa = fabs(a), aap = fabs(ap), aam = fabs(am);
-  const T nr = fabs(ap - a), dr = aap + aa + eps;
-  const T nl = fabs(a - am), dl = aa + aam + eps;
-  const T nc = fabs(ap - T(2) * a + am), dc = aap + T(2) * aa + aam + eps;
-  near = near || ratio_near(nr, dr, thr, tol) || ratio_near(nl, dl, thr, tol) ||
-         ratio_near(nc, dc, thr, tol);
-  return ratio_gt(nr, dr, thr) || ratio_gt(nl, dl, thr) || ratio_gt(nc, dc, thr);
+// Two-point jump |b - a| / (|b| + |a| + eps) > thr of the pair (a, b): the
+// reference's right jump of a and left jump of b are the same expression
+// (OOP/spatial_operator.py:149-153), so it is evaluated once per edge.
+template <typename T, bool NEAR>
+__device__ __forceinline__ bool pair_gt(T a, T b, T eps, T thr, T tol, bool& near) {
+  const T num = fabs(b - a), den = fabs(b) + fabs(a) + eps;
+  if (NEAR) near = near || ratio_near(num, den, thr, tol);
+  return ratio_gt(num, den, thr);
+}
+
+// Curvature |ap - 2a + am| / (|ap| + 2|a| + |am| + eps) > thr (OOP/spatial_operator.py:155-165).
+template <typename T, bool NEAR>
+__device__ __forceinline__ bool curv_gt(T am, T a, T ap, T eps, T thr, T tol, bool& near) {
+  const T num = fabs(ap - T(2) * a + am), den = fabs(ap) + T(2) * fabs(a) + fabs(am) + eps;
+  if (NEAR) near = near || ratio_near(num, den, thr, tol);
+  return ratio_gt(num, den, thr);
 }
 
 __host__ __device__ inline int sensor_halo(int width) { return width + 1 > 2 ? width + 1 : 2; }
@@ -66,9 +77,11 @@ __host__ __device__ inline size_t sensor_smem_bytes(int width, int elem) {
   const int hw = sensor_halo(width);
   const size_t sx = kSenTX + 2 * hw, sy = kSenTY + 2 * hw;
   const size_t prim = 5 * sx * sy * (size_t)elem;
-  const size_t raw = (size_t)(kSenTY + 2 * width) * (kSenTX + 2 * width);
-  const size_t row = (size_t)(kSenTY + 2 * width) * kSenTX;
-  return prim + raw + row + 16;
+  const size_t rx = kSenTX + 2 * width, ry = kSenTY + 2 * width;
+  const size_t raw = ry * rx;
+  const size_t row = ry * kSenTX;
+  const size_t edges = ry * (rx + 1) + (ry + 1) * rx;
+  return prim + raw + row + edges + 32;
 }
 
 // Central difference quotient of the sensor.  FP64 divides by 2h exactly as
@@ -79,10 +92,21 @@ __device__ __forceinline__ T dq(T a, T b, T h2, T ih2) {
   else return (a - b) * ih2;
 }
 
+// Row / column of a flattened index in a table of row length `w`, with the
+// float reciprocal `iw` = 1 / w (exact for the index ranges used here).
+__device__ __forceinline__ int row_of(int idx, int w, float iw) {
+  int r = __float2int_rd(((float)idx + 0.5f) * iw);
+  if (r * w > idx) --r;
+  else if ((r + 1) * w <= idx) ++r;
+  return r;
+}
+
 // sel: 0 q, 1 q1, 2 q2, 3 hyperviscosity input (stage-3 output q1, runs only on
-// hyperviscosity steps).  want_visc: also write the viscous terms.
-template <typename T>
-__global__ void __launch_bounds__(kStencilThreads)
+// hyperviscosity steps).  want_visc: also write the viscous terms.  NEAR:
+// count nodes within roundoff of a threshold (sensor API; off in the fused
+// step).
+template <typename T, bool NEAR>
+__global__ void __launch_bounds__(kSensorThreads, 2)
     sensor_kernel(const SolveDev* __restrict__ solves, const Work* __restrict__ work, int sel,
                   int enf, int want_visc, Bind bind, uint8_t* __restrict__ mask_out) {
   extern __shared__ __align__(16) unsigned char smem[];
@@ -102,29 +126,54 @@ __global__ void __launch_bounds__(kStencilThreads)
   const int x0 = wk.a, y0 = wk.b;
   const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5, nty = blockDim.x >> 5;
   const T g = T(S.gamma);
+  const T igm1 = T(1.0 / (S.gamma - 1.0));
   T* RHO = reinterpret_cast<T*>(smem);
   T* U = RHO + SX * SY;
   T* V = U + SX * SY;
   T* P = V + SX * SY;
   T* E = P + SX * SY;
-  uint8_t* RAW = reinterpret_cast<uint8_t*>(E + SX * SY);
   const int RX = kSenTX + 2 * W, RY = kSenTY + 2 * W;
+  uint8_t* RAW = reinterpret_cast<uint8_t*>(E + SX * SY);
   uint8_t* ROW = RAW + RX * RY;
+  uint8_t* EXF = ROW + RY * kSenTX;       // [RY][RX + 1]: edge left of raw column br
+  uint8_t* EYF = EXF + RY * (RX + 1);     // [RY + 1][RX]: edge below raw row ar
+  const int off = HW - W;                 // smem offset of raw index 0
 
-  for (int a = ty; a < SY; a += nty) {
-    const int gj = fold_node(y0 - HW + a, ny, per);
-    for (int b = tx; b < SX; b += 32) {
-      const int gi = fold_node(x0 - HW + b, nx, per);
-      const size_t o = (size_t)gj * nx + gi;
-      T q0 = T(q[o]), q1 = T(q[o + plane]), q2 = T(q[o + 2 * plane]), q3 = T(q[o + 3 * plane]);
+  // ---- staged primitives of the tile and its (width + 1) halo ----
+  const float isx = 1.0f / (float)SX;
+  for (int idx = threadIdx.x; idx < SX * SY; idx += blockDim.x) {
+    const int a = row_of(idx, SX, isx), b = idx - a * SX;
+    const int gj = fold_node(y0 - HW + a, ny, per), gi = fold_node(x0 - HW + b, nx, per);
+    const size_t o = (size_t)gj * nx + gi;
+    T q0 = T(q[o]), q1 = T(q[o + plane]), q2 = T(q[o + 2 * plane]), q3 = T(q[o + 3 * plane]);
+    if constexpr (sizeof(T) == 8) {
       if (enf) enforce_node(q0, q1, q2, q3, g);
       const Prim<T> p = primitives(q0, q1, q2, q3, g);
-      const int k = a * SX + b;
-      RHO[k] = p.rho;
-      U[k] = p.u;
-      V[k] = p.v;
-      P[k] = p.p;
-      E[k] = p.p / (p.rho * (g - T(1)));
+      RHO[idx] = p.rho;
+      U[idx] = p.u;
+      V[idx] = p.v;
+      P[idx] = p.p;
+      E[idx] = p.p / (p.rho * (g - T(1)));
+    } else {
+      const T rho = q0 > T(kRhoFloor) ? q0 : T(kRhoFloor);
+      const T rinv = __frcp_rn(rho);
+      T u = q1 * rinv, v = q2 * rinv;
+      const T kin = T(0.5) * rho * (u * u + v * v);
+      T pr = (g - T(1)) * (q3 - kin);
+      if (enf) {
+        q1 = rho * u;
+        q2 = rho * v;
+        q3 = pr > T(kPFloor) ? q3 : T(kPFloor) / (g - T(1)) + kin;
+        u = q1 * rinv;
+        v = q2 * rinv;
+        pr = (g - T(1)) * (q3 - T(0.5) * rho * (u * u + v * v));
+      }
+      pr = pr > T(kPFloor) ? pr : T(kPFloor);
+      RHO[idx] = rho;
+      U[idx] = u;
+      V[idx] = v;
+      P[idx] = pr;
+      E[idx] = pr * rinv * igm1;
     }
   }
   __syncthreads();
@@ -136,63 +185,93 @@ __global__ void __launch_bounds__(kStencilThreads)
   const T tdx = T(2.0 * S.dx), tdy = T(2.0 * S.dy), hx = T(S.dx), hy = T(S.dy);
   const T itdx = T(1.0 / (2.0 * S.dx)), itdy = T(1.0 / (2.0 * S.dy));
   const T tol = T(32) * type_eps<T>();
-  int near_count = 0;
-  for (int ar = ty; ar < RY; ar += nty) {
-    const int gj = y0 - W + ar;
-    for (int br = tx; br < RX; br += 32) {
-      const int gi = x0 - W + br;
-      const bool inside = gj >= 0 && gj < ny && gi >= 0 && gi < nx;
-      const int idx = ar * RX + br;
-      if (!per && !inside) {
-        RAW[idx] = 0;
-        continue;
-      }
-      const int c = (ar + HW - W) * SX + br + HW - W;
-      bool near = false;
-      bool m = false;
-      // sensor velocity gradients: central; first-order one-sided at outflow edges
-      T dudx = T(0), dvdx = T(0), dudy = T(0), dvdy = T(0);
-      const bool cx = per || (gi > 0 && gi < nx - 1), cy = per || (gj > 0 && gj < ny - 1);
-      if (comp_on || shear_on) {
-        if (cx) dudx = dq(U[c + 1], U[c - 1], tdx, itdx);
-        else if (nx > 1) dudx = gi == 0 ? (U[c + 1] - U[c]) / hx : (U[c] - U[c - 1]) / hx;
-        if (cy) dvdy = dq(V[c + SX], V[c - SX], tdy, itdy);
-        else if (ny > 1) dvdy = gj == 0 ? (V[c + SX] - V[c]) / hy : (V[c] - V[c - SX]) / hy;
-      }
-      if (comp_on) {
-        const T div = dudx + dvdy;
-        m = div < comp_lim;
-        near = near || fabs(div - comp_lim) <= tol * fabs(comp_lim);
-      }
-      if (shear_on) {
-        if (cx) dvdx = dq(V[c + 1], V[c - 1], tdx, itdx);
-        else if (nx > 1) dvdx = gi == 0 ? (V[c + 1] - V[c]) / hx : (V[c] - V[c - 1]) / hx;
-        if (cy) dudy = dq(U[c + SX], U[c - SX], tdy, itdy);
-        else if (ny > 1) dudy = gj == 0 ? (U[c + SX] - U[c]) / hy : (U[c] - U[c - SX]) / hy;
-        const T av = fabs(dvdx - dudy);
-        m = m || av > shear_lim;
-        near = near || fabs(av - shear_lim) <= tol * shear_lim;
-      }
-      m = jump_gt(RHO[c - 1], RHO[c], RHO[c + 1], eps_r, thr, tol, near) || m;
-      m = jump_gt(RHO[c - SX], RHO[c], RHO[c + SX], eps_r, thr, tol, near) || m;
-      m = jump_gt(P[c - 1], P[c], P[c + 1], eps_p, thr, tol, near) || m;
-      m = jump_gt(P[c - SX], P[c], P[c + SX], eps_p, thr, tol, near) || m;
-      m = jump_gt(E[c - 1], E[c], E[c + 1], eps_e, thr, tol, near) || m;
-      m = jump_gt(E[c - SX], E[c], E[c + SX], eps_e, thr, tol, near) || m;
-      if (!per && S.boundary_guard > 0) {
-        const int bg = S.boundary_guard;
-        if (gj < bg || gj >= ny - bg || gi < bg || gi >= nx - bg) m = true;
-      }
-      RAW[idx] = m ? 1 : 0;
-      // nodes of this tile whose metric sits within roundoff of a threshold
-      if (near && inside && ar >= W && ar < W + kSenTY && br >= W && br < W + kSenTX) ++near_count;
-    }
+  bool near_any = false;  // only used when NEAR
+
+  // ---- two-point jumps, once per edge (x edges, then y edges) ----
+  const int nex = RY * (RX + 1);
+  const float iex = 1.0f / (float)(RX + 1);
+  for (int idx = threadIdx.x; idx < nex; idx += blockDim.x) {
+    const int ar = row_of(idx, RX + 1, iex), be = idx - ar * (RX + 1);
+    const int c = (ar + off) * SX + be + off;  // right node of the edge
+    bool nr = false;
+    const bool f = pair_gt<T, NEAR>(RHO[c - 1], RHO[c], eps_r, thr, tol, nr) |
+                   pair_gt<T, NEAR>(P[c - 1], P[c], eps_p, thr, tol, nr) |
+                   pair_gt<T, NEAR>(E[c - 1], E[c], eps_e, thr, tol, nr);
+    EXF[idx] = (f ? 1 : 0) | (nr ? 2 : 0);
+  }
+  const int ney = (RY + 1) * RX;
+  const float irx = 1.0f / (float)RX;
+  for (int idx = threadIdx.x; idx < ney; idx += blockDim.x) {
+    const int ae = row_of(idx, RX, irx), br = idx - ae * RX;
+    const int c = (ae + off) * SX + br + off;  // upper node of the edge
+    bool nr = false;
+    const bool f = pair_gt<T, NEAR>(RHO[c - SX], RHO[c], eps_r, thr, tol, nr) |
+                   pair_gt<T, NEAR>(P[c - SX], P[c], eps_p, thr, tol, nr) |
+                   pair_gt<T, NEAR>(E[c - SX], E[c], eps_e, thr, tol, nr);
+    EYF[idx] = (f ? 1 : 0) | (nr ? 2 : 0);
   }
   __syncthreads();
-  for (int ar = ty; ar < RY; ar += nty) {
+
+  // ---- raw flags on the tile plus a width-wide ring ----
+  int near_count = 0;
+  for (int idx = threadIdx.x; idx < RX * RY; idx += blockDim.x) {
+    const int ar = row_of(idx, RX, irx), br = idx - ar * RX;
+    const int gj = y0 - W + ar, gi = x0 - W + br;
+    const bool inside = gj >= 0 && gj < ny && gi >= 0 && gi < nx;
+    if (!per && !inside) {
+      RAW[idx] = 0;
+      continue;
+    }
+    const int c = (ar + off) * SX + br + off;
+    const uint8_t ef = EXF[ar * (RX + 1) + br] | EXF[ar * (RX + 1) + br + 1] |
+                       EYF[ar * RX + br] | EYF[(ar + 1) * RX + br];
+    bool near = NEAR && (ef & 2);
+    bool m = (ef & 1) != 0;
+    // sensor velocity gradients: central; first-order one-sided at outflow edges
+    const bool cx = per || (gi > 0 && gi < nx - 1), cy = per || (gj > 0 && gj < ny - 1);
+    if (comp_on) {
+      T dudx = T(0), dvdy = T(0);
+      if (cx) dudx = dq(U[c + 1], U[c - 1], tdx, itdx);
+      else if (nx > 1) dudx = gi == 0 ? (U[c + 1] - U[c]) / hx : (U[c] - U[c - 1]) / hx;
+      if (cy) dvdy = dq(V[c + SX], V[c - SX], tdy, itdy);
+      else if (ny > 1) dvdy = gj == 0 ? (V[c + SX] - V[c]) / hy : (V[c] - V[c - SX]) / hy;
+      const T div = dudx + dvdy;
+      m = m || div < comp_lim;
+      if (NEAR) near = near || fabs(div - comp_lim) <= tol * fabs(comp_lim);
+    }
+    if (shear_on) {
+      T dvdx = T(0), dudy = T(0);
+      if (cx) dvdx = dq(V[c + 1], V[c - 1], tdx, itdx);
+      else if (nx > 1) dvdx = gi == 0 ? (V[c + 1] - V[c]) / hx : (V[c] - V[c - 1]) / hx;
+      if (cy) dudy = dq(U[c + SX], U[c - SX], tdy, itdy);
+      else if (ny > 1) dudy = gj == 0 ? (U[c + SX] - U[c]) / hy : (U[c] - U[c - SX]) / hy;
+      const T av = fabs(dvdx - dudy);
+      m = m || av > shear_lim;
+      if (NEAR) near = near || fabs(av - shear_lim) <= tol * shear_lim;
+    }
+    if (!m || NEAR) {
+      m = curv_gt<T, NEAR>(RHO[c - 1], RHO[c], RHO[c + 1], eps_r, thr, tol, near) || m;
+      m = curv_gt<T, NEAR>(RHO[c - SX], RHO[c], RHO[c + SX], eps_r, thr, tol, near) || m;
+      m = curv_gt<T, NEAR>(P[c - 1], P[c], P[c + 1], eps_p, thr, tol, near) || m;
+      m = curv_gt<T, NEAR>(P[c - SX], P[c], P[c + SX], eps_p, thr, tol, near) || m;
+      m = curv_gt<T, NEAR>(E[c - 1], E[c], E[c + 1], eps_e, thr, tol, near) || m;
+      m = curv_gt<T, NEAR>(E[c - SX], E[c], E[c + SX], eps_e, thr, tol, near) || m;
+    }
+    if (!per && S.boundary_guard > 0) {
+      const int bg = S.boundary_guard;
+      if (gj < bg || gj >= ny - bg || gi < bg || gi >= nx - bg) m = true;
+    }
+    RAW[idx] = m ? 1 : 0;
+    // nodes of this tile whose metric sits within roundoff of a threshold
+    if (NEAR && near && inside && ar >= W && ar < W + kSenTY && br >= W && br < W + kSenTX)
+      ++near_count;
+  }
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < RY * kSenTX; idx += blockDim.x) {
+    const int ar = idx >> 5, bx = idx & 31;
     uint8_t v = 0;
-    for (int d = 0; d <= 2 * W; ++d) v |= RAW[ar * RX + tx + d];
-    ROW[ar * kSenTX + tx] = v;
+    for (int d = 0; d <= 2 * W; ++d) v |= RAW[ar * RX + bx + d];
+    ROW[idx] = v;
   }
   __syncthreads();
   for (int a = ty; a < kSenTY; a += nty) {
@@ -202,8 +281,11 @@ __global__ void __launch_bounds__(kStencilThreads)
     for (int d = 0; d <= 2 * W; ++d) v |= ROW[(a + d) * kSenTX + tx];
     mask[(size_t)gj * nx + gi] = v;
   }
-  near_count = warp_sum(near_count);
-  if (tx == 0 && near_count > 0) atomicAdd(S.near_count, near_count);
+  if (NEAR) {
+    near_count = warp_sum(near_count);
+    if (tx == 0 && near_count > 0) atomicAdd(S.near_count, near_count);
+  }
+  (void)near_any;
 
   if (!want_visc || S.mu == 0.0) return;
   // viscous stress and heat-flux divergence, central differences (periodic)

@@ -13,10 +13,11 @@
 
 namespace hitb200 {
 
-constexpr int kRedThreads = 256;
+constexpr int kRedThreads = 512;
 constexpr int kRedWarps = kRedThreads / 32;
-constexpr int kTileX = 32;   // prepass / noise / synth tile: 32 x 16 cells
-constexpr int kTileY = 16;
+constexpr int kTileX = 32;   // prepass / noise / synth / diagnostics tile: 32 x 32 cells
+constexpr int kTileY = 32;
+constexpr int kCellsPerThread = kTileY / kRedWarps;  // rows of the tile per thread
 
 enum RedOp : int { OP_SUM = 0, OP_MAX = 1 };
 
