@@ -99,11 +99,13 @@ ModeTables build_modes(const hitb200_desc& d) {
   return t;
 }
 
+constexpr size_t kSweepSmemMax = 227 * 1024;  // opt-in shared memory per CTA on sm_100
+
 int lines_per_cta(int n, int nlines, int elem) {
-  // Largest R in {8, 4, 2, 1} whose shared memory lets two CTAs share an SM
-  // and that still leaves at least two CTAs per SM worth of lines.
+  // R = 2 when its shared memory lets two CTAs share an SM and the grid still
+  // has at least two CTAs per SM worth of lines; otherwise 1.
   int best = 1;
-  for (int R : {8, 4, 2, 1}) {
+  for (int R : {2, 1}) {
     const size_t b = elem == 4 ? SweepLayout<float>(n, R).bytes() : SweepLayout<double>(n, R).bytes();
     if (b > 110 * 1024) continue;
     if ((nlines + R - 1) / R < 2 * 148 && R > 1) continue;
@@ -153,6 +155,7 @@ struct hitb200_batch {
   Work *d_tiles = nullptr, *d_tiles32 = nullptr, *d_xlines = nullptr, *d_ylines = nullptr;
   int* d_partner = nullptr;
   int n_tiles = 0, n_tiles32 = 0, n_x = 0, n_y = 0, elem = 8, mch_x = 4, mch_y = 4, guard_blocks = 1;
+  int rx_max = 1, ry_max = 1;
   size_t smem_x = 0, smem_y = 0, smem_sensor = 0;
   int any_outflow = 0, any_forcing = 0, any_hv = 0, any_noise_upload = 0;
   cudaGraphExec_t graph = nullptr;
@@ -168,6 +171,7 @@ struct LaunchSet {
   const Work *tiles, *tiles32, *xl, *yl;
   const int* partner;
   int n_tiles, n_tiles32, n_x, n_y, elem, mch_x, mch_y, guard_blocks;
+  int thr_x, thr_y;  // sweep CTA sizes: kLineThreads per line of the widest work item
   size_t smem_x, smem_y, smem_sensor;
   cudaStream_t st;
   // cells of all solves, and of the solves carrying viscous / forcing terms
@@ -229,10 +233,11 @@ void launch_sweep_t(const LaunchSet& L, int stage, int mode, const Bind& b) {
   const int nb = AXIS == 0 ? L.n_x : L.n_y;
   const size_t sm = AXIS == 0 ? L.smem_x : L.smem_y;
   const Work* w = AXIS == 0 ? L.xl : L.yl;
+  const int thr = AXIS == 0 ? L.thr_x : L.thr_y;
 #define HB_SWEEP(M)                                                                   \
   case M:                                                                             \
     set_sweep_attr<T, AXIS, M>(sm);                                                   \
-    sweep_kernel<T, AXIS, M><<<nb, kStencilThreads, sm, L.st>>>(L.solves, w, stage, mode, b); \
+    sweep_kernel<T, AXIS, M><<<nb, thr, sm, L.st>>>(L.solves, w, stage, mode, b);     \
     break;
   switch (mch) {
     HB_SWEEP(4)
@@ -296,14 +301,11 @@ int launch_step_sequence(const LaunchSet& L, int any_forcing, int noise_upload, 
     }
     PMARK("sensor", 33 * N + 3 * e * L.cells_visc);
     launch_sensor(L, stage, 1, 1, nb, nullptr);
-    PMARK("sweep_x", 33 * N + 3 * e * L.cells_visc + 16 * L.cells_force + 4 * e * N);
-    launch_sweep(L, 0, stage, SW_STAGE, nb);
-    PMARK("sweep_y", (stage == 0 ? 65 : 97) * N + 4 * e * N);
+    // y sweep: q, mask -> -dG/dy; x sweep: q, mask, -dG/dy, sources (, q) -> stage state
+    PMARK("sweep_y", 33 * N + 4 * e * N);
     launch_sweep(L, 1, stage, SW_STAGE, nb);
-    if (any_outflow) {
-      PMARK("guard", 0.0);
-      guard_kernel<<<dim3(L.guard_blocks, L.nsolves), 256, 0, L.st>>>(L.solves, L.nsolves, stage == 2 ? 3 : stage + 1, nb);
-    }
+    PMARK("sweep_x", (stage == 0 ? 65 : 97) * N + 4 * e * N + 3 * e * L.cells_visc + 16 * L.cells_force);
+    launch_sweep(L, 0, stage, SW_STAGE, nb);
   }
   if (any_hv) {
     PMARK("hv_prepass", 32 * N);
@@ -362,6 +364,8 @@ LaunchSet plan_launch_set(hitb200_plan* p, cudaStream_t st) {
   L.elem = p->elem;
   L.mch_x = mch_for(p->desc.nx);
   L.mch_y = mch_for(p->desc.ny);
+  L.thr_x = kLineThreads * p->Rx;
+  L.thr_y = kLineThreads * p->Ry;
   L.smem_x = p->smem_x;
   L.smem_y = p->smem_y;
   L.smem_sensor = p->smem_sensor;
@@ -549,12 +553,19 @@ int hitb200_plan_create(const hitb200_desc* d, hitb200_plan** out) {
   p->n_tiles = ntx * nty;
   p->Rx = lines_per_cta(nx, ny, p->elem);
   p->Ry = lines_per_cta(ny, nx, p->elem);
-  if (p->Ry < 2 && nx >= 2) p->Ry = 2;  // y panels: at least 16-byte row segments
+  // y panels: at least 16-byte row segments where the shared memory allows
+  if (p->Ry < 2 && nx >= 2 &&
+      (p->elem == 4 ? SweepLayout<float>(ny, 2).bytes() : SweepLayout<double>(ny, 2).bytes()) <= kSweepSmemMax)
+    p->Ry = 2;
   p->n_x = (ny + p->Rx - 1) / p->Rx;
   p->n_y = (nx + p->Ry - 1) / p->Ry;
   p->smem_x = p->elem == 4 ? SweepLayout<float>(nx, p->Rx).bytes() : SweepLayout<double>(nx, p->Rx).bytes();
   p->smem_y = p->elem == 4 ? SweepLayout<float>(ny, p->Ry).bytes() : SweepLayout<double>(ny, p->Ry).bytes();
   p->smem_sensor = sensor_smem_bytes(d->sensor_width, p->elem);
+  if (p->smem_x > kSweepSmemMax || p->smem_y > kSweepSmemMax) {
+    delete p;
+    return (g_last_error = "grid lines too long for the sweep's shared memory", HITB200_ERR_UNSUPPORTED);
+  }
 
   // ---- arena layout ----
   Arena a;
@@ -736,6 +747,16 @@ int hitb200_plan_create(const hitb200_desc* d, hitb200_plan** out) {
     return cuda_fail(e, "cudaMemset(counters)");
   }
   prime_attributes(p->elem, mch_for(nx), mch_for(ny), p->smem_x, p->smem_y, p->smem_sensor);
+  {
+    // powers of the compact-solve root for the non-periodic end corrections
+    double tab[kPowTab];
+    for (int k = 0; k < kPowTab; ++k) tab[k] = std::pow(kRhoSolve, (double)k);
+    const cudaError_t e = cudaMemcpyToSymbol(g_rho_pow, tab, sizeof(tab));
+    if (e != cudaSuccess) {
+      hitb200_plan_destroy(p);
+      return cuda_fail(e, "cudaMemcpyToSymbol(rho powers)");
+    }
+  }
   *out = p;
   return HITB200_OK;
 }
@@ -821,8 +842,8 @@ int hitb200_rhs(hitb200_plan* p, const double* q, int terms, const double* fx, c
   b.terms = terms;
   launch_prepass(L, 0, PRE_STAGE, 1, b);
   launch_sensor(L, 0, 1, (terms & HITB200_TERM_VISCOUS) ? 1 : 0, b, p->hs.mask);
-  launch_sweep(L, 0, 0, SW_RHS, b);
   launch_sweep(L, 1, 0, SW_RHS, b);
+  launch_sweep(L, 0, 0, SW_RHS, b);
   HB_LAUNCHED("rhs");
   return HITB200_OK;
 }
@@ -1093,6 +1114,8 @@ int hitb200_batch_create(const hitb200_desc* descs, int32_t n, hitb200_batch** o
     b->elem = p->elem;
     b->mch_x = std::max(b->mch_x, mch_for(p->desc.nx));
     b->mch_y = std::max(b->mch_y, mch_for(p->desc.ny));
+    b->rx_max = std::max(b->rx_max, p->Rx);
+    b->ry_max = std::max(b->ry_max, p->Ry);
     b->smem_x = std::max(b->smem_x, p->smem_x);
     b->smem_y = std::max(b->smem_y, p->smem_y);
     b->smem_sensor = std::max(b->smem_sensor, p->smem_sensor);
@@ -1219,6 +1242,8 @@ static LaunchSet batch_launch_set(hitb200_batch* b, cudaStream_t st) {
   L.elem = b->elem;
   L.mch_x = b->mch_x;
   L.mch_y = b->mch_y;
+  L.thr_x = kLineThreads * b->rx_max;
+  L.thr_y = kLineThreads * b->ry_max;
   L.smem_x = b->smem_x;
   L.smem_y = b->smem_y;
   L.smem_sensor = b->smem_sensor;

@@ -176,6 +176,21 @@ __device__ __forceinline__ void enforce_node(T& q0, T& q1, T& q2, T& q3, T gamma
   q3 = p > T(kPFloor) ? q3 : T(kPFloor) / (gamma - T(1)) + kin;
 }
 
+// enforce_node with one reciprocal instead of two quotients (results within
+// two ulp of the quotient form); used for the stage states the step writes.
+template <typename T>
+__device__ __forceinline__ void enforce_node_rcp(T& q0, T& q1, T& q2, T& q3, T gamma) {
+  const T rho = q0 > T(kRhoFloor) ? q0 : T(kRhoFloor);
+  const T rinv = T(1) / rho;
+  const T u = q1 * rinv, v = q2 * rinv;
+  const T kin = T(0.5) * rho * (u * u + v * v);
+  const T p = (gamma - T(1)) * (q3 - kin);
+  q0 = rho;
+  q1 = rho * u;
+  q2 = rho * v;
+  q3 = p > T(kPFloor) ? q3 : T(kPFloor) / (gamma - T(1)) + kin;
+}
+
 template <typename T>
 __device__ __forceinline__ T warp_sum(T v) {
 #pragma unroll

@@ -13,6 +13,7 @@ constexpr unsigned kFull = 0xffffffffu;
 
 
 constexpr int kStencilThreads = 256;
+constexpr int kLineThreads = 128;  // sweep threads per grid line of a CTA
 constexpr int kSenTX = 32, kSenTY = 32;  // sensor tile
 constexpr int kSensorThreads = 512;
 constexpr int kHvTX = 32, kHvTY = 16;    // hyperviscosity tile
@@ -351,8 +352,15 @@ __global__ void __launch_bounds__(kSensorThreads, 2)
 // =============================================================================
 constexpr double kRhoSolve = -0.45141622964513645;  // (sqrt(7) - 4) / 3
 constexpr double kSolveScale = 1.2037766123870306;  // -rho / a
-constexpr int kMaxTasks = 16;                        // H-phase tasks per warp
-constexpr int kNodesPerTask = 29;
+constexpr int kPowTab = 128;                         // rho^k below 1e-43 beyond this
+
+// rho^k, k in [0, kPowTab); filled once by the host (hitb200_plan_create).
+__device__ double g_rho_pow[kPowTab];
+
+template <typename T>
+__device__ __forceinline__ T rho_pow(int k) {
+  return (k >= 0 && k < kPowTab) ? T(__ldg(&g_rho_pow[k])) : T(0);
+}
 
 template <typename T>
 __host__ __device__ inline int pad_index(int i) {
@@ -360,24 +368,32 @@ __host__ __device__ inline int pad_index(int i) {
 }
 
 // Shared memory of one sweep CTA holding R lines of n nodes:
-//   FQ [R][8][LS]  flux F_c (c < 4) and enforced state Q_c (c >= 4) of every
-//                  node plus a 5-node halo on each side (LS = n + 10)
-//   RB [R][4][LQ]  face differences raw_i, solved in place into d_i (padded
-//                  index so that the chunked solve reads without bank conflicts)
-//   MK [R][n + 2]  sensor mask of nodes -1 .. n
+//   FQ  [R][8][LS]  flux F_c (c < 4) and enforced state Q_c (c >= 4) of every
+//                   node plus a 5-node halo on each side (LS = n + 10); reused
+//                   by the x-sweep epilogue for the new rows (FP64) when
+//                   guard cells are written
+//   WB  [R][4][LW]  WENO face fluxes W_{il+1/2}, il in [-2, n], of needed faces
+//   HB  [R][4][LW]  hybrid face fluxes H_{il+1/2}, il in [-1, n-1]
+//   RB  [R][4][LQ]  face differences raw_i, solved in place into d_i (padded
+//                   index so that the chunked solve reads without bank conflicts)
+//   MK  [R][n + 2]  sensor mask of nodes -1 .. n
 template <typename T>
 struct SweepLayout {
-  int n, LS, LQ, R;
+  int n, LS, LQ, LW, R;
   __host__ __device__ SweepLayout(int n_, int R_) : n(n_), R(R_) {
     LS = n + 2 * kHalo;
     LS = (LS + 1) & ~1;
     LQ = pad_index<T>(n - 1) + 1;
     LQ = (LQ + 3) & ~3;
+    LW = (n + 3 + 3) & ~3;
   }
+  // byte offsets of the regions; the kernel and the host use the same ones
+  __host__ __device__ size_t off_wb() const { return (size_t)R * 8 * LS * sizeof(T); }
+  __host__ __device__ size_t off_hb() const { return off_wb() + (size_t)R * 4 * LW * sizeof(T); }
+  __host__ __device__ size_t off_rb() const { return off_hb() + (size_t)R * 4 * LW * sizeof(T); }
+  __host__ __device__ size_t off_mk() const { return off_rb() + (size_t)R * 4 * LQ * sizeof(T); }
   __host__ __device__ size_t bytes() const {
-    size_t b = (size_t)R * (8 * LS + 4 * LQ) * sizeof(T);
-    b += (size_t)R * (n + 2);
-    return (b + 15) & ~(size_t)15;
+    return (off_mk() + (size_t)R * (n + 2) + 15) & ~(size_t)15;
   }
 };
 
@@ -514,14 +530,14 @@ __device__ __forceinline__ void line_solve(T* line, int n, int per) {
     if (n == 1) {
       if (len > 0) x[0] = rfirst;
     } else {
-      const T e = T(pow(double(kRhoSolve), double(n - 1)));
+      const T e = rho_pow<T>(n - 1);
       const T r0 = rfirst - pfirst, r1 = rlast - plast;
       const T den = T(1) - e * e;
       const T ca = (r0 - e * r1) / den, cb = (r1 - e * r0) / den;
       // the homogeneous terms are below roundoff beyond ~80 nodes from an end
       if (len > 0 && (start < 96 || start + len > n - 96)) {
-        T pa = T(pow(double(kRhoSolve), double(start)));
-        T pb = T(pow(double(kRhoSolve), double(n - start - len)));
+        T pa = rho_pow<T>(start);
+        T pb = rho_pow<T>(n - start - len);
         T pbk[MCH];
 #pragma unroll
         for (int k = MCH - 1; k >= 0; --k)
@@ -543,14 +559,40 @@ __device__ __forceinline__ void line_solve(T* line, int n, int per) {
     if (k < len) line[pad_index<T>(start + k)] = x[k];
 }
 
-// stage: 0, 1, 2 (SSP-RK3 stage); mode: SweepMode.  For AXIS 1 with
-// mode SW_STAGE the epilogue writes the stage state
+// Position of the j-th (0-based) set bit of `mask` (j < popc(mask)).
+__device__ __forceinline__ int nth_set_bit(unsigned mask, int j) {
+  int pos = 0;
+#pragma unroll
+  for (int w = 16; w > 0; w >>= 1) {
+    const unsigned lo = mask & ((1u << w) - 1u);
+    const int c = __popc(lo);
+    if (j >= c) {
+      j -= c;
+      mask >>= w;
+      pos += w;
+    } else {
+      mask = lo;
+    }
+  }
+  return pos;
+}
+
+// Outflow guard source index: guard cells copy cell g (n-g-1), riemann_config3.py:419-429.
+__device__ __forceinline__ int guard_src(int i, int n, int g) {
+  return i < g ? g : (i > n - g - 1 ? n - g - 1 : i);
+}
+
+// One sweep of the split RHS over R whole grid lines (rows for AXIS 0, columns
+// for AXIS 1), 128 threads per line.  The y sweep runs first and leaves
+// -dG/dy in the partial-rhs buffer; the x sweep runs second and, in mode
+// SW_STAGE, finishes the stage:
 //   stage 0: q1 = clean(q + dt L)
 //   stage 1: q2 = clean(3/4 q + 1/4 (q1 + dt L))
 //   stage 2:      clean(1/3 q + 2/3 (q2 + dt L))     (OOP/time_operator.py:21-26)
-// R (lines per CTA) is a power of two.
+// with L = -dF/dx - dG/dy + viscous + forcing + drag + cooling and clean the
+// enforce filter plus, on outflow grids, the guard cells.
 template <typename T, int AXIS, int MCH>
-__global__ void __launch_bounds__(kStencilThreads, 2)
+__global__ void __launch_bounds__(256, 2)
     sweep_kernel(const SolveDev* __restrict__ solves, const Work* __restrict__ work, int stage,
                  int mode, Bind bind) {
   extern __shared__ __align__(16) unsigned char smem[];
@@ -562,18 +604,20 @@ __global__ void __launch_bounds__(kStencilThreads, 2)
   const int n = AXIS == 0 ? nx : ny;
   const size_t plane = (size_t)nx * ny;
   const int line0 = wk.a, R = wk.b;
-  const int rsh = R > 4 ? 3 : (R > 2 ? 2 : (R > 1 ? 1 : 0));  // ceil(log2 R)
-  const SweepLayout<T> L(n, 1 << rsh);
-  const int LS = L.LS, LQ = L.LQ;
+  const int rsh = R > 1 ? 1 : 0;  // R is 1 or 2
+  const int RL = 1 << rsh;
+  const SweepLayout<T> L(n, RL);
+  const int LS = L.LS, LQ = L.LQ, LW = L.LW;
   const T g = T(S.gamma);
   const double h = AXIS == 0 ? S.dx : S.dy;
   const double* qin = bind.use ? bind.qin : stage_in(S, stage);
   const uint8_t* mask = bind.use ? bind.mask : S.mask;
   const T alpha = T(AXIS == 0 ? sc[S_ALPHA_X] : sc[S_ALPHA_Y]);
-  const int RL = 1 << rsh;  // layout lines (>= R: the last CTA may hold fewer)
   T* FQ = reinterpret_cast<T*>(smem);
-  T* RB = FQ + (size_t)RL * 8 * LS;
-  uint8_t* MK = reinterpret_cast<uint8_t*>(RB + (size_t)RL * 4 * LQ);
+  T* WB = reinterpret_cast<T*>(smem + L.off_wb());
+  T* HB = reinterpret_cast<T*>(smem + L.off_hb());
+  T* RB = reinterpret_cast<T*>(smem + L.off_rb());
+  uint8_t* MK = smem + L.off_mk();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
 
   // ---- L: stage flux and enforced state of the lines ---------------------------
@@ -583,12 +627,8 @@ __global__ void __launch_bounds__(kStencilThreads, 2)
   for (int idx = threadIdx.x; idx < nl; idx += blockDim.x) {
     int r, p;
     if (AXIS == 0) {
-      r = 0;
-      p = idx;
-      while (p >= LS) {
-        p -= LS;
-        ++r;
-      }
+      r = idx >= LS ? 1 : 0;
+      p = idx - r * LS;
     } else {
       r = idx & (RL - 1);
       p = idx >> rsh;
@@ -626,12 +666,8 @@ __global__ void __launch_bounds__(kStencilThreads, 2)
   for (int idx = threadIdx.x; idx < nm; idx += blockDim.x) {
     int r, p;
     if (AXIS == 0) {
-      r = 0;
-      p = idx;
-      while (p >= n + 2) {
-        p -= n + 2;
-        ++r;
-      }
+      r = idx >= n + 2 ? 1 : 0;
+      p = idx - r * (n + 2);
     } else {
       r = idx & (RL - 1);
       p = idx >> rsh;
@@ -643,39 +679,65 @@ __global__ void __launch_bounds__(kStencilThreads, 2)
   }
   __syncthreads();
 
-  // ---- H: face fluxes and their differences --------------------------------------
-  // Warp task = (line, component, 29 consecutive nodes): lanes hold faces
-  // base-2 .. base+29, exchange neighbour faces by shuffles and write
-  // raw_i = (H_{i+1/2} - H_{i-1/2}) / h of nodes base .. base+28.
-  const int tpl = (n + kNodesPerTask - 1) / kNodesPerTask;
-  const int ntask = R * 4 * tpl;
-  const T inv_h = T(1.0 / h);
-#pragma unroll 1
-  for (int task = warp; task < ntask; task += nwarp) {
-    const int rc = task / tpl, seg = task - rc * tpl;
-    const int r = rc >> 2, c = rc & 3;
-    const int il = seg * kNodesPerTask - 2 + lane;  // this lane's face il + 1/2
-    const T* F = FQ + (size_t)(r * 8 + c) * LS + kHalo;
-    const T* Q = FQ + (size_t)(r * 8 + 4 + c) * LS + kHalo;
+  // face il + 1/2 (il in [-1, n-1]) is flagged when node il or il + 1 is
+  auto flagged = [&](const uint8_t* mk, int f) -> bool {
+    return f >= -1 && f <= n - 1 && (mk[f] | mk[f + 1]);
+  };
+
+  // ---- H1: WENO fluxes where a flagged face needs them ---------------------------
+  // Warp task = 32 consecutive faces of one line; the faces that need W (a
+  // flagged face among itself and its neighbours) are found by ballot and
+  // their (face, component) pairs are spread over the warp's lanes.
+  const int nch = (n + 3 + 31) >> 5;
+  for (int task = warp; task < R * nch; task += nwarp) {
+    const int r = task >= nch ? 1 : 0, ch = task - r * nch;
     const uint8_t* mk = MK + r * (n + 2) + 1;  // mk[i] = node i, i in [-1, n]
-    auto flg = [&](int f) -> bool { return f >= -1 && f <= n - 1 && (mk[f] | mk[f + 1]); };
-    const bool f0 = flg(il);
-    const bool need = flg(il - 1) || f0 || flg(il + 1);
-    T wv = T(0);
-    if (need) wv = weno_face<T>(F, Q, per ? il : min(max(il, -1), n - 1), alpha);
-    const T wp = __shfl_down_sync(kFull, wv, 1), wm = __shfl_up_sync(kFull, wv, 1);
-    T hf = T(0);
-    if (il >= -1 && il <= n - 1) {
-      if (f0) {
-        hf = T(kCompactA) * wp + wv;
-        hf = hf + T(kCompactA) * wm;
-      } else {
-        hf = compact_face<T>(F, il);
-      }
+    const int il0 = ch * 32 - 2;
+    const int il = il0 + lane;
+    const bool need = il <= n && (flagged(mk, il - 1) || flagged(mk, il) || flagged(mk, il + 1));
+    const unsigned bal = __ballot_sync(kFull, need);
+    const int items = 4 * __popc(bal);
+    for (int k = lane; k < items; k += 32) {
+      const int c = k & 3, f = il0 + nth_set_bit(bal, k >> 2);
+      const T* F = FQ + (size_t)(r * 8 + c) * LS + kHalo;
+      const T* Q = FQ + (size_t)(r * 8 + 4 + c) * LS + kHalo;
+      const int fe = per ? f : min(max(f, -1), n - 1);
+      WB[(size_t)(r * 4 + c) * LW + f + 2] = weno_face<T>(F, Q, fe, alpha);
     }
-    const T hm = __shfl_up_sync(kFull, hf, 1);
-    if (lane >= 2 && lane <= 30 && il >= 0 && il < n)
-      RB[(size_t)(r * 4 + c) * LQ + pad_index<T>(il)] = (hf - hm) * inv_h;
+  }
+  __syncthreads();
+
+  // ---- H2: hybrid face fluxes, then raw_i = (H_{i+1/2} - H_{i-1/2}) / h -----------
+  const int nf = R * 4 * (n + 1);
+  for (int idx = threadIdx.x; idx < nf; idx += blockDim.x) {
+    int rc = 0, f = idx;
+    while (f >= n + 1) {
+      f -= n + 1;
+      ++rc;
+    }
+    const int il = f - 1, r = rc >> 2, c = rc & 3;
+    const uint8_t* mk = MK + r * (n + 2) + 1;
+    T hf;
+    if (flagged(mk, il)) {
+      const T* Wc = WB + (size_t)rc * LW + 2;
+      hf = T(kCompactA) * Wc[il + 1] + Wc[il];
+      hf = hf + T(kCompactA) * Wc[il - 1];
+    } else {
+      hf = compact_face<T>(FQ + (size_t)(r * 8 + c) * LS + kHalo, il);
+    }
+    HB[(size_t)rc * LW + f] = hf;  // HB[il + 1]
+  }
+  __syncthreads();
+  const T inv_h = T(1.0 / h);
+  const int nr = R * 4 * n;
+  for (int idx = threadIdx.x; idx < nr; idx += blockDim.x) {
+    int rc = 0, i = idx;
+    while (i >= n) {
+      i -= n;
+      ++rc;
+    }
+    const T* H = HB + (size_t)rc * LW;
+    RB[(size_t)rc * LQ + pad_index<T>(i)] = (H[i + 1] - H[i]) * inv_h;
   }
   __syncthreads();
 
@@ -685,95 +747,116 @@ __global__ void __launch_bounds__(kStencilThreads, 2)
   __syncthreads();
 
   // ---- E: epilogue ----------------------------------------------------------------------
-  const double fs = sc[S_F_SCALE];
   const int terms = bind.use ? bind.terms : fused_terms(S);
-  const int ne = AXIS == 0 ? R * n : (n << rsh);
-  for (int idx = threadIdx.x; idx < ne; idx += blockDim.x) {
-    int r, p;
-    if (AXIS == 0) {
-      r = 0;
-      p = idx;
-      while (p >= n) {
-        p -= n;
-        ++r;
+  if (AXIS == 1 || mode == SW_DERIV) {
+    // y sweep: partial rhs -dG/dy (or the bare derivative for the API)
+    const int ne = AXIS == 0 ? R * n : (n << rsh);
+    T* rx = reinterpret_cast<T*>(S.rx);
+    for (int idx = threadIdx.x; idx < ne; idx += blockDim.x) {
+      int r, p;
+      if (AXIS == 0) {
+        r = idx >= n ? 1 : 0;
+        p = idx - r * n;
+      } else {
+        r = idx & (RL - 1);
+        p = idx >> rsh;
+        if (r >= R) continue;
       }
-    } else {
-      r = idx & (RL - 1);
-      p = idx >> rsh;
-      if (r >= R) continue;
-    }
-    const int row = AXIS == 0 ? line0 + r : p, col = AXIS == 0 ? p : line0 + r;
-    const size_t o = (size_t)row * nx + col;
-    const T* dl = RB + (size_t)r * 4 * LQ + pad_index<T>(p);
-    T d[4];
-#pragma unroll
-    for (int c = 0; c < 4; ++c) d[c] = (terms & 1) ? dl[c * LQ] : T(0);
-    if (mode == SW_DERIV) {
-#pragma unroll
-      for (int c = 0; c < 4; ++c) bind.out[c * plane + o] = double(dl[c * LQ]);
-      continue;
-    }
-    if (AXIS == 0) {
-      T v[4] = {-d[0], -d[1], -d[2], -d[3]};
-      if ((terms & 2) && S.mu > 0.0) {
-        const T* vis = reinterpret_cast<const T*>(S.vis);
-        v[1] += vis[o];
-        v[2] += vis[plane + o];
-        v[3] += vis[2 * plane + o];
-      }
-      if (terms & (4 | 8)) {
-        const Prim<double> pr = primitives(qin[o], qin[o + plane], qin[o + 2 * plane], qin[o + 3 * plane], S.gamma);
-        if (terms & 4) {
-          const T fxv = bind.use ? T(bind.fx[o]) : T(fs * S.fx[o]);
-          const T fyv = bind.use ? T(bind.fy[o]) : T(fs * S.fy[o]);
-          const T rho = T(pr.rho), u = T(pr.u), vv = T(pr.v);
-          v[1] += rho * fxv;
-          v[2] += rho * fyv;
-          v[3] += rho * (u * fxv + vv * fyv);
-        }
-        if ((terms & 8) && S.drag_on) {
-          T lx = T(0), ly = T(0);
-          for (int md = 0; md < S.n_drag; ++md) {
-            const int2 k = S.modes[md];
-            const double2 ex = S.twx[mode_index(k.x, col, nx)], ey = S.twy[mode_index(k.y, row, ny)];
-            const T er = T(cmul_re(ex, ey)), ei = T(-cmul_im(ex, ey));
-            const double* cf = sc + S_DRAG + 4 * md;
-            lx += T(cf[0]) * er - T(cf[1]) * ei;
-            ly += T(cf[2]) * er - T(cf[3]) * ei;
-          }
-          v[1] += lx;
-          v[2] += ly;
-          v[3] += T(pr.u) * lx + T(pr.v) * ly;
-        }
-      }
-      if (terms & 16) v[3] += T(sc[S_COOL]);
-      T* rx = reinterpret_cast<T*>(S.rx);
-#pragma unroll
-      for (int c = 0; c < 4; ++c) rx[c * plane + o] = v[c];
-    } else {
-      const T* rx = reinterpret_cast<const T*>(S.rx);
-      double rhs[4];
-#pragma unroll
-      for (int c = 0; c < 4; ++c) rhs[c] = double(rx[c * plane + o]) - double(d[c]);
-      if (mode == SW_RHS) {
-#pragma unroll
-        for (int c = 0; c < 4; ++c) bind.out[c * plane + o] = rhs[c];
-        continue;
-      }
-      const double dt = sc[S_DT];
-      const double* q0 = bind.use ? bind.q0 : S.q;
-      double* qo = bind.use ? bind.qout : stage_out(S, stage);
-      double sv[4];
+      const int row = AXIS == 0 ? line0 + r : p, col = AXIS == 0 ? p : line0 + r;
+      const size_t o = (size_t)row * nx + col;
+      const T* dl = RB + (size_t)r * 4 * LQ + pad_index<T>(p);
 #pragma unroll
       for (int c = 0; c < 4; ++c) {
-        const double t = qin[c * plane + o] + dt * rhs[c];
-        if (stage == 0) sv[c] = t;
-        else if (stage == 1) sv[c] = 0.75 * q0[c * plane + o] + 0.25 * t;
-        else sv[c] = (1.0 / 3.0) * q0[c * plane + o] + (2.0 / 3.0) * t;
+        if (mode == SW_DERIV) bind.out[c * plane + o] = double(dl[c * LQ]);
+        else rx[c * plane + o] = (terms & 1) ? -dl[c * LQ] : T(0);
       }
-      enforce_node(sv[0], sv[1], sv[2], sv[3], S.gamma);
+    }
+    return;
+  }
+  // x sweep: full rhs, then the stage combine and the clean filter
+  const double fs = sc[S_F_SCALE];
+  const double dt = sc[S_DT];
+  const double* q0 = bind.use ? bind.q0 : S.q;
+  double* qo = bind.use ? bind.qout : stage_out(S, stage);
+  const T* ry = reinterpret_cast<const T*>(S.rx);
+  const int gc = (mode == SW_STAGE && !per) ? S.guard : 0;
+  double* ST = reinterpret_cast<double*>(smem);  // new rows (guard staging), reuses FQ
+  for (int idx = threadIdx.x; idx < R * n; idx += blockDim.x) {
+    const int r = idx >= n ? 1 : 0, col = idx - r * n, row = line0 + r;
+    const size_t o = (size_t)row * nx + col;
+    const T* dl = RB + (size_t)r * 4 * LQ + pad_index<T>(col);
+    double rhs[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) rhs[c] = double(ry[c * plane + o]) - ((terms & 1) ? double(dl[c * LQ]) : 0.0);
+    if ((terms & 2) && S.mu > 0.0) {
+      const T* vis = reinterpret_cast<const T*>(S.vis);
+      rhs[1] += double(vis[o]);
+      rhs[2] += double(vis[plane + o]);
+      rhs[3] += double(vis[2 * plane + o]);
+    }
+    if (terms & (4 | 8)) {
+      const Prim<double> pr = primitives(qin[o], qin[o + plane], qin[o + 2 * plane], qin[o + 3 * plane], S.gamma);
+      if (terms & 4) {
+        const double fxv = bind.use ? bind.fx[o] : fs * S.fx[o];
+        const double fyv = bind.use ? bind.fy[o] : fs * S.fy[o];
+        const T rho = T(pr.rho), u = T(pr.u), vv = T(pr.v), tfx = T(fxv), tfy = T(fyv);
+        rhs[1] += double(rho * tfx);
+        rhs[2] += double(rho * tfy);
+        rhs[3] += double(rho * (u * tfx + vv * tfy));
+      }
+      if ((terms & 8) && S.drag_on) {
+        T lx = T(0), ly = T(0);
+        for (int md = 0; md < S.n_drag; ++md) {
+          const int2 k = S.modes[md];
+          const double2 ex = S.twx[mode_index(k.x, col, nx)], ey = S.twy[mode_index(k.y, row, ny)];
+          const T er = T(cmul_re(ex, ey)), ei = T(-cmul_im(ex, ey));
+          const double* cf = sc + S_DRAG + 4 * md;
+          lx += T(cf[0]) * er - T(cf[1]) * ei;
+          ly += T(cf[2]) * er - T(cf[3]) * ei;
+        }
+        rhs[1] += double(lx);
+        rhs[2] += double(ly);
+        rhs[3] += double(T(pr.u) * lx + T(pr.v) * ly);
+      }
+    }
+    if (terms & 16) rhs[3] += sc[S_COOL];
+    if (mode == SW_RHS) {
+#pragma unroll
+      for (int c = 0; c < 4; ++c) bind.out[c * plane + o] = rhs[c];
+      continue;
+    }
+    double sv[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      const double t = qin[c * plane + o] + dt * rhs[c];
+      if (stage == 0) sv[c] = t;
+      else if (stage == 1) sv[c] = 0.75 * q0[c * plane + o] + 0.25 * t;
+      else sv[c] = (1.0 / 3.0) * q0[c * plane + o] + (2.0 / 3.0) * t;
+    }
+    enforce_node_rcp(sv[0], sv[1], sv[2], sv[3], S.gamma);
+    if (gc == 0) {
 #pragma unroll
       for (int c = 0; c < 4; ++c) qo[c * plane + o] = sv[c];
+    } else {
+#pragma unroll
+      for (int c = 0; c < 4; ++c) ST[(size_t)(r * 4 + c) * n + col] = sv[c];
+    }
+  }
+  if (gc == 0 || mode != SW_STAGE) return;
+  // Outflow guard fused: every row j takes row J(j) = clamp(j, g, ny-g-1) and
+  // every column i column I(i); the CTA owning row J(j) writes row j.
+  __syncthreads();
+  for (int r = 0; r < R; ++r) {
+    const int j0 = line0 + r;
+    if (j0 != guard_src(j0, ny, gc)) continue;  // a guard row: written by its source
+    const int jlo = j0 == gc ? 0 : j0, jhi = j0 == ny - gc - 1 ? ny - 1 : j0;
+    const int cnt = (jhi - jlo + 1) * nx;
+    for (int idx = threadIdx.x; idx < cnt; idx += blockDim.x) {
+      const int jj = idx / nx, i = idx - jj * nx;
+      const size_t o = (size_t)(jlo + jj) * nx + i;
+      const int si = guard_src(i, nx, gc);
+#pragma unroll
+      for (int c = 0; c < 4; ++c) qo[c * plane + o] = ST[(size_t)(r * 4 + c) * n + si];
     }
   }
 }
