@@ -103,6 +103,9 @@ SIGNATURES = [
     ("hitb200_stable_time_step", ctypes.c_int,
      [_VP, _DP, ctypes.c_double, ctypes.c_double, ctypes.POINTER(ctypes.c_double)]),
     ("hitb200_validate", ctypes.c_int, [_VP, _DP]),
+    ("hitb200_stable_time_step_noalloc", ctypes.c_int,
+     [_DP, ctypes.c_int32, ctypes.c_int32, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+      ctypes.c_double, ctypes.c_double, _DP, _VP]),
     ("hitb200_forcing_update", ctypes.c_int,
      [_VP, _DP, _DP, ctypes.c_double, ctypes.c_double, _DP, _DP, _VP]),
     ("hitb200_step", ctypes.c_int, [_VP, _DP, _DP, _VP]),

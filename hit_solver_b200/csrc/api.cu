@@ -11,6 +11,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1293,3 +1294,133 @@ int hitb200_batch_run(hitb200_batch* b, int32_t nsteps, void* stream) {
 }
 
 }  // extern "C"
+
+// =============================================================================
+// Stable time step without a plan and without allocating.
+//
+// Who needs it: a caller that must not allocate device memory at the point
+// where it wants the CFL time step.  Creating a plan allocates its arena with
+// cudaMalloc, and destroying one calls cudaFree, which synchronises the whole
+// device; a serving loop that shares the GPU with other streams, or a process
+// whose device memory is already reserved by its own caching pool, cannot
+// afford either.  This entry point keeps its reduction scratch in one
+// fixed-size array in the library's own device memory instead.
+//
+// Scratch (g_dt_scratch, 256 + 8 * kDtScratchTiles bytes on every device that
+// loads the library, held until the process exits):
+//   bytes [0, 4)      ticket counter of the last-CTA reduction.  It MUST be
+//                     zero when a call starts: it is zero when the module is
+//                     loaded and every call leaves it at zero again.
+//   bytes [256, ...)  one partial maximum (double) per 32 x 32-cell tile;
+//                     written before it is read, needs no initial value.
+// Every call on a device uses the same scratch and it keeps the last call's
+// contents, so two calls whose kernels may overlap on the GPU (different
+// streams, or different host threads without ordering) race and give wrong
+// results; calls on one stream are ordered and safe.
+// =============================================================================
+namespace {
+
+constexpr int kDtScratchTiles = 1024;  // up to 1024 tiles of 32 x 32 cells (1,048,576 cells)
+constexpr int kDtScratchHead = 256;
+constexpr int kMaxScratchDevices = 64;
+
+static __device__ __align__(256) unsigned char g_dt_scratch[kDtScratchHead + 8 * kDtScratchTiles];
+
+std::mutex g_dt_scratch_mu;
+unsigned char* g_dt_scratch_addr[kMaxScratchDevices] = {};
+
+// Device address of g_dt_scratch on the current device.  In host code the
+// name g_dt_scratch is only a host-side stand-in, so the address is looked up
+// once per device with that device current (the first call on a device may
+// also load the module there) and then passed to the kernel.
+int dt_scratch_address(unsigned char** out) {
+  int dev = 0;
+  HB_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kMaxScratchDevices)
+    return invalid("device ordinal out of range for the static time-step scratch");
+  std::lock_guard<std::mutex> lock(g_dt_scratch_mu);
+  if (!g_dt_scratch_addr[dev]) {
+    void* p = nullptr;
+    HB_CUDA(cudaGetSymbolAddress(&p, g_dt_scratch));
+    g_dt_scratch_addr[dev] = static_cast<unsigned char*>(p);
+  }
+  *out = g_dt_scratch_addr[dev];
+  return HITB200_OK;
+}
+
+// Spectral-radius maximum of the raw state (the time-step reduction of the
+// prepass, OOP/spatial_operator.py:369-377), one CTA per 32 x 32 tile; the
+// last CTA reduces the partials and writes dt = min(cfl / max, remaining).
+__global__ void __launch_bounds__(kRedThreads)
+    dt_scratch_kernel(const double* __restrict__ q, int nx, int ny, double dx, double dy,
+                      double g, double cfl, double remaining, unsigned char* scratch,
+                      double* dt_out) {
+  unsigned* ticket = reinterpret_cast<unsigned*>(scratch);
+  double* part = reinterpret_cast<double*>(scratch + kDtScratchHead);
+  const int ntx = (nx + kTileX - 1) / kTileX;
+  const int x0 = (blockIdx.x % ntx) * kTileX, y0 = (blockIdx.x / ntx) * kTileY;
+  const int tx = threadIdx.x & 31, ty0 = threadIdx.x >> 5;
+  const size_t plane = (size_t)nx * ny;
+  const double idx_ = 1.0 / dx, idy_ = 1.0 / dy;
+  double sr = 0.0;
+  for (int a = ty0; a < kTileY; a += kRedWarps) {
+    const int gj = y0 + a, gi = x0 + tx;
+    if (gj >= ny || gi >= nx) continue;
+    const size_t o = (size_t)gj * nx + gi;
+    const double q0 = q[o], q1 = q[o + plane], q2 = q[o + 2 * plane], q3 = q[o + 3 * plane];
+    const double rho = q0 > kRhoFloor ? q0 : kRhoFloor;
+    const double rinv = 1.0 / rho;
+    const double ur = q1 * rinv, vr = q2 * rinv;
+    const double kin = 0.5 * rho * (ur * ur + vr * vr);
+    const double p_raw = (g - 1.0) * (q3 - kin);
+    const double pr = p_raw > kPFloor ? p_raw : kPFloor;
+    const double cr = sqrt(g * pr * rinv);
+    sr = fmax(sr, (fabs(ur) + cr) * idx_ + (fabs(vr) + cr) * idy_);
+  }
+  __shared__ double sm[kRedWarps];
+  sr = warp_max(sr);
+  if (tx == 0) sm[ty0] = sr;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double m = sm[0];
+    for (int w = 1; w < kRedWarps; ++w) m = fmax(m, sm[w]);
+    part[blockIdx.x] = m;
+  }
+  if (!last_block(ticket, gridDim.x)) return;
+  if (threadIdx.x >= 32) return;
+  double m = 0.0;
+  for (int b = tx; b < (int)gridDim.x; b += 32) m = fmax(m, __ldcg(part + b));
+  m = warp_max(m);
+  if (tx == 0) {
+    double dt = cfl / m;
+    if (!isnan(remaining)) dt = fmin(dt, remaining);
+    *dt_out = dt;
+  }
+}
+
+}  // namespace
+
+extern "C" int hitb200_stable_time_step_noalloc(const double* q, int32_t nx, int32_t ny, double dx,
+                                                double dy, double gamma, double cfl,
+                                                double remaining_time, double* dt_out,
+                                                void* stream) {
+  if (!q || !dt_out) return invalid("NULL argument");
+  if (nx <= 0 || ny <= 0) return invalid("nx and ny must be positive");
+  if (!(dx > 0.0) || !(dy > 0.0)) return invalid("dx and dy must be positive");
+  if (!(gamma > 1.0)) return invalid("gamma must exceed 1");
+  if (!(cfl > 0.0)) return invalid("cfl must be positive");
+  const long long tiles = (long long)((nx + kTileX - 1) / kTileX) * ((ny + kTileY - 1) / kTileY);
+  if (tiles > kDtScratchTiles) {
+    g_last_error = "grid of " + std::to_string(nx) + " x " + std::to_string(ny) + " cells needs " +
+                   std::to_string(tiles) + " tiles of 32 x 32 cells; the static scratch of "
+                   "hitb200_stable_time_step_noalloc holds at most 1024";
+    return HITB200_ERR_UNSUPPORTED;
+  }
+  unsigned char* scratch = nullptr;
+  const int st = dt_scratch_address(&scratch);
+  if (st != HITB200_OK) return st;
+  dt_scratch_kernel<<<(unsigned)tiles, kRedThreads, 0, (cudaStream_t)stream>>>(
+      q, nx, ny, dx, dy, gamma, cfl, remaining_time, scratch, dt_out);
+  HB_LAUNCHED("dt_scratch_kernel");
+  return HITB200_OK;
+}

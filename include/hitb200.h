@@ -176,6 +176,26 @@ int hitb200_stable_time_step(hitb200_plan* plan, const double* q, double cfl,
 /* validate_raw_physical_state (riemann_config3.py:442-452); synchronises and
  * returns HITB200_ERR_NONFINITE / HITB200_ERR_NONPOSITIVE. */
 int hitb200_validate(hitb200_plan* plan, const double* q);
+/* Stable time step without a plan, allocating nothing.  No counterpart in the
+ * reference (its NumPy stable_time_step allocates freely).  For callers that
+ * must not allocate device memory where they need the CFL step: creating a
+ * plan calls cudaMalloc and destroying it cudaFree, which synchronises the
+ * device; a serving loop sharing the GPU, or a process whose device memory is
+ * reserved by its own pool, can take neither.
+ * Writes min(cfl / max_cells((|u|+c)/dx + (|v|+c)/dy), remaining_time) (NaN
+ * remaining_time: no limit), the value hitb200_stable_time_step returns, to
+ * the device double *dt_out, asynchronously on `stream`.  q: device double
+ * [4][ny][nx].  The reduction scratch is a static device array of 8448 bytes
+ * (held by every GPU that loads the library until exit): grids of more than
+ * 1024 tiles of 32 x 32 cells are rejected with HITB200_ERR_UNSUPPORTED.  Its
+ * ticket counter must be zero when a call starts; it is zero at module load
+ * and each call leaves it zero.  The first call on a device looks up the
+ * scratch address (and may load the module): make it before any stream
+ * capture.  All calls on a device share the scratch, so calls that may
+ * overlap on the GPU (other streams or threads) race. */
+int hitb200_stable_time_step_noalloc(const double* q, int32_t nx, int32_t ny, double dx,
+                                     double dy, double gamma, double cfl,
+                                     double remaining_time, double* dt_out, void* stream);
 
 /* ---- forcing ---------------------------------------------------------------- */
 /* IsotropicShellOUForcing2D.update (OOP/forcing.py:70-130) for the state q
