@@ -65,6 +65,9 @@ def parse_args():
     p.add_argument("--batch", type=int, default=8, help="solves in the batched measurement")
     p.add_argument("--cpu-steps", type=int, default=3, help="oracle steps in the cpu_baseline sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--only", choices=("all", "single"), default="all",
+                   help="single: only the FP32-bulk single-solve steps, no JSON line "
+                        "(a short launch sequence for profilers)")
     return p.parse_args()
 
 
@@ -117,20 +120,63 @@ def dist_finish(world: int) -> None:
 # clocks sampled during the timed region
 # ----------------------------------------------------------------------------------
 class ClockSampler:
+    """SM clock and clock-event reasons sampled during the timed region:
+    NVML polled from a thread every 10 ms (falls back to nvidia-smi -lms 200)."""
+
     QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    # NVML clocks-event reason bits
+    REASONS = {0x4: "sw_power_cap", 0x8: "hw_slowdown", 0x20: "sw_thermal_slowdown",
+               0x40: "hw_thermal_slowdown"}
 
-    def __init__(self, gpu_index: int):
-        self.path = Path(tempfile.mkstemp(prefix="clocks_", suffix=".csv")[1])
-        self.gpu = gpu_index
+    def __init__(self, cuda_index: int):
+        self.cuda_index = cuda_index
+        self.samples = []
+        self.max_mhz = None
         self.proc = None
+        self.thread = None
+        self.path = None
+
+    def _nvml_handle(self):
+        import pynvml
+        import torch
+
+        pynvml.nvmlInit()
+        try:
+            uuid = str(torch.cuda.get_device_properties(self.cuda_index).uuid)
+            return pynvml, pynvml.nvmlDeviceGetHandleByUUID("GPU-" + uuid)
+        except Exception:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.cuda_index)
 
     def __enter__(self):
+        import threading
+
         try:
+            nv, h = self._nvml_handle()
+            self.max_mhz = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+            self.stop = threading.Event()
+
+            def poll():
+                while not self.stop.is_set():
+                    try:
+                        mhz = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                        bits = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                        self.samples.append((float(mhz), int(bits)))
+                    except Exception:
+                        pass
+                    self.stop.wait(0.01)
+
+            self.thread = threading.Thread(target=poll, daemon=True)
+            self.thread.start()
+            return self
+        except Exception:
+            self.thread = None
+        try:
+            self.path = Path(tempfile.mkstemp(prefix="clocks_", suffix=".csv")[1])
             self.fh = open(self.path, "w")
             self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.QUERY}",
+                ["nvidia-smi", f"--id={self.cuda_index}", f"--query-gpu={self.QUERY}",
                  "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.fh,
                 stderr=subprocess.DEVNULL)
         except (OSError, FileNotFoundError):
@@ -138,6 +184,9 @@ class ClockSampler:
         return self
 
     def __exit__(self, *exc):
+        if self.thread is not None:
+            self.stop.set()
+            self.thread.join(timeout=5)
         if self.proc is not None:
             self.proc.terminate()
             try:
@@ -147,7 +196,15 @@ class ClockSampler:
             self.fh.close()
 
     def summary(self):
-        if self.proc is None or not self.path.exists():
+        if self.thread is not None:
+            if not self.samples:
+                return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": ["no samples"]}
+            reasons = sorted({name for _, bits in self.samples
+                              for bit, name in self.REASONS.items() if bits & bit})
+            return {"sm_mhz": statistics.median(m for m, _ in self.samples),
+                    "sm_max_mhz": self.max_mhz, "reasons": reasons,
+                    "samples": len(self.samples), "source": "nvml"}
+        if self.proc is None or self.path is None or not self.path.exists():
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         rows = []
         for line in self.path.read_text().splitlines():
@@ -162,7 +219,7 @@ class ClockSampler:
         reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i] == "Active"})
         return {"sm_mhz": statistics.median(sm) if sm else None,
                 "sm_max_mhz": max(smax) if smax else None, "reasons": reasons,
-                "samples": len(rows)}
+                "samples": len(rows), "source": "nvidia-smi"}
 
 
 def measured_peak():
@@ -272,6 +329,8 @@ def run_b200(args, world, rank, local):
         torch.cuda.synchronize()
     dist_barrier(world)
     t32 = dist_max(t32, world)
+    if args.only == "single":
+        return None
     launches_per_step = len(s32.plan.step_profile(s32.q))
 
     # ---- plain FP64 single solve ----
