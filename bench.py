@@ -65,6 +65,10 @@ def parse_args():
     p.add_argument("--batch", type=int, default=8, help="solves in the batched measurement")
     p.add_argument("--cpu-steps", type=int, default=3, help="oracle steps in the cpu_baseline sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--serve-requests", type=int, default=24,
+                   help="requests in the serving measurement (0: skip)")
+    p.add_argument("--serve-rate", type=float, default=20.0, help="mean arrivals per second")
+    p.add_argument("--serve-round", type=int, default=16, help="steps between admission points")
     p.add_argument("--only", choices=("all", "single"), default="all",
                    help="single: only the FP32-bulk single-solve steps, no JSON line "
                         "(a short launch sequence for profilers)")
@@ -357,6 +361,14 @@ def run_b200(args, world, rank, local):
     batch.run(W)
     tb = dist_max(timed_steps(lambda: batch.run(1), max(K // 4, 5), flush), world)
     kb = max(K // 4, 5)
+    batch.close()
+    del batch, states
+
+    # ---- 512^2 production HIT: plain FP64 single solve vs FP32-bulk batch ----
+    hit = hit_forms(K, W, B, flush, world)
+
+    # ---- serving: a seeded Poisson stream through the continuous-batching loop ----
+    serve = serving_run(args) if args.serve_requests > 0 else None
 
     # ---- roofline of the dominant kernel (FP32-bulk solve) ----
     per = profile_steps(lambda: s32.plan.step_profile(s32.q), 5, flush)
@@ -410,6 +422,8 @@ def run_b200(args, world, rank, local):
         "batched": {"value": world * B * cells * kb / tb, "ms_per_step": 1e3 * tb / kb,
                     "solves": B, "dtype": "fp32 (fp64 state)",
                     "speedup_vs_plain_fp64": (B * cells * kb / tb) / (cells * K / t64)},
+        "batched_hit": hit,
+        "serving": serve,
         "e2e": {"value": world * cells * K / te2e, "unit": "cell-updates/s",
                 "h2d_bytes_per_step": state_bytes / K,
                 "d2h_bytes_per_step": 8 * _lib.S_COUNT + state_bytes / K},
@@ -431,6 +445,59 @@ def run_b200(args, world, rank, local):
     if cpu is not None:
         line["cpu_baseline"] = cpu
     return line
+
+
+def hit_forms(K: int, W: int, B: int, flush, world: int):
+    """512^2 production forced HIT (device forcing noise): the plain FP64
+    single solve and B FP32-bulk solves (seeds 0..B-1, Mach 0.1..0.4) in one
+    batch, both device-timed with L2 flushes."""
+    import torch
+
+    from hit_solver_b200 import _lib
+    from hit_solver_b200.batch import Batch
+    from hit_solver_b200.hit2d import HITSolver
+    from hit_solver_b200.serving import hit_request_config
+
+    n = NX
+    s64 = HITSolver(hit_request_config(n, 1234, 0.25, 10 ** 9, "fp64"))
+    s64.advance(W)
+    k64 = max(K // 2, 5)
+    t64 = dist_max(timed_steps(lambda: s64.advance(1), k64, flush), world)
+    del s64
+    solvers = [HITSolver(hit_request_config(n, i, 0.1 + 0.3 * i / max(B - 1, 1), 10 ** 9,
+                                            "fp32-bulk")) for i in range(B)]
+    batch = Batch.from_plans([s.plan for s in solvers], [s.q for s in solvers])
+    batch.run(W)
+    kb = max(K // 4, 5)
+    tb = dist_max(timed_steps(lambda: batch.run(1), kb, flush), world)
+    status = max(int(m.scalars()[_lib.S_STATUS]) for m in batch.members)
+    batch.close()
+    del solvers
+    torch.cuda.synchronize()
+    plain = world * n * n * k64 / t64
+    batched = world * B * n * n * kb / tb
+    return {"workload": "hit_production_512x512 (nu 7.5e-4, OU 3..5, Mach control, drag, cooling)",
+            "plain_fp64": {"value": plain, "ms_per_step": 1e3 * t64 / k64},
+            "batched_fp32": {"value": batched, "ms_per_step": 1e3 * tb / kb, "solves": B},
+            "speedup_batched_vs_plain": batched / plain, "status_bits": status}
+
+
+def serving_run(args):
+    """Continuous batching of a seeded Poisson stream (Riemann config 3/6 on
+    256..1024^2 to tfinal, HIT 128..512^2 for 200 steps)."""
+    import torch
+
+    from hit_solver_b200 import serving
+
+    reqs = serving.poisson_requests(args.serve_requests, args.serve_rate, seed=2024)
+    server = serving.SolveServer("fp32-bulk", steps_per_round=args.serve_round)
+    results = server.serve(reqs)
+    torch.cuda.synchronize()
+    st = dict(server.stats)
+    st.update({"rate_per_s": args.serve_rate, "unit": "cell-updates/s",
+               "mix": {k: sum(1 for r in reqs if r.kind == k) for k in serving.KINDS},
+               "failed": sum(1 for r in results if r.status != 0)})
+    return st
 
 
 def cpu_baseline(steps: int):

@@ -125,6 +125,8 @@ SIGNATURES = [
     ("hitb200_batch_create", ctypes.c_int,
      [ctypes.POINTER(Desc), ctypes.c_int32, ctypes.POINTER(_VP)]),
     ("hitb200_batch_destroy", ctypes.c_int, [_VP]),
+    ("hitb200_batch_from_plans", ctypes.c_int,
+     [ctypes.POINTER(_VP), ctypes.c_int32, ctypes.POINTER(_VP)]),
     ("hitb200_batch_plan", _VP, [_VP, ctypes.c_int32]),
     ("hitb200_batch_bind", ctypes.c_int, [_VP, ctypes.POINTER(_VP)]),
     ("hitb200_batch_step", ctypes.c_int, [_VP, _VP]),

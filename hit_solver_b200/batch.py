@@ -58,6 +58,33 @@ class Batch:
         self.members = [MemberPlan(self.lib, self.lib.hitb200_batch_plan(h, i)) for i in range(n)]
         self.states: list[torch.Tensor] = []
 
+    @classmethod
+    def from_plans(cls, plans, states) -> "Batch":
+        """A batch over existing plans (hitb200_batch_from_plans) with their
+        resident states bound.  The plans stay owned by their Plan objects:
+        close() hands them back for use alone or in a later batch."""
+        self = cls.__new__(cls)
+        self.lib = _lib.load()
+        n = len(plans)
+        if n == 0:
+            raise ValueError("batch needs at least one plan")
+        arr = (ctypes.c_void_p * n)(*[p.handle.value for p in plans])
+        h = ctypes.c_void_p()
+        torch.cuda.synchronize()
+        _lib.check(self.lib.hitb200_batch_from_plans(arr, n, ctypes.byref(h)))
+        self.handle = h
+        self._plans = list(plans)  # the plans outlive the batch
+        self._finalizer = weakref.finalize(self, Batch._destroy, self.lib, h.value)
+        self.descs = [p.desc for p in plans]
+        self.members = [MemberPlan(self.lib, p.handle.value) for p in plans]
+        self.states = []
+        self.bind(states)
+        return self
+
+    def close(self) -> None:
+        """Destroy the native batch now (waits for the device)."""
+        self._finalizer()
+
     @staticmethod
     def _destroy(lib, handle):
         if handle:

@@ -148,10 +148,12 @@ struct hitb200_plan {
   cudaStream_t graph_stream = nullptr;
   const double* graph_q = nullptr;
   bool in_batch = false;
+  SolveDev* own_solve = nullptr;  // the arena's descriptor (d_solve points into a batch table while batched)
 };
 
 struct hitb200_batch {
   std::vector<hitb200_plan*> plans;
+  bool owns_plans = true;  // false for hitb200_batch_from_plans
   SolveDev* d_solves = nullptr;
   Work *d_tiles = nullptr, *d_tiles32 = nullptr, *d_xlines = nullptr, *d_ylines = nullptr;
   int* d_partner = nullptr;
@@ -681,6 +683,7 @@ int hitb200_plan_create(const hitb200_desc* d, hitb200_plan** out) {
   s.near_count = reinterpret_cast<int*>(s.counters + 8);
   s.diag_out = reinterpret_cast<double*>(base + o_cnt + 64);
   p->d_solve = reinterpret_cast<SolveDev*>(base + o_solve);
+  p->own_solve = p->d_solve;
   p->d_partner = reinterpret_cast<int*>(base + o_partner);
   p->d_tiles = reinterpret_cast<Work*>(base + o_tiles);
   p->d_tiles32 = reinterpret_cast<Work*>(base + o_tiles32);
@@ -984,6 +987,7 @@ int hitb200_step(hitb200_plan* p, double* q, const double* noise, void* stream) 
 
 int hitb200_run(hitb200_plan* p, double* q, int32_t nsteps, void* stream) {
   if (!p || !q) return invalid("NULL argument");
+  if (p->in_batch) return invalid("plan belongs to a batch; use hitb200_batch_run");
   if (nsteps < 0) return invalid("nsteps must be >= 0");
   if (p->desc.forcing_on && p->desc.noise_mode == 0)
     return invalid("hitb200_run needs noise_mode 1 (device noise) when forcing is on");
@@ -1080,24 +1084,14 @@ int hitb200_diagnostics(hitb200_plan* p, const double* q, double* out, int32_t n
 }
 
 // ---- batched form ---------------------------------------------------------------------
-int hitb200_batch_create(const hitb200_desc* descs, int32_t n, hitb200_batch** out) {
-  if (!descs || !out || n <= 0) return invalid("batch needs at least one descriptor");
-  *out = nullptr;
-  for (int i = 1; i < n; ++i)
-    if (descs[i].precision != descs[0].precision) return invalid("batch members must share precision");
-  hitb200_batch* b = new hitb200_batch();
+// Work lists, descriptor table and launch shape of a batch over b->plans.
+static int batch_build(hitb200_batch* b) {
   std::vector<SolveDev> hs;
   std::vector<Work> tiles, tiles32, xl, yl;
   std::vector<int> partner;
+  const int n = (int)b->plans.size();
   for (int i = 0; i < n; ++i) {
-    hitb200_plan* p = nullptr;
-    int r = hitb200_plan_create(&descs[i], &p);
-    if (r != HITB200_OK) {
-      hitb200_batch_destroy(b);
-      return r;
-    }
-    p->in_batch = true;
-    b->plans.push_back(p);
+    hitb200_plan* p = b->plans[i];
     hs.push_back(p->hs);
     const int ntx = (p->desc.nx + kHvTX - 1) / kHvTX, nty = (p->desc.ny + kHvTY - 1) / kHvTY;
     int k = 0;
@@ -1125,30 +1119,23 @@ int hitb200_batch_create(const hitb200_desc* descs, int32_t n, hitb200_batch** o
     b->any_hv |= p->hs.hv_interval > 0;
     b->any_noise_upload |= (p->desc.forcing_on && p->desc.noise_mode == 0);
   }
-  if (b->any_noise_upload) {
-    hitb200_batch_destroy(b);
-    return invalid("batched solves draw forcing noise on the device (noise_mode 1)");
-  }
+  if (b->any_noise_upload) return invalid("batched solves draw forcing noise on the device (noise_mode 1)");
   b->n_tiles = (int)tiles.size();
   b->n_tiles32 = (int)tiles32.size();
   b->n_x = (int)xl.size();
   b->n_y = (int)yl.size();
-  // interleave the sweep work of different solves so that large grids start first
-  cudaError_t e;
   size_t bytes = hs.size() * sizeof(SolveDev) +
                  (tiles.size() + tiles32.size() + xl.size() + yl.size()) * sizeof(Work) +
-                 partner.size() * sizeof(int) + 1024;
+                 partner.size() * sizeof(int) + 1024 + 6 * 256;
   unsigned char* buf = nullptr;
-  e = cudaMalloc(&buf, bytes);
-  if (e != cudaSuccess) {
-    hitb200_batch_destroy(b);
-    return cuda_fail(e, "cudaMalloc(batch tables)");
-  }
+  cudaError_t e = cudaMalloc(&buf, bytes);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(batch tables)");
   size_t off = 0;
+  cudaError_t ce = cudaSuccess;
   auto put = [&](const void* src, size_t nbytes) -> unsigned char* {
     unsigned char* d = buf + off;
     off += (nbytes + 255) & ~(size_t)255;
-    cudaMemcpy(d, src, nbytes, cudaMemcpyHostToDevice);
+    if (nbytes > 0 && ce == cudaSuccess) ce = cudaMemcpy(d, src, nbytes, cudaMemcpyHostToDevice);
     return d;
   };
   b->d_solves = reinterpret_cast<SolveDev*>(put(hs.data(), hs.size() * sizeof(SolveDev)));
@@ -1157,23 +1144,89 @@ int hitb200_batch_create(const hitb200_desc* descs, int32_t n, hitb200_batch** o
   b->d_xlines = reinterpret_cast<Work*>(put(xl.data(), xl.size() * sizeof(Work)));
   b->d_ylines = reinterpret_cast<Work*>(put(yl.data(), yl.size() * sizeof(Work)));
   b->d_partner = reinterpret_cast<int*>(put(partner.data(), partner.size() * sizeof(int)));
+  if (ce != cudaSuccess) return cuda_fail(ce, "cudaMemcpy(batch tables)");
   prime_attributes(b->elem, b->mch_x, b->mch_y, b->smem_x, b->smem_y, b->smem_sensor);
-  // member plans keep their own descriptors pointing at the batch copy
-  for (int i = 0; i < n; ++i) b->plans[i]->d_solve = b->d_solves + i;
+  // member plans use the batch's copy of their descriptor while batched
+  for (int i = 0; i < n; ++i) {
+    b->plans[i]->d_solve = b->d_solves + i;
+    b->plans[i]->in_batch = true;
+  }
+  return HITB200_OK;
+}
+
+int hitb200_batch_create(const hitb200_desc* descs, int32_t n, hitb200_batch** out) {
+  if (!descs || !out || n <= 0) return invalid("batch needs at least one descriptor");
+  *out = nullptr;
+  for (int i = 1; i < n; ++i)
+    if (descs[i].precision != descs[0].precision) return invalid("batch members must share precision");
+  hitb200_batch* b = new hitb200_batch();
+  for (int i = 0; i < n; ++i) {
+    hitb200_plan* p = nullptr;
+    int r = hitb200_plan_create(&descs[i], &p);
+    if (r != HITB200_OK) {
+      hitb200_batch_destroy(b);
+      return r;
+    }
+    b->plans.push_back(p);
+  }
+  const int r = batch_build(b);
+  if (r != HITB200_OK) {
+    hitb200_batch_destroy(b);
+    return r;
+  }
+  *out = b;
+  return HITB200_OK;
+}
+
+int hitb200_batch_from_plans(hitb200_plan* const* plans, int32_t n, hitb200_batch** out) {
+  if (!plans || !out || n <= 0) return invalid("batch needs at least one plan");
+  *out = nullptr;
+  for (int i = 0; i < n; ++i) {
+    if (!plans[i]) return invalid("NULL plan");
+    if (plans[i]->in_batch) return invalid("plan already belongs to a batch");
+    if (plans[i]->desc.precision != plans[0]->desc.precision)
+      return invalid("batch members must share precision");
+    for (int j = 0; j < i; ++j)
+      if (plans[j] == plans[i]) return invalid("plan listed twice");
+  }
+  hitb200_batch* b = new hitb200_batch();
+  b->owns_plans = false;
+  b->plans.assign(plans, plans + n);
+  const int r = batch_build(b);
+  if (r != HITB200_OK) {
+    hitb200_batch_destroy(b);
+    return r;
+  }
   *out = b;
   return HITB200_OK;
 }
 
 int hitb200_batch_destroy(hitb200_batch* b) {
   if (!b) return HITB200_OK;
+  int status = HITB200_OK;
   if (b->graph) cudaGraphExecDestroy(b->graph);
-  if (b->d_solves) cudaFree(b->d_solves);
+  if (b->d_solves) {
+    // the tables may still be read by queued launches of this batch
+    const cudaError_t e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) status = cuda_fail(e, "cudaDeviceSynchronize(batch destroy)");
+    cudaFree(b->d_solves);
+  }
   for (hitb200_plan* p : b->plans) {
-    p->d_solve = nullptr;
-    hitb200_plan_destroy(p);
+    if (b->owns_plans) {
+      p->d_solve = nullptr;
+      hitb200_plan_destroy(p);
+    } else if (p->d_solve != p->own_solve) {
+      // hand the plan back with its own descriptor, carrying the state bound meanwhile
+      p->d_solve = p->own_solve;
+      p->in_batch = false;
+      const cudaError_t e = cudaMemcpy(&p->own_solve->q, &p->hs.q, sizeof(double*), cudaMemcpyHostToDevice);
+      if (e != cudaSuccess && status == HITB200_OK) status = cuda_fail(e, "cudaMemcpy(plan state)");
+    } else {
+      p->in_batch = false;
+    }
   }
   delete b;
-  return HITB200_OK;
+  return status;
 }
 
 hitb200_plan* hitb200_batch_plan(hitb200_batch* b, int32_t i) {

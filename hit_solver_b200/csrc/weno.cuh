@@ -41,6 +41,10 @@ HITB200_WENO_IS(weno_is3, 2107.0, 1083920.0 / 2107.0, 203060.0 / 13549.0, -2594.
 // value needs one division (the scaled weights stay within 1e-60 .. 1e40).
 // FP32: that product would underflow, so each weight uses a fast reciprocal
 // (2 ulp), which perturbs the convex combination far below FP32 flux error.
+// The reference's IS_0 can be negative, so eps + IS_0 can cancel to (nearly)
+// zero; its square is floored at 1e-30 so that the fast reciprocal stays
+// finite.  The floored weight then exceeds every other by at least 1e10, so
+// the face value is q_0 to FP32 precision, the exact limit of the weights.
 template <typename T>
 __device__ __forceinline__ T weno7(T v0, T v1, T v2, T v3, T v4, T v5, T v6) {
   const T eps = T(1e-10);
@@ -61,8 +65,10 @@ __device__ __forceinline__ T weno7(T v0, T v1, T v2, T v3, T v4, T v5, T v6) {
     const T w3 = T(4.0 / 35.0) * s2 * p01;
     return (w0 * q0 + w1 * q1 + w2 * q2 + w3 * q3) / (w0 + w1 + w2 + w3);
   } else {
-    const float a0 = __fdividef(1.0f / 35.0f, s0), a1 = __fdividef(12.0f / 35.0f, s1);
-    const float a2 = __fdividef(18.0f / 35.0f, s2), a3 = __fdividef(4.0f / 35.0f, s3);
+    const float a0 = __fdividef(1.0f / 35.0f, fmaxf(s0, 1e-30f));
+    const float a1 = __fdividef(12.0f / 35.0f, fmaxf(s1, 1e-30f));
+    const float a2 = __fdividef(18.0f / 35.0f, fmaxf(s2, 1e-30f));
+    const float a3 = __fdividef(4.0f / 35.0f, fmaxf(s3, 1e-30f));
     return __fdividef(a0 * q0 + a1 * q1 + a2 * q2 + a3 * q3, a0 + a1 + a2 + a3);
   }
 }

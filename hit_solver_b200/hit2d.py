@@ -470,8 +470,9 @@ class HITSolver:
         q = initialize_hit_2d(config, self.domain, self.equation, rng)
         self.q = self.equation.enforce_physical_state(q)
         self.plan.set_time(0.0, 0, 0.0, -1 if config.max_steps is None else config.max_steps)
-        self._noise_dev = torch.empty((config.ny, config.nx), dtype=torch.float64, device="cuda")
-        self._noise_host = torch.empty((config.ny, config.nx), dtype=torch.float64).pin_memory()
+        if config.forcing_noise == "numpy":
+            self._noise_dev = torch.empty((config.ny, config.nx), dtype=torch.float64, device="cuda")
+            self._noise_host = torch.empty((config.ny, config.nx), dtype=torch.float64).pin_memory()
 
     def advance(self, nsteps: int) -> None:
         """Issue nsteps steps; steps past tfinal / max_steps are device no-ops."""

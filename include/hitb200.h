@@ -249,6 +249,14 @@ int hitb200_diagnostics(hitb200_plan* plan, const double* q, double* out, int32_
  * share precision. */
 typedef struct hitb200_batch hitb200_batch;
 int hitb200_batch_create(const hitb200_desc* descs, int32_t n, hitb200_batch** batch);
+/* A batch over existing plans (no counterpart in the reference: the serving
+ * loop regroups resident solves as they arrive and finish).  The batch does
+ * not own the plans: hitb200_batch_destroy hands them back, with their
+ * scalars and bound states, usable alone or in a later batch.  A plan belongs
+ * to at most one batch at a time and is advanced only through it meanwhile.
+ * Bind the members' states with hitb200_batch_bind before stepping. */
+int hitb200_batch_from_plans(hitb200_plan* const* plans, int32_t n, hitb200_batch** batch);
+/* Destroys the batch (waits for the device first) and the plans it owns. */
 int hitb200_batch_destroy(hitb200_batch* batch);
 /* The member plan of solve i (for per-solve set_time / read_scalars). */
 hitb200_plan* hitb200_batch_plan(hitb200_batch* batch, int32_t i);

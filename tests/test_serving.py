@@ -1,0 +1,68 @@
+"""Continuous-batching request loop (hit_solver_b200.serving).
+
+The GPU test runs a small mixed stream (Riemann configurations 3 and 6 and
+forced HIT, uneven grid sizes, staggered arrivals, a memory budget that
+forces queueing) and checks that every request's final state equals the same
+request run alone through the plain single-solve path.  The stated tolerance
+is exact equality: each solve's kernels and reductions touch only its own
+data in a fixed order, so batching must not change a single bit.
+"""
+
+import pytest
+import torch
+
+from hit_solver_b200 import serving
+
+
+def test_poisson_stream_is_seeded_and_in_range():
+    a = serving.poisson_requests(40, 20.0, seed=3)
+    b = serving.poisson_requests(40, 20.0, seed=3)
+    assert [(r.kind, r.n, r.arrival, r.split, r.seed, r.mach) for r in a] == \
+           [(r.kind, r.n, r.arrival, r.split, r.seed, r.mach) for r in b]
+    arr = [r.arrival for r in a]
+    assert arr == sorted(arr) and arr[0] > 0.0
+    for r in a:
+        assert r.kind in serving.KINDS
+        if r.kind == "hit":
+            assert 128 <= r.n <= 512 and 0.1 <= r.mach <= 0.4 and r.steps == 200
+        else:
+            assert 256 <= r.n <= 1024 and 0.3 <= r.split <= 0.8
+        assert r.n % 64 == 0
+
+
+def test_footprint_grows_with_grid():
+    small = serving.footprint(serving.Request(0, "riemann3", 64), "fp32-bulk")
+    large = serving.footprint(serving.Request(1, "riemann3", 128), "fp32-bulk")
+    hit = serving.footprint(serving.Request(2, "hit", 64), "fp32-bulk")
+    assert 0 < small < large
+    assert hit > 4 * 64 * 64 * 8
+
+
+def test_unknown_kind_rejected():
+    with pytest.raises(ValueError):
+        serving.make_solver(serving.Request(0, "sod", 32), "fp32-bulk")
+
+
+@pytest.mark.gpu
+def test_mixed_stream_matches_solo_runs():
+    reqs = [
+        serving.Request(0, "riemann3", 64, 0.00, split=0.5),
+        serving.Request(1, "hit", 48, 0.00, seed=11, mach=0.2, steps=23),
+        serving.Request(2, "riemann6", 40, 0.01, split=0.4),
+        serving.Request(3, "hit", 64, 0.02, seed=5, mach=0.3, steps=37),
+        serving.Request(4, "riemann3", 32, 0.03, split=0.7),
+    ]
+    # room for about three of them at a time: later arrivals queue for memory
+    budget = sum(sorted(serving.footprint(r, "fp32-bulk") for r in reqs)[-3:])
+    server = serving.SolveServer("fp32-bulk", hbm_budget=budget, steps_per_round=8,
+                                 keep_states=True)
+    results = server.serve(reqs)
+    assert sorted(r.rid for r in results) == [0, 1, 2, 3, 4]
+    assert server.stats["rounds"] > 1 and server.stats["p99_s"] >= server.stats["p50_s"] > 0.0
+    for res in results:
+        req = reqs[res.rid]
+        assert res.status == 0
+        if req.kind == "hit":
+            assert res.steps == req.steps
+        solo = serving.run_alone(req, "fp32-bulk")
+        assert torch.equal(res.state, solo), f"request {res.rid} differs from its solo run"
