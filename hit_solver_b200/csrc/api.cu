@@ -276,7 +276,10 @@ void launch_hv(const LaunchSet& L, const Bind& b) {
   else hv_kernel<double><<<L.n_tiles, kStencilThreads, 0, L.st>>>(L.solves, L.tiles, b);
 }
 void launch_prepass(const LaunchSet& L, int buf, int mode, int enf, const Bind& b) {
-  prepass_kernel<<<L.n_tiles32, kRedThreads, 0, L.st>>>(L.solves, L.tiles32, buf, mode, enf, b);
+  if (L.elem == 4)
+    prepass_kernel<float><<<L.n_tiles32, kPreThreads, 0, L.st>>>(L.solves, L.tiles32, buf, mode, enf, b);
+  else
+    prepass_kernel<double><<<L.n_tiles32, kPreThreads, 0, L.st>>>(L.solves, L.tiles32, buf, mode, enf, b);
 }
 
 // The reference's loop body (OOP/hit2d.py:828-879; riemann_config3.py:728-740).
@@ -546,6 +549,11 @@ int hitb200_plan_create(const hitb200_desc* d, hitb200_plan** out) {
   if ((int)mt.force.size() > kMaxForce)
     return (g_last_error = "forcing shell holds more than 128 modes", HITB200_ERR_UNSUPPORTED);
   if (d->forcing_on && mt.force.empty()) return invalid("forcing shell contains no Fourier modes on this grid");
+  for (const std::vector<int2>* v : {&mt.drag, &mt.force})
+    for (const int2& m : *v)
+      if (std::abs(m.x) > kMaxKx)
+        return (g_last_error = "drag / forcing modes beyond |kx| = 16 grid bins are not supported",
+                HITB200_ERR_UNSUPPORTED);
 
   hitb200_plan* p = new hitb200_plan();
   p->desc = *d;
@@ -638,6 +646,9 @@ int hitb200_plan_create(const hitb200_desc* d, hitb200_plan** out) {
   s.cooling_pref = is_none(d->cooling_target_pressure) ? 1.0 / d->gamma : d->cooling_target_pressure;
   s.forcing_on = d->forcing_on;
   s.n_force = (int)mt.force.size();
+  s.kx_drag = s.kx_force = 0;
+  for (const int2& m : mt.drag) s.kx_drag = std::max(s.kx_drag, std::abs(m.x));
+  for (const int2& m : mt.force) s.kx_force = std::max(s.kx_force, std::abs(m.x));
   s.f_tau = d->forcing_correlation_time;
   s.f_rms = d->forcing_rms;
   s.f_has_target = !is_none(d->target_power);

@@ -24,6 +24,7 @@ constexpr int kMaxLine = 1024;        // longest supported grid line
 constexpr int kMaxDrag = 32;          // max drag modes (|k| <= kmax band)
 constexpr int kMaxForce = 128;        // max forcing shell modes
 constexpr int kMaxWidth = 8;          // max sensor dilation width
+constexpr int kMaxKx = 16;            // max |x wavenumber bin| of drag / forcing modes
 
 // ---- reduction slots of the per-stage prepass -------------------------------
 enum Red : int {
@@ -83,6 +84,7 @@ struct SolveDev {
   int guard;
   // sources
   int drag_on, n_drag;
+  int kx_drag, kx_force;  // max |x bin| of the drag / forcing modes
   double drag_coef;
   int cooling_on;
   double cooling_tau, cooling_pref;

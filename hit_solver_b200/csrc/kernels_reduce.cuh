@@ -97,10 +97,75 @@ __device__ void step_control(const SolveDev& S, const double* red, double* sc) {
 }
 
 // Prepass: one pass over a stage state computing every global quantity the
-// RHS needs before its flux pass.
-//   ENF = 1: sensor/LF quantities on enforce_physical_state(q), as
+// RHS needs before its flux pass.  One CTA per 32 x 32 tile, 256 threads,
+// each thread owning one column's 4 cells (rows warp, warp + 8, ...).
+//   enf = 1: sensor/LF quantities on enforce_physical_state(q), as
 //   PeriodicHybridEuler2DOperator.rhs does (OOP/spatial_operator.py:345-346).
-__global__ void __launch_bounds__(kRedThreads, 2)
+// T is the arithmetic type of the sensor/Lax-Friedrichs quantities (float in
+// the FP32-bulk form); the raw-state reductions that drive the time step,
+// Mach control and validation are FP64 in both forms, and every sum is
+// accumulated in FP64.
+constexpr int kPreThreads = 256;
+constexpr int kPreWarps = kPreThreads / 32;
+constexpr int kPreRows = kTileY / kPreWarps;  // own cells per thread
+
+// Enforced-state primitives of one node (enforce_physical_state followed by
+// primitive_from_conservative) in T arithmetic; rinv64 is the node's FP64
+// 1 / rho when the caller has it (FP64 form), else ignored.
+template <typename T>
+struct EnfPrim {
+  T u, v, p, rinv, rho;
+};
+template <typename T>
+__device__ __forceinline__ EnfPrim<T> enforced_prim(double q0, double q1, double q2, double q3,
+                                                    double g, int enf) {
+  EnfPrim<T> r;
+  if constexpr (sizeof(T) == 8) {
+    const double rho = q0 > kRhoFloor ? q0 : kRhoFloor;
+    const double rinv = 1.0 / rho;
+    const double ur = q1 * rinv, vr = q2 * rinv;
+    const double kin = 0.5 * rho * (ur * ur + vr * vr);
+    const double p_raw = (g - 1.0) * (q3 - kin);
+    double ue = ur, ve = vr, pe = p_raw;
+    if (enf) {
+      const double e1 = rho * ur, e2 = rho * vr;
+      const double e3 = p_raw > kPFloor ? q3 : kPFloor / (g - 1.0) + kin;
+      ue = e1 * rinv;
+      ve = e2 * rinv;
+      pe = (g - 1.0) * (e3 - 0.5 * rho * (ue * ue + ve * ve));
+    }
+    r.u = ue;
+    r.v = ve;
+    r.p = pe > kPFloor ? pe : kPFloor;
+    r.rinv = rinv;
+    r.rho = rho;
+  } else {
+    const float gf = (float)g;
+    const float rho = (float)q0 > (float)kRhoFloor ? (float)q0 : (float)kRhoFloor;
+    const float rinv = __frcp_rn(rho);
+    float a1 = (float)q1, a2 = (float)q2, a3 = (float)q3;
+    float u = a1 * rinv, v = a2 * rinv;
+    const float kin = 0.5f * rho * (u * u + v * v);
+    float pr = (gf - 1.0f) * (a3 - kin);
+    if (enf) {
+      a1 = rho * u;
+      a2 = rho * v;
+      a3 = pr > (float)kPFloor ? a3 : (float)kPFloor / (gf - 1.0f) + kin;
+      u = a1 * rinv;
+      v = a2 * rinv;
+      pr = (gf - 1.0f) * (a3 - 0.5f * rho * (u * u + v * v));
+    }
+    r.u = u;
+    r.v = v;
+    r.p = pr > (float)kPFloor ? pr : (float)kPFloor;
+    r.rinv = rinv;
+    r.rho = rho;
+  }
+  return r;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kPreThreads)
     prepass_kernel(const SolveDev* __restrict__ solves, const Work* __restrict__ work, int buf,
                    int mode, int enf, Bind bind) {
   const Work w = work[blockIdx.x];
@@ -112,121 +177,142 @@ __global__ void __launch_bounds__(kRedThreads, 2)
   const int nx = S.nx, ny = S.ny, per = S.periodic;
   const size_t plane = (size_t)nx * ny;
   const double g = S.gamma;
-  const double igm1 = 1.0 / (g - 1.0), idx_ = 1.0 / S.dx, idy_ = 1.0 / S.dy;
-  const double ih2x = 1.0 / (2.0 * S.dx), ih2y = 1.0 / (2.0 * S.dy);
+  const T gT = T(g);
+  const T igm1 = T(1.0 / (g - 1.0));
+  const double idx_ = 1.0 / S.dx, idy_ = 1.0 / S.dy;
+  const T hx = T(S.dx), hy = T(S.dy);
+  const T ih2x = T(1.0 / (2.0 * S.dx)), ih2y = T(1.0 / (2.0 * S.dy));
   const int x0 = w.a, y0 = w.b;
+  const bool grads = mode != PRE_CHECK;
+  const bool rawq = mode == PRE_STEP || mode == PRE_CHECK;  // time step, Mach, validation
+  const bool psum = S.cooling_on && (mode == PRE_STAGE || mode == PRE_STEP);
+  const int nslots = (mode == PRE_STAGE || mode == PRE_STEP) ? S.nred : R_FIXED;
+  const int ndrag = nslots > R_FIXED ? S.n_drag : 0;
 
-  __shared__ double su[kTileY + 2][kTileX + 2];
-  __shared__ double sv[kTileY + 2][kTileX + 2];
-  __shared__ double sm[kRedWarps * (R_FIXED + 4 * kMaxDrag)];
+  __shared__ T su[kTileY + 2][kTileX + 2];
+  __shared__ T sv[kTileY + 2][kTileX + 2];
+  __shared__ double2 tw[kTileY][kMaxDrag];  // e^{-i ky y} of the tile's rows, per drag mode
+  __shared__ double sm[kPreWarps * (R_FIXED + 4 * kMaxDrag)];
   __shared__ double red[R_FIXED + 4 * kMaxDrag];
-  const bool need_grad = (mode != PRE_CHECK);
-  const int tx = threadIdx.x & 31, ty0 = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+
+  for (int t = threadIdx.x; t < kTileY * ndrag; t += kPreThreads) {
+    const int a = t / ndrag, m = t - a * ndrag;
+    const int gj = min(y0 + a, ny - 1);
+    tw[a][m] = S.twy[mode_index(S.modes[m].y, gj, ny)];
+  }
 
   double ax = 0, ay = 0, div2 = 0, vort2 = 0, mr = 0, mp = 0, me = 0, ps = 0, sr = 0, vel2 = 0,
          cs = 0;
   int bad = 0;  // validation flags: 1 non-finite, 2 rho <= 0, 4 p <= 0
-  // Every node of the tile and its one-node halo is loaded once; tile nodes
-  // also feed the pointwise reductions here.
-  for (int a = ty0; a < kTileY + 2; a += kRedWarps) {
-    const int gy = y0 + a - 1;
-    const int gj = fold_node(gy, ny, per);
-    for (int b = tx; b < kTileX + 2; b += 32) {
-      const int gx = x0 + b - 1;
-      const bool own = a >= 1 && a <= kTileY && b >= 1 && b <= kTileX && gy < ny && gx < nx;
-      if (!need_grad && !own) continue;
-      const int gi = fold_node(gx, nx, per);
-      const size_t o = (size_t)gj * nx + gi;
-      const double q0 = q[o], q1 = q[o + plane], q2 = q[o + 2 * plane], q3 = q[o + 3 * plane];
-      // One reciprocal and one square root per node serve the enforced state
-      // (sensor / Lax-Friedrichs quantities) and the raw state (time step,
-      // Mach, cooling); both share the floored density.
+  const int gi = x0 + lane;
+  double m0[kPreRows], m1[kPreRows];
+#pragma unroll
+  for (int k = 0; k < kPreRows; ++k) {
+    const int a = warp + kPreWarps * k, gj = y0 + a;
+    m0[k] = m1[k] = 0.0;
+    if (gj >= ny || gi >= nx) {
+      // beyond the grid in a partial tile: the folded node is the halo of
+      // the last row / column
+      if (grads) {
+        const size_t o = (size_t)fold_node(gj, ny, per) * nx + fold_node(gi, nx, per);
+        const EnfPrim<T> e = enforced_prim<T>(q[o], q[o + plane], q[o + 2 * plane], q[o + 3 * plane], g, enf);
+        su[a + 1][lane + 1] = e.u;
+        sv[a + 1][lane + 1] = e.v;
+      }
+      continue;
+    }
+    const size_t o = (size_t)gj * nx + gi;
+    const double q0 = q[o], q1 = q[o + plane], q2 = q[o + 2 * plane], q3 = q[o + 3 * plane];
+    m0[k] = q1;
+    m1[k] = q2;
+    if (mode != PRE_CHECK) {
+      const EnfPrim<T> e = enforced_prim<T>(q0, q1, q2, q3, g, enf);
+      su[a + 1][lane + 1] = e.u;
+      sv[a + 1][lane + 1] = e.v;
+      const T c = sqrt(gT * e.p * e.rinv);
+      ax = fmax(ax, double(fabs(e.u) + c));
+      ay = fmax(ay, double(fabs(e.v) + c));
+      mr = fmax(mr, double(e.rho));
+      mp = fmax(mp, double(e.p));
+      me = fmax(me, double(e.p * e.rinv * igm1));
+    }
+    if (rawq || psum) {
       const double rho = q0 > kRhoFloor ? q0 : kRhoFloor;
       const double rinv = 1.0 / rho;
       const double ur = q1 * rinv, vr = q2 * rinv;
-      const double kin = 0.5 * rho * (ur * ur + vr * vr);
-      const double p_raw = (g - 1.0) * (q3 - kin);
-      double ue = ur, ve = vr, pe = p_raw;
-      if (need_grad && enf) {
-        const double e1 = rho * ur, e2 = rho * vr;
-        const double e3 = p_raw > kPFloor ? q3 : kPFloor / (g - 1.0) + kin;
-        ue = e1 * rinv;
-        ve = e2 * rinv;
-        pe = (g - 1.0) * (e3 - 0.5 * rho * (ue * ue + ve * ve));
-      }
-      pe = pe > kPFloor ? pe : kPFloor;
+      const double p_raw = (g - 1.0) * (q3 - 0.5 * rho * (ur * ur + vr * vr));
       const double pr = p_raw > kPFloor ? p_raw : kPFloor;
-      const double cr = sqrt(g * pr * rinv);
-      if (need_grad) {
-        su[a][b] = ue;
-        sv[a][b] = ve;
-        if (own) {
-          const double c = enf ? sqrt(g * pe * rinv) : cr;
-          ax = fmax(ax, fabs(ue) + c);
-          ay = fmax(ay, fabs(ve) + c);
-          mr = fmax(mr, rho);
-          mp = fmax(mp, pe);
-          me = fmax(me, pe * rinv * igm1);
-        }
-      }
-      if (!own) continue;
-      // raw state: time step, Mach, cooling, validation
       ps += pr;
-      sr = fmax(sr, (fabs(ur) + cr) * idx_ + (fabs(vr) + cr) * idy_);
-      vel2 += ur * ur + vr * vr;
-      cs += cr;
-      // validate_raw_physical_state: p = (g-1)(E - (m_x^2 + m_y^2) / (2 rho)) on
-      // the unfloored density; its sign is that of 2 rho E - |m|^2 when rho > 0
-      const bool fin = isfinite(q0) && isfinite(q1) && isfinite(q2) && isfinite(q3);
-      const double pp = 2.0 * q0 * q3 - (q1 * q1 + q2 * q2);
-      if (!fin || !isfinite(pp)) bad |= 1;
-      if (q0 <= 0.0) bad |= 2;
-      else if (pp <= 0.0) bad |= 4;
+      if (rawq) {
+        const double cr = sqrt(g * pr * rinv);
+        sr = fmax(sr, (fabs(ur) + cr) * idx_ + (fabs(vr) + cr) * idy_);
+        vel2 += ur * ur + vr * vr;
+        cs += cr;
+        // validate_raw_physical_state: p = (g-1)(E - (m_x^2 + m_y^2) / (2 rho)) on
+        // the unfloored density; its sign is that of 2 rho E - |m|^2 when rho > 0
+        const bool fin = isfinite(q0) && isfinite(q1) && isfinite(q2) && isfinite(q3);
+        const double pp = 2.0 * q0 * q3 - (q1 * q1 + q2 * q2);
+        if (!fin || !isfinite(pp)) bad |= 1;
+        if (q0 <= 0.0) bad |= 2;
+        else if (pp <= 0.0) bad |= 4;
+      }
     }
   }
-  if (need_grad) __syncthreads();
-  int cj[kCellsPerThread], ci[kCellsPerThread];
-  bool valid[kCellsPerThread];
+  if (grads) {
+    // one-node ring for the central differences (corners are not used)
+    if (threadIdx.x < 4 * kTileX) {
+      const int side = threadIdx.x >> 5, t = threadIdx.x & 31;
+      int a, b;  // smem coordinates
+      if (side == 0) { a = 0; b = t + 1; }
+      else if (side == 1) { a = kTileY + 1; b = t + 1; }
+      else if (side == 2) { a = t + 1; b = 0; }
+      else { a = t + 1; b = kTileX + 1; }
+      const int gj = fold_node(y0 + a - 1, ny, per), gx = fold_node(x0 + b - 1, nx, per);
+      const size_t o = (size_t)gj * nx + gx;
+      const EnfPrim<T> e = enforced_prim<T>(q[o], q[o + plane], q[o + 2 * plane], q[o + 3 * plane], g, enf);
+      su[a][b] = e.u;
+      sv[a][b] = e.v;
+    }
+    __syncthreads();
 #pragma unroll
-  for (int k = 0; k < kCellsPerThread; ++k) {
-    const int ty = ty0 + kRedWarps * k;
-    const int gj = y0 + ty, gi = x0 + tx;
-    cj[k] = gj;
-    ci[k] = gi;
-    valid[k] = (gj < ny && gi < nx);
-    if (!valid[k] || !need_grad) continue;
-    // sensor divergence / vorticity: central, one-sided at outflow edges
-    const int a = ty + 1, b = tx + 1;
-    double dudx, dvdx, dudy, dvdy;
-    if (per || (gi > 0 && gi < nx - 1)) {
-      dudx = (su[a][b + 1] - su[a][b - 1]) * ih2x;
-      dvdx = (sv[a][b + 1] - sv[a][b - 1]) * ih2x;
-    } else if (nx == 1) {
-      dudx = dvdx = 0.0;
-    } else if (gi == 0) {
-      dudx = (su[a][b + 1] - su[a][b]) * idx_;
-      dvdx = (sv[a][b + 1] - sv[a][b]) * idx_;
-    } else {
-      dudx = (su[a][b] - su[a][b - 1]) * idx_;
-      dvdx = (sv[a][b] - sv[a][b - 1]) * idx_;
+    for (int k = 0; k < kPreRows; ++k) {
+      const int a0 = warp + kPreWarps * k, gj = y0 + a0;
+      if (gj >= ny || gi >= nx) continue;
+      // sensor divergence / vorticity: central, one-sided at outflow edges
+      const int a = a0 + 1, b = lane + 1;
+      T dudx, dvdx, dudy, dvdy;
+      if (per || (gi > 0 && gi < nx - 1)) {
+        dudx = (su[a][b + 1] - su[a][b - 1]) * ih2x;
+        dvdx = (sv[a][b + 1] - sv[a][b - 1]) * ih2x;
+      } else if (nx == 1) {
+        dudx = dvdx = T(0);
+      } else if (gi == 0) {
+        dudx = (su[a][b + 1] - su[a][b]) / hx;
+        dvdx = (sv[a][b + 1] - sv[a][b]) / hx;
+      } else {
+        dudx = (su[a][b] - su[a][b - 1]) / hx;
+        dvdx = (sv[a][b] - sv[a][b - 1]) / hx;
+      }
+      if (per || (gj > 0 && gj < ny - 1)) {
+        dudy = (su[a + 1][b] - su[a - 1][b]) * ih2y;
+        dvdy = (sv[a + 1][b] - sv[a - 1][b]) * ih2y;
+      } else if (ny == 1) {
+        dudy = dvdy = T(0);
+      } else if (gj == 0) {
+        dudy = (su[a + 1][b] - su[a][b]) / hy;
+        dvdy = (sv[a + 1][b] - sv[a][b]) / hy;
+      } else {
+        dudy = (su[a][b] - su[a - 1][b]) / hy;
+        dvdy = (sv[a][b] - sv[a - 1][b]) / hy;
+      }
+      const T dv = dudx + dvdy, vo = dvdx - dudy;
+      div2 += double(dv * dv);
+      vort2 += double(vo * vo);
     }
-    if (per || (gj > 0 && gj < ny - 1)) {
-      dudy = (su[a + 1][b] - su[a - 1][b]) * ih2y;
-      dvdy = (sv[a + 1][b] - sv[a - 1][b]) * ih2y;
-    } else if (ny == 1) {
-      dudy = dvdy = 0.0;
-    } else if (gj == 0) {
-      dudy = (su[a + 1][b] - su[a][b]) * idy_;
-      dvdy = (sv[a + 1][b] - sv[a][b]) * idy_;
-    } else {
-      dudy = (su[a][b] - su[a - 1][b]) * idy_;
-      dvdy = (sv[a][b] - sv[a - 1][b]) * idy_;
-    }
-    const double dv = dudx + dvdy, vo = dvdx - dudy;
-    div2 += dv * dv;
-    vort2 += vo * vo;
+  } else {
+    __syncthreads();  // tw table
   }
-  const int nslots = (mode == PRE_STAGE || mode == PRE_STEP) ? S.nred : R_FIXED;
   warp_to_smem<OP_MAX>(ax, sm, R_AX, nslots);
   warp_to_smem<OP_MAX>(ay, sm, R_AY, nslots);
   warp_to_smem<OP_SUM>(div2, sm, R_DIV2, nslots);
@@ -239,37 +325,39 @@ __global__ void __launch_bounds__(kRedThreads, 2)
   warp_to_smem<OP_SUM>(vel2, sm, R_VEL2, nslots);
   warp_to_smem<OP_SUM>(cs, sm, R_CSUM, nslots);
   bad = __reduce_or_sync(kFullMask, bad);
-  if ((threadIdx.x & 31) == 0) {
-    sm[(threadIdx.x >> 5) * nslots + R_NONFINITE] = (bad & 1) ? 1.0 : 0.0;
-    sm[(threadIdx.x >> 5) * nslots + R_NONPOS_RHO] = (bad & 2) ? 1.0 : 0.0;
-    sm[(threadIdx.x >> 5) * nslots + R_NONPOS_P] = (bad & 4) ? 1.0 : 0.0;
+  if (lane == 0) {
+    sm[warp * nslots + R_NONFINITE] = (bad & 1) ? 1.0 : 0.0;
+    sm[warp * nslots + R_NONPOS_RHO] = (bad & 2) ? 1.0 : 0.0;
+    sm[warp * nslots + R_NONPOS_P] = (bad & 4) ? 1.0 : 0.0;
   }
-  if (nslots > R_FIXED) {
-    // low-k momentum transform of the drag band filter (OOP/hit2d.py:352-399)
-    for (int m = 0; m < S.n_drag; ++m) {
-      const int2 md = S.modes[m];
-      double v[4] = {0, 0, 0, 0};
+  // low-k momentum transform of the drag band filter (OOP/hit2d.py:352-399):
+  // sum_y e^{-i ky y} m(x, y) over the thread's cells, then times e^{-i kx x}
+  for (int md = 0; md < ndrag; ++md) {
+    double cr0 = 0.0, ci0 = 0.0, cr1 = 0.0, ci1 = 0.0;
 #pragma unroll
-      for (int k = 0; k < kCellsPerThread; ++k) {
-        if (!valid[k]) continue;
-        const size_t o = (size_t)cj[k] * nx + ci[k];
-        const double m0 = q[o + plane], m1 = q[o + 2 * plane];
-        const double2 ex = S.twx[mode_index(md.x, ci[k], nx)], ey = S.twy[mode_index(md.y, cj[k], ny)];
-        const double2 e = make_double2(cmul_re(ex, ey), cmul_im(ex, ey));  // e^{-i theta}
-        v[0] += m0 * e.x;
-        v[1] += m0 * e.y;
-        v[2] += m1 * e.x;
-        v[3] += m1 * e.y;
-      }
-#pragma unroll
-      for (int k = 0; k < 4; ++k) warp_to_smem<OP_SUM>(v[k], sm, R_FIXED + 4 * m + k, nslots);
+    for (int k = 0; k < kPreRows; ++k) {
+      const double2 ey = tw[warp + kPreWarps * k][md];
+      cr0 += m0[k] * ey.x;
+      ci0 += m0[k] * ey.y;
+      cr1 += m1[k] * ey.x;
+      ci1 += m1[k] * ey.y;
     }
+    double v[4] = {0.0, 0.0, 0.0, 0.0};
+    if (gi < nx) {
+      const double2 ex = S.twx[mode_index(S.modes[md].x, gi, nx)];
+      v[0] = ex.x * cr0 - ex.y * ci0;
+      v[1] = ex.x * ci0 + ex.y * cr0;
+      v[2] = ex.x * cr1 - ex.y * ci1;
+      v[3] = ex.x * ci1 + ex.y * cr1;
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) warp_to_smem<OP_SUM>(v[k], sm, R_FIXED + 4 * md + k, nslots);
   }
   __syncthreads();
   for (int t = threadIdx.x; t < nslots; t += blockDim.x) {
     const int op = pre_op(t);
     double acc = sm[t];
-    for (int ww = 1; ww < kRedWarps; ++ww) {
+    for (int ww = 1; ww < kPreWarps; ++ww) {
       const double x = sm[ww * nslots + t];
       acc = op == OP_SUM ? acc + x : fmax(acc, x);
     }
@@ -279,8 +367,7 @@ __global__ void __launch_bounds__(kRedThreads, 2)
 
   // ---- last CTA of this solve: fixed-order final reduction + scalar logic ----
   {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int t = warp; t < nslots; t += kRedWarps) {
+    for (int t = warp; t < nslots; t += kPreWarps) {
       const int op = pre_op(t);
       double acc = op == OP_SUM ? 0.0 : -INFINITY;
 #pragma unroll 8
@@ -461,7 +548,10 @@ __global__ void noise_rng_kernel(const SolveDev* __restrict__ solves, int nsolve
 
 // Forcing synthesis: f_hat = (i ky phi, -i kx phi), fx = Re ifft2 (forcing.py:
 // 82-85) evaluated directly on the shell modes, plus the sums the rescaling
-// needs (forcing.py:87-118), then the scalar rescaling logic.
+// needs (forcing.py:87-118), then the scalar rescaling logic.  The synthesis
+// is separable: for each row y of the tile the modes are first folded into
+// P_k(y) = sum over modes with |kx| = k of c_m e^{i ky y} (conjugated for
+// kx < 0), so that a cell needs only Re sum_k P_k(y) e^{i k x}, k = 0..max|kx|.
 __global__ void __launch_bounds__(kRedThreads)
     force_synth_kernel(const SolveDev* __restrict__ solves, const Work* __restrict__ work,
                        Bind bind) {
@@ -471,11 +561,12 @@ __global__ void __launch_bounds__(kRedThreads)
   if (!S.forcing_on) return;
   if (!bind.use && sc[S_ACTIVE] == 0.0) return;
   const double* q = bind.use ? bind.qin : S.q;
-  const int nx = S.nx, ny = S.ny, nf = S.n_force;
+  const int nx = S.nx, ny = S.ny, nf = S.n_force, K = S.kx_force;
   const size_t plane = (size_t)nx * ny;
   const int2* modes = S.modes + S.n_drag;
   const double invN = 1.0 / ((double)nx * (double)ny);
   __shared__ double2 ca[kMaxForce], cb[kMaxForce];
+  __shared__ double2 px[kTileY][kMaxKx + 1], py[kTileY][kMaxKx + 1];
   __shared__ double sm[kRedWarps * 4];
   __shared__ double red[4];
   for (int m = threadIdx.x; m < nf; m += blockDim.x) {
@@ -485,20 +576,46 @@ __global__ void __launch_bounds__(kRedThreads)
     cb[m] = make_double2(kv.x * pi * invN, -kv.x * pr * invN);   // (-i kx phi)/N
   }
   __syncthreads();
-  const int tx = threadIdx.x & 31, ty0 = threadIdx.x >> 5;
-  double sxx = 0, syy = 0, sxy = 0, spow = 0;
-#pragma unroll
-  for (int k = 0; k < kCellsPerThread; ++k) {
-    const int gj = w.b + ty0 + kRedWarps * k, gi = w.a + tx;
-    if (gj >= ny || gi >= nx) continue;
-    double fx = 0.0, fy = 0.0;
+  for (int t = threadIdx.x; t < kTileY * (K + 1); t += blockDim.x) {
+    const int a = t / (K + 1), k = t - a * (K + 1);
+    const int gj = min(w.b + a, ny - 1);
+    double2 sx = make_double2(0.0, 0.0), sy = make_double2(0.0, 0.0);
     for (int m = 0; m < nf; ++m) {
       const int2 md = modes[m];
-      const double2 ex = S.twx[mode_index(md.x, gi, nx)], ey = S.twy[mode_index(md.y, gj, ny)];
-      // e^{+i theta} = conj(e^{-i theta})
-      const double er = cmul_re(ex, ey), ei = -cmul_im(ex, ey);
-      fx += ca[m].x * er - ca[m].y * ei;
-      fy += cb[m].x * er - cb[m].y * ei;
+      if (abs(md.x) != k) continue;
+      const double2 e = S.twy[mode_index(md.y, gj, ny)];  // e^{-i ky y}
+      const double er = e.x, ei = -e.y;                   // e^{+i ky y}
+      double ar = ca[m].x * er - ca[m].y * ei, ai = ca[m].x * ei + ca[m].y * er;
+      double br = cb[m].x * er - cb[m].y * ei, bi = cb[m].x * ei + cb[m].y * er;
+      if (md.x < 0) {
+        ai = -ai;
+        bi = -bi;
+      }
+      sx.x += ar;
+      sx.y += ai;
+      sy.x += br;
+      sy.y += bi;
+    }
+    px[a][k] = sx;
+    py[a][k] = sy;
+  }
+  __syncthreads();
+  const int tx = threadIdx.x & 31, ty0 = threadIdx.x >> 5;
+  const int gi = w.a + tx;
+  double sxx = 0, syy = 0, sxy = 0, spow = 0;
+#pragma unroll
+  for (int kk = 0; kk < kCellsPerThread; ++kk) {
+    const int a = ty0 + kRedWarps * kk, gj = w.b + a;
+    if (gj >= ny || gi >= nx) continue;
+    double fx = px[a][0].x, fy = py[a][0].x;
+    int ix = 0;
+    for (int k = 1; k <= K; ++k) {
+      ix += gi;
+      if (ix >= nx) ix -= nx;                 // (k x) mod nx
+      const double2 e = S.twx[ix];             // e^{-i k x}
+      const double er = e.x, ei = -e.y;       // e^{+i k x}
+      fx += px[a][k].x * er - px[a][k].y * ei;
+      fy += py[a][k].x * er - py[a][k].y * ei;
     }
     const size_t o = (size_t)gj * nx + gi;
     S.fx[o] = fx;

@@ -780,6 +780,39 @@ __global__ void __launch_bounds__(256, 2)
   double* qo = bind.use ? bind.qout : stage_out(S, stage);
   const T* ry = reinterpret_cast<const T*>(S.rx);
   const int gc = (mode == SW_STAGE && !per) ? S.guard : 0;
+  // drag band S = -c lowpass(m) (OOP/hit2d.py:352-399) of the CTA's rows:
+  // P_k(y) = sum over modes with |kx| = k of C_m e^{i ky y} (conjugated for
+  // kx < 0), C_m the mode's scaled transform from the prepass
+  __shared__ double2 dpx[2][kMaxKx + 1], dpy[2][kMaxKx + 1];
+  const bool drag = (terms & 8) && S.drag_on;
+  if (drag) {
+    const int K = S.kx_drag;
+    for (int t = threadIdx.x; t < R * (K + 1); t += blockDim.x) {
+      const int r = t / (K + 1), k = t - r * (K + 1);
+      const int row = line0 + r;
+      double2 sx = make_double2(0.0, 0.0), sy = make_double2(0.0, 0.0);
+      for (int md = 0; md < S.n_drag; ++md) {
+        const int2 km = S.modes[md];
+        if (abs(km.x) != k) continue;
+        const double2 e = S.twy[mode_index(km.y, row, ny)];
+        const double er = e.x, ei = -e.y;  // e^{+i ky y}
+        const double* cf = sc + S_DRAG + 4 * md;
+        double ar = cf[0] * er - cf[1] * ei, ai = cf[0] * ei + cf[1] * er;
+        double br = cf[2] * er - cf[3] * ei, bi = cf[2] * ei + cf[3] * er;
+        if (km.x < 0) {
+          ai = -ai;
+          bi = -bi;
+        }
+        sx.x += ar;
+        sx.y += ai;
+        sy.x += br;
+        sy.y += bi;
+      }
+      dpx[r][k] = sx;
+      dpy[r][k] = sy;
+    }
+    __syncthreads();
+  }
   double* ST = reinterpret_cast<double*>(smem);  // new rows (guard staging), reuses FQ
   for (int idx = threadIdx.x; idx < R * n; idx += blockDim.x) {
     const int r = idx >= n ? 1 : 0, col = idx - r * n, row = line0 + r;
@@ -804,19 +837,21 @@ __global__ void __launch_bounds__(256, 2)
         rhs[2] += double(rho * tfy);
         rhs[3] += double(rho * (u * tfx + vv * tfy));
       }
-      if ((terms & 8) && S.drag_on) {
-        T lx = T(0), ly = T(0);
-        for (int md = 0; md < S.n_drag; ++md) {
-          const int2 k = S.modes[md];
-          const double2 ex = S.twx[mode_index(k.x, col, nx)], ey = S.twy[mode_index(k.y, row, ny)];
-          const T er = T(cmul_re(ex, ey)), ei = T(-cmul_im(ex, ey));
-          const double* cf = sc + S_DRAG + 4 * md;
-          lx += T(cf[0]) * er - T(cf[1]) * ei;
-          ly += T(cf[2]) * er - T(cf[3]) * ei;
+      if (drag) {
+        // Re sum_k P_k(row) e^{i k x}: the drag band synthesised per row
+        double lx = dpx[r][0].x, ly = dpy[r][0].x;
+        int ix = 0;
+        for (int k = 1; k <= S.kx_drag; ++k) {
+          ix += col;
+          if (ix >= nx) ix -= nx;  // (k x) mod nx
+          const double2 e = S.twx[ix];
+          const double er = e.x, ei = -e.y;  // e^{+i k x}
+          lx += dpx[r][k].x * er - dpx[r][k].y * ei;
+          ly += dpy[r][k].x * er - dpy[r][k].y * ei;
         }
-        rhs[1] += double(lx);
-        rhs[2] += double(ly);
-        rhs[3] += double(T(pr.u) * lx + T(pr.v) * ly);
+        rhs[1] += lx;
+        rhs[2] += ly;
+        rhs[3] += pr.u * lx + pr.v * ly;
       }
     }
     if (terms & 16) rhs[3] += sc[S_COOL];
