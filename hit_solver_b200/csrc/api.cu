@@ -122,9 +122,9 @@ int guard_blocks_for(const hitb200_desc& d) {
   return (int)std::max(1L, std::min(64L, (band + 255) / 256));
 }
 
+// Sweep nodes per thread (128 threads per line).
 int mch_for(int n) {
-  const int m = (n + 31) / 32;
-  return m <= 4 ? 4 : m <= 8 ? 8 : m <= 16 ? 16 : 32;
+  return n <= 128 ? 1 : n <= 256 ? 2 : n <= 512 ? 4 : 8;
 }
 
 }  // namespace
@@ -157,7 +157,7 @@ struct hitb200_batch {
   SolveDev* d_solves = nullptr;
   Work *d_tiles = nullptr, *d_tiles32 = nullptr, *d_xlines = nullptr, *d_ylines = nullptr;
   int* d_partner = nullptr;
-  int n_tiles = 0, n_tiles32 = 0, n_x = 0, n_y = 0, elem = 8, mch_x = 4, mch_y = 4, guard_blocks = 1;
+  int n_tiles = 0, n_tiles32 = 0, n_x = 0, n_y = 0, elem = 8, mch_x = 1, mch_y = 1, guard_blocks = 1;
   int rx_max = 1, ry_max = 1;
   size_t smem_x = 0, smem_y = 0, smem_sensor = 0;
   int any_outflow = 0, any_forcing = 0, any_hv = 0, any_noise_upload = 0;
@@ -243,10 +243,10 @@ void launch_sweep_t(const LaunchSet& L, int stage, int mode, const Bind& b) {
     sweep_kernel<T, AXIS, M><<<nb, thr, sm, L.st>>>(L.solves, w, stage, mode, b);     \
     break;
   switch (mch) {
+    HB_SWEEP(1)
+    HB_SWEEP(2)
     HB_SWEEP(4)
     HB_SWEEP(8)
-    HB_SWEEP(16)
-    HB_SWEEP(32)
   }
 #undef HB_SWEEP
 }
@@ -393,7 +393,7 @@ void prime_attributes(int elem, int mch_x, int mch_y, size_t smem_x, size_t smem
     if (axis == 0) set_sweep_attr<T, 0, M>(bytes);                    \
     else set_sweep_attr<T, 1, M>(bytes);                              \
   }
-    HB_ATTR(4) HB_ATTR(8) HB_ATTR(16) HB_ATTR(32)
+    HB_ATTR(1) HB_ATTR(2) HB_ATTR(4) HB_ATTR(8)
 #undef HB_ATTR
   };
   if (elem == 4) {

@@ -329,17 +329,23 @@ __global__ void __launch_bounds__(kSensorThreads, 2)
 
 // =============================================================================
 // Line sweeps.  A CTA owns R whole grid lines (rows for x, columns for y) of
-// one solve and runs, in shared memory:
-//   L  stage the enforced state, normal velocity and pressure of every node
-//      of the lines plus a 5-node halo (periodic wrap or clamped edge);
-//   H  per component: the hybrid face flux (6-point compact flux, or the
-//      compactised WENO7 flux on flagged faces) by warps that each own 29
-//      consecutive nodes, exchanging neighbour faces by shuffles, and the
-//      face difference raw_i = (H_{i+1/2} - H_{i-1/2}) / h;
-//   S  the compact tridiagonal solve 3/8 d_{i-1} + d_i + 3/8 d_{i+1} = raw_i,
-//      one warp per (line, component), as two first-order recurrences
-//      (factorisation below) evaluated by a chunked warp scan;
-//   E  the fused epilogue (partial rhs for x; RK stage combine + clean for y).
+// one solve, 128 threads per line; thread t of a line owns the MN
+// consecutive nodes [t MN, t MN + MN) and keeps them in registers from the
+// face fluxes to the epilogue:
+//   L  stage the flux and enforced state of every node of the lines plus a
+//      halo (periodic wrap or clamped edge) in shared memory, and the mask;
+//   W  the WENO7 face fluxes that a flagged face needs, compacted by warp
+//      ballots over 32-face chunks;
+//   H  per component, the hybrid face fluxes of the thread's MN + 1 faces
+//      (6-point compact flux, or the compactised WENO7 flux on flagged
+//      faces) and raw_i = (H_{i+1/2} - H_{i-1/2}) / h of its nodes;
+//   S  the compact tridiagonal solve 3/8 d_{i-1} + d_i + 3/8 d_{i+1} = raw_i
+//      as two first-order recurrences (factorisation below): each thread runs
+//      them over its nodes, and a scan of the per-thread affine maps across
+//      the line (warp shuffles, then the line's 4 warps through shared
+//      memory) supplies each thread's carry-in;
+//   E  the fused epilogue (y: partial rhs -dG/dy; x: full rhs, sources, RK
+//      stage combine, clean filter and outflow guard).
 //
 // Factorisation: a s^-1 + 1 + a s = (-a/rho)(1 - rho s^-1)(1 - rho s) with
 // rho = (sqrt(1 - 4 a^2) - 1) / (2 a) = (sqrt(7) - 4) / 3 for a = 3/8, so
@@ -362,36 +368,26 @@ __device__ __forceinline__ T rho_pow(int k) {
   return (k >= 0 && k < kPowTab) ? T(__ldg(&g_rho_pow[k])) : T(0);
 }
 
-template <typename T>
-__host__ __device__ inline int pad_index(int i) {
-  return sizeof(T) == 4 ? i + (i >> 5) : i + (i >> 4);
-}
+constexpr int kSweepHalo = 8;  // staged nodes left of node 0 (WENO reads 5)
 
 // Shared memory of one sweep CTA holding R lines of n nodes:
-//   FQ  [R][8][LS]  flux F_c (c < 4) and enforced state Q_c (c >= 4) of every
-//                   node plus a 5-node halo on each side (LS = n + 10); reused
-//                   by the x-sweep epilogue for the new rows (FP64) when
-//                   guard cells are written
-//   WB  [R][4][LW]  WENO face fluxes W_{il+1/2}, il in [-2, n], of needed faces
-//   HB  [R][4][LW]  hybrid face fluxes H_{il+1/2}, il in [-1, n-1]
-//   RB  [R][4][LQ]  face differences raw_i, solved in place into d_i (padded
-//                   index so that the chunked solve reads without bank conflicts)
+//   FQ  [R][8][LS]  flux F_c (c < 4) and enforced state Q_c (c >= 4) of nodes
+//                   -8 .. LS - 9; node i at index i + 8 so that each
+//                   thread's nodes start on a 16-byte boundary.  Reused by
+//                   the x-sweep epilogue for the new rows (FP64) when guard
+//                   cells are written.
+//   WB  [R][4][LW]  WENO face fluxes W_{f+1/2}, f in [-2, n], of needed faces
 //   MK  [R][n + 2]  sensor mask of nodes -1 .. n
 template <typename T>
 struct SweepLayout {
-  int n, LS, LQ, LW, R;
+  int n, LS, LW, R;
   __host__ __device__ SweepLayout(int n_, int R_) : n(n_), R(R_) {
-    LS = n + 2 * kHalo;
-    LS = (LS + 1) & ~1;
-    LQ = pad_index<T>(n - 1) + 1;
-    LQ = (LQ + 3) & ~3;
+    LS = (kSweepHalo + n + 16 + 7) & ~7;
     LW = (n + 3 + 3) & ~3;
   }
   // byte offsets of the regions; the kernel and the host use the same ones
   __host__ __device__ size_t off_wb() const { return (size_t)R * 8 * LS * sizeof(T); }
-  __host__ __device__ size_t off_hb() const { return off_wb() + (size_t)R * 4 * LW * sizeof(T); }
-  __host__ __device__ size_t off_rb() const { return off_hb() + (size_t)R * 4 * LW * sizeof(T); }
-  __host__ __device__ size_t off_mk() const { return off_rb() + (size_t)R * 4 * LQ * sizeof(T); }
+  __host__ __device__ size_t off_mk() const { return off_wb() + (size_t)R * 4 * LW * sizeof(T); }
   __host__ __device__ size_t bytes() const {
     return (off_mk() + (size_t)R * (n + 2) + 15) & ~(size_t)15;
   }
@@ -431,134 +427,6 @@ __device__ __forceinline__ T weno_face(const T* F, const T* Q, int s, T alpha) {
          weno7(fm[7], fm[6], fm[5], fm[4], fm[3], fm[2], fm[1]);
 }
 
-// Warp-cooperative solve of one line held at line[pad(i)], i in [0, n).
-template <typename T, int MCH>
-__device__ __forceinline__ void line_solve(T* line, int n, int per) {
-  const int lane = threadIdx.x & 31;
-  const int m = (n + 31) >> 5;
-  const int start = lane * m;
-  const int len = max(0, min(m, n - start));
-  const T rho = T(kRhoSolve);
-  T x[MCH];
-  T rfirst = T(0), rlast = T(0);
-#pragma unroll
-  for (int k = 0; k < MCH; ++k) {
-    x[k] = (k < len) ? line[pad_index<T>(start + k)] : T(0);
-    if (k < len && start + k == n - 1) rlast = x[k];
-  }
-  rfirst = x[0];
-  // forward y_i = raw_i + rho y_{i-1}
-  T acc = T(0), M = T(1);
-#pragma unroll
-  for (int k = 0; k < MCH; ++k)
-    if (k < len) {
-      acc = x[k] + rho * acc;
-      x[k] = acc;
-      M *= rho;
-    }
-  T A = acc;
-#pragma unroll
-  for (int off = 1; off < 32; off <<= 1) {
-    const T Mo = __shfl_up_sync(kFull, M, off), Ao = __shfl_up_sync(kFull, A, off);
-    if (lane >= off) {
-      A = M * Ao + A;
-      M = M * Mo;
-    }
-  }
-  {
-    T Me = __shfl_up_sync(kFull, M, 1), Ae = __shfl_up_sync(kFull, A, 1);
-    if (lane == 0) {
-      Me = T(1);
-      Ae = T(0);
-    }
-    const T Mt = __shfl_sync(kFull, M, 31), At = __shfl_sync(kFull, A, 31);
-    const T yin = per ? Me * (At / (T(1) - Mt)) + Ae : Ae;
-    T pw = rho;
-#pragma unroll
-    for (int k = 0; k < MCH; ++k)
-      if (k < len) {
-        x[k] += pw * yin;
-        pw *= rho;
-      }
-  }
-  // backward z_i = y_i + rho z_{i+1}
-  acc = T(0);
-  M = T(1);
-#pragma unroll
-  for (int k = MCH - 1; k >= 0; --k)
-    if (k < len) {
-      acc = x[k] + rho * acc;
-      x[k] = acc;
-      M *= rho;
-    }
-  A = acc;
-#pragma unroll
-  for (int off = 1; off < 32; off <<= 1) {
-    const T Mo = __shfl_down_sync(kFull, M, off), Ao = __shfl_down_sync(kFull, A, off);
-    if (lane + off < 32) {
-      A = M * Ao + A;
-      M = M * Mo;
-    }
-  }
-  {
-    T Me = __shfl_down_sync(kFull, M, 1), Ae = __shfl_down_sync(kFull, A, 1);
-    if (lane == 31) {
-      Me = T(1);
-      Ae = T(0);
-    }
-    const T Mt = __shfl_sync(kFull, M, 0), At = __shfl_sync(kFull, A, 0);
-    const T zin = per ? Me * (At / (T(1) - Mt)) + Ae : Ae;
-    T pw = rho;
-#pragma unroll
-    for (int k = MCH - 1; k >= 0; --k)
-      if (k < len) {
-        x[k] = T(kSolveScale) * (x[k] + pw * zin);
-        pw *= rho;
-      }
-  }
-  if (!per) {
-    // identity end rows: d = p + A rho^i + B rho^(n-1-i)
-    const int llast = (n - 1) / m;
-    rfirst = __shfl_sync(kFull, rfirst, 0);
-    rlast = __shfl_sync(kFull, rlast, llast);
-    T plast = T(0);
-#pragma unroll
-    for (int k = 0; k < MCH; ++k)
-      if (k < len && start + k == n - 1) plast = x[k];
-    const T pfirst = __shfl_sync(kFull, x[0], 0);
-    plast = __shfl_sync(kFull, plast, llast);
-    if (n == 1) {
-      if (len > 0) x[0] = rfirst;
-    } else {
-      const T e = rho_pow<T>(n - 1);
-      const T r0 = rfirst - pfirst, r1 = rlast - plast;
-      const T den = T(1) - e * e;
-      const T ca = (r0 - e * r1) / den, cb = (r1 - e * r0) / den;
-      // the homogeneous terms are below roundoff beyond ~80 nodes from an end
-      if (len > 0 && (start < 96 || start + len > n - 96)) {
-        T pa = rho_pow<T>(start);
-        T pb = rho_pow<T>(n - start - len);
-        T pbk[MCH];
-#pragma unroll
-        for (int k = MCH - 1; k >= 0; --k)
-          if (k < len) {
-            pbk[k] = pb;
-            pb *= rho;
-          }
-#pragma unroll
-        for (int k = 0; k < MCH; ++k)
-          if (k < len) {
-            x[k] += ca * pa + cb * pbk[k];
-            pa *= rho;
-          }
-      }
-    }
-  }
-#pragma unroll
-  for (int k = 0; k < MCH; ++k)
-    if (k < len) line[pad_index<T>(start + k)] = x[k];
-}
-
 // Position of the j-th (0-based) set bit of `mask` (j < popc(mask)).
 __device__ __forceinline__ int nth_set_bit(unsigned mask, int j) {
   int pos = 0;
@@ -582,20 +450,57 @@ __device__ __forceinline__ int guard_src(int i, int n, int g) {
   return i < g ? g : (i > n - g - 1 ? n - g - 1 : i);
 }
 
+// Affine map y -> m y + a[c] of the recurrence over a run of nodes (one
+// multiplier for all four components, which share rho).
+template <typename T>
+struct Affine {
+  T m, a[4];
+};
+
+// Loads v[j] = row[base + j], j < N, from shared memory; 16-byte vector loads
+// when the start is aligned (always, for the thread layout of the sweep).
+template <typename T, int N>
+__device__ __forceinline__ void load_run(const T* row, int base, T (&v)[N]) {
+  constexpr int VEC = 16 / sizeof(T);
+  if constexpr (N % VEC == 0) {
+    if (((base * (int)sizeof(T)) & 15) == 0) {
+#pragma unroll
+      for (int j = 0; j < N; j += VEC) {
+        if constexpr (sizeof(T) == 4) {
+          const float4 f = *reinterpret_cast<const float4*>(row + base + j);
+          v[j] = f.x;
+          v[j + 1] = f.y;
+          v[j + 2] = f.z;
+          v[j + 3] = f.w;
+        } else {
+          const double2 f = *reinterpret_cast<const double2*>(row + base + j);
+          v[j] = f.x;
+          v[j + 1] = f.y;
+        }
+      }
+      return;
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < N; ++j) v[j] = row[base + j];
+}
+
 // One sweep of the split RHS over R whole grid lines (rows for AXIS 0, columns
-// for AXIS 1), 128 threads per line.  The y sweep runs first and leaves
-// -dG/dy in the partial-rhs buffer; the x sweep runs second and, in mode
-// SW_STAGE, finishes the stage:
+// for AXIS 1), 128 threads per line, MN nodes per thread.  The y sweep runs
+// first and leaves -dG/dy in the partial-rhs buffer; the x sweep runs second
+// and, in mode SW_STAGE, finishes the stage:
 //   stage 0: q1 = clean(q + dt L)
 //   stage 1: q2 = clean(3/4 q + 1/4 (q1 + dt L))
 //   stage 2:      clean(1/3 q + 2/3 (q2 + dt L))     (OOP/time_operator.py:21-26)
 // with L = -dF/dx - dG/dy + viscous + forcing + drag + cooling and clean the
 // enforce filter plus, on outflow grids, the guard cells.
-template <typename T, int AXIS, int MCH>
+template <typename T, int AXIS, int MN>
 __global__ void __launch_bounds__(256, 2)
     sweep_kernel(const SolveDev* __restrict__ solves, const Work* __restrict__ work, int stage,
                  int mode, Bind bind) {
   extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ Affine<T> scan_f[2][4], scan_b[2][4];  // per line, per warp totals
+  __shared__ T ends[2][4][4];                          // raw_0, raw_n-1, p_0, p_n-1
   const Work wk = work[blockIdx.x];
   const SolveDev& S = solves[wk.solve];
   const double* sc = S.scal;
@@ -607,7 +512,7 @@ __global__ void __launch_bounds__(256, 2)
   const int rsh = R > 1 ? 1 : 0;  // R is 1 or 2
   const int RL = 1 << rsh;
   const SweepLayout<T> L(n, RL);
-  const int LS = L.LS, LQ = L.LQ, LW = L.LW;
+  const int LS = L.LS, LW = L.LW;
   const T g = T(S.gamma);
   const double h = AXIS == 0 ? S.dx : S.dy;
   const double* qin = bind.use ? bind.qin : stage_in(S, stage);
@@ -615,8 +520,6 @@ __global__ void __launch_bounds__(256, 2)
   const T alpha = T(AXIS == 0 ? sc[S_ALPHA_X] : sc[S_ALPHA_Y]);
   T* FQ = reinterpret_cast<T*>(smem);
   T* WB = reinterpret_cast<T*>(smem + L.off_wb());
-  T* HB = reinterpret_cast<T*>(smem + L.off_hb());
-  T* RB = reinterpret_cast<T*>(smem + L.off_rb());
   uint8_t* MK = smem + L.off_mk();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
 
@@ -634,7 +537,7 @@ __global__ void __launch_bounds__(256, 2)
       p = idx >> rsh;
       if (r >= R) continue;
     }
-    const int gp = fold_node(p - kHalo, n, per);
+    const int gp = fold_node(p - kSweepHalo, n, per);
     const size_t o = AXIS == 0 ? (size_t)(line0 + r) * nx + gp : (size_t)gp * nx + line0 + r;
     T a0 = T(qin[o]), a1 = T(qin[o + plane]), a2 = T(qin[o + 2 * plane]), a3 = T(qin[o + 3 * plane]);
     // enforce_physical_state, then primitive_from_conservative of the result
@@ -684,7 +587,7 @@ __global__ void __launch_bounds__(256, 2)
     return f >= -1 && f <= n - 1 && (mk[f] | mk[f + 1]);
   };
 
-  // ---- H1: WENO fluxes where a flagged face needs them ---------------------------
+  // ---- W: WENO fluxes where a flagged face needs them ----------------------------
   // Warp task = 32 consecutive faces of one line; the faces that need W (a
   // flagged face among itself and its neighbours) are found by ballot and
   // their (face, component) pairs are spread over the warp's lanes.
@@ -699,76 +602,267 @@ __global__ void __launch_bounds__(256, 2)
     const int items = 4 * __popc(bal);
     for (int k = lane; k < items; k += 32) {
       const int c = k & 3, f = il0 + nth_set_bit(bal, k >> 2);
-      const T* F = FQ + (size_t)(r * 8 + c) * LS + kHalo;
-      const T* Q = FQ + (size_t)(r * 8 + 4 + c) * LS + kHalo;
+      const T* F = FQ + (size_t)(r * 8 + c) * LS + kSweepHalo;
+      const T* Q = FQ + (size_t)(r * 8 + 4 + c) * LS + kSweepHalo;
       const int fe = per ? f : min(max(f, -1), n - 1);
       WB[(size_t)(r * 4 + c) * LW + f + 2] = weno_face<T>(F, Q, fe, alpha);
     }
   }
   __syncthreads();
 
-  // ---- H2: hybrid face fluxes, then raw_i = (H_{i+1/2} - H_{i-1/2}) / h -----------
-  const int nf = R * 4 * (n + 1);
-  for (int idx = threadIdx.x; idx < nf; idx += blockDim.x) {
-    int rc = 0, f = idx;
-    while (f >= n + 1) {
-      f -= n + 1;
-      ++rc;
-    }
-    const int il = f - 1, r = rc >> 2, c = rc & 3;
-    const uint8_t* mk = MK + r * (n + 2) + 1;
-    T hf;
-    if (flagged(mk, il)) {
-      const T* Wc = WB + (size_t)rc * LW + 2;
-      hf = T(kCompactA) * Wc[il + 1] + Wc[il];
-      hf = hf + T(kCompactA) * Wc[il - 1];
-    } else {
-      hf = compact_face<T>(FQ + (size_t)(r * 8 + c) * LS + kHalo, il);
-    }
-    HB[(size_t)rc * LW + f] = hf;  // HB[il + 1]
-  }
-  __syncthreads();
+  // ---- H: this thread's faces and raw differences, in registers ------------------
+  const int r = threadIdx.x >> 7;         // line of the CTA
+  const int tl = threadIdx.x & 127;       // thread within the line
+  const int lw = tl >> 5;                 // warp within the line
+  const int i0 = tl * MN;                 // first node
+  const int len = r < R ? max(0, min(MN, n - i0)) : 0;
   const T inv_h = T(1.0 / h);
-  const int nr = R * 4 * n;
-  for (int idx = threadIdx.x; idx < nr; idx += blockDim.x) {
-    int rc = 0, i = idx;
-    while (i >= n) {
-      i -= n;
-      ++rc;
+  const T rho = T(kRhoSolve);
+  T x[4][MN];
+  bool fl[MN + 1];
+  {
+    const uint8_t* mk = MK + min(r, R - 1) * (n + 2) + 1;
+#pragma unroll
+    for (int j = 0; j <= MN; ++j) {
+      const int f = i0 - 1 + j;  // face f + 1/2
+      fl[j] = len > 0 && f <= n - 1 && flagged(mk, f);
     }
-    const T* H = HB + (size_t)rc * LW;
-    RB[(size_t)rc * LQ + pad_index<T>(i)] = (H[i + 1] - H[i]) * inv_h;
+  }
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    T H[MN + 1];
+    if (len > 0) {
+      T fv[MN + 8];  // F_c of nodes i0 - 4 .. i0 + MN + 3
+      load_run<T, MN + 8>(FQ + (size_t)(r * 8 + c) * LS, kSweepHalo + i0 - 4, fv);
+      const T* Wc = WB + (size_t)(r * 4 + c) * LW + 2;
+#pragma unroll
+      for (int j = 0; j <= MN; ++j) {
+        if (fl[j]) {
+          const int f = i0 - 1 + j;
+          T hf = T(kCompactA) * Wc[f + 1] + Wc[f];
+          H[j] = hf + T(kCompactA) * Wc[f - 1];
+        } else {
+          // 6-point compact flux of face i0 - 1 + j (OOP/spatial_operator.py:179-189)
+          H[j] = T(-1.0 / 480.0) * (fv[j + 6] + fv[j + 1]) + T(kB1C1) * (fv[j + 5] + fv[j + 2]) +
+                 T(kA1B1C1) * (fv[j + 4] + fv[j + 3]);
+        }
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < MN; ++k) x[c][k] = (k < len) ? (H[k + 1] - H[k]) * inv_h : T(0);
+  }
+
+  // ---- S: forward recurrence y_i = raw_i + rho y_{i-1} ------------------------------
+  T raw0[4], rawl[4];
+  const int owner_last = (n - 1) / MN, k_last = (n - 1) - owner_last * MN;
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    raw0[c] = x[c][0];
+    T v = T(0);
+#pragma unroll
+    for (int k = 0; k < MN; ++k)
+      if (k == k_last) v = x[c][k];
+    rawl[c] = v;
+  }
+  Affine<T> fw;
+  fw.m = T(1);
+#pragma unroll
+  for (int c = 0; c < 4; ++c) fw.a[c] = T(0);
+#pragma unroll
+  for (int k = 0; k < MN; ++k)
+    if (k < len) {
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        fw.a[c] = x[c][k] + rho * fw.a[c];
+        x[c][k] = fw.a[c];
+      }
+      fw.m *= rho;
+    }
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const T mo = __shfl_up_sync(kFull, fw.m, off);
+    T ao[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) ao[c] = __shfl_up_sync(kFull, fw.a[c], off);
+    if (lane >= off) {
+#pragma unroll
+      for (int c = 0; c < 4; ++c) fw.a[c] = fw.m * ao[c] + fw.a[c];
+      fw.m *= mo;
+    }
+  }
+  if (lane == 31 && r < 2) scan_f[r][lw] = fw;
+  // exclusive prefix within the warp
+  Affine<T> fe;
+  fe.m = __shfl_up_sync(kFull, fw.m, 1);
+#pragma unroll
+  for (int c = 0; c < 4; ++c) fe.a[c] = __shfl_up_sync(kFull, fw.a[c], 1);
+  if (lane == 0) {
+    fe.m = T(1);
+#pragma unroll
+    for (int c = 0; c < 4; ++c) fe.a[c] = T(0);
   }
   __syncthreads();
+  {
+    const int rr = min(r, 1);
+    Affine<T> pre, tot;  // maps of the warps before this one, and of the whole line
+    pre.m = tot.m = T(1);
+#pragma unroll
+    for (int c = 0; c < 4; ++c) pre.a[c] = tot.a[c] = T(0);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const Affine<T> wj = scan_f[rr][j];
+      if (j < lw) {
+#pragma unroll
+        for (int c = 0; c < 4; ++c) pre.a[c] = wj.m * pre.a[c] + wj.a[c];
+        pre.m *= wj.m;
+      }
+#pragma unroll
+      for (int c = 0; c < 4; ++c) tot.a[c] = wj.m * tot.a[c] + wj.a[c];
+      tot.m *= wj.m;
+    }
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      // periodic: y_{-1} = y_{n-1} closes the cycle exactly
+      const T ybnd = per ? tot.a[c] / (T(1) - tot.m) : T(0);
+      const T yin = fe.m * (pre.m * ybnd + pre.a[c]) + fe.a[c];
+      T pw = rho;
+#pragma unroll
+      for (int k = 0; k < MN; ++k)
+        if (k < len) {
+          x[c][k] += pw * yin;
+          pw *= rho;
+        }
+    }
+  }
 
-  // ---- S: compact solves -------------------------------------------------------------
-  for (int item = warp; item < 4 * R; item += nwarp)
-    line_solve<T, MCH>(RB + (size_t)item * LQ, n, per);
+  // ---- S: backward recurrence z_i = y_i + rho z_{i+1} -------------------------------
+  Affine<T> bw;
+  bw.m = T(1);
+#pragma unroll
+  for (int c = 0; c < 4; ++c) bw.a[c] = T(0);
+#pragma unroll
+  for (int k = MN - 1; k >= 0; --k)
+    if (k < len) {
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        bw.a[c] = x[c][k] + rho * bw.a[c];
+        x[c][k] = bw.a[c];
+      }
+      bw.m *= rho;
+    }
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const T mo = __shfl_down_sync(kFull, bw.m, off);
+    T ao[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) ao[c] = __shfl_down_sync(kFull, bw.a[c], off);
+    if (lane + off < 32) {
+#pragma unroll
+      for (int c = 0; c < 4; ++c) bw.a[c] = bw.m * ao[c] + bw.a[c];
+      bw.m *= mo;
+    }
+  }
+  if (lane == 0 && r < 2) scan_b[r][lw] = bw;
+  Affine<T> be;
+  be.m = __shfl_down_sync(kFull, bw.m, 1);
+#pragma unroll
+  for (int c = 0; c < 4; ++c) be.a[c] = __shfl_down_sync(kFull, bw.a[c], 1);
+  if (lane == 31) {
+    be.m = T(1);
+#pragma unroll
+    for (int c = 0; c < 4; ++c) be.a[c] = T(0);
+  }
   __syncthreads();
+  {
+    const int rr = min(r, 1);
+    Affine<T> post, tot;  // maps of the warps after this one (innermost last), whole line
+    post.m = tot.m = T(1);
+#pragma unroll
+    for (int c = 0; c < 4; ++c) post.a[c] = tot.a[c] = T(0);
+#pragma unroll
+    for (int j = 3; j >= 0; --j) {
+      const Affine<T> wj = scan_b[rr][j];
+      if (j > lw) {
+#pragma unroll
+        for (int c = 0; c < 4; ++c) post.a[c] = wj.m * post.a[c] + wj.a[c];
+        post.m *= wj.m;
+      }
+#pragma unroll
+      for (int c = 0; c < 4; ++c) tot.a[c] = wj.m * tot.a[c] + wj.a[c];
+      tot.m *= wj.m;
+    }
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      const T zbnd = per ? tot.a[c] / (T(1) - tot.m) : T(0);
+      const T zin = be.m * (post.m * zbnd + post.a[c]) + be.a[c];
+      T pw = rho;
+#pragma unroll
+      for (int k = MN - 1; k >= 0; --k)
+        if (k < len) {
+          x[c][k] = T(kSolveScale) * (x[c][k] + pw * zin);
+          pw *= rho;
+        }
+    }
+  }
+
+  if (!per) {
+    // identity end rows (riemann_config3.py:244-264): d = p + A rho^i + B rho^(n-1-i)
+    if (len > 0 && tl == 0) {
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        ends[r][c][0] = raw0[c];
+        ends[r][c][2] = x[c][0];
+      }
+    }
+    if (len > 0 && tl == owner_last) {
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        T pl = T(0);
+#pragma unroll
+        for (int k = 0; k < MN; ++k)
+          if (k == k_last) pl = x[c][k];
+        ends[r][c][1] = rawl[c];
+        ends[r][c][3] = pl;
+      }
+    }
+    __syncthreads();
+    // the homogeneous terms are below roundoff beyond ~80 nodes from an end
+    if (len > 0 && (i0 < 96 || i0 + len > n - 96)) {
+      if (n == 1) {
+        x[0][0] = ends[r][0][0];
+        x[1][0] = ends[r][1][0];
+        x[2][0] = ends[r][2][0];
+        x[3][0] = ends[r][3][0];
+      } else {
+        const T e = rho_pow<T>(n - 1);
+        const T den = T(1) - e * e;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+          const T r0 = ends[r][c][0] - ends[r][c][2], r1 = ends[r][c][1] - ends[r][c][3];
+          const T ca = (r0 - e * r1) / den, cb = (r1 - e * r0) / den;
+#pragma unroll
+          for (int k = 0; k < MN; ++k)
+            if (k < len) x[c][k] += ca * rho_pow<T>(i0 + k) + cb * rho_pow<T>(n - 1 - i0 - k);
+        }
+      }
+    }
+  }
 
   // ---- E: epilogue ----------------------------------------------------------------------
   const int terms = bind.use ? bind.terms : fused_terms(S);
   if (AXIS == 1 || mode == SW_DERIV) {
     // y sweep: partial rhs -dG/dy (or the bare derivative for the API)
-    const int ne = AXIS == 0 ? R * n : (n << rsh);
     T* rx = reinterpret_cast<T*>(S.rx);
-    for (int idx = threadIdx.x; idx < ne; idx += blockDim.x) {
-      int r, p;
-      if (AXIS == 0) {
-        r = idx >= n ? 1 : 0;
-        p = idx - r * n;
-      } else {
-        r = idx & (RL - 1);
-        p = idx >> rsh;
-        if (r >= R) continue;
-      }
+#pragma unroll
+    for (int k = 0; k < MN; ++k) {
+      if (k >= len) continue;
+      const int p = i0 + k;
       const int row = AXIS == 0 ? line0 + r : p, col = AXIS == 0 ? p : line0 + r;
       const size_t o = (size_t)row * nx + col;
-      const T* dl = RB + (size_t)r * 4 * LQ + pad_index<T>(p);
 #pragma unroll
       for (int c = 0; c < 4; ++c) {
-        if (mode == SW_DERIV) bind.out[c * plane + o] = double(dl[c * LQ]);
-        else rx[c * plane + o] = (terms & 1) ? -dl[c * LQ] : T(0);
+        if (mode == SW_DERIV) bind.out[c * plane + o] = double(x[c][k]);
+        else rx[c * plane + o] = (terms & 1) ? -x[c][k] : T(0);
       }
     }
     return;
@@ -788,8 +882,8 @@ __global__ void __launch_bounds__(256, 2)
   if (drag) {
     const int K = S.kx_drag;
     for (int t = threadIdx.x; t < R * (K + 1); t += blockDim.x) {
-      const int r = t / (K + 1), k = t - r * (K + 1);
-      const int row = line0 + r;
+      const int rr = t / (K + 1), k = t - rr * (K + 1);
+      const int row = line0 + rr;
       double2 sx = make_double2(0.0, 0.0), sy = make_double2(0.0, 0.0);
       for (int md = 0; md < S.n_drag; ++md) {
         const int2 km = S.modes[md];
@@ -808,19 +902,20 @@ __global__ void __launch_bounds__(256, 2)
         sy.x += br;
         sy.y += bi;
       }
-      dpx[r][k] = sx;
-      dpy[r][k] = sy;
+      dpx[rr][k] = sx;
+      dpy[rr][k] = sy;
     }
-    __syncthreads();
   }
+  if (drag || gc) __syncthreads();  // drag table ready; FQ free for the guard staging
   double* ST = reinterpret_cast<double*>(smem);  // new rows (guard staging), reuses FQ
-  for (int idx = threadIdx.x; idx < R * n; idx += blockDim.x) {
-    const int r = idx >= n ? 1 : 0, col = idx - r * n, row = line0 + r;
+#pragma unroll
+  for (int k = 0; k < MN; ++k) {
+    if (k >= len) continue;
+    const int col = i0 + k, row = line0 + r;
     const size_t o = (size_t)row * nx + col;
-    const T* dl = RB + (size_t)r * 4 * LQ + pad_index<T>(col);
     double rhs[4];
 #pragma unroll
-    for (int c = 0; c < 4; ++c) rhs[c] = double(ry[c * plane + o]) - ((terms & 1) ? double(dl[c * LQ]) : 0.0);
+    for (int c = 0; c < 4; ++c) rhs[c] = double(ry[c * plane + o]) - ((terms & 1) ? double(x[c][k]) : 0.0);
     if ((terms & 2) && S.mu > 0.0) {
       const T* vis = reinterpret_cast<const T*>(S.vis);
       rhs[1] += double(vis[o]);
@@ -832,22 +927,22 @@ __global__ void __launch_bounds__(256, 2)
       if (terms & 4) {
         const double fxv = bind.use ? bind.fx[o] : fs * S.fx[o];
         const double fyv = bind.use ? bind.fy[o] : fs * S.fy[o];
-        const T rho = T(pr.rho), u = T(pr.u), vv = T(pr.v), tfx = T(fxv), tfy = T(fyv);
-        rhs[1] += double(rho * tfx);
-        rhs[2] += double(rho * tfy);
-        rhs[3] += double(rho * (u * tfx + vv * tfy));
+        const T rho_ = T(pr.rho), u = T(pr.u), vv = T(pr.v), tfx = T(fxv), tfy = T(fyv);
+        rhs[1] += double(rho_ * tfx);
+        rhs[2] += double(rho_ * tfy);
+        rhs[3] += double(rho_ * (u * tfx + vv * tfy));
       }
       if (drag) {
         // Re sum_k P_k(row) e^{i k x}: the drag band synthesised per row
         double lx = dpx[r][0].x, ly = dpy[r][0].x;
         int ix = 0;
-        for (int k = 1; k <= S.kx_drag; ++k) {
+        for (int kk = 1; kk <= S.kx_drag; ++kk) {
           ix += col;
           if (ix >= nx) ix -= nx;  // (k x) mod nx
           const double2 e = S.twx[ix];
           const double er = e.x, ei = -e.y;  // e^{+i k x}
-          lx += dpx[r][k].x * er - dpx[r][k].y * ei;
-          ly += dpy[r][k].x * er - dpy[r][k].y * ei;
+          lx += dpx[r][kk].x * er - dpx[r][kk].y * ei;
+          ly += dpy[r][kk].x * er - dpy[r][kk].y * ei;
         }
         rhs[1] += lx;
         rhs[2] += ly;
@@ -868,7 +963,7 @@ __global__ void __launch_bounds__(256, 2)
       else if (stage == 1) sv[c] = 0.75 * q0[c * plane + o] + 0.25 * t;
       else sv[c] = (1.0 / 3.0) * q0[c * plane + o] + (2.0 / 3.0) * t;
     }
-    enforce_node_rcp(sv[0], sv[1], sv[2], sv[3], S.gamma);
+    enforce_node(sv[0], sv[1], sv[2], sv[3], S.gamma);
     if (gc == 0) {
 #pragma unroll
       for (int c = 0; c < 4; ++c) qo[c * plane + o] = sv[c];
@@ -881,8 +976,8 @@ __global__ void __launch_bounds__(256, 2)
   // Outflow guard fused: every row j takes row J(j) = clamp(j, g, ny-g-1) and
   // every column i column I(i); the CTA owning row J(j) writes row j.
   __syncthreads();
-  for (int r = 0; r < R; ++r) {
-    const int j0 = line0 + r;
+  for (int rr = 0; rr < R; ++rr) {
+    const int j0 = line0 + rr;
     if (j0 != guard_src(j0, ny, gc)) continue;  // a guard row: written by its source
     const int jlo = j0 == gc ? 0 : j0, jhi = j0 == ny - gc - 1 ? ny - 1 : j0;
     const int cnt = (jhi - jlo + 1) * nx;
@@ -891,7 +986,7 @@ __global__ void __launch_bounds__(256, 2)
       const size_t o = (size_t)(jlo + jj) * nx + i;
       const int si = guard_src(i, nx, gc);
 #pragma unroll
-      for (int c = 0; c < 4; ++c) qo[c * plane + o] = ST[(size_t)(r * 4 + c) * n + si];
+      for (int c = 0; c < 4; ++c) qo[c * plane + o] = ST[(size_t)(rr * 4 + c) * n + si];
     }
   }
 }
