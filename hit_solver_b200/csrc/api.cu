@@ -572,7 +572,7 @@ int hitb200_plan_create(const hitb200_desc* d, hitb200_plan** out) {
   p->n_y = (nx + p->Ry - 1) / p->Ry;
   p->smem_x = p->elem == 4 ? SweepLayout<float>(nx, p->Rx).bytes() : SweepLayout<double>(nx, p->Rx).bytes();
   p->smem_y = p->elem == 4 ? SweepLayout<float>(ny, p->Ry).bytes() : SweepLayout<double>(ny, p->Ry).bytes();
-  p->smem_sensor = sensor_smem_bytes(d->sensor_width, p->elem);
+  p->smem_sensor = sensor_smem_bytes(d->sensor_width, p->elem, d->viscosity > 0.0);
   if (p->smem_x > kSweepSmemMax || p->smem_y > kSweepSmemMax) {
     delete p;
     return (g_last_error = "grid lines too long for the sweep's shared memory", HITB200_ERR_UNSUPPORTED);

@@ -74,7 +74,10 @@ __device__ __forceinline__ bool curv_gt(T am, T a, T ap, T eps, T thr, T tol, bo
 
 __host__ __device__ inline int sensor_halo(int width) { return width + 1 > 2 ? width + 1 : 2; }
 
-__host__ __device__ inline size_t sensor_smem_bytes(int width, int elem) {
+// Viscous stage: stresses and energy fluxes of the tile plus a one-node ring.
+constexpr int kVisX = kSenTX + 2, kVisY = kSenTY + 2;
+
+__host__ __device__ inline size_t sensor_flag_end(int width, int elem) {
   const int hw = sensor_halo(width);
   const size_t sx = kSenTX + 2 * hw, sy = kSenTY + 2 * hw;
   const size_t prim = 5 * sx * sy * (size_t)elem;
@@ -82,7 +85,13 @@ __host__ __device__ inline size_t sensor_smem_bytes(int width, int elem) {
   const size_t raw = ry * rx;
   const size_t row = ry * kSenTX;
   const size_t edges = ry * (rx + 1) + (ry + 1) * rx;
-  return prim + raw + row + edges + 32;
+  return (prim + raw + row + edges + 32 + 15) & ~(size_t)15;
+}
+
+// Dynamic shared memory of the sensor kernel; `viscous` adds the five
+// stress / flux arrays of the viscous terms.
+__host__ __device__ inline size_t sensor_smem_bytes(int width, int elem, bool viscous) {
+  return sensor_flag_end(width, elem) + (viscous ? 5 * (size_t)kVisX * kVisY * elem : 0);
 }
 
 // Central difference quotient of the sensor.  FP64 divides by 2h exactly as
@@ -289,37 +298,46 @@ __global__ void __launch_bounds__(kSensorThreads, 2)
   (void)near_any;
 
   if (!want_visc || S.mu == 0.0) return;
-  // viscous stress and heat-flux divergence, central differences (periodic)
+  // viscous stress and heat-flux divergence (OOP/equations.py:232-267), as the
+  // reference evaluates it: velocity / temperature gradients, then stresses
+  // and energy fluxes at every node of the tile plus a one-node ring, then
+  // their central differences.
   const T mu = T(S.mu), kap = T(S.kappa), rgas = T(S.gas_r);
   const T two3 = T(2.0 / 3.0);
+  T* TXX = reinterpret_cast<T*>(smem + sensor_flag_end(W, (int)sizeof(T)));
+  T* TYY = TXX + kVisX * kVisY;
+  T* TXY = TYY + kVisX * kVisY;
+  T* QX = TXY + kVisX * kVisY;
+  T* QY = QX + kVisX * kVisY;
+  __syncthreads();  // E (internal energy) is free: the mask is complete
+  for (int idx = threadIdx.x; idx < SX * SY; idx += blockDim.x) E[idx] = P[idx] / (RHO[idx] * rgas);
+  __syncthreads();
+  const float ivx = 1.0f / (float)kVisX;
+  for (int idx = threadIdx.x; idx < kVisX * kVisY; idx += blockDim.x) {
+    const int a = row_of(idx, kVisX, ivx), b = idx - a * kVisX;
+    const int c = (a + HW - 1) * SX + (b + HW - 1);
+    const T ux = dq(U[c + 1], U[c - 1], tdx, itdx), vx = dq(V[c + 1], V[c - 1], tdx, itdx);
+    const T uy = dq(U[c + SX], U[c - SX], tdy, itdy), vy = dq(V[c + SX], V[c - SX], tdy, itdy);
+    const T dv = ux + vy;
+    const T txx = T(2) * mu * ux - two3 * mu * dv;
+    const T tyy = T(2) * mu * vy - two3 * mu * dv;
+    const T txy = mu * (uy + vx);
+    const T tx_ = dq(E[c + 1], E[c - 1], tdx, itdx), ty_ = dq(E[c + SX], E[c - SX], tdy, itdy);
+    TXX[idx] = txx;
+    TYY[idx] = tyy;
+    TXY[idx] = txy;
+    QX[idx] = U[c] * txx + V[c] * txy + kap * tx_;
+    QY[idx] = U[c] * txy + V[c] * tyy + kap * ty_;
+  }
+  __syncthreads();
   T* visp = reinterpret_cast<T*>(S.vis);
   for (int a = ty; a < kSenTY; a += nty) {
     const int gj = y0 + a, gi = x0 + tx;
     if (gj >= ny || gi >= nx) continue;
-    const int c = (a + HW) * SX + tx + HW;
-    auto ddx = [&](const T* f, int o) { return (f[o + 1] - f[o - 1]) / tdx; };
-    auto ddy = [&](const T* f, int o) { return (f[o + SX] - f[o - SX]) / tdy; };
-    auto temp = [&](int o) { return P[o] / (RHO[o] * rgas); };
-    auto txx = [&](int o) {
-      const T ux = ddx(U, o);
-      return T(2) * mu * ux - two3 * mu * (ux + ddy(V, o));
-    };
-    auto tyy = [&](int o) {
-      const T vy = ddy(V, o);
-      return T(2) * mu * vy - two3 * mu * (ddx(U, o) + vy);
-    };
-    auto txy = [&](int o) { return mu * (ddy(U, o) + ddx(V, o)); };
-    auto efx = [&](int o) {
-      const T dtx = (temp(o + 1) - temp(o - 1)) / tdx;
-      return U[o] * txx(o) + V[o] * txy(o) + kap * dtx;
-    };
-    auto efy = [&](int o) {
-      const T dty = (temp(o + SX) - temp(o - SX)) / tdy;
-      return U[o] * txy(o) + V[o] * tyy(o) + kap * dty;
-    };
-    const T r1 = (txx(c + 1) - txx(c - 1)) / tdx + (txy(c + SX) - txy(c - SX)) / tdy;
-    const T r2 = (txy(c + 1) - txy(c - 1)) / tdx + (tyy(c + SX) - tyy(c - SX)) / tdy;
-    const T r3 = (efx(c + 1) - efx(c - 1)) / tdx + (efy(c + SX) - efy(c - SX)) / tdy;
+    const int i = (a + 1) * kVisX + tx + 1;
+    const T r1 = dq(TXX[i + 1], TXX[i - 1], tdx, itdx) + dq(TXY[i + kVisX], TXY[i - kVisX], tdy, itdy);
+    const T r2 = dq(TXY[i + 1], TXY[i - 1], tdx, itdx) + dq(TYY[i + kVisX], TYY[i - kVisX], tdy, itdy);
+    const T r3 = dq(QX[i + 1], QX[i - 1], tdx, itdx) + dq(QY[i + kVisX], QY[i - kVisX], tdy, itdy);
     const size_t o = (size_t)gj * nx + gi;
     visp[o] = r1;
     visp[plane + o] = r2;
