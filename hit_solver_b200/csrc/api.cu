@@ -551,8 +551,8 @@ int hitb200_plan_create(const hitb200_desc* d, hitb200_plan** out) {
   if (d->forcing_on && mt.force.empty()) return invalid("forcing shell contains no Fourier modes on this grid");
   for (const std::vector<int2>* v : {&mt.drag, &mt.force})
     for (const int2& m : *v)
-      if (std::abs(m.x) > kMaxKx)
-        return (g_last_error = "drag / forcing modes beyond |kx| = 16 grid bins are not supported",
+      if (std::abs(m.x) > kMaxKx || (v == &mt.drag && std::abs(m.y) > kMaxKyDrag))
+        return (g_last_error = "drag / forcing modes beyond |kx| = 16 (drag |ky| = 4) grid bins are not supported",
                 HITB200_ERR_UNSUPPORTED);
 
   hitb200_plan* p = new hitb200_plan();
@@ -648,6 +648,8 @@ int hitb200_plan_create(const hitb200_desc* d, hitb200_plan** out) {
   s.n_force = (int)mt.force.size();
   s.kx_drag = s.kx_force = 0;
   for (const int2& m : mt.drag) s.kx_drag = std::max(s.kx_drag, std::abs(m.x));
+  s.ky_drag = 0;
+  for (const int2& m : mt.drag) s.ky_drag = std::max(s.ky_drag, std::abs(m.y));
   for (const int2& m : mt.force) s.kx_force = std::max(s.kx_force, std::abs(m.x));
   s.f_tau = d->forcing_correlation_time;
   s.f_rms = d->forcing_rms;

@@ -25,6 +25,7 @@ constexpr int kMaxDrag = 32;          // max drag modes (|k| <= kmax band)
 constexpr int kMaxForce = 128;        // max forcing shell modes
 constexpr int kMaxWidth = 8;          // max sensor dilation width
 constexpr int kMaxKx = 16;            // max |x wavenumber bin| of drag / forcing modes
+constexpr int kMaxKyDrag = 4;         // max |y wavenumber bin| of drag modes
 
 // ---- reduction slots of the per-stage prepass -------------------------------
 enum Red : int {
@@ -85,6 +86,7 @@ struct SolveDev {
   // sources
   int drag_on, n_drag;
   int kx_drag, kx_force;  // max |x bin| of the drag / forcing modes
+  int ky_drag;            // max |y bin| of the drag modes
   double drag_coef;
   int cooling_on;
   double cooling_tau, cooling_pref;

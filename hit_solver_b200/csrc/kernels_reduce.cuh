@@ -191,21 +191,40 @@ __global__ void __launch_bounds__(kPreThreads)
 
   __shared__ T su[kTileY + 2][kTileX + 2];
   __shared__ T sv[kTileY + 2][kTileX + 2];
-  __shared__ double2 tw[kTileY][kMaxDrag];  // e^{-i ky y} of the tile's rows, per drag mode
+  __shared__ double2 tw[kTileY][kMaxKyDrag + 1];  // e^{-i k y}, k = 0..ky_drag, of the tile's rows
+  __shared__ double cbuf[kPreWarps][4][32];          // per-warp column partials of one k
+  __shared__ double ctab[kMaxKyDrag + 1][4][32];     // C_k(x) = sum_y m(x, y) e^{-i k y}
   __shared__ double sm[kPreWarps * (R_FIXED + 4 * kMaxDrag)];
   __shared__ double red[R_FIXED + 4 * kMaxDrag];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 
-  for (int t = threadIdx.x; t < kTileY * ndrag; t += kPreThreads) {
-    const int a = t / ndrag, m = t - a * ndrag;
+  const int KY = ndrag > 0 ? S.ky_drag : -1;
+  for (int t = threadIdx.x; t < kTileY * (KY + 1); t += kPreThreads) {
+    const int a = t / (KY + 1), k = t - a * (KY + 1);
     const int gj = min(y0 + a, ny - 1);
-    tw[a][m] = S.twy[mode_index(S.modes[m].y, gj, ny)];
+    tw[a][k] = S.twy[mode_index(k, gj, ny)];
   }
 
   double ax = 0, ay = 0, div2 = 0, vort2 = 0, mr = 0, mp = 0, me = 0, ps = 0, sr = 0, vel2 = 0,
          cs = 0;
   int bad = 0;  // validation flags: 1 non-finite, 2 rho <= 0, 4 p <= 0
   const int gi = x0 + lane;
+  // one-node ring for the central differences (corners are not used), loaded
+  // first so that its latency overlaps the tile's
+  const bool ring = grads && threadIdx.x < 4 * kTileX;
+  int ra = 0, rb = 0;  // smem coordinates
+  double rq[4] = {0.0, 0.0, 0.0, 0.0};
+  if (ring) {
+    const int side = threadIdx.x >> 5, t = threadIdx.x & 31;
+    if (side == 0) { ra = 0; rb = t + 1; }
+    else if (side == 1) { ra = kTileY + 1; rb = t + 1; }
+    else if (side == 2) { ra = t + 1; rb = 0; }
+    else { ra = t + 1; rb = kTileX + 1; }
+    const int gj = fold_node(y0 + ra - 1, ny, per), gx = fold_node(x0 + rb - 1, nx, per);
+    const size_t o = (size_t)gj * nx + gx;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) rq[c] = q[o + c * plane];
+  }
   double m0[kPreRows], m1[kPreRows];
 #pragma unroll
   for (int k = 0; k < kPreRows; ++k) {
@@ -226,8 +245,10 @@ __global__ void __launch_bounds__(kPreThreads)
     const double q0 = q[o], q1 = q[o + plane], q2 = q[o + 2 * plane], q3 = q[o + 3 * plane];
     m0[k] = q1;
     m1[k] = q2;
+    T ep = T(0);
     if (mode != PRE_CHECK) {
       const EnfPrim<T> e = enforced_prim<T>(q0, q1, q2, q3, g, enf);
+      ep = e.p;
       su[a + 1][lane + 1] = e.u;
       sv[a + 1][lane + 1] = e.v;
       const T c = sqrt(gT * e.p * e.rinv);
@@ -237,7 +258,11 @@ __global__ void __launch_bounds__(kPreThreads)
       mp = fmax(mp, double(e.p));
       me = fmax(me, double(e.p * e.rinv * igm1));
     }
-    if (rawq || psum) {
+    // cooling's mean pressure: the FP32-bulk form takes it from its enforced
+    // pressure (equal to the floored raw pressure up to rounding)
+    const bool psum64 = psum && (sizeof(T) == 8 || rawq);
+    if (psum && !psum64) ps += double(ep);
+    if (rawq || psum64) {
       const double rho = q0 > kRhoFloor ? q0 : kRhoFloor;
       const double rinv = 1.0 / rho;
       const double ur = q1 * rinv, vr = q2 * rinv;
@@ -260,19 +285,10 @@ __global__ void __launch_bounds__(kPreThreads)
     }
   }
   if (grads) {
-    // one-node ring for the central differences (corners are not used)
-    if (threadIdx.x < 4 * kTileX) {
-      const int side = threadIdx.x >> 5, t = threadIdx.x & 31;
-      int a, b;  // smem coordinates
-      if (side == 0) { a = 0; b = t + 1; }
-      else if (side == 1) { a = kTileY + 1; b = t + 1; }
-      else if (side == 2) { a = t + 1; b = 0; }
-      else { a = t + 1; b = kTileX + 1; }
-      const int gj = fold_node(y0 + a - 1, ny, per), gx = fold_node(x0 + b - 1, nx, per);
-      const size_t o = (size_t)gj * nx + gx;
-      const EnfPrim<T> e = enforced_prim<T>(q[o], q[o + plane], q[o + 2 * plane], q[o + 3 * plane], g, enf);
-      su[a][b] = e.u;
-      sv[a][b] = e.v;
+    if (ring) {
+      const EnfPrim<T> e = enforced_prim<T>(rq[0], rq[1], rq[2], rq[3], g, enf);
+      su[ra][rb] = e.u;
+      sv[ra][rb] = e.v;
     }
     __syncthreads();
 #pragma unroll
@@ -313,16 +329,9 @@ __global__ void __launch_bounds__(kPreThreads)
   } else {
     __syncthreads();  // tw table
   }
-  warp_to_smem<OP_MAX>(ax, sm, R_AX, nslots);
-  warp_to_smem<OP_MAX>(ay, sm, R_AY, nslots);
-  warp_to_smem<OP_SUM>(div2, sm, R_DIV2, nslots);
-  warp_to_smem<OP_SUM>(vort2, sm, R_VORT2, nslots);
-  warp_to_smem<OP_MAX>(mr, sm, R_RHO, nslots);
-  warp_to_smem<OP_MAX>(mp, sm, R_P, nslots);
-  warp_to_smem<OP_MAX>(me, sm, R_E, nslots);
-  warp_to_smem<OP_SUM>(ps, sm, R_PSUM, nslots);
-  warp_to_smem<OP_MAX>(sr, sm, R_SR, nslots);
-  warp_to_smem<OP_SUM>(vel2, sm, R_VEL2, nslots);
+  warp_to_smem4<OP_MAX>(ax, ay, mr, mp, sm, make_int4(R_AX, R_AY, R_RHO, R_P), nslots);
+  warp_to_smem4<OP_MAX>(me, sr, 0.0, 0.0, sm, make_int4(R_E, R_SR, -1, -1), nslots);
+  warp_to_smem4<OP_SUM>(div2, vort2, ps, vel2, sm, make_int4(R_DIV2, R_VORT2, R_PSUM, R_VEL2), nslots);
   warp_to_smem<OP_SUM>(cs, sm, R_CSUM, nslots);
   bad = __reduce_or_sync(kFullMask, bad);
   if (lane == 0) {
@@ -330,31 +339,55 @@ __global__ void __launch_bounds__(kPreThreads)
     sm[warp * nslots + R_NONPOS_RHO] = (bad & 2) ? 1.0 : 0.0;
     sm[warp * nslots + R_NONPOS_P] = (bad & 4) ? 1.0 : 0.0;
   }
-  // low-k momentum transform of the drag band filter (OOP/hit2d.py:352-399):
-  // sum_y e^{-i ky y} m(x, y) over the thread's cells, then times e^{-i kx x}
-  for (int md = 0; md < ndrag; ++md) {
-    double cr0 = 0.0, ci0 = 0.0, cr1 = 0.0, ci1 = 0.0;
+  // low-k momentum transform of the drag band filter (OOP/hit2d.py:352-399),
+  // separable: C_k(x) = sum_y m(x, y) e^{-i k y} per column for k = 0..ky_drag
+  // (C_{-k} = conj C_k for real m), then per mode sum_x e^{-i kx x} C_ky(x).
+  // Each mode is reduced by one warp and its partials go straight to the
+  // CTA's row of partials.
+  for (int k = 0; k <= KY; ++k) {
+    double v[4] = {0.0, 0.0, 0.0, 0.0};  // Re, Im of m0; Re, Im of m1
 #pragma unroll
-    for (int k = 0; k < kPreRows; ++k) {
-      const double2 ey = tw[warp + kPreWarps * k][md];
-      cr0 += m0[k] * ey.x;
-      ci0 += m0[k] * ey.y;
-      cr1 += m1[k] * ey.x;
-      ci1 += m1[k] * ey.y;
+    for (int kk = 0; kk < kPreRows; ++kk) {
+      const double2 ey = tw[warp + kPreWarps * kk][k];
+      v[0] += m0[kk] * ey.x;
+      v[1] += m0[kk] * ey.y;
+      v[2] += m1[kk] * ey.x;
+      v[3] += m1[kk] * ey.y;
     }
+#pragma unroll
+    for (int j = 0; j < 4; ++j) cbuf[warp][j][lane] = v[j];
+    __syncthreads();
+    if (warp < 4) {
+      double acc = cbuf[0][warp][lane];
+#pragma unroll
+      for (int ww = 1; ww < kPreWarps; ++ww) acc += cbuf[ww][warp][lane];
+      ctab[k][warp][lane] = acc;
+    }
+    __syncthreads();
+  }
+  for (int md = warp; md < ndrag; md += kPreWarps) {
+    const int2 km = S.modes[md];
+    const int ky = abs(km.y);
+    const double sy = km.y < 0 ? -1.0 : 1.0;  // conjugate for negative ky
+    const double c0r = ctab[ky][0][lane], c0i = sy * ctab[ky][1][lane];
+    const double c1r = ctab[ky][2][lane], c1i = sy * ctab[ky][3][lane];
     double v[4] = {0.0, 0.0, 0.0, 0.0};
     if (gi < nx) {
-      const double2 ex = S.twx[mode_index(S.modes[md].x, gi, nx)];
-      v[0] = ex.x * cr0 - ex.y * ci0;
-      v[1] = ex.x * ci0 + ex.y * cr0;
-      v[2] = ex.x * cr1 - ex.y * ci1;
-      v[3] = ex.x * ci1 + ex.y * cr1;
+      const double2 ex = S.twx[mode_index(km.x, gi, nx)];
+      v[0] = ex.x * c0r - ex.y * c0i;
+      v[1] = ex.x * c0i + ex.y * c0r;
+      v[2] = ex.x * c1r - ex.y * c1i;
+      v[3] = ex.x * c1i + ex.y * c1r;
     }
-#pragma unroll
-    for (int k = 0; k < 4; ++k) warp_to_smem<OP_SUM>(v[k], sm, R_FIXED + 4 * md + k, nslots);
+    // warp total of the four sums into lanes 0, 8, 16, 24 of sm row `warp`,
+    // then straight to this CTA's partials
+    const int sl = R_FIXED + 4 * md;
+    warp_to_smem4<OP_SUM>(v[0], v[1], v[2], v[3], sm, make_int4(sl, sl + 1, sl + 2, sl + 3), nslots);
+    __syncwarp();
+    if (lane < 4) S.part_pre[(size_t)w.c * nslots + sl + lane] = sm[warp * nslots + sl + lane];
   }
   __syncthreads();
-  for (int t = threadIdx.x; t < nslots; t += blockDim.x) {
+  for (int t = threadIdx.x; t < R_FIXED; t += blockDim.x) {
     const int op = pre_op(t);
     double acc = sm[t];
     for (int ww = 1; ww < kPreWarps; ++ww) {
@@ -366,17 +399,31 @@ __global__ void __launch_bounds__(kPreThreads)
   if (!last_block(&S.counters[0], S.nblk_pre)) return;
 
   // ---- last CTA of this solve: fixed-order final reduction + scalar logic ----
+  // Every thread takes one slot and every C-th block (C = threads / slots),
+  // with many loads in flight; the C partials of a slot are then combined in
+  // a fixed order.
   {
-    for (int t = warp; t < nslots; t += kPreWarps) {
-      const int op = pre_op(t);
-      double acc = op == OP_SUM ? 0.0 : -INFINITY;
+    __shared__ double chunk[kPreThreads];
+    const int C = max(1, kPreThreads / nslots);
+    const int t = threadIdx.x % nslots, j = threadIdx.x / nslots;
+    const int op = pre_op(t);
+    double acc = op == OP_SUM ? 0.0 : -INFINITY;
+    if (j < C) {
 #pragma unroll 8
-      for (int b = lane; b < S.nblk_pre; b += 32) {
+      for (int b = j; b < S.nblk_pre; b += C) {
         const double x = __ldcg(S.part_pre + (size_t)b * nslots + t);
         acc = op == OP_SUM ? acc + x : fmax(acc, x);
       }
-      acc = op == OP_SUM ? warp_sum(acc) : warp_max(acc);
-      if (lane == 0) red[t] = acc;
+      chunk[j * nslots + t] = acc;
+    }
+    __syncthreads();
+    if (threadIdx.x < nslots) {
+      double v = chunk[threadIdx.x];
+      for (int jj = 1; jj < C; ++jj) {
+        const double x = chunk[jj * nslots + threadIdx.x];
+        v = op == OP_SUM ? v + x : fmax(v, x);
+      }
+      red[threadIdx.x] = v;
     }
     __syncthreads();
   }
@@ -626,10 +673,7 @@ __global__ void __launch_bounds__(kRedThreads)
     sxy += fx * fy;
     spow += p.rho * (fx * p.u + fy * p.v);
   }
-  warp_to_smem<OP_SUM>(sxx, sm, 0, 4);
-  warp_to_smem<OP_SUM>(syy, sm, 1, 4);
-  warp_to_smem<OP_SUM>(sxy, sm, 2, 4);
-  warp_to_smem<OP_SUM>(spow, sm, 3, 4);
+  warp_to_smem4<OP_SUM>(sxx, syy, sxy, spow, sm, make_int4(0, 1, 2, 3), 4);
   __syncthreads();
   if (threadIdx.x < 4) {
     double acc = sm[threadIdx.x];

@@ -503,6 +503,34 @@ __device__ __forceinline__ void load_run(const T* row, int base, T (&v)[N]) {
   for (int j = 0; j < N; ++j) v[j] = row[base + j];
 }
 
+// v[j] = p[j] for j < len (0 beyond), with 16-byte vector loads through the
+// read-only path when the whole run is present and aligned.
+template <typename T, int N>
+__device__ __forceinline__ void gload_run(const T* p, int len, T (&v)[N]) {
+  constexpr int VEC = 16 / sizeof(T);
+  if constexpr (N % VEC == 0) {
+    if (len == N && (reinterpret_cast<uintptr_t>(p) & 15) == 0) {
+#pragma unroll
+      for (int j = 0; j < N; j += VEC) {
+        if constexpr (sizeof(T) == 4) {
+          const float4 f = __ldg(reinterpret_cast<const float4*>(p + j));
+          v[j] = f.x;
+          v[j + 1] = f.y;
+          v[j + 2] = f.z;
+          v[j + 3] = f.w;
+        } else {
+          const double2 f = __ldg(reinterpret_cast<const double2*>(p + j));
+          v[j] = f.x;
+          v[j + 1] = f.y;
+        }
+      }
+      return;
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < N; ++j) v[j] = j < len ? p[j] : T(0);
+}
+
 // One sweep of the split RHS over R whole grid lines (rows for AXIS 0, columns
 // for AXIS 1), 128 threads per line, MN nodes per thread.  The y sweep runs
 // first and leaves -dG/dy in the partial-rhs buffer; the x sweep runs second
@@ -926,6 +954,15 @@ __global__ void __launch_bounds__(256, 2)
   }
   if (drag || gc) __syncthreads();  // drag table ready; FQ free for the guard staging
   double* ST = reinterpret_cast<double*>(smem);  // new rows (guard staging), reuses FQ
+  const size_t o0 = (size_t)(line0 + min(r, R - 1)) * nx + i0;
+  // the thread's stage inputs and partial rhs, loaded together up front
+  double qa[4][MN];
+  T rya[4][MN];
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    gload_run<double, MN>(qin + c * plane + o0, len, qa[c]);
+    gload_run<T, MN>(ry + c * plane + o0, len, rya[c]);
+  }
 #pragma unroll
   for (int k = 0; k < MN; ++k) {
     if (k >= len) continue;
@@ -933,7 +970,7 @@ __global__ void __launch_bounds__(256, 2)
     const size_t o = (size_t)row * nx + col;
     double rhs[4];
 #pragma unroll
-    for (int c = 0; c < 4; ++c) rhs[c] = double(ry[c * plane + o]) - ((terms & 1) ? double(x[c][k]) : 0.0);
+    for (int c = 0; c < 4; ++c) rhs[c] = double(rya[c][k]) - ((terms & 1) ? double(x[c][k]) : 0.0);
     if ((terms & 2) && S.mu > 0.0) {
       const T* vis = reinterpret_cast<const T*>(S.vis);
       rhs[1] += double(vis[o]);
@@ -941,7 +978,10 @@ __global__ void __launch_bounds__(256, 2)
       rhs[3] += double(vis[2 * plane + o]);
     }
     if (terms & (4 | 8)) {
-      const Prim<double> pr = primitives(qin[o], qin[o + plane], qin[o + 2 * plane], qin[o + 3 * plane], S.gamma);
+      // rho, u, v of primitive_from_conservative (one reciprocal)
+      const double prho = qa[0][k] > kRhoFloor ? qa[0][k] : kRhoFloor;
+      const double prinv = 1.0 / prho;
+      const Prim<double> pr{prho, qa[1][k] * prinv, qa[2][k] * prinv, 0.0};
       if (terms & 4) {
         const double fxv = bind.use ? bind.fx[o] : fs * S.fx[o];
         const double fyv = bind.use ? bind.fy[o] : fs * S.fy[o];
@@ -976,12 +1016,12 @@ __global__ void __launch_bounds__(256, 2)
     double sv[4];
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
-      const double t = qin[c * plane + o] + dt * rhs[c];
+      const double t = qa[c][k] + dt * rhs[c];
       if (stage == 0) sv[c] = t;
       else if (stage == 1) sv[c] = 0.75 * q0[c * plane + o] + 0.25 * t;
       else sv[c] = (1.0 / 3.0) * q0[c * plane + o] + (2.0 / 3.0) * t;
     }
-    enforce_node(sv[0], sv[1], sv[2], sv[3], S.gamma);
+    enforce_node_rcp(sv[0], sv[1], sv[2], sv[3], S.gamma);
     if (gc == 0) {
 #pragma unroll
       for (int c = 0; c < 4; ++c) qo[c * plane + o] = sv[c];

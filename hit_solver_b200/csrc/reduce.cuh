@@ -28,6 +28,35 @@ __device__ __forceinline__ void warp_to_smem(double v, double* sm, int slot, int
   if ((threadIdx.x & 31) == 0) sm[(threadIdx.x >> 5) * nslots + slot] = v;
 }
 
+// Reduce four values over the warp with 6 exchanges instead of 20: after two
+// halving steps each lane carries one of the four partial sums, then a
+// butterfly over the low three lane bits completes it.  Lanes 0, 8, 16 and 24
+// hold the totals of v0, v1, v2 and v3 and store them in sm[warp][slot_j]
+// (slot_j < 0: not stored).
+template <int OP>
+__device__ __forceinline__ void warp_to_smem4(double v0, double v1, double v2, double v3, double* sm,
+                                              int4 slot, int nslots) {
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  auto op = [](double a, double b) { return OP == OP_SUM ? a + b : fmax(a, b); };
+  const bool hi4 = lane & 16, hi3 = lane & 8;
+  double a0 = hi4 ? v2 : v0, a1 = hi4 ? v3 : v1;
+  const double s0 = hi4 ? v0 : v2, s1 = hi4 ? v1 : v3;
+  a0 = op(a0, __shfl_xor_sync(full, s0, 16));
+  a1 = op(a1, __shfl_xor_sync(full, s1, 16));
+  double b = hi3 ? a1 : a0;
+  const double t = hi3 ? a0 : a1;
+  b = op(b, __shfl_xor_sync(full, t, 8));
+  b = op(b, __shfl_xor_sync(full, b, 4));
+  b = op(b, __shfl_xor_sync(full, b, 2));
+  b = op(b, __shfl_xor_sync(full, b, 1));
+  if ((lane & 7) == 0) {
+    const int j = lane >> 3;
+    const int sl = j == 0 ? slot.x : j == 1 ? slot.y : j == 2 ? slot.z : slot.w;
+    if (sl >= 0) sm[(threadIdx.x >> 5) * nslots + sl] = b;
+  }
+}
+
 // After __syncthreads: threads t < nslots combine the warps and store row `blk`.
 __device__ __forceinline__ void smem_to_partials(const double* sm, int nslots,
                                                  const int* ops, double* part, int blk) {
