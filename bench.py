@@ -323,8 +323,12 @@ def run_b200(args, world, rank, local):
     flush = flush_buffer()
     cells = NX * NY
 
+    from hit_solver_b200 import autotune
+
+    tuning = {}
     # ---- FP32-bulk single solve (value) ----
     s32 = make_solver("fp32-bulk")
+    tuning["single_fp32"] = autotune.tune_plan(s32.plan, s32.q)
     s32.advance(W)
     torch.cuda.synchronize()
     dist_barrier(world)
@@ -339,6 +343,7 @@ def run_b200(args, world, rank, local):
 
     # ---- plain FP64 single solve ----
     s64 = make_solver("fp64")
+    tuning["plain_fp64"] = autotune.tune_plan(s64.plan, s64.q)
     s64.advance(W)
     t64 = dist_max(timed_steps(lambda: s64.advance(1), K, flush), world)
 
@@ -358,6 +363,7 @@ def run_b200(args, world, rank, local):
     batch.bind(states)
     for m, dt in zip(batch.members, dts):
         m.set_time(0.0, 0, dt, -1)
+    tuning["batched"] = batch.autotune()
     batch.run(W)
     tb = dist_max(timed_steps(lambda: batch.run(1), max(K // 4, 5), flush), world)
     kb = max(K // 4, 5)
@@ -366,6 +372,7 @@ def run_b200(args, world, rank, local):
 
     # ---- 512^2 production HIT: plain FP64 single solve vs FP32-bulk batch ----
     hit = hit_forms(K, W, B, flush, world)
+    hit["tuning"] = hit.pop("_tuning")
 
     # ---- serving: a seeded Poisson stream through the continuous-batching loop ----
     serve = serving_run(args) if args.serve_requests > 0 else None
@@ -439,6 +446,8 @@ def run_b200(args, world, rank, local):
                                      "gbs": round(v["bytes_per_launch"] / (v["ms_per_launch"] / 1e3) / 1e9, 1)
                                      if v["bytes_per_launch"] > 0 else None}
                                  for k, v in sorted(per.items(), key=lambda kv: -kv[1]["ms_per_step"])}},
+        "tuning": {"knobs": "sweep_x, sweep_y, prepass: 0 latency / 1 throughput variant "
+                            "(hit_solver_b200.autotune)", **tuning},
         "gpu_launches": K * launches_per_step,
         "clocks": clk.summary(),
     }
@@ -459,14 +468,19 @@ def hit_forms(K: int, W: int, B: int, flush, world: int):
     from hit_solver_b200.serving import hit_request_config
 
     n = NX
+    from hit_solver_b200 import autotune
+
     s64 = HITSolver(hit_request_config(n, 1234, 0.25, 10 ** 9, "fp64"))
+    t64 = autotune.tune_plan(s64.plan, s64.q)
     s64.advance(W)
     k64 = max(K // 2, 5)
+    tune64 = t64
     t64 = dist_max(timed_steps(lambda: s64.advance(1), k64, flush), world)
     del s64
     solvers = [HITSolver(hit_request_config(n, i, 0.1 + 0.3 * i / max(B - 1, 1), 10 ** 9,
                                             "fp32-bulk")) for i in range(B)]
     batch = Batch.from_plans([s.plan for s in solvers], [s.q for s in solvers])
+    tuneb = batch.autotune()
     batch.run(W)
     kb = max(K // 4, 5)
     tb = dist_max(timed_steps(lambda: batch.run(1), kb, flush), world)
@@ -479,7 +493,8 @@ def hit_forms(K: int, W: int, B: int, flush, world: int):
     return {"workload": "hit_production_512x512 (nu 7.5e-4, OU 3..5, Mach control, drag, cooling)",
             "plain_fp64": {"value": plain, "ms_per_step": 1e3 * t64 / k64},
             "batched_fp32": {"value": batched, "ms_per_step": 1e3 * tb / kb, "solves": B},
-            "speedup_batched_vs_plain": batched / plain, "status_bits": status}
+            "speedup_batched_vs_plain": batched / plain, "status_bits": status,
+            "_tuning": {"plain_fp64": tune64, "batched_fp32": tuneb}}
 
 
 def serving_run(args):

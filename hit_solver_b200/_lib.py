@@ -28,6 +28,7 @@ S_ALPHA_X, S_ALPHA_Y, S_DIV_RMS, S_VORT_RMS, S_DT, S_TIME, S_STEP, S_ACTIVE, S_M
  S_F_FXX, S_F_FYY, S_F_FXY, S_F_AF, S_F_DECAY, S_F_SCALE, S_MAX_STEPS, S_STATUS,
  S_NEAR_THRESHOLD, S_HV_APPLIED) = range(9, 25)
 S_COUNT = 32
+TUNE_SWEEP_X, TUNE_SWEEP_Y, TUNE_PREPASS, TUNE_COUNT = 0, 1, 2, 3
 
 NAN = float("nan")
 
@@ -127,6 +128,10 @@ SIGNATURES = [
     ("hitb200_batch_destroy", ctypes.c_int, [_VP]),
     ("hitb200_batch_from_plans", ctypes.c_int,
      [ctypes.POINTER(_VP), ctypes.c_int32, ctypes.POINTER(_VP)]),
+    ("hitb200_plan_set_tuning", ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int32), ctypes.c_int32]),
+    ("hitb200_plan_get_tuning", ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int32), ctypes.c_int32]),
+    ("hitb200_batch_set_tuning", ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int32), ctypes.c_int32]),
+    ("hitb200_batch_get_tuning", ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int32), ctypes.c_int32]),
     ("hitb200_batch_plan", _VP, [_VP, ctypes.c_int32]),
     ("hitb200_batch_bind", ctypes.c_int, [_VP, ctypes.POINTER(_VP)]),
     ("hitb200_batch_step", ctypes.c_int, [_VP, _VP]),

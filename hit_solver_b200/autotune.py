@@ -1,0 +1,115 @@
+"""Autotuner of the kernel variants.
+
+Three kernel families have two compiled variants each: the x sweep, the y
+sweep and the prepass.  The latency variant keeps more registers per thread
+and suits launches that cannot fill the GPU (one 512^2 solve); the
+throughput variant fits more CTAs per SM and suits launches over many solves.
+Plans and batches start from a default picked by launch size.  The tuner
+measures instead: it builds a copy of the batch (same descriptors, copies of
+the member states, the members' time and step size), times a few steps of
+each variant with per-launch CUDA events, keeps the faster variant of every
+family, and applies it to the real batch.  The choice only changes speed, not
+results, and is cached per batch signature (precision and each member's grid
+and physics switches), so a serving loop that meets the same mix again pays
+nothing.
+"""
+
+from __future__ import annotations
+
+import threading
+
+import torch
+
+from . import _lib, core
+
+_cache: dict = {}
+_lock = threading.Lock()
+
+# profile labels of each knob's kernels (hitb200_step_profile names)
+_FAMILIES = {
+    _lib.TUNE_SWEEP_X: ("sweep_x",),
+    _lib.TUNE_SWEEP_Y: ("sweep_y",),
+    _lib.TUNE_PREPASS: ("prepass", "hv_prepass"),
+}
+
+
+def signature(descs) -> tuple:
+    """Cache key: what the launch shapes and the work per cell depend on."""
+    members = sorted(
+        (d.nx, d.ny, d.periodic, d.scheme, d.sensor_width, int(d.viscosity > 0.0),
+         int(d.forcing_on), int(d.drag_coefficient > 0.0), d.hv_interval)
+        for d in descs)
+    return (descs[0].precision, tuple(members))
+
+
+def _family_ms(profile_fn, trials: int) -> dict:
+    """Mean device time per step of each knob's kernels over `trials` steps."""
+    tot = {k: 0.0 for k in _FAMILIES}
+    for _ in range(trials):
+        for name, ms, _ in profile_fn():
+            for k, names in _FAMILIES.items():
+                if name in names:
+                    tot[k] += ms
+    return {k: v / trials for k, v in tot.items()}
+
+
+def _choose(profile_fn, set_fn, trials: int) -> list[int]:
+    ms = {}
+    for variant in (0, 1):
+        set_fn([variant] * _lib.TUNE_COUNT)
+        profile_fn()  # warm-up step of this variant
+        ms[variant] = _family_ms(profile_fn, trials)
+    return [0 if ms[0][k] <= ms[1][k] else 1 for k in range(_lib.TUNE_COUNT)]
+
+
+def tune_batch(batch, trials: int = 3, use_cache: bool = True) -> list[int]:
+    """Tune `batch` (a hit_solver_b200.batch.Batch with bound states)."""
+    from .batch import Batch
+
+    key = signature(batch.descs)
+    with _lock:
+        best = _cache.get(key) if use_cache else None
+    if best is None:
+        plans = [core.Plan(d) for d in batch.descs]
+        states = [s.clone() for s in batch.states]
+        scratch = Batch.from_plans(plans, states)
+        try:
+            for m, src in zip(scratch.members, batch.members):
+                sc = src.scalars()
+                m.set_time(sc[_lib.S_TIME], int(sc[_lib.S_STEP]), sc[_lib.S_DT], -1)
+            best = _choose(scratch.step_profile, scratch.set_tuning, trials)
+        finally:
+            scratch.close()
+            del scratch, plans, states
+            torch.cuda.synchronize()
+        with _lock:
+            _cache[key] = best
+    batch.set_tuning(best)
+    return best
+
+
+def tune_plan(plan, q, trials: int = 3, use_cache: bool = True) -> list[int]:
+    """Tune a single plan on a copy of its state q.  Plans whose forcing noise
+    is uploaded per step (noise_mode 0) keep their default variants."""
+    if plan.desc.forcing_on and plan.desc.noise_mode == 0:
+        return plan.tuning
+    key = signature([plan.desc]) + ("single",)
+    with _lock:
+        best = _cache.get(key) if use_cache else None
+    if best is None:
+        scratch = core.Plan(plan.desc)
+        qc = q.clone()
+        sc = plan.scalars()
+        scratch.set_time(sc[_lib.S_TIME], int(sc[_lib.S_STEP]), sc[_lib.S_DT], -1)
+        best = _choose(lambda: scratch.step_profile(qc), scratch.set_tuning, trials)
+        del scratch, qc
+        torch.cuda.synchronize()
+        with _lock:
+            _cache[key] = best
+    plan.set_tuning(best)
+    return best
+
+
+def clear_cache() -> None:
+    with _lock:
+        _cache.clear()

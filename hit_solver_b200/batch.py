@@ -116,6 +116,21 @@ class Batch:
     def run(self, nsteps: int) -> None:
         _lib.check(self.lib.hitb200_batch_run(self.handle, int(nsteps), core.stream_handle()))
 
+    @property
+    def tuning(self) -> list[int]:
+        """Kernel variant knobs (see hit_solver_b200.autotune)."""
+        return core.get_tuning(self.lib.hitb200_batch_get_tuning, self.handle)
+
+    def set_tuning(self, knobs) -> None:
+        core.set_tuning(self.lib.hitb200_batch_set_tuning, self.handle, knobs)
+
+    def autotune(self, trials: int = 3) -> list[int]:
+        """Pick each kernel family's variant by timing both on a copy of this
+        batch (hit_solver_b200.autotune.tune_batch)."""
+        from .autotune import tune_batch
+
+        return tune_batch(self, trials=trials)
+
     def step_profile(self):
         return core.profile_call(lambda ms, b, cap, cnt, names, size:
                                  self.lib.hitb200_batch_step_profile(

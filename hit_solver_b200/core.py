@@ -167,11 +167,31 @@ class Plan:
         _lib.check(self.lib.hitb200_read_scalars(self.handle, buf, n))
         return list(buf)
 
+    @property
+    def tuning(self) -> list[int]:
+        """Kernel variant knobs (see hit_solver_b200.autotune)."""
+        return get_tuning(self.lib.hitb200_plan_get_tuning, self.handle)
+
+    def set_tuning(self, knobs) -> None:
+        set_tuning(self.lib.hitb200_plan_set_tuning, self.handle, knobs)
+
     def diagnostics(self, q) -> list[float]:
         buf = (ctypes.c_double * 17)()
         torch.cuda.current_stream().synchronize()
         _lib.check(self.lib.hitb200_diagnostics(self.handle, q.data_ptr(), buf, 17))
         return list(buf)
+
+
+def get_tuning(fn, handle) -> list[int]:
+    buf = (ctypes.c_int32 * _lib.TUNE_COUNT)()
+    _lib.check(fn(handle, buf, _lib.TUNE_COUNT))
+    return list(buf)
+
+
+def set_tuning(fn, handle, knobs) -> None:
+    knobs = list(knobs)
+    buf = (ctypes.c_int32 * len(knobs))(*[int(k) for k in knobs])
+    _lib.check(fn(handle, buf, len(knobs)))
 
 
 def profile_call(fn, cap: int = 64):

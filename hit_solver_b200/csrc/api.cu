@@ -127,6 +127,18 @@ int mch_for(int n) {
   return n <= 128 ? 1 : n <= 256 ? 2 : n <= 512 ? 4 : 8;
 }
 
+// Default kernel variants from the launch sizes: the throughput variants
+// (more resident CTAs, fewer registers) once a launch has several waves of
+// CTAs per SM, the latency variants below that.
+void default_tuning(int n_x, int n_y, int n_tiles32, int* t) {
+  int dev = 0, sms = 148;
+  if (cudaGetDevice(&dev) == cudaSuccess)
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  t[HITB200_TUNE_SWEEP_X] = n_x >= 6 * sms;
+  t[HITB200_TUNE_SWEEP_Y] = n_y >= 4 * sms;
+  t[HITB200_TUNE_PREPASS] = n_tiles32 >= 4 * sms;
+}
+
 }  // namespace
 
 struct hitb200_plan {
@@ -148,12 +160,14 @@ struct hitb200_plan {
   cudaStream_t graph_stream = nullptr;
   const double* graph_q = nullptr;
   bool in_batch = false;
-  SolveDev* own_solve = nullptr;  // the arena's descriptor (d_solve points into a batch table while batched)
+  SolveDev* own_solve = nullptr;
+  int tuning[HITB200_TUNE_COUNT] = {0, 0, 0};  // kernel variants (0 latency, 1 throughput)  // the arena's descriptor (d_solve points into a batch table while batched)
 };
 
 struct hitb200_batch {
   std::vector<hitb200_plan*> plans;
   bool owns_plans = true;  // false for hitb200_batch_from_plans
+  int tuning[HITB200_TUNE_COUNT] = {0, 0, 0};
   SolveDev* d_solves = nullptr;
   Work *d_tiles = nullptr, *d_tiles32 = nullptr, *d_xlines = nullptr, *d_ylines = nullptr;
   int* d_partner = nullptr;
@@ -175,6 +189,7 @@ struct LaunchSet {
   const int* partner;
   int n_tiles, n_tiles32, n_x, n_y, elem, mch_x, mch_y, guard_blocks;
   int thr_x, thr_y;  // sweep CTA sizes: kLineThreads per line of the widest work item
+  int occ_x, occ_y, occ_pre;  // kernel variants: 0 latency, 1 throughput (tuning knobs)
   size_t smem_x, smem_y, smem_sensor;
   cudaStream_t st;
   // cells of all solves, and of the solves carrying viscous / forcing terms
@@ -210,11 +225,11 @@ struct Prof {
 #define PMARK(name, b) \
   if (prof) prof->mark(name, b)
 
-template <typename T, int AXIS, int MCH>
+template <typename T, int AXIS, int MCH, int OCC>
 void set_sweep_attr(size_t bytes) {
   static size_t done = 0;
   if (bytes > done) {
-    cudaFuncSetAttribute(sweep_kernel<T, AXIS, MCH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaFuncSetAttribute(sweep_kernel<T, AXIS, MCH, OCC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)bytes);
     done = bytes;
   }
@@ -237,10 +252,16 @@ void launch_sweep_t(const LaunchSet& L, int stage, int mode, const Bind& b) {
   const size_t sm = AXIS == 0 ? L.smem_x : L.smem_y;
   const Work* w = AXIS == 0 ? L.xl : L.yl;
   const int thr = AXIS == 0 ? L.thr_x : L.thr_y;
-#define HB_SWEEP(M)                                                                   \
-  case M:                                                                             \
-    set_sweep_attr<T, AXIS, M>(sm);                                                   \
-    sweep_kernel<T, AXIS, M><<<nb, thr, sm, L.st>>>(L.solves, w, stage, mode, b);     \
+  const int occ = AXIS == 0 ? L.occ_x : L.occ_y;
+#define HB_SWEEP(M)                                                                        \
+  case M:                                                                                  \
+    if (occ) {                                                                             \
+      set_sweep_attr<T, AXIS, M, 1>(sm);                                                   \
+      sweep_kernel<T, AXIS, M, 1><<<nb, thr, sm, L.st>>>(L.solves, w, stage, mode, b);     \
+    } else {                                                                               \
+      set_sweep_attr<T, AXIS, M, 0>(sm);                                                   \
+      sweep_kernel<T, AXIS, M, 0><<<nb, thr, sm, L.st>>>(L.solves, w, stage, mode, b);     \
+    }                                                                                      \
     break;
   switch (mch) {
     HB_SWEEP(1)
@@ -276,10 +297,16 @@ void launch_hv(const LaunchSet& L, const Bind& b) {
   else hv_kernel<double><<<L.n_tiles, kStencilThreads, 0, L.st>>>(L.solves, L.tiles, b);
 }
 void launch_prepass(const LaunchSet& L, int buf, int mode, int enf, const Bind& b) {
-  if (L.elem == 4)
-    prepass_kernel<float><<<L.n_tiles32, kPreThreads, 0, L.st>>>(L.solves, L.tiles32, buf, mode, enf, b);
-  else
-    prepass_kernel<double><<<L.n_tiles32, kPreThreads, 0, L.st>>>(L.solves, L.tiles32, buf, mode, enf, b);
+#define HB_PRE(TT, O) \
+  prepass_kernel<TT, O><<<L.n_tiles32, kPreThreads, 0, L.st>>>(L.solves, L.tiles32, buf, mode, enf, b)
+  if (L.elem == 4) {
+    if (L.occ_pre) HB_PRE(float, 1);
+    else HB_PRE(float, 0);
+  } else {
+    if (L.occ_pre) HB_PRE(double, 1);
+    else HB_PRE(double, 0);
+  }
+#undef HB_PRE
 }
 
 // The reference's loop body (OOP/hit2d.py:828-879; riemann_config3.py:728-740).
@@ -372,6 +399,9 @@ LaunchSet plan_launch_set(hitb200_plan* p, cudaStream_t st) {
   L.mch_y = mch_for(p->desc.ny);
   L.thr_x = kLineThreads * p->Rx;
   L.thr_y = kLineThreads * p->Ry;
+  L.occ_x = p->tuning[HITB200_TUNE_SWEEP_X];
+  L.occ_y = p->tuning[HITB200_TUNE_SWEEP_Y];
+  L.occ_pre = p->tuning[HITB200_TUNE_PREPASS];
   L.smem_x = p->smem_x;
   L.smem_y = p->smem_y;
   L.smem_sensor = p->smem_sensor;
@@ -390,8 +420,13 @@ void prime_attributes(int elem, int mch_x, int mch_y, size_t smem_x, size_t smem
     using T = decltype(tag);
 #define HB_ATTR(M)                                                    \
   if (mch == M) {                                                     \
-    if (axis == 0) set_sweep_attr<T, 0, M>(bytes);                    \
-    else set_sweep_attr<T, 1, M>(bytes);                              \
+    if (axis == 0) {                                                  \
+      set_sweep_attr<T, 0, M, 0>(bytes);                              \
+      set_sweep_attr<T, 0, M, 1>(bytes);                              \
+    } else {                                                          \
+      set_sweep_attr<T, 1, M, 0>(bytes);                              \
+      set_sweep_attr<T, 1, M, 1>(bytes);                              \
+    }                                                                 \
   }
     HB_ATTR(1) HB_ATTR(2) HB_ATTR(4) HB_ATTR(8)
 #undef HB_ATTR
@@ -570,6 +605,7 @@ int hitb200_plan_create(const hitb200_desc* d, hitb200_plan** out) {
     p->Ry = 2;
   p->n_x = (ny + p->Rx - 1) / p->Rx;
   p->n_y = (nx + p->Ry - 1) / p->Ry;
+  default_tuning(p->n_x, p->n_y, ((nx + kSenTX - 1) / kSenTX) * ((ny + kSenTY - 1) / kSenTY), p->tuning);
   p->smem_x = p->elem == 4 ? SweepLayout<float>(nx, p->Rx).bytes() : SweepLayout<double>(nx, p->Rx).bytes();
   p->smem_y = p->elem == 4 ? SweepLayout<float>(ny, p->Ry).bytes() : SweepLayout<double>(ny, p->Ry).bytes();
   p->smem_sensor = sensor_smem_bytes(d->sensor_width, p->elem, d->viscosity > 0.0);
@@ -1137,6 +1173,7 @@ static int batch_build(hitb200_batch* b) {
   b->n_tiles32 = (int)tiles32.size();
   b->n_x = (int)xl.size();
   b->n_y = (int)yl.size();
+  default_tuning(b->n_x, b->n_y, b->n_tiles32, b->tuning);
   size_t bytes = hs.size() * sizeof(SolveDev) +
                  (tiles.size() + tiles32.size() + xl.size() + yl.size()) * sizeof(Work) +
                  partner.size() * sizeof(int) + 1024 + 6 * 256;
@@ -1311,6 +1348,9 @@ static LaunchSet batch_launch_set(hitb200_batch* b, cudaStream_t st) {
   L.mch_y = b->mch_y;
   L.thr_x = kLineThreads * b->rx_max;
   L.thr_y = kLineThreads * b->ry_max;
+  L.occ_x = b->tuning[HITB200_TUNE_SWEEP_X];
+  L.occ_y = b->tuning[HITB200_TUNE_SWEEP_Y];
+  L.occ_pre = b->tuning[HITB200_TUNE_PREPASS];
   L.smem_x = b->smem_x;
   L.smem_y = b->smem_y;
   L.smem_sensor = b->smem_sensor;
@@ -1360,6 +1400,53 @@ int hitb200_batch_run(hitb200_batch* b, int32_t nsteps, void* stream) {
 }
 
 }  // extern "C"
+
+// ---- kernel variants (autotuner knobs) -------------------------------------------
+static int tuning_set(int* dst, const int32_t* knobs, int32_t n, int n_x, int n_y, int n_tiles32) {
+  if (!knobs || n <= 0 || n > HITB200_TUNE_COUNT) return invalid("tuning knobs: 1..HITB200_TUNE_COUNT values");
+  int def[HITB200_TUNE_COUNT];
+  default_tuning(n_x, n_y, n_tiles32, def);
+  for (int i = 0; i < n; ++i) {
+    if (knobs[i] < -1 || knobs[i] > 1) return invalid("tuning knob must be -1 (default), 0 or 1");
+    dst[i] = knobs[i] < 0 ? def[i] : knobs[i];
+  }
+  return HITB200_OK;
+}
+
+extern "C" int hitb200_plan_set_tuning(hitb200_plan* p, const int32_t* knobs, int32_t n) {
+  if (!p) return invalid("NULL argument");
+  if (p->in_batch) return invalid("plan belongs to a batch; tune the batch");
+  const int r = tuning_set(p->tuning, knobs, n, p->n_x, p->n_y, p->n_tiles32);
+  if (r == HITB200_OK && p->graph) {
+    cudaGraphExecDestroy(p->graph);
+    p->graph = nullptr;
+  }
+  return r;
+}
+
+extern "C" int hitb200_plan_get_tuning(const hitb200_plan* p, int32_t* knobs, int32_t n) {
+  if (!p || !knobs) return invalid("NULL argument");
+  if (n <= 0 || n > HITB200_TUNE_COUNT) return invalid("tuning knobs: 1..HITB200_TUNE_COUNT values");
+  for (int i = 0; i < n; ++i) knobs[i] = p->tuning[i];
+  return HITB200_OK;
+}
+
+extern "C" int hitb200_batch_set_tuning(hitb200_batch* b, const int32_t* knobs, int32_t n) {
+  if (!b) return invalid("NULL argument");
+  const int r = tuning_set(b->tuning, knobs, n, b->n_x, b->n_y, b->n_tiles32);
+  if (r == HITB200_OK && b->graph) {
+    cudaGraphExecDestroy(b->graph);
+    b->graph = nullptr;
+  }
+  return r;
+}
+
+extern "C" int hitb200_batch_get_tuning(const hitb200_batch* b, int32_t* knobs, int32_t n) {
+  if (!b || !knobs) return invalid("NULL argument");
+  if (n <= 0 || n > HITB200_TUNE_COUNT) return invalid("tuning knobs: 1..HITB200_TUNE_COUNT values");
+  for (int i = 0; i < n; ++i) knobs[i] = b->tuning[i];
+  return HITB200_OK;
+}
 
 // =============================================================================
 // Stable time step without a plan and without allocating.

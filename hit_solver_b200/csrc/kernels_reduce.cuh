@@ -106,6 +106,11 @@ __device__ void step_control(const SolveDev& S, const double* red, double* sc) {
 // Mach control and validation are FP64 in both forms, and every sum is
 // accumulated in FP64.
 constexpr int kPreThreads = 256;
+// CTAs per SM of the prepass's throughput variant (OCC = 1; the latency
+// variant keeps 2).
+#ifndef HITB200_PRE_MIN_BLOCKS
+#define HITB200_PRE_MIN_BLOCKS 4
+#endif
 constexpr int kPreWarps = kPreThreads / 32;
 constexpr int kPreRows = kTileY / kPreWarps;  // own cells per thread
 
@@ -164,8 +169,8 @@ __device__ __forceinline__ EnfPrim<T> enforced_prim(double q0, double q1, double
   return r;
 }
 
-template <typename T>
-__global__ void __launch_bounds__(kPreThreads)
+template <typename T, int OCC>
+__global__ void __launch_bounds__(kPreThreads, OCC ? HITB200_PRE_MIN_BLOCKS : 2)
     prepass_kernel(const SolveDev* __restrict__ solves, const Work* __restrict__ work, int buf,
                    int mode, int enf, Bind bind) {
   const Work w = work[blockIdx.x];

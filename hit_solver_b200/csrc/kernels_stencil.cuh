@@ -14,6 +14,18 @@ constexpr unsigned kFull = 0xffffffffu;
 
 constexpr int kStencilThreads = 256;
 constexpr int kLineThreads = 128;  // sweep threads per grid line of a CTA
+// Occupancy targets of the throughput variant of the sweeps (OCC = 1; CTAs
+// of 256 threads per SM): they bound the registers per thread, so that many
+// solves' lines share an SM.  The latency variant (OCC = 0) keeps 2, for
+// launches too small to fill the GPU twice over.
+#ifndef HITB200_SWEEP_MIN_BLOCKS_X
+#define HITB200_SWEEP_MIN_BLOCKS_X 4
+#endif
+#ifndef HITB200_SWEEP_MIN_BLOCKS_Y
+#define HITB200_SWEEP_MIN_BLOCKS_Y 3
+#endif
+constexpr int kSweepMinBlocksX = HITB200_SWEEP_MIN_BLOCKS_X;
+constexpr int kSweepMinBlocksY = HITB200_SWEEP_MIN_BLOCKS_Y;
 constexpr int kSenTX = 32, kSenTY = 32;  // sensor tile
 constexpr int kSensorThreads = 512;
 constexpr int kHvTX = 32, kHvTY = 16;    // hyperviscosity tile
@@ -115,8 +127,11 @@ __device__ __forceinline__ int row_of(int idx, int w, float iw) {
 // hyperviscosity steps).  want_visc: also write the viscous terms.  NEAR:
 // count nodes within roundoff of a threshold (sensor API; off in the fused
 // step).
+#ifndef HITB200_SENSOR_MIN_BLOCKS
+#define HITB200_SENSOR_MIN_BLOCKS 2
+#endif
 template <typename T, bool NEAR>
-__global__ void __launch_bounds__(kSensorThreads, 2)
+__global__ void __launch_bounds__(kSensorThreads, HITB200_SENSOR_MIN_BLOCKS)
     sensor_kernel(const SolveDev* __restrict__ solves, const Work* __restrict__ work, int sel,
                   int enf, int want_visc, Bind bind, uint8_t* __restrict__ mask_out) {
   extern __shared__ __align__(16) unsigned char smem[];
@@ -540,8 +555,8 @@ __device__ __forceinline__ void gload_run(const T* p, int len, T (&v)[N]) {
 //   stage 2:      clean(1/3 q + 2/3 (q2 + dt L))     (OOP/time_operator.py:21-26)
 // with L = -dF/dx - dG/dy + viscous + forcing + drag + cooling and clean the
 // enforce filter plus, on outflow grids, the guard cells.
-template <typename T, int AXIS, int MN>
-__global__ void __launch_bounds__(256, 2)
+template <typename T, int AXIS, int MN, int OCC>
+__global__ void __launch_bounds__(256, OCC ? (AXIS == 0 ? kSweepMinBlocksX : kSweepMinBlocksY) : 2)
     sweep_kernel(const SolveDev* __restrict__ solves, const Work* __restrict__ work, int stage,
                  int mode, Bind bind) {
   extern __shared__ __align__(16) unsigned char smem[];

@@ -264,6 +264,22 @@ hitb200_plan* hitb200_batch_plan(hitb200_batch* batch, int32_t i);
 int hitb200_batch_bind(hitb200_batch* batch, double* const* q);
 int hitb200_batch_step(hitb200_batch* batch, void* stream);
 int hitb200_batch_run(hitb200_batch* batch, int32_t nsteps, void* stream);
+/* ---- kernel variants (autotuner knobs; no counterpart in the reference) -------- */
+/* Each knob picks the variant of one kernel family: 0 = latency variant
+ * (more registers per thread, for launches that cannot fill the GPU), 1 =
+ * throughput variant (more resident CTAs per SM, for many solves per
+ * launch).  Plans and batches start from a default chosen by launch size;
+ * -1 restores that default.  Results do not depend on the knobs, only
+ * speed.  Setting a knob drops the captured graph (recaptured on the next
+ * run). */
+#define HITB200_TUNE_SWEEP_X 0
+#define HITB200_TUNE_SWEEP_Y 1
+#define HITB200_TUNE_PREPASS 2
+#define HITB200_TUNE_COUNT 3
+int hitb200_plan_set_tuning(hitb200_plan* plan, const int32_t* knobs, int32_t n);
+int hitb200_plan_get_tuning(const hitb200_plan* plan, int32_t* knobs, int32_t n);
+int hitb200_batch_set_tuning(hitb200_batch* batch, const int32_t* knobs, int32_t n);
+int hitb200_batch_get_tuning(const hitb200_batch* batch, int32_t* knobs, int32_t n);
 /* hitb200_step_profile for a batch (launches cover all member solves). */
 int hitb200_batch_step_profile(hitb200_batch* batch, float* ms, double* bytes, int32_t cap,
                                int32_t* count, char* names, size_t names_size, void* stream);

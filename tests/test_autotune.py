@@ -1,0 +1,81 @@
+"""Kernel variants and the autotuner (hit_solver_b200.autotune).
+
+The variants differ only in register budgets and CTAs per SM, so the state
+after any number of steps must be bit-identical whichever variants run; the
+tuner must return one valid choice per kernel family and apply it.
+"""
+
+import pytest
+import torch
+
+from hit_solver_b200 import _lib, autotune, serving
+from hit_solver_b200.batch import Batch
+
+
+def _mixed(n_hit=48, n_riem=40):
+    hit = serving.make_solver(serving.Request(0, "hit", n_hit, seed=3, mach=0.3, steps=10 ** 6),
+                              "fp32-bulk")
+    riem = serving.make_solver(serving.Request(1, "riemann3", n_riem, split=0.45), "fp32-bulk")
+    return [hit, riem]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["fp32-bulk", "fp64"])
+def test_variants_give_identical_states(precision):
+    finals = []
+    for knobs in ([0, 0, 0], [1, 1, 1], [1, 0, 1]):
+        sv = [serving.make_solver(serving.Request(0, "hit", 48, seed=3, mach=0.3, steps=10 ** 6), precision),
+              serving.make_solver(serving.Request(1, "riemann3", 40, split=0.45), precision)]
+        b = Batch.from_plans([s.plan for s in sv], [s.q for s in sv])
+        b.set_tuning(knobs)
+        assert b.tuning == knobs
+        b.run(7)
+        torch.cuda.synchronize()
+        finals.append([s.q.clone() for s in sv])
+        b.close()
+    for other in finals[1:]:
+        for a, c in zip(finals[0], other):
+            assert torch.equal(a, c)
+
+
+@pytest.mark.gpu
+def test_single_plan_variants_identical():
+    out = []
+    for knobs in ([0, 0, 0], [1, 1, 1]):
+        s = serving.make_solver(serving.Request(0, "riemann6", 64, split=0.5), "fp32-bulk")
+        s.plan.set_tuning(knobs)
+        assert s.plan.tuning == knobs
+        s.advance(5)
+        out.append(s.q.clone())
+    assert torch.equal(out[0], out[1])
+
+
+@pytest.mark.gpu
+def test_autotune_batch_and_plan():
+    autotune.clear_cache()
+    sv = _mixed()
+    b = Batch.from_plans([s.plan for s in sv], [s.q for s in sv])
+    before = [s.q.clone() for s in sv]
+    knobs = b.autotune(trials=1)
+    assert len(knobs) == _lib.TUNE_COUNT and set(knobs) <= {0, 1}
+    assert b.tuning == knobs
+    # tuning ran on copies: the batch's own states are untouched
+    for a, c in zip(before, [s.q for s in sv]):
+        assert torch.equal(a, c)
+    # cached: same answer without timing again
+    assert autotune.tune_batch(b) == knobs
+    b.close()
+    s = serving.make_solver(serving.Request(2, "riemann3", 64, split=0.5), "fp32-bulk")
+    k2 = autotune.tune_plan(s.plan, s.q, trials=1)
+    assert s.plan.tuning == k2
+
+
+@pytest.mark.gpu
+def test_tuning_knob_validation():
+    s = serving.make_solver(serving.Request(0, "riemann3", 32), "fp32-bulk")
+    with pytest.raises(ValueError):
+        s.plan.set_tuning([2, 0, 0])
+    with pytest.raises(ValueError):
+        s.plan.set_tuning([0, 0, 0, 0])
+    s.plan.set_tuning([-1, -1, -1])  # back to the launch-size default
+    assert set(s.plan.tuning) <= {0, 1}
