@@ -65,6 +65,8 @@ def parse_args():
     p.add_argument("--batch", type=int, default=8, help="solves in the batched measurement")
     p.add_argument("--cpu-steps", type=int, default=3, help="oracle steps in the cpu_baseline sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--ref-procs", type=int, default=0,
+                   help="reference arm: host processes (0: one per core, at most 32)")
     p.add_argument("--serve-requests", type=int, default=24,
                    help="requests in the serving measurement (0: skip)")
     p.add_argument("--serve-rate", type=float, default=20.0, help="mean arrivals per second")
@@ -101,7 +103,8 @@ def dist_max(x: float, world: int) -> float:
     import torch
     import torch.distributed as dist
 
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -558,6 +561,8 @@ def run_reference(args, world, rank):
     os.environ.setdefault("OMP_NUM_THREADS", "1")
     cores = os.cpu_count() or 1
     procs = max(1, min(cores, 32))  # each process holds ~0.5 GB of NumPy temporaries
+    if args.ref_procs > 0:
+        procs = min(procs, args.ref_procs)
     # bounded sample: each process advances the 512^2 workload a few steps;
     # ~4 s per step per process, so the run stays within a few minutes
     steps = max(1, min(args.steps, 8))
