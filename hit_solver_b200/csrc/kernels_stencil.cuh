@@ -53,6 +53,9 @@ __device__ __noinline__ bool quotient_gt(T num, T den, T thr) {
 // ~8 ulp of the threshold (then the quotient itself is formed).
 template <typename T>
 __device__ __forceinline__ bool ratio_gt(T num, T den, T thr) {
+  // FP32-bulk form: the product test (its masks already differ from the
+  // FP64 ones at nodes within FP32 roundoff of a threshold)
+  if constexpr (sizeof(T) == 4) return num > thr * den;
   const T t = thr * den;
   const T d = num - t;
   if (fabs(d) > T(8) * type_eps<T>() * t) return d > T(0);
@@ -96,8 +99,7 @@ __host__ __device__ inline size_t sensor_flag_end(int width, int elem) {
   const size_t rx = kSenTX + 2 * width, ry = kSenTY + 2 * width;
   const size_t raw = ry * rx;
   const size_t row = ry * kSenTX;
-  const size_t edges = ry * (rx + 1) + (ry + 1) * rx;
-  return (prim + raw + row + edges + 32 + 15) & ~(size_t)15;
+  return (prim + raw + row + 32 + 15) & ~(size_t)15;
 }
 
 // Dynamic shared memory of the sensor kernel; `viscous` adds the five
@@ -127,11 +129,14 @@ __device__ __forceinline__ int row_of(int idx, int w, float iw) {
 // hyperviscosity steps).  want_visc: also write the viscous terms.  NEAR:
 // count nodes within roundoff of a threshold (sensor API; off in the fused
 // step).
+// CTAs per SM the FP32 sensor is compiled for; the FP64 one holds one CTA
+// per SM anyway (its staged tile and viscous arrays take ~120 KB) and gets
+// the full register budget instead.
 #ifndef HITB200_SENSOR_MIN_BLOCKS
 #define HITB200_SENSOR_MIN_BLOCKS 2
 #endif
 template <typename T, bool NEAR>
-__global__ void __launch_bounds__(kSensorThreads, HITB200_SENSOR_MIN_BLOCKS)
+__global__ void __launch_bounds__(kSensorThreads, sizeof(T) == 8 ? 1 : HITB200_SENSOR_MIN_BLOCKS)
     sensor_kernel(const SolveDev* __restrict__ solves, const Work* __restrict__ work, int sel,
                   int enf, int want_visc, Bind bind, uint8_t* __restrict__ mask_out) {
   extern __shared__ __align__(16) unsigned char smem[];
@@ -160,8 +165,6 @@ __global__ void __launch_bounds__(kSensorThreads, HITB200_SENSOR_MIN_BLOCKS)
   const int RX = kSenTX + 2 * W, RY = kSenTY + 2 * W;
   uint8_t* RAW = reinterpret_cast<uint8_t*>(E + SX * SY);
   uint8_t* ROW = RAW + RX * RY;
-  uint8_t* EXF = ROW + RY * kSenTX;       // [RY][RX + 1]: edge left of raw column br
-  uint8_t* EYF = EXF + RY * (RX + 1);     // [RY + 1][RX]: edge below raw row ar
   const int off = HW - W;                 // smem offset of raw index 0
 
   // ---- staged primitives of the tile and its (width + 1) halo ----
@@ -210,86 +213,96 @@ __global__ void __launch_bounds__(kSensorThreads, HITB200_SENSOR_MIN_BLOCKS)
   const T tdx = T(2.0 * S.dx), tdy = T(2.0 * S.dy), hx = T(S.dx), hy = T(S.dy);
   const T itdx = T(1.0 / (2.0 * S.dx)), itdy = T(1.0 / (2.0 * S.dy));
   const T tol = T(32) * type_eps<T>();
-  bool near_any = false;  // only used when NEAR
-
-  // ---- two-point jumps, once per edge (x edges, then y edges) ----
-  const int nex = RY * (RX + 1);
-  const float iex = 1.0f / (float)(RX + 1);
-  for (int idx = threadIdx.x; idx < nex; idx += blockDim.x) {
-    const int ar = row_of(idx, RX + 1, iex), be = idx - ar * (RX + 1);
-    const int c = (ar + off) * SX + be + off;  // right node of the edge
-    bool nr = false;
-    const bool f = pair_gt<T, NEAR>(RHO[c - 1], RHO[c], eps_r, thr, tol, nr) |
-                   pair_gt<T, NEAR>(P[c - 1], P[c], eps_p, thr, tol, nr) |
-                   pair_gt<T, NEAR>(E[c - 1], E[c], eps_e, thr, tol, nr);
-    EXF[idx] = (f ? 1 : 0) | (nr ? 2 : 0);
-  }
-  const int ney = (RY + 1) * RX;
-  const float irx = 1.0f / (float)RX;
-  for (int idx = threadIdx.x; idx < ney; idx += blockDim.x) {
-    const int ae = row_of(idx, RX, irx), br = idx - ae * RX;
-    const int c = (ae + off) * SX + br + off;  // upper node of the edge
-    bool nr = false;
-    const bool f = pair_gt<T, NEAR>(RHO[c - SX], RHO[c], eps_r, thr, tol, nr) |
-                   pair_gt<T, NEAR>(P[c - SX], P[c], eps_p, thr, tol, nr) |
-                   pair_gt<T, NEAR>(E[c - SX], E[c], eps_e, thr, tol, nr);
-    EYF[idx] = (f ? 1 : 0) | (nr ? 2 : 0);
-  }
-  __syncthreads();
 
   // ---- raw flags on the tile plus a width-wide ring ----
+  // Thread task: a strip of up to 4 consecutive raw rows of one raw column.
+  // The strip's column values (rows -1 .. +4) and its left / right
+  // neighbours stay in registers; each y edge of the strip is tested once,
+  // x edges and curvatures per node, with the reference's operand order.
   int near_count = 0;
-  for (int idx = threadIdx.x; idx < RX * RY; idx += blockDim.x) {
-    const int ar = row_of(idx, RX, irx), br = idx - ar * RX;
-    const int gj = y0 - W + ar, gi = x0 - W + br;
-    const bool inside = gj >= 0 && gj < ny && gi >= 0 && gi < nx;
-    if (!per && !inside) {
-      RAW[idx] = 0;
-      continue;
+  const int nstrip = (RY + 3) >> 2;
+  const float irx = 1.0f / (float)RX;
+  for (int t = threadIdx.x; t < RX * nstrip; t += blockDim.x) {
+    const int s = row_of(t, RX, irx), br = t - s * RX;
+    const int ar0 = 4 * s, nrow = min(4, RY - ar0);
+    const int gi = x0 - W + br;
+    const int c0 = (ar0 + off) * SX + br + off;  // staged index of raw node (ar0, br)
+    bool m[4] = {false, false, false, false}, nr[4] = {false, false, false, false};
+    // jumps and curvatures of one staged quantity
+    auto quantity = [&](const T* A, T eps) {
+      T col[6], lf[4], rt[4];
+#pragma unroll
+      for (int j = 0; j < 6; ++j) col[j] = j <= nrow + 1 ? A[c0 + (j - 1) * SX] : T(0);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        lf[k] = k < nrow ? A[c0 + k * SX - 1] : T(0);
+        rt[k] = k < nrow ? A[c0 + k * SX + 1] : T(0);
+      }
+      bool ey[5];
+#pragma unroll
+      for (int j = 0; j < 5; ++j) {
+        bool nn = false;
+        ey[j] = j <= nrow && pair_gt<T, NEAR>(col[j], col[j + 1], eps, thr, tol, nn);
+        if (NEAR && j <= nrow) {
+          if (j < 4) nr[j] = nr[j] || nn;
+          if (j > 0) nr[j - 1] = nr[j - 1] || nn;
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        if (k >= nrow) continue;
+        bool nn = false;
+        bool f = ey[k] | ey[k + 1];
+        f |= pair_gt<T, NEAR>(lf[k], col[k + 1], eps, thr, tol, nn);
+        f |= pair_gt<T, NEAR>(col[k + 1], rt[k], eps, thr, tol, nn);
+        f |= curv_gt<T, NEAR>(lf[k], col[k + 1], rt[k], eps, thr, tol, nn);
+        f |= curv_gt<T, NEAR>(col[k], col[k + 1], col[k + 2], eps, thr, tol, nn);
+        m[k] = m[k] || f;
+        if (NEAR) nr[k] = nr[k] || nn;
+      }
+    };
+    quantity(RHO, eps_r);
+    quantity(P, eps_p);
+    quantity(E, eps_e);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      if (k >= nrow) continue;
+      const int ar = ar0 + k, gj = y0 - W + ar;
+      const bool inside = gj >= 0 && gj < ny && gi >= 0 && gi < nx;
+      const int c = c0 + k * SX;
+      bool mk = m[k], near = NEAR && nr[k];
+      // sensor velocity gradients: central; first-order one-sided at outflow edges
+      const bool cx = per || (gi > 0 && gi < nx - 1), cy = per || (gj > 0 && gj < ny - 1);
+      if (comp_on) {
+        T dudx = T(0), dvdy = T(0);
+        if (cx) dudx = dq(U[c + 1], U[c - 1], tdx, itdx);
+        else if (nx > 1) dudx = gi == 0 ? (U[c + 1] - U[c]) / hx : (U[c] - U[c - 1]) / hx;
+        if (cy) dvdy = dq(V[c + SX], V[c - SX], tdy, itdy);
+        else if (ny > 1) dvdy = gj == 0 ? (V[c + SX] - V[c]) / hy : (V[c] - V[c - SX]) / hy;
+        const T div = dudx + dvdy;
+        mk = mk || div < comp_lim;
+        if (NEAR) near = near || fabs(div - comp_lim) <= tol * fabs(comp_lim);
+      }
+      if (shear_on) {
+        T dvdx = T(0), dudy = T(0);
+        if (cx) dvdx = dq(V[c + 1], V[c - 1], tdx, itdx);
+        else if (nx > 1) dvdx = gi == 0 ? (V[c + 1] - V[c]) / hx : (V[c] - V[c - 1]) / hx;
+        if (cy) dudy = dq(U[c + SX], U[c - SX], tdy, itdy);
+        else if (ny > 1) dudy = gj == 0 ? (U[c + SX] - U[c]) / hy : (U[c] - U[c - SX]) / hy;
+        const T av = fabs(dvdx - dudy);
+        mk = mk || av > shear_lim;
+        if (NEAR) near = near || fabs(av - shear_lim) <= tol * shear_lim;
+      }
+      if (!per && S.boundary_guard > 0) {
+        const int bg = S.boundary_guard;
+        if (gj < bg || gj >= ny - bg || gi < bg || gi >= nx - bg) mk = true;
+      }
+      if (!per && !inside) mk = false;
+      RAW[ar * RX + br] = mk ? 1 : 0;
+      // nodes of this tile whose metric sits within roundoff of a threshold
+      if (NEAR && near && inside && ar >= W && ar < W + kSenTY && br >= W && br < W + kSenTX)
+        ++near_count;
     }
-    const int c = (ar + off) * SX + br + off;
-    const uint8_t ef = EXF[ar * (RX + 1) + br] | EXF[ar * (RX + 1) + br + 1] |
-                       EYF[ar * RX + br] | EYF[(ar + 1) * RX + br];
-    bool near = NEAR && (ef & 2);
-    bool m = (ef & 1) != 0;
-    // sensor velocity gradients: central; first-order one-sided at outflow edges
-    const bool cx = per || (gi > 0 && gi < nx - 1), cy = per || (gj > 0 && gj < ny - 1);
-    if (comp_on) {
-      T dudx = T(0), dvdy = T(0);
-      if (cx) dudx = dq(U[c + 1], U[c - 1], tdx, itdx);
-      else if (nx > 1) dudx = gi == 0 ? (U[c + 1] - U[c]) / hx : (U[c] - U[c - 1]) / hx;
-      if (cy) dvdy = dq(V[c + SX], V[c - SX], tdy, itdy);
-      else if (ny > 1) dvdy = gj == 0 ? (V[c + SX] - V[c]) / hy : (V[c] - V[c - SX]) / hy;
-      const T div = dudx + dvdy;
-      m = m || div < comp_lim;
-      if (NEAR) near = near || fabs(div - comp_lim) <= tol * fabs(comp_lim);
-    }
-    if (shear_on) {
-      T dvdx = T(0), dudy = T(0);
-      if (cx) dvdx = dq(V[c + 1], V[c - 1], tdx, itdx);
-      else if (nx > 1) dvdx = gi == 0 ? (V[c + 1] - V[c]) / hx : (V[c] - V[c - 1]) / hx;
-      if (cy) dudy = dq(U[c + SX], U[c - SX], tdy, itdy);
-      else if (ny > 1) dudy = gj == 0 ? (U[c + SX] - U[c]) / hy : (U[c] - U[c - SX]) / hy;
-      const T av = fabs(dvdx - dudy);
-      m = m || av > shear_lim;
-      if (NEAR) near = near || fabs(av - shear_lim) <= tol * shear_lim;
-    }
-    if (!m || NEAR) {
-      m = curv_gt<T, NEAR>(RHO[c - 1], RHO[c], RHO[c + 1], eps_r, thr, tol, near) || m;
-      m = curv_gt<T, NEAR>(RHO[c - SX], RHO[c], RHO[c + SX], eps_r, thr, tol, near) || m;
-      m = curv_gt<T, NEAR>(P[c - 1], P[c], P[c + 1], eps_p, thr, tol, near) || m;
-      m = curv_gt<T, NEAR>(P[c - SX], P[c], P[c + SX], eps_p, thr, tol, near) || m;
-      m = curv_gt<T, NEAR>(E[c - 1], E[c], E[c + 1], eps_e, thr, tol, near) || m;
-      m = curv_gt<T, NEAR>(E[c - SX], E[c], E[c + SX], eps_e, thr, tol, near) || m;
-    }
-    if (!per && S.boundary_guard > 0) {
-      const int bg = S.boundary_guard;
-      if (gj < bg || gj >= ny - bg || gi < bg || gi >= nx - bg) m = true;
-    }
-    RAW[idx] = m ? 1 : 0;
-    // nodes of this tile whose metric sits within roundoff of a threshold
-    if (NEAR && near && inside && ar >= W && ar < W + kSenTY && br >= W && br < W + kSenTX)
-      ++near_count;
   }
   __syncthreads();
   for (int idx = threadIdx.x; idx < RY * kSenTX; idx += blockDim.x) {
@@ -310,7 +323,6 @@ __global__ void __launch_bounds__(kSensorThreads, HITB200_SENSOR_MIN_BLOCKS)
     near_count = warp_sum(near_count);
     if (tx == 0 && near_count > 0) atomicAdd(S.near_count, near_count);
   }
-  (void)near_any;
 
   if (!want_visc || S.mu == 0.0) return;
   // viscous stress and heat-flux divergence (OOP/equations.py:232-267), as the
