@@ -67,6 +67,7 @@ def parse_args():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--ref-procs", type=int, default=0,
                    help="reference arm: host processes (0: one per core, at most 32)")
+    p.add_argument("--ensemble", type=int, default=64, help="solves in the ensemble leg (0: skip)")
     p.add_argument("--serve-requests", type=int, default=24,
                    help="requests in the serving measurement (0: skip)")
     p.add_argument("--serve-rate", type=float, default=20.0, help="mean arrivals per second")
@@ -376,6 +377,9 @@ def run_b200(args, world, rank, local):
     # ---- 512^2 production HIT: plain FP64 single solve vs FP32-bulk batch ----
     hit = hit_forms(K, W, B, flush, world)
     hit["tuning"] = hit.pop("_tuning")
+    ens = ensemble_run(K, W, flush, world, args.ensemble) if args.ensemble > 0 else None
+    if ens is not None:
+        ens["speedup_vs_plain_fp64_hit_512"] = ens["value"] / hit["plain_fp64"]["value"]
 
     # ---- serving: a seeded Poisson stream through the continuous-batching loop ----
     serve = serving_run(args) if args.serve_requests > 0 else None
@@ -433,6 +437,7 @@ def run_b200(args, world, rank, local):
                     "solves": B, "dtype": "fp32 (fp64 state)",
                     "speedup_vs_plain_fp64": (B * cells * kb / tb) / (cells * K / t64)},
         "batched_hit": hit,
+        "ensemble": ens,
         "serving": serve,
         "e2e": {"value": world * cells * K / te2e, "unit": "cell-updates/s",
                 "h2d_bytes_per_step": state_bytes / K,
@@ -498,6 +503,40 @@ def hit_forms(K: int, W: int, B: int, flush, world: int):
             "batched_fp32": {"value": batched, "ms_per_step": 1e3 * tb / kb, "solves": B},
             "speedup_batched_vs_plain": batched / plain, "status_bits": status,
             "_tuning": {"plain_fp64": tune64, "batched_fp32": tuneb}}
+
+
+def ensemble_run(K: int, W: int, flush, world: int, count: int):
+    """The batched-ensemble configuration: `count` production-physics HIT
+    solves with grids drawn from {128, 256, 384, 512}^2, seeds 0..count-1 and
+    turbulent Mach uniform in [0.1, 0.4] (fixed meta-seed), FP32-bulk, one
+    launch per kernel of the step for all of them, autotuned."""
+    import numpy as np
+    import torch
+
+    from hit_solver_b200.batch import Batch
+    from hit_solver_b200.hit2d import HITSolver
+    from hit_solver_b200.serving import hit_request_config
+
+    rng = np.random.default_rng(64)
+    sizes = rng.choice([128, 256, 384, 512], size=count)
+    machs = rng.uniform(0.1, 0.4, size=count)
+    solvers = [HITSolver(hit_request_config(int(n), i, float(m), 10 ** 9, "fp32-bulk"))
+               for i, (n, m) in enumerate(zip(sizes, machs))]
+    batch = Batch.from_plans([s.plan for s in solvers], [s.q for s in solvers])
+    knobs = batch.autotune()
+    batch.run(W)
+    k = max(K // 8, 5)
+    t = dist_max(timed_steps(lambda: batch.run(1), k, flush), world)
+    from hit_solver_b200 import _lib
+
+    status = max(int(m.scalars()[_lib.S_STATUS]) for m in batch.members)
+    cells = int(sum(int(n) * int(n) for n in sizes))
+    batch.close()
+    del solvers
+    torch.cuda.synchronize()
+    return {"workload": f"{count} HIT solves, grids from {{128,256,384,512}}^2, Mach U[0.1,0.4]",
+            "value": world * cells * k / t, "unit": "cell-updates/s", "ms_per_step": 1e3 * t / k,
+            "cells": cells, "solves": count, "steps": k, "tuning": knobs, "status_bits": status}
 
 
 def serving_run(args):

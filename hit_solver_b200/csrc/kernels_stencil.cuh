@@ -169,6 +169,7 @@ __global__ void __launch_bounds__(kSensorThreads, sizeof(T) == 8 ? 1 : HITB200_S
 
   // ---- staged primitives of the tile and its (width + 1) halo ----
   const float isx = 1.0f / (float)SX;
+#pragma unroll 2
   for (int idx = threadIdx.x; idx < SX * SY; idx += blockDim.x) {
     const int a = row_of(idx, SX, isx), b = idx - a * SX;
     const int gj = fold_node(y0 - HW + a, ny, per), gi = fold_node(x0 - HW + b, nx, per);
@@ -600,6 +601,7 @@ __global__ void __launch_bounds__(256, OCC ? (AXIS == 0 ? kSweepMinBlocksX : kSw
   // x lines: consecutive threads take consecutive nodes of a row; y lines:
   // consecutive threads take the R columns of a row, then the next row.
   const int nl = AXIS == 0 ? R * LS : (LS << rsh);
+#pragma unroll 4
   for (int idx = threadIdx.x; idx < nl; idx += blockDim.x) {
     int r, p;
     if (AXIS == 0) {
@@ -639,6 +641,7 @@ __global__ void __launch_bounds__(256, OCC ? (AXIS == 0 ? kSweepMinBlocksX : kSw
   }
   const int weno_all = S.scheme == 1;
   const int nm = AXIS == 0 ? R * (n + 2) : ((n + 2) << rsh);
+#pragma unroll 4
   for (int idx = threadIdx.x; idx < nm; idx += blockDim.x) {
     int r, p;
     if (AXIS == 0) {
@@ -979,39 +982,52 @@ __global__ void __launch_bounds__(256, OCC ? (AXIS == 0 ? kSweepMinBlocksX : kSw
       dpy[rr][k] = sy;
     }
   }
-  if (drag || gc) __syncthreads();  // drag table ready; FQ free for the guard staging
+  // The derivatives go to shared memory (the WENO buffer is free once the
+  // faces are formed) and the epilogue walks the rows with consecutive
+  // threads on consecutive nodes, so that every global access is coalesced.
+  T* XS = WB;  // [R][4][LW]
+#pragma unroll
+  for (int k = 0; k < MN; ++k)
+    if (k < len) {
+#pragma unroll
+      for (int c = 0; c < 4; ++c) XS[(r * 4 + c) * LW + i0 + k] = x[c][k];
+    }
+  __syncthreads();  // derivatives and drag table ready; FQ free for the guard staging
   double* ST = reinterpret_cast<double*>(smem);  // new rows (guard staging), reuses FQ
-  const size_t o0 = (size_t)(line0 + min(r, R - 1)) * nx + i0;
-  // the thread's stage inputs and partial rhs, loaded together up front
-  double qa[4][MN];
-  T rya[4][MN];
-#pragma unroll
-  for (int c = 0; c < 4; ++c) {
-    gload_run<double, MN>(qin + c * plane + o0, len, qa[c]);
-    gload_run<T, MN>(ry + c * plane + o0, len, rya[c]);
-  }
-#pragma unroll
-  for (int k = 0; k < MN; ++k) {
-    if (k >= len) continue;
-    const int col = i0 + k, row = line0 + r;
+  // Solve fields in registers and read-only inputs behind restrict-qualified
+  // pointers: the stores to the stage output below cannot force reloads.
+  const double gam = S.gamma, cool = (terms & 16) ? sc[S_COOL] : 0.0;
+  const bool visc = (terms & 2) && S.mu > 0.0;
+  const int kxd = S.kx_drag;
+  const T* __restrict__ visp = reinterpret_cast<const T*>(S.vis);
+  const double* __restrict__ fxp = bind.use ? bind.fx : S.fx;
+  const double* __restrict__ fyp = bind.use ? bind.fy : S.fy;
+  const double fsc = bind.use ? 1.0 : fs;
+  const double2* __restrict__ twx = S.twx;
+  const double* __restrict__ qinr = qin;
+  const T* __restrict__ ryr = ry;
+  for (int idx = threadIdx.x; idx < R * n; idx += blockDim.x) {
+    const int rr = idx >= n ? 1 : 0, col = idx - rr * n, row = line0 + rr;
     const size_t o = (size_t)row * nx + col;
-    double rhs[4];
+    double qa[4], rhs[4];
 #pragma unroll
-    for (int c = 0; c < 4; ++c) rhs[c] = double(rya[c][k]) - ((terms & 1) ? double(x[c][k]) : 0.0);
-    if ((terms & 2) && S.mu > 0.0) {
-      const T* vis = reinterpret_cast<const T*>(S.vis);
-      rhs[1] += double(vis[o]);
-      rhs[2] += double(vis[plane + o]);
-      rhs[3] += double(vis[2 * plane + o]);
+    for (int c = 0; c < 4; ++c) {
+      qa[c] = qinr[c * plane + o];
+      rhs[c] = double(ryr[c * plane + o]) - ((terms & 1) ? double(XS[(rr * 4 + c) * LW + col]) : 0.0);
+    }
+    if (visc) {
+      rhs[1] += double(visp[o]);
+      rhs[2] += double(visp[plane + o]);
+      rhs[3] += double(visp[2 * plane + o]);
     }
     if (terms & (4 | 8)) {
       // rho, u, v of primitive_from_conservative (one reciprocal)
-      const double prho = qa[0][k] > kRhoFloor ? qa[0][k] : kRhoFloor;
+      const double prho = qa[0] > kRhoFloor ? qa[0] : kRhoFloor;
       const double prinv = 1.0 / prho;
-      const Prim<double> pr{prho, qa[1][k] * prinv, qa[2][k] * prinv, 0.0};
+      const Prim<double> pr{prho, qa[1] * prinv, qa[2] * prinv, 0.0};
       if (terms & 4) {
-        const double fxv = bind.use ? bind.fx[o] : fs * S.fx[o];
-        const double fyv = bind.use ? bind.fy[o] : fs * S.fy[o];
+        const double fxv = fsc * fxp[o];
+        const double fyv = fsc * fyp[o];
         const T rho_ = T(pr.rho), u = T(pr.u), vv = T(pr.v), tfx = T(fxv), tfy = T(fyv);
         rhs[1] += double(rho_ * tfx);
         rhs[2] += double(rho_ * tfy);
@@ -1019,22 +1035,22 @@ __global__ void __launch_bounds__(256, OCC ? (AXIS == 0 ? kSweepMinBlocksX : kSw
       }
       if (drag) {
         // Re sum_k P_k(row) e^{i k x}: the drag band synthesised per row
-        double lx = dpx[r][0].x, ly = dpy[r][0].x;
+        double lx = dpx[rr][0].x, ly = dpy[rr][0].x;
         int ix = 0;
-        for (int kk = 1; kk <= S.kx_drag; ++kk) {
+        for (int kk = 1; kk <= kxd; ++kk) {
           ix += col;
           if (ix >= nx) ix -= nx;  // (k x) mod nx
-          const double2 e = S.twx[ix];
+          const double2 e = twx[ix];
           const double er = e.x, ei = -e.y;  // e^{+i k x}
-          lx += dpx[r][kk].x * er - dpx[r][kk].y * ei;
-          ly += dpy[r][kk].x * er - dpy[r][kk].y * ei;
+          lx += dpx[rr][kk].x * er - dpx[rr][kk].y * ei;
+          ly += dpy[rr][kk].x * er - dpy[rr][kk].y * ei;
         }
         rhs[1] += lx;
         rhs[2] += ly;
         rhs[3] += pr.u * lx + pr.v * ly;
       }
     }
-    if (terms & 16) rhs[3] += sc[S_COOL];
+    if (terms & 16) rhs[3] += cool;
     if (mode == SW_RHS) {
 #pragma unroll
       for (int c = 0; c < 4; ++c) bind.out[c * plane + o] = rhs[c];
@@ -1043,18 +1059,18 @@ __global__ void __launch_bounds__(256, OCC ? (AXIS == 0 ? kSweepMinBlocksX : kSw
     double sv[4];
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
-      const double t = qa[c][k] + dt * rhs[c];
+      const double t = qa[c] + dt * rhs[c];
       if (stage == 0) sv[c] = t;
       else if (stage == 1) sv[c] = 0.75 * q0[c * plane + o] + 0.25 * t;
       else sv[c] = (1.0 / 3.0) * q0[c * plane + o] + (2.0 / 3.0) * t;
     }
-    enforce_node_rcp(sv[0], sv[1], sv[2], sv[3], S.gamma);
+    enforce_node_rcp(sv[0], sv[1], sv[2], sv[3], gam);
     if (gc == 0) {
 #pragma unroll
       for (int c = 0; c < 4; ++c) qo[c * plane + o] = sv[c];
     } else {
 #pragma unroll
-      for (int c = 0; c < 4; ++c) ST[(size_t)(r * 4 + c) * n + col] = sv[c];
+      for (int c = 0; c < 4; ++c) ST[(size_t)(rr * 4 + c) * n + col] = sv[c];
     }
   }
   if (gc == 0 || mode != SW_STAGE) return;
