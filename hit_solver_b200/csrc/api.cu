@@ -1139,6 +1139,22 @@ static int batch_build(hitb200_batch* b) {
   std::vector<Work> tiles, tiles32, xl, yl;
   std::vector<int> partner;
   const int n = (int)b->plans.size();
+  // y panels of 4 columns (full 32-byte row segments of the FP64 state)
+  // when the batch has enough columns for several waves of such CTAs and
+  // every member's panel fits in shared memory; else each plan's own width
+  int ry4 = 1;
+  {
+    int dev = 0, sms = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    long cols = 0;
+    for (hitb200_plan* p : b->plans) {
+      cols += (p->desc.nx + 3) / 4;
+      const size_t by = p->elem == 4 ? SweepLayout<float>(p->desc.ny, 4).bytes()
+                                     : SweepLayout<double>(p->desc.ny, 4).bytes();
+      if (by > 110 * 1024 || p->desc.nx < 4) ry4 = 0;
+    }
+    if (cols < 4L * sms) ry4 = 0;
+  }
   for (int i = 0; i < n; ++i) {
     hitb200_plan* p = b->plans[i];
     hs.push_back(p->hs);
@@ -1152,16 +1168,19 @@ static int batch_build(hitb200_batch* b) {
       for (int tx = 0; tx < ntx32; ++tx) tiles32.push_back({i, tx * kSenTX, ty * kSenTY, k32++});
     b->guard_blocks = std::max(b->guard_blocks, guard_blocks_for(p->desc));
     for (int r0 = 0; r0 < p->desc.ny; r0 += p->Rx) xl.push_back({i, r0, std::min(p->Rx, p->desc.ny - r0), 0});
-    for (int c0 = 0; c0 < p->desc.nx; c0 += p->Ry) yl.push_back({i, c0, std::min(p->Ry, p->desc.nx - c0), 0});
+    const int ry = ry4 ? 4 : p->Ry;
+    for (int c0 = 0; c0 < p->desc.nx; c0 += ry) yl.push_back({i, c0, std::min(ry, p->desc.nx - c0), 0});
     ModeTables mt = build_modes(p->desc);
     partner.insert(partner.end(), mt.partner.begin(), mt.partner.end());
     b->elem = p->elem;
     b->mch_x = std::max(b->mch_x, mch_for(p->desc.nx));
     b->mch_y = std::max(b->mch_y, mch_for(p->desc.ny));
     b->rx_max = std::max(b->rx_max, p->Rx);
-    b->ry_max = std::max(b->ry_max, p->Ry);
+    b->ry_max = std::max(b->ry_max, ry);
     b->smem_x = std::max(b->smem_x, p->smem_x);
-    b->smem_y = std::max(b->smem_y, p->smem_y);
+    b->smem_y = std::max(b->smem_y, ry4 ? (p->elem == 4 ? SweepLayout<float>(p->desc.ny, 4).bytes()
+                                                         : SweepLayout<double>(p->desc.ny, 4).bytes())
+                                         : p->smem_y);
     b->smem_sensor = std::max(b->smem_sensor, p->smem_sensor);
     b->any_outflow |= !p->desc.periodic;
     b->any_forcing |= p->desc.forcing_on;

@@ -14,15 +14,16 @@ constexpr unsigned kFull = 0xffffffffu;
 
 constexpr int kStencilThreads = 256;
 constexpr int kLineThreads = 128;  // sweep threads per grid line of a CTA
-// Occupancy targets of the throughput variant of the sweeps (OCC = 1; CTAs
-// of 256 threads per SM): they bound the registers per thread, so that many
-// solves' lines share an SM.  The latency variant (OCC = 0) keeps 2, for
+// Occupancy targets of the throughput variant of the sweeps (OCC = 1): CTAs
+// per SM, of 256 threads for x (up to 2 lines) and 512 for y (up to 4
+// lines); they bound the registers per thread, so that many solves' lines
+// share an SM.  The latency variants keep 128 registers per thread, for
 // launches too small to fill the GPU twice over.
 #ifndef HITB200_SWEEP_MIN_BLOCKS_X
 #define HITB200_SWEEP_MIN_BLOCKS_X 4
 #endif
 #ifndef HITB200_SWEEP_MIN_BLOCKS_Y
-#define HITB200_SWEEP_MIN_BLOCKS_Y 3
+#define HITB200_SWEEP_MIN_BLOCKS_Y 2
 #endif
 constexpr int kSweepMinBlocksX = HITB200_SWEEP_MIN_BLOCKS_X;
 constexpr int kSweepMinBlocksY = HITB200_SWEEP_MIN_BLOCKS_Y;
@@ -569,12 +570,13 @@ __device__ __forceinline__ void gload_run(const T* p, int len, T (&v)[N]) {
 // with L = -dF/dx - dG/dy + viscous + forcing + drag + cooling and clean the
 // enforce filter plus, on outflow grids, the guard cells.
 template <typename T, int AXIS, int MN, int OCC>
-__global__ void __launch_bounds__(256, OCC ? (AXIS == 0 ? kSweepMinBlocksX : kSweepMinBlocksY) : 2)
+__global__ void __launch_bounds__(AXIS == 0 ? 256 : 512,
+                                  AXIS == 0 ? (OCC ? kSweepMinBlocksX : 2) : (OCC ? kSweepMinBlocksY : 1))
     sweep_kernel(const SolveDev* __restrict__ solves, const Work* __restrict__ work, int stage,
                  int mode, Bind bind) {
   extern __shared__ __align__(16) unsigned char smem[];
-  __shared__ Affine<T> scan_f[2][4], scan_b[2][4];  // per line, per warp totals
-  __shared__ T ends[2][4][4];                          // raw_0, raw_n-1, p_0, p_n-1
+  __shared__ Affine<T> scan_f[4][4], scan_b[4][4];  // per line, per warp totals
+  __shared__ T ends[4][4][4];                          // raw_0, raw_n-1, p_0, p_n-1
   const Work wk = work[blockIdx.x];
   const SolveDev& S = solves[wk.solve];
   const double* sc = S.scal;
@@ -583,7 +585,7 @@ __global__ void __launch_bounds__(256, OCC ? (AXIS == 0 ? kSweepMinBlocksX : kSw
   const int n = AXIS == 0 ? nx : ny;
   const size_t plane = (size_t)nx * ny;
   const int line0 = wk.a, R = wk.b;
-  const int rsh = R > 1 ? 1 : 0;  // R is 1 or 2
+  const int rsh = R > 2 ? 2 : (R > 1 ? 1 : 0);  // R is 1 or 2 (x lines), up to 4 (y lines)
   const int RL = 1 << rsh;
   const SweepLayout<T> L(n, RL);
   const int LS = L.LS, LW = L.LW;
@@ -669,7 +671,11 @@ __global__ void __launch_bounds__(256, OCC ? (AXIS == 0 ? kSweepMinBlocksX : kSw
   // their (face, component) pairs are spread over the warp's lanes.
   const int nch = (n + 3 + 31) >> 5;
   for (int task = warp; task < R * nch; task += nwarp) {
-    const int r = task >= nch ? 1 : 0, ch = task - r * nch;
+    int r = 0, ch = task;
+    while (ch >= nch) {
+      ch -= nch;
+      ++r;
+    }
     const uint8_t* mk = MK + r * (n + 2) + 1;  // mk[i] = node i, i in [-1, n]
     const int il0 = ch * 32 - 2;
     const int il = il0 + lane;
@@ -766,7 +772,7 @@ __global__ void __launch_bounds__(256, OCC ? (AXIS == 0 ? kSweepMinBlocksX : kSw
       fw.m *= mo;
     }
   }
-  if (lane == 31 && r < 2) scan_f[r][lw] = fw;
+  if (lane == 31 && r < 4) scan_f[r][lw] = fw;
   // exclusive prefix within the warp
   Affine<T> fe;
   fe.m = __shfl_up_sync(kFull, fw.m, 1);
@@ -779,7 +785,7 @@ __global__ void __launch_bounds__(256, OCC ? (AXIS == 0 ? kSweepMinBlocksX : kSw
   }
   __syncthreads();
   {
-    const int rr = min(r, 1);
+    const int rr = min(r, 3);
     Affine<T> pre, tot;  // maps of the warps before this one, and of the whole line
     pre.m = tot.m = T(1);
 #pragma unroll
@@ -838,7 +844,7 @@ __global__ void __launch_bounds__(256, OCC ? (AXIS == 0 ? kSweepMinBlocksX : kSw
       bw.m *= mo;
     }
   }
-  if (lane == 0 && r < 2) scan_b[r][lw] = bw;
+  if (lane == 0 && r < 4) scan_b[r][lw] = bw;
   Affine<T> be;
   be.m = __shfl_down_sync(kFull, bw.m, 1);
 #pragma unroll
@@ -850,7 +856,7 @@ __global__ void __launch_bounds__(256, OCC ? (AXIS == 0 ? kSweepMinBlocksX : kSw
   }
   __syncthreads();
   {
-    const int rr = min(r, 1);
+    const int rr = min(r, 3);
     Affine<T> post, tot;  // maps of the warps after this one (innermost last), whole line
     post.m = tot.m = T(1);
 #pragma unroll
@@ -926,8 +932,34 @@ __global__ void __launch_bounds__(256, OCC ? (AXIS == 0 ? kSweepMinBlocksX : kSw
 
   // ---- E: epilogue ----------------------------------------------------------------------
   const int terms = bind.use ? bind.terms : fused_terms(S);
-  if (AXIS == 1 || mode == SW_DERIV) {
-    // y sweep: partial rhs -dG/dy (or the bare derivative for the API)
+  if (AXIS == 1) {
+    // y sweep: partial rhs -dG/dy (or the bare derivative for the API),
+    // staged in shared memory and written with consecutive threads on the
+    // R columns of a row, then the next row
+    T* XS = WB;  // [R][4][LW]
+#pragma unroll
+    for (int k = 0; k < MN; ++k)
+      if (k < len) {
+#pragma unroll
+        for (int c = 0; c < 4; ++c) XS[(r * 4 + c) * LW + i0 + k] = x[c][k];
+      }
+    __syncthreads();
+    T* rx = reinterpret_cast<T*>(S.rx);
+    for (int idx = threadIdx.x; idx < (n << rsh); idx += blockDim.x) {
+      const int rr = idx & (RL - 1), p = idx >> rsh;
+      if (rr >= R) continue;
+      const size_t o = (size_t)p * nx + line0 + rr;
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        const T d = XS[(rr * 4 + c) * LW + p];
+        if (mode == SW_DERIV) bind.out[c * plane + o] = double(d);
+        else rx[c * plane + o] = (terms & 1) ? -d : T(0);
+      }
+    }
+    return;
+  }
+  if (mode == SW_DERIV) {
+    // x derivative for the API
     T* rx = reinterpret_cast<T*>(S.rx);
 #pragma unroll
     for (int k = 0; k < MN; ++k) {
