@@ -687,6 +687,14 @@ int hitb200_plan_create(const hitb200_desc* d, hitb200_plan** out) {
   s.ky_drag = 0;
   for (const int2& m : mt.drag) s.ky_drag = std::max(s.ky_drag, std::abs(m.y));
   for (const int2& m : mt.force) s.kx_force = std::max(s.kx_force, std::abs(m.x));
+  {
+    int pos = 0;
+    for (int k = 0; k <= kMaxKx + 1; ++k) {
+      s.f_kofs[k] = (short)pos;
+      for (size_t m = 0; m < mt.force.size(); ++m)
+        if (std::abs(mt.force[m].x) == k) s.f_order[pos++] = (unsigned char)m;
+    }
+  }
   s.f_tau = d->forcing_correlation_time;
   s.f_rms = d->forcing_rms;
   s.f_has_target = !is_none(d->target_power);

@@ -87,6 +87,8 @@ struct SolveDev {
   int drag_on, n_drag;
   int kx_drag, kx_force;  // max |x bin| of the drag / forcing modes
   int ky_drag;            // max |y bin| of the drag modes
+  unsigned char f_order[kMaxForce];  // forcing modes ordered by |x bin| ...
+  short f_kofs[kMaxKx + 2];          // ... with |x bin| = k at f_order[f_kofs[k] .. f_kofs[k+1])
   double drag_coef;
   int cooling_on;
   double cooling_tau, cooling_pref;

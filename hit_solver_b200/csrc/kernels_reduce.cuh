@@ -632,9 +632,9 @@ __global__ void __launch_bounds__(kRedThreads)
     const int a = t / (K + 1), k = t - a * (K + 1);
     const int gj = min(w.b + a, ny - 1);
     double2 sx = make_double2(0.0, 0.0), sy = make_double2(0.0, 0.0);
-    for (int m = 0; m < nf; ++m) {
+    for (int j = S.f_kofs[k]; j < S.f_kofs[k + 1]; ++j) {
+      const int m = S.f_order[j];
       const int2 md = modes[m];
-      if (abs(md.x) != k) continue;
       const double2 e = S.twy[mode_index(md.y, gj, ny)];  // e^{-i ky y}
       const double er = e.x, ei = -e.y;                   // e^{+i ky y}
       double ar = ca[m].x * er - ca[m].y * ei, ai = ca[m].x * ei + ca[m].y * er;
