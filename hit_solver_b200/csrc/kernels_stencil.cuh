@@ -1154,6 +1154,12 @@ __global__ void __launch_bounds__(kStencilThreads)
   }
   __syncthreads();
   const T dx2 = T(S.dx * S.dx), dy2 = T(S.dy * S.dy);
+  const T idx2 = T(1.0 / (S.dx * S.dx)), idy2 = T(1.0 / (S.dy * S.dy));
+  // second differences: FP64 divides by h^2 as the reference; FP32 multiplies
+  auto d2 = [&](T a, T b, T c, T h2, T ih2) -> T {
+    if constexpr (sizeof(T) == 8) return (a - T(2) * b + c) / h2;
+    else return (a - T(2) * b + c) * ih2;
+  };
   for (int idx = threadIdx.x; idx < LX * LY; idx += blockDim.x) {
     int a = idx / LX, b = idx % LX;
     // outflow: the Laplacian is itself edge-padded before the second pass
@@ -1167,12 +1173,15 @@ __global__ void __launch_bounds__(kStencilThreads)
     const int qa = a + 1, qb = b + 1;
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
-      const T lx = (Qs[c][qa][qb + 1] - T(2) * Qs[c][qa][qb] + Qs[c][qa][qb - 1]) / dx2;
-      const T ly = (Qs[c][qa + 1][qb] - T(2) * Qs[c][qa][qb] + Qs[c][qa - 1][qb]) / dy2;
+      const T lx = d2(Qs[c][qa][qb + 1], Qs[c][qa][qb], Qs[c][qa][qb - 1], dx2, idx2);
+      const T ly = d2(Qs[c][qa + 1][qb], Qs[c][qa][qb], Qs[c][qa - 1][qb], dy2, idy2);
       Ls[c][idx / LX][idx % LX] = lx + ly;
     }
   }
   __syncthreads();
+  // solve fields in registers: the stores below cannot force reloads
+  const double gam = S.gamma;
+  const double hc[4] = {S.hv_coef[0], S.hv_coef[1], S.hv_coef[2], S.hv_coef[3]};
   for (int idx = threadIdx.x; idx < kHvTX * kHvTY; idx += blockDim.x) {
     const int ty = idx / kHvTX, tx = idx % kHvTX;
     const int gj = y0 + ty, gi = x0 + tx;
@@ -1183,12 +1192,12 @@ __global__ void __launch_bounds__(kStencilThreads)
     double s[4];
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
-      const T bx = (Ls[c][a][b + 1] - T(2) * Ls[c][a][b] + Ls[c][a][b - 1]) / dx2;
-      const T by = (Ls[c][a + 1][b] - T(2) * Ls[c][a][b] + Ls[c][a - 1][b]) / dy2;
+      const T bx = d2(Ls[c][a][b + 1], Ls[c][a][b], Ls[c][a][b - 1], dx2, idx2);
+      const T by = d2(Ls[c][a + 1][b], Ls[c][a][b], Ls[c][a - 1][b], dy2, idy2);
       const double bih = double(bx + by);
-      s[c] = q[c * plane + o] - (active ? S.hv_coef[c] : 0.0) * bih;
+      s[c] = q[c * plane + o] - (active ? hc[c] : 0.0) * bih;
     }
-    enforce_node(s[0], s[1], s[2], s[3], S.gamma);
+    enforce_node_rcp(s[0], s[1], s[2], s[3], gam);
 #pragma unroll
     for (int c = 0; c < 4; ++c) out[c * plane + o] = s[c];
   }
