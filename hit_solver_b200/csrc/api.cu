@@ -346,11 +346,7 @@ int launch_step_sequence(const LaunchSet& L, int any_forcing, int noise_upload, 
     PMARK("hv_sensor", 33 * N);
     launch_sensor(L, 3, 0, 0, nb, nullptr);
     PMARK("hv", 65 * N);
-    launch_hv(L, nb);
-    if (any_outflow) {
-      PMARK("guard", 0.0);
-      guard_kernel<<<dim3(L.guard_blocks, L.nsolves), 256, 0, L.st>>>(L.solves, L.nsolves, 0, nb);
-    }
+    launch_hv(L, nb);  // applies the outflow guard of outflow solves too
   }
   if (prof) prof->end();
   HB_LAUNCHED("step kernels");

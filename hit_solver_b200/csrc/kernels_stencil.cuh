@@ -1181,6 +1181,7 @@ __global__ void __launch_bounds__(kStencilThreads)
   __syncthreads();
   // solve fields in registers: the stores below cannot force reloads
   const double gam = S.gamma;
+  const int gcell = (!bind.use && !per) ? S.guard : 0;  // fused outflow guard of the step
   const double hc[4] = {S.hv_coef[0], S.hv_coef[1], S.hv_coef[2], S.hv_coef[3]};
   for (int idx = threadIdx.x; idx < kHvTX * kHvTY; idx += blockDim.x) {
     const int ty = idx / kHvTX, tx = idx % kHvTX;
@@ -1198,8 +1199,24 @@ __global__ void __launch_bounds__(kStencilThreads)
       s[c] = q[c * plane + o] - (active ? hc[c] : 0.0) * bih;
     }
     enforce_node_rcp(s[0], s[1], s[2], s[3], gam);
+    if (gcell == 0) {
 #pragma unroll
-    for (int c = 0; c < 4; ++c) out[c * plane + o] = s[c];
+      for (int c = 0; c < 4; ++c) out[c * plane + o] = s[c];
+      continue;
+    }
+    // Outflow guard fused (riemann_config3.py:419-429): guard cells are not
+    // written by their own threads; the thread of each source cell writes
+    // its value to itself and to the guard cells that copy it.
+    const bool guard_cell = gj < gcell || gj >= ny - gcell || gi < gcell || gi >= nx - gcell;
+    if (guard_cell) continue;
+    const int jlo = gj == gcell ? 0 : gj, jhi = gj == ny - gcell - 1 ? ny - 1 : gj;
+    const int ilo = gi == gcell ? 0 : gi, ihi = gi == nx - gcell - 1 ? nx - 1 : gi;
+    for (int jj = jlo; jj <= jhi; ++jj)
+      for (int ii = ilo; ii <= ihi; ++ii) {
+        const size_t od = (size_t)jj * nx + ii;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) out[c * plane + od] = s[c];
+      }
   }
 }
 
