@@ -225,23 +225,38 @@ struct Prof {
 #define PMARK(name, b) \
   if (prof) prof->mark(name, b)
 
+// Dynamic shared-memory opt-ins are per device; each kernel remembers the
+// largest size it was granted on each device.
+constexpr int kMaxAttrDevices = 64;
+std::mutex g_attr_mu;
+
+inline int attr_device() {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxAttrDevices) dev = 0;
+  return dev;
+}
+
 template <typename T, int AXIS, int MCH, int OCC>
 void set_sweep_attr(size_t bytes) {
-  static size_t done = 0;
-  if (bytes > done) {
+  static size_t done[kMaxAttrDevices] = {};
+  const int dev = attr_device();
+  std::lock_guard<std::mutex> lock(g_attr_mu);
+  if (bytes > done[dev]) {
     cudaFuncSetAttribute(sweep_kernel<T, AXIS, MCH, OCC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)bytes);
-    done = bytes;
+    done[dev] = bytes;
   }
 }
 
 template <typename T>
 void set_sensor_attr(size_t bytes) {
-  static size_t done = 0;
-  if (bytes > done) {
+  static size_t done[kMaxAttrDevices] = {};
+  const int dev = attr_device();
+  std::lock_guard<std::mutex> lock(g_attr_mu);
+  if (bytes > done[dev]) {
     cudaFuncSetAttribute(sensor_kernel<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
     cudaFuncSetAttribute(sensor_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-    done = bytes;
+    done[dev] = bytes;
   }
 }
 
@@ -618,8 +633,8 @@ int hitb200_plan_create(const hitb200_desc* d, hitb200_plan** out) {
   const size_t o_rx = a.take(4 * N * p->elem);
   const size_t o_vis = d->viscosity > 0.0 ? a.take(3 * N * p->elem) : 0;
   const size_t o_mask = a.take(N);
-  const size_t o_fx = d->forcing_on ? a.take(N * sizeof(double)) : 0;
-  const size_t o_fy = d->forcing_on ? a.take(N * sizeof(double)) : 0;
+  const size_t o_fx = d->forcing_on ? a.take(N * p->elem) : 0;
+  const size_t o_fy = d->forcing_on ? a.take(N * p->elem) : 0;
   const size_t o_noise = (d->forcing_on && d->noise_mode == 0) ? a.take(N * sizeof(double)) : 0;
   const size_t o_tw = a.take((nx + ny) * sizeof(double2));
   const size_t o_modes = a.take((mt.drag.size() + mt.force.size() + 1) * sizeof(int2));
@@ -720,8 +735,8 @@ int hitb200_plan_create(const hitb200_desc* d, hitb200_plan** out) {
   s.rx = base + o_rx;
   s.vis = d->viscosity > 0.0 ? (void*)(base + o_vis) : nullptr;
   s.mask = base + o_mask;
-  s.fx = d->forcing_on ? reinterpret_cast<double*>(base + o_fx) : nullptr;
-  s.fy = d->forcing_on ? reinterpret_cast<double*>(base + o_fy) : nullptr;
+  s.fx = d->forcing_on ? reinterpret_cast<void*>(base + o_fx) : nullptr;
+  s.fy = d->forcing_on ? reinterpret_cast<void*>(base + o_fy) : nullptr;
   s.noise = o_noise ? reinterpret_cast<double*>(base + o_noise) : nullptr;
   s.twx = reinterpret_cast<double2*>(base + o_tw);
   s.twy = s.twx + nx;
@@ -1016,8 +1031,13 @@ int hitb200_forcing_update(hitb200_plan* p, const double* q, const double* noise
   force_synth_kernel<<<L.n_tiles32, kRedThreads, 0, st>>>(L.solves, L.tiles32, b2);
   const size_t plane = (size_t)p->desc.nx * p->desc.ny;
   const int nb = (int)std::min<size_t>((plane + 255) / 256, 4096);
-  scale_copy_kernel<<<nb, 256, 0, st>>>(p->hs.fx, fx, p->hs.scal, S_F_SCALE, plane);
-  scale_copy_kernel<<<nb, 256, 0, st>>>(p->hs.fy, fy, p->hs.scal, S_F_SCALE, plane);
+  if (p->elem == 4) {
+    scale_copy_kernel<<<nb, 256, 0, st>>>((const float*)p->hs.fx, fx, p->hs.scal, S_F_SCALE, plane);
+    scale_copy_kernel<<<nb, 256, 0, st>>>((const float*)p->hs.fy, fy, p->hs.scal, S_F_SCALE, plane);
+  } else {
+    scale_copy_kernel<<<nb, 256, 0, st>>>((const double*)p->hs.fx, fx, p->hs.scal, S_F_SCALE, plane);
+    scale_copy_kernel<<<nb, 256, 0, st>>>((const double*)p->hs.fy, fy, p->hs.scal, S_F_SCALE, plane);
+  }
   HB_LAUNCHED("forcing_update");
   HB_CUDA(cudaStreamSynchronize(st));  // host-side scalars above live on this stack frame
   return HITB200_OK;

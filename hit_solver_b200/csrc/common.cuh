@@ -109,7 +109,7 @@ struct SolveDev {
   double *q, *q1, *q2;
   void *rx, *vis;
   uint8_t *mask;
-  double *fx, *fy;
+  void *fx, *fy;             // unit-rms forcing shape, T [ny][nx] (T = float in the FP32-bulk form)
   const double *noise;
   double2 *twx, *twy;        // e^{-2 pi i j / n}, j in [0, n)
   int2 *modes;               // n_drag drag modes, then n_force forcing modes (integer mx, my)

@@ -670,8 +670,13 @@ __global__ void __launch_bounds__(kRedThreads)
       fy += py[a][k].x * er - py[a][k].y * ei;
     }
     const size_t o = (size_t)gj * nx + gi;
-    S.fx[o] = fx;
-    S.fy[o] = fy;
+    if (S.precision == 1) {
+      static_cast<float*>(S.fx)[o] = (float)fx;
+      static_cast<float*>(S.fy)[o] = (float)fy;
+    } else {
+      static_cast<double*>(S.fx)[o] = fx;
+      static_cast<double*>(S.fy)[o] = fy;
+    }
     const Prim<double> p = primitives(q[o], q[o + plane], q[o + 2 * plane], q[o + 3 * plane], S.gamma);
     sxx += fx * fx;
     syy += fy * fy;

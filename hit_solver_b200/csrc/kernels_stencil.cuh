@@ -1032,9 +1032,11 @@ __global__ void __launch_bounds__(AXIS == 0 ? 256 : 512,
   const bool visc = (terms & 2) && S.mu > 0.0;
   const int kxd = S.kx_drag;
   const T* __restrict__ visp = reinterpret_cast<const T*>(S.vis);
-  const double* __restrict__ fxp = bind.use ? bind.fx : S.fx;
-  const double* __restrict__ fyp = bind.use ? bind.fy : S.fy;
-  const double fsc = bind.use ? 1.0 : fs;
+  // caller's FP64 accelerations (API) or the solve's scaled unit-rms shape (T)
+  const double* __restrict__ bfx = bind.fx;
+  const double* __restrict__ bfy = bind.fy;
+  const T* __restrict__ sfx = static_cast<const T*>(S.fx);
+  const T* __restrict__ sfy = static_cast<const T*>(S.fy);
   const double2* __restrict__ twx = S.twx;
   const double* __restrict__ qinr = qin;
   const T* __restrict__ ryr = ry;
@@ -1058,8 +1060,8 @@ __global__ void __launch_bounds__(AXIS == 0 ? 256 : 512,
       const double prinv = 1.0 / prho;
       const Prim<double> pr{prho, qa[1] * prinv, qa[2] * prinv, 0.0};
       if (terms & 4) {
-        const double fxv = fsc * fxp[o];
-        const double fyv = fsc * fyp[o];
+        const double fxv = bind.use ? bfx[o] : fs * double(sfx[o]);
+        const double fyv = bind.use ? bfy[o] : fs * double(sfy[o]);
         const T rho_ = T(pr.rho), u = T(pr.u), vv = T(pr.v), tfx = T(fxv), tfy = T(fyv);
         rhs[1] += double(rho_ * tfx);
         rhs[2] += double(rho_ * tfy);
@@ -1268,12 +1270,13 @@ __global__ void enforce_kernel(const double* __restrict__ q, double* __restrict_
 }
 
 // out[c] = scale * a  (forcing accelerations for the API, viscous copy)
-__global__ void scale_copy_kernel(const double* __restrict__ a, double* __restrict__ out,
+template <typename A>
+__global__ void scale_copy_kernel(const A* __restrict__ a, double* __restrict__ out,
                                   const double* __restrict__ scal, int slot, size_t n) {
   const double s = slot >= 0 ? scal[slot] : 1.0;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
        i += (size_t)gridDim.x * blockDim.x)
-    out[i] = s * a[i];
+    out[i] = s * double(a[i]);
 }
 
 template <typename T>
