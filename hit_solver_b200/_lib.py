@@ -28,7 +28,7 @@ S_ALPHA_X, S_ALPHA_Y, S_DIV_RMS, S_VORT_RMS, S_DT, S_TIME, S_STEP, S_ACTIVE, S_M
  S_F_FXX, S_F_FYY, S_F_FXY, S_F_AF, S_F_DECAY, S_F_SCALE, S_MAX_STEPS, S_STATUS,
  S_NEAR_THRESHOLD, S_HV_APPLIED) = range(9, 25)
 S_COUNT = 32
-TUNE_SWEEP_X, TUNE_SWEEP_Y, TUNE_PREPASS, TUNE_COUNT = 0, 1, 2, 3
+TUNE_SWEEP_X, TUNE_SWEEP_Y, TUNE_PREPASS, TUNE_FUSED_SENSOR, TUNE_COUNT = 0, 1, 2, 3, 4
 
 NAN = float("nan")
 

@@ -1,7 +1,8 @@
 """Autotuner of the kernel variants.
 
 Three kernel families have two compiled variants each: the x sweep, the y
-sweep and the prepass.  The latency variant keeps more registers per thread
+sweep and the prepass; a fourth knob fuses each prepass into the following
+sensor launch (single solves whose tiles all fit on the GPU at once).  The latency variant keeps more registers per thread
 and suits launches that cannot fill the GPU (one 512^2 solve); the
 throughput variant fits more CTAs per SM and suits launches over many solves.
 Plans and batches start from a default picked by launch size.  The tuner
@@ -25,12 +26,13 @@ from . import _lib, core
 _cache: dict = {}
 _lock = threading.Lock()
 
-# profile labels of each knob's kernels (hitb200_step_profile names)
+# profile labels of each variant knob's kernels (hitb200_step_profile names)
 _FAMILIES = {
     _lib.TUNE_SWEEP_X: ("sweep_x",),
     _lib.TUNE_SWEEP_Y: ("sweep_y",),
     _lib.TUNE_PREPASS: ("prepass", "hv_prepass"),
 }
+_VARIANT_KNOBS = (_lib.TUNE_SWEEP_X, _lib.TUNE_SWEEP_Y, _lib.TUNE_PREPASS)
 
 
 def signature(descs) -> tuple:
@@ -42,24 +44,51 @@ def signature(descs) -> tuple:
     return (descs[0].precision, tuple(members))
 
 
-def _family_ms(profile_fn, trials: int) -> dict:
-    """Mean device time per step of each knob's kernels over `trials` steps."""
-    tot = {k: 0.0 for k in _FAMILIES}
+def _profile_ms(profile_fn, trials: int):
+    """Mean device time per step of each knob's kernels, and of the whole
+    step, over `trials` steps."""
+    fam = {k: 0.0 for k in _FAMILIES}
+    total = 0.0
     for _ in range(trials):
         for name, ms, _ in profile_fn():
+            total += ms
             for k, names in _FAMILIES.items():
                 if name in names:
-                    tot[k] += ms
-    return {k: v / trials for k, v in tot.items()}
+                    fam[k] += ms
+    return {k: v / trials for k, v in fam.items()}, total / trials
 
 
-def _choose(profile_fn, set_fn, trials: int) -> list[int]:
+def _graph_ms(run_fn, steps: int) -> float:
+    """Device time per step of `steps` graph-replayed steps."""
+    st = torch.cuda.current_stream()
+    run_fn(1)  # capture
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(st)
+    run_fn(steps)
+    b.record(st)
+    torch.cuda.synchronize()
+    return a.elapsed_time(b) / steps
+
+
+def _choose(profile_fn, set_fn, trials: int, run_fn=None) -> list[int]:
+    """Variant knobs: each family's faster variant by per-launch times (fused
+    sensor off); then, where run_fn can replay the plan's steps and the plan
+    can fuse its prepasses into the sensors, whichever of fused / unfused
+    gives the shorter graph-replayed step (launch gaps matter there)."""
     ms = {}
     for variant in (0, 1):
-        set_fn([variant] * _lib.TUNE_COUNT)
+        set_fn([variant, variant, variant, 0])
         profile_fn()  # warm-up step of this variant
-        ms[variant] = _family_ms(profile_fn, trials)
-    return [0 if ms[0][k] <= ms[1][k] else 1 for k in range(_lib.TUNE_COUNT)]
+        ms[variant] = _profile_ms(profile_fn, trials)[0]
+    best = [0 if ms[0][k] <= ms[1][k] else 1 for k in _VARIANT_KNOBS] + [0]
+    if run_fn is not None:
+        step = {}
+        for fused in (0, 1):
+            set_fn(best[:3] + [fused])
+            step[fused] = _graph_ms(run_fn, max(4, 2 * trials))
+        best[_lib.TUNE_FUSED_SENSOR] = 0 if step[0] <= step[1] else 1
+    set_fn(best)
+    return best
 
 
 def tune_batch(batch, trials: int = 3, use_cache: bool = True) -> list[int]:
@@ -101,7 +130,10 @@ def tune_plan(plan, q, trials: int = 3, use_cache: bool = True) -> list[int]:
         qc = q.clone()
         sc = plan.scalars()
         scratch.set_time(sc[_lib.S_TIME], int(sc[_lib.S_STEP]), sc[_lib.S_DT], -1)
-        best = _choose(lambda: scratch.step_profile(qc), scratch.set_tuning, trials)
+        run = None
+        if not (plan.desc.forcing_on and plan.desc.noise_mode == 0):
+            run = lambda n: scratch.run(qc, n)  # noqa: E731
+        best = _choose(lambda: scratch.step_profile(qc), scratch.set_tuning, trials, run)
         del scratch, qc
         torch.cuda.synchronize()
         with _lock:

@@ -137,6 +137,7 @@ void default_tuning(int n_x, int n_y, int n_tiles32, int* t) {
   t[HITB200_TUNE_SWEEP_X] = n_x >= 6 * sms;
   t[HITB200_TUNE_SWEEP_Y] = n_y >= 4 * sms;
   t[HITB200_TUNE_PREPASS] = n_tiles32 >= 4 * sms;
+  t[HITB200_TUNE_FUSED_SENSOR] = 0;  // measured slower at 512^2; the autotuner decides
 }
 
 }  // namespace
@@ -160,14 +161,15 @@ struct hitb200_plan {
   cudaStream_t graph_stream = nullptr;
   const double* graph_q = nullptr;
   bool in_batch = false;
-  SolveDev* own_solve = nullptr;
-  int tuning[HITB200_TUNE_COUNT] = {0, 0, 0};  // kernel variants (0 latency, 1 throughput)  // the arena's descriptor (d_solve points into a batch table while batched)
+  SolveDev* own_solve = nullptr;  // the arena's descriptor (d_solve points into a batch table while batched)
+  int tuning[HITB200_TUNE_COUNT] = {0, 0, 0, 0};  // kernel variants (tuning knobs)
+  bool fuse_ok = false;  // all of the fused sensor's CTAs fit on the GPU at once
 };
 
 struct hitb200_batch {
   std::vector<hitb200_plan*> plans;
   bool owns_plans = true;  // false for hitb200_batch_from_plans
-  int tuning[HITB200_TUNE_COUNT] = {0, 0, 0};
+  int tuning[HITB200_TUNE_COUNT] = {0, 0, 0, 0};
   SolveDev* d_solves = nullptr;
   Work *d_tiles = nullptr, *d_tiles32 = nullptr, *d_xlines = nullptr, *d_ylines = nullptr;
   int* d_partner = nullptr;
@@ -190,6 +192,7 @@ struct LaunchSet {
   int n_tiles, n_tiles32, n_x, n_y, elem, mch_x, mch_y, guard_blocks;
   int thr_x, thr_y;  // sweep CTA sizes: kLineThreads per line of the widest work item
   int occ_x, occ_y, occ_pre;  // kernel variants: 0 latency, 1 throughput (tuning knobs)
+  int fused;                  // prepass fused into the sensor (single solves, tuning knob)
   size_t smem_x, smem_y, smem_sensor;
   cudaStream_t st;
   // cells of all solves, and of the solves carrying viscous / forcing terms
@@ -254,8 +257,9 @@ void set_sensor_attr(size_t bytes) {
   const int dev = attr_device();
   std::lock_guard<std::mutex> lock(g_attr_mu);
   if (bytes > done[dev]) {
-    cudaFuncSetAttribute(sensor_kernel<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-    cudaFuncSetAttribute(sensor_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    cudaFuncSetAttribute(sensor_kernel<T, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    cudaFuncSetAttribute(sensor_kernel<T, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    cudaFuncSetAttribute(sensor_kernel<T, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
     done[dev] = bytes;
   }
 }
@@ -297,16 +301,42 @@ void launch_sweep(const LaunchSet& L, int axis, int stage, int mode, const Bind&
 template <typename T>
 void launch_sensor_t(const LaunchSet& L, int sel, int enf, int visc, const Bind& b, uint8_t* mo) {
   if (b.use)
-    sensor_kernel<T, true><<<L.n_tiles32, kSensorThreads, L.smem_sensor, L.st>>>(
+    sensor_kernel<T, true, false><<<L.n_tiles32, kSensorThreads, L.smem_sensor, L.st>>>(
         L.solves, L.tiles32, sel, enf, visc, b, mo);
   else
-    sensor_kernel<T, false><<<L.n_tiles32, kSensorThreads, L.smem_sensor, L.st>>>(
+    sensor_kernel<T, false, false><<<L.n_tiles32, kSensorThreads, L.smem_sensor, L.st>>>(
         L.solves, L.tiles32, sel, enf, visc, b, mo);
 }
 void launch_sensor(const LaunchSet& L, int sel, int enf, int visc, const Bind& b, uint8_t* mo) {
   if (L.elem == 4) launch_sensor_t<float>(L, sel, enf, visc, b, mo);
   else launch_sensor_t<double>(L, sel, enf, visc, b, mo);
 }
+// The prepass of `sel`'s state fused with its sensor: one cooperative launch
+// of the FUSED sensor (single solves whose tiles are all resident at once).
+template <typename T>
+void launch_presensor_t(const LaunchSet& L, int sel) {
+  Bind nb{};
+  uint8_t* mo = nullptr;
+  int enf = sel == 3 ? 0 : 1, visc = sel == 3 ? 0 : 1;
+  void* args[] = {(void*)&L.solves, (void*)&L.tiles32, (void*)&sel, (void*)&enf, (void*)&visc,
+                  (void*)&nb, (void*)&mo};
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(L.n_tiles32);
+  cfg.blockDim = dim3(kSensorThreads);
+  cfg.dynamicSmemBytes = L.smem_sensor;
+  cfg.stream = L.st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelExC(&cfg, (const void*)sensor_kernel<T, false, true>, args);
+}
+void launch_presensor(const LaunchSet& L, int sel) {
+  if (L.elem == 4) launch_presensor_t<float>(L, sel);
+  else launch_presensor_t<double>(L, sel);
+}
+
 void launch_hv(const LaunchSet& L, const Bind& b) {
   if (L.elem == 4) hv_kernel<float><<<L.n_tiles, kStencilThreads, 0, L.st>>>(L.solves, L.tiles, b);
   else hv_kernel<double><<<L.n_tiles, kStencilThreads, 0, L.st>>>(L.solves, L.tiles, b);
@@ -329,8 +359,13 @@ int launch_step_sequence(const LaunchSet& L, int any_forcing, int noise_upload, 
                          int any_hv, Prof* prof = nullptr) {
   Bind nb{};
   const double N = L.cells, e = L.elem;
-  PMARK("prepass", 32 * N);
-  launch_prepass(L, 0, PRE_STEP, 1, nb);
+  if (L.fused) {
+    PMARK("presensor", 65 * N + 3 * e * L.cells_visc);
+    launch_presensor(L, 0);  // the step's prepass and the first stage's sensor
+  } else {
+    PMARK("prepass", 32 * N);
+    launch_prepass(L, 0, PRE_STEP, 1, nb);
+  }
   if (any_forcing) {
     if (noise_upload) {
       PMARK("noise_dft", 8 * L.cells_force);
@@ -343,12 +378,19 @@ int launch_step_sequence(const LaunchSet& L, int any_forcing, int noise_upload, 
     force_synth_kernel<<<L.n_tiles32, kRedThreads, 0, L.st>>>(L.solves, L.tiles32, nb);
   }
   for (int stage = 0; stage < 3; ++stage) {
-    if (stage > 0) {
-      PMARK("prepass", 32 * N);
-      launch_prepass(L, stage, PRE_STAGE, 1, nb);
+    if (L.fused) {
+      if (stage > 0) {
+        PMARK("presensor", 65 * N + 3 * e * L.cells_visc);
+        launch_presensor(L, stage);
+      }
+    } else {
+      if (stage > 0) {
+        PMARK("prepass", 32 * N);
+        launch_prepass(L, stage, PRE_STAGE, 1, nb);
+      }
+      PMARK("sensor", 33 * N + 3 * e * L.cells_visc);
+      launch_sensor(L, stage, 1, 1, nb, nullptr);
     }
-    PMARK("sensor", 33 * N + 3 * e * L.cells_visc);
-    launch_sensor(L, stage, 1, 1, nb, nullptr);
     // y sweep: q, mask -> -dG/dy; x sweep: q, mask, -dG/dy, sources (, q) -> stage state
     PMARK("sweep_y", 33 * N + 4 * e * N);
     launch_sweep(L, 1, stage, SW_STAGE, nb);
@@ -356,10 +398,15 @@ int launch_step_sequence(const LaunchSet& L, int any_forcing, int noise_upload, 
     launch_sweep(L, 0, stage, SW_STAGE, nb);
   }
   if (any_hv) {
-    PMARK("hv_prepass", 32 * N);
-    launch_prepass(L, 1, PRE_SENSOR, 0, nb);
-    PMARK("hv_sensor", 33 * N);
-    launch_sensor(L, 3, 0, 0, nb, nullptr);
+    if (L.fused) {
+      PMARK("hv_presensor", 65 * N);
+      launch_presensor(L, 3);
+    } else {
+      PMARK("hv_prepass", 32 * N);
+      launch_prepass(L, 1, PRE_SENSOR, 0, nb);
+      PMARK("hv_sensor", 33 * N);
+      launch_sensor(L, 3, 0, 0, nb, nullptr);
+    }
     PMARK("hv", 65 * N);
     launch_hv(L, nb);  // applies the outflow guard of outflow solves too
   }
@@ -413,6 +460,7 @@ LaunchSet plan_launch_set(hitb200_plan* p, cudaStream_t st) {
   L.occ_x = p->tuning[HITB200_TUNE_SWEEP_X];
   L.occ_y = p->tuning[HITB200_TUNE_SWEEP_Y];
   L.occ_pre = p->tuning[HITB200_TUNE_PREPASS];
+  L.fused = p->tuning[HITB200_TUNE_FUSED_SENSOR] && p->fuse_ok;
   L.smem_x = p->smem_x;
   L.smem_y = p->smem_y;
   L.smem_sensor = p->smem_sensor;
@@ -819,6 +867,21 @@ int hitb200_plan_create(const hitb200_desc* d, hitb200_plan** out) {
     return cuda_fail(e, "cudaMemset(counters)");
   }
   prime_attributes(p->elem, mch_for(nx), mch_for(ny), p->smem_x, p->smem_y, p->smem_sensor);
+  {
+    // the fused sensor needs every tile's CTA resident at once (grid barrier)
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaError_t oe = p->elem == 4
+        ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sensor_kernel<float, false, true>,
+                                                        kSensorThreads, p->smem_sensor)
+        : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sensor_kernel<double, false, true>,
+                                                        kSensorThreads, p->smem_sensor);
+    int coop = 0;
+    cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
+    p->fuse_ok = oe == cudaSuccess && coop && (long)per_sm * sms >= p->n_tiles32;
+    cudaGetLastError();
+  }
   {
     // powers of the compact-solve root for the non-periodic end corrections
     double tab[kPowTab];
@@ -1394,6 +1457,7 @@ static LaunchSet batch_launch_set(hitb200_batch* b, cudaStream_t st) {
   L.occ_x = b->tuning[HITB200_TUNE_SWEEP_X];
   L.occ_y = b->tuning[HITB200_TUNE_SWEEP_Y];
   L.occ_pre = b->tuning[HITB200_TUNE_PREPASS];
+  L.fused = 0;  // the fused sensor's grid barrier spans one solve
   L.smem_x = b->smem_x;
   L.smem_y = b->smem_y;
   L.smem_sensor = b->smem_sensor;

@@ -67,7 +67,7 @@ enum Scal : int {
 };
 
 // Status bits accumulated in S_STATUS.
-enum StatusBits : int { ST_NONFINITE = 1, ST_NONPOS_RHO = 2, ST_NONPOS_P = 4 };
+enum StatusBits : int { ST_NONFINITE = 1, ST_NONPOS_RHO = 2, ST_NONPOS_P = 4, ST_BARRIER = 8 };
 
 // ---- per-solve descriptor (device resident, read-only in kernels) -------------
 struct SolveDev {
@@ -116,7 +116,7 @@ struct SolveDev {
   double2 *kvec;             // physical (kx, ky) of the forcing modes
   double *scal;
   double *part_pre, *part_noise, *part_synth, *part_diag;
-  unsigned *counters;        // [0] prepass, [1] noise, [2] synth, [3] diag
+  unsigned *counters;        // [0] prepass, [1] noise, [2] synth, [3] diag, [4..6] grid barrier
   int *near_count;
   double *diag_out;          // diagnostics results (device)
 };

@@ -169,15 +169,14 @@ __device__ __forceinline__ EnfPrim<T> enforced_prim(double q0, double q1, double
   return r;
 }
 
-template <typename T, int OCC>
-__global__ void __launch_bounds__(kPreThreads, OCC ? HITB200_PRE_MIN_BLOCKS : 2)
-    prepass_kernel(const SolveDev* __restrict__ solves, const Work* __restrict__ work, int buf,
-                   int mode, int enf, Bind bind) {
-  const Work w = work[blockIdx.x];
-  const SolveDev& S = solves[w.solve];
-  double* sc = S.scal;
-  if (mode == PRE_SENSOR && !bind.use && sc[S_HV_STEP] == 0.0) return;  // no hyperviscosity this step
-  if (mode == PRE_STAGE && !bind.use && sc[S_ACTIVE] == 0.0) return;
+// One tile of the prepass: every quantity it reduces, for the tile's cells,
+// into this CTA's row of partials (S.part_pre[w.c][*]); returns the number of
+// slots.  Runs on the first kPreThreads threads of the CTA; every thread of
+// the CTA must call it (it synchronises the CTA).
+template <typename T>
+__device__ int prepass_tile(const SolveDev& S, const Work& w, int buf, int mode, int enf,
+                            const Bind& bind) {
+  const bool act = threadIdx.x < kPreThreads;
   const double* q = bind.use ? bind.qin : stage_in(S, buf);
   const int nx = S.nx, ny = S.ny, per = S.periodic;
   const size_t plane = (size_t)nx * ny;
@@ -200,11 +199,10 @@ __global__ void __launch_bounds__(kPreThreads, OCC ? HITB200_PRE_MIN_BLOCKS : 2)
   __shared__ double cbuf[kPreWarps][4][32];          // per-warp column partials of one k
   __shared__ double ctab[kMaxKyDrag + 1][4][32];     // C_k(x) = sum_y m(x, y) e^{-i k y}
   __shared__ double sm[kPreWarps * (R_FIXED + 4 * kMaxDrag)];
-  __shared__ double red[R_FIXED + 4 * kMaxDrag];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 
   const int KY = ndrag > 0 ? S.ky_drag : -1;
-  for (int t = threadIdx.x; t < kTileY * (KY + 1); t += kPreThreads) {
+  for (int t = threadIdx.x; act && t < kTileY * (KY + 1); t += kPreThreads) {
     const int a = t / (KY + 1), k = t - a * (KY + 1);
     const int gj = min(y0 + a, ny - 1);
     tw[a][k] = S.twy[mode_index(k, gj, ny)];
@@ -216,7 +214,7 @@ __global__ void __launch_bounds__(kPreThreads, OCC ? HITB200_PRE_MIN_BLOCKS : 2)
   const int gi = x0 + lane;
   // one-node ring for the central differences (corners are not used), loaded
   // first so that its latency overlaps the tile's
-  const bool ring = grads && threadIdx.x < 4 * kTileX;
+  const bool ring = grads && threadIdx.x < 4 * kTileX;  // within the first kPreThreads
   int ra = 0, rb = 0;  // smem coordinates
   double rq[4] = {0.0, 0.0, 0.0, 0.0};
   if (ring) {
@@ -235,6 +233,7 @@ __global__ void __launch_bounds__(kPreThreads, OCC ? HITB200_PRE_MIN_BLOCKS : 2)
   for (int k = 0; k < kPreRows; ++k) {
     const int a = warp + kPreWarps * k, gj = y0 + a;
     m0[k] = m1[k] = 0.0;
+    if (!act) continue;
     if (gj >= ny || gi >= nx) {
       // beyond the grid in a partial tile: the folded node is the halo of
       // the last row / column
@@ -299,7 +298,7 @@ __global__ void __launch_bounds__(kPreThreads, OCC ? HITB200_PRE_MIN_BLOCKS : 2)
 #pragma unroll
     for (int k = 0; k < kPreRows; ++k) {
       const int a0 = warp + kPreWarps * k, gj = y0 + a0;
-      if (gj >= ny || gi >= nx) continue;
+      if (!act || gj >= ny || gi >= nx) continue;
       // sensor divergence / vorticity: central, one-sided at outflow edges
       const int a = a0 + 1, b = lane + 1;
       T dudx, dvdx, dudy, dvdy;
@@ -334,6 +333,7 @@ __global__ void __launch_bounds__(kPreThreads, OCC ? HITB200_PRE_MIN_BLOCKS : 2)
   } else {
     __syncthreads();  // tw table
   }
+  if (act) {
   warp_to_smem4<OP_MAX>(ax, ay, mr, mp, sm, make_int4(R_AX, R_AY, R_RHO, R_P), nslots);
   warp_to_smem4<OP_MAX>(me, sr, 0.0, 0.0, sm, make_int4(R_E, R_SR, -1, -1), nslots);
   warp_to_smem4<OP_SUM>(div2, vort2, ps, vel2, sm, make_int4(R_DIV2, R_VORT2, R_PSUM, R_VEL2), nslots);
@@ -344,6 +344,7 @@ __global__ void __launch_bounds__(kPreThreads, OCC ? HITB200_PRE_MIN_BLOCKS : 2)
     sm[warp * nslots + R_NONPOS_RHO] = (bad & 2) ? 1.0 : 0.0;
     sm[warp * nslots + R_NONPOS_P] = (bad & 4) ? 1.0 : 0.0;
   }
+  }
   // low-k momentum transform of the drag band filter (OOP/hit2d.py:352-399),
   // separable: C_k(x) = sum_y m(x, y) e^{-i k y} per column for k = 0..ky_drag
   // (C_{-k} = conj C_k for real m), then per mode sum_x e^{-i kx x} C_ky(x).
@@ -353,6 +354,7 @@ __global__ void __launch_bounds__(kPreThreads, OCC ? HITB200_PRE_MIN_BLOCKS : 2)
     double v[4] = {0.0, 0.0, 0.0, 0.0};  // Re, Im of m0; Re, Im of m1
 #pragma unroll
     for (int kk = 0; kk < kPreRows; ++kk) {
+      if (!act) break;
       const double2 ey = tw[warp + kPreWarps * kk][k];
       v[0] += m0[kk] * ey.x;
       v[1] += m0[kk] * ey.y;
@@ -360,7 +362,8 @@ __global__ void __launch_bounds__(kPreThreads, OCC ? HITB200_PRE_MIN_BLOCKS : 2)
       v[3] += m1[kk] * ey.y;
     }
 #pragma unroll
-    for (int j = 0; j < 4; ++j) cbuf[warp][j][lane] = v[j];
+    for (int j = 0; j < 4; ++j)
+      if (act) cbuf[warp][j][lane] = v[j];
     __syncthreads();
     if (warp < 4) {
       double acc = cbuf[0][warp][lane];
@@ -370,7 +373,7 @@ __global__ void __launch_bounds__(kPreThreads, OCC ? HITB200_PRE_MIN_BLOCKS : 2)
     }
     __syncthreads();
   }
-  for (int md = warp; md < ndrag; md += kPreWarps) {
+  for (int md = warp; act && md < ndrag; md += kPreWarps) {
     const int2 km = S.modes[md];
     const int ky = abs(km.y);
     const double sy = km.y < 0 ? -1.0 : 1.0;  // conjugate for negative ky
@@ -392,7 +395,8 @@ __global__ void __launch_bounds__(kPreThreads, OCC ? HITB200_PRE_MIN_BLOCKS : 2)
     if (lane < 4) S.part_pre[(size_t)w.c * nslots + sl + lane] = sm[warp * nslots + sl + lane];
   }
   __syncthreads();
-  for (int t = threadIdx.x; t < R_FIXED; t += blockDim.x) {
+  for (int t = threadIdx.x; t < R_FIXED; t += kPreThreads) {
+    if (!act) break;
     const int op = pre_op(t);
     double acc = sm[t];
     for (int ww = 1; ww < kPreWarps; ++ww) {
@@ -401,39 +405,44 @@ __global__ void __launch_bounds__(kPreThreads, OCC ? HITB200_PRE_MIN_BLOCKS : 2)
     }
     S.part_pre[(size_t)w.c * nslots + t] = acc;
   }
-  if (!last_block(&S.counters[0], S.nblk_pre)) return;
+  return nslots;
+}
 
-  // ---- last CTA of this solve: fixed-order final reduction + scalar logic ----
-  // Every thread takes one slot and every C-th block (C = threads / slots),
-  // with many loads in flight; the C partials of a slot are then combined in
-  // a fixed order.
-  {
-    __shared__ double chunk[kPreThreads];
-    const int C = max(1, kPreThreads / nslots);
-    const int t = threadIdx.x % nslots, j = threadIdx.x / nslots;
-    const int op = pre_op(t);
-    double acc = op == OP_SUM ? 0.0 : -INFINITY;
-    if (j < C) {
+// Fixed-order final reduction of the prepass partials of solve S into red[]:
+// every thread takes one slot and every C-th block (C = kPreThreads / slots),
+// with many loads in flight, and the C partials of a slot are combined in a
+// fixed order.  Every thread of the CTA must call it; the first kPreThreads
+// work.  The result is the same whichever CTA computes it.
+__device__ void prepass_finalize(const SolveDev& S, int nslots, double* red) {
+  __shared__ double chunk[kPreThreads];
+  const int C = max(1, kPreThreads / nslots);
+  const int t = threadIdx.x % nslots, j = threadIdx.x / nslots;
+  const int op = pre_op(t);
+  double acc = op == OP_SUM ? 0.0 : -INFINITY;
+  if (threadIdx.x < kPreThreads && j < C) {
 #pragma unroll 8
-      for (int b = j; b < S.nblk_pre; b += C) {
-        const double x = __ldcg(S.part_pre + (size_t)b * nslots + t);
-        acc = op == OP_SUM ? acc + x : fmax(acc, x);
-      }
-      chunk[j * nslots + t] = acc;
+    for (int b = j; b < S.nblk_pre; b += C) {
+      const double x = __ldcg(S.part_pre + (size_t)b * nslots + t);
+      acc = op == OP_SUM ? acc + x : fmax(acc, x);
     }
-    __syncthreads();
-    if (threadIdx.x < nslots) {
-      double v = chunk[threadIdx.x];
-      for (int jj = 1; jj < C; ++jj) {
-        const double x = chunk[jj * nslots + threadIdx.x];
-        v = op == OP_SUM ? v + x : fmax(v, x);
-      }
-      red[threadIdx.x] = v;
-    }
-    __syncthreads();
+    chunk[j * nslots + t] = acc;
   }
-  if (threadIdx.x != 0) return;
-  const double N = (double)nx * (double)ny;
+  __syncthreads();
+  if (threadIdx.x < nslots) {
+    double v = chunk[threadIdx.x];
+    for (int jj = 1; jj < C; ++jj) {
+      const double x = chunk[jj * nslots + threadIdx.x];
+      v = op == OP_SUM ? v + x : fmax(v, x);
+    }
+    red[threadIdx.x] = v;
+  }
+  __syncthreads();
+}
+
+// The scalar logic of one prepass from its reductions (one thread).
+__device__ void prepass_scalars(const SolveDev& S, const double* red, double* sc, int mode,
+                                bool api) {
+  const double N = (double)S.nx * (double)S.ny;
   int status = 0;
   if (red[R_NONFINITE] > 0.0) status |= ST_NONFINITE;
   if (red[R_NONPOS_RHO] > 0.0) status |= ST_NONPOS_RHO;
@@ -455,7 +464,7 @@ __global__ void __launch_bounds__(kPreThreads, OCC ? HITB200_PRE_MIN_BLOCKS : 2)
   sc[S_EPS_P] = 1e-14 + 1e-12 * red[R_P];
   sc[S_EPS_E] = 1e-14 + 1e-12 * red[R_E];
   if (mode == PRE_SENSOR) {
-    if (!bind.use) sc[S_HV_APPLIED] += 1.0;  // this prepass runs only on hyperviscosity steps
+    if (!api) sc[S_HV_APPLIED] += 1.0;  // this prepass runs only on hyperviscosity steps
     return;
   }
   // cooling_source (OOP/hit2d.py:402-426)
@@ -466,6 +475,24 @@ __global__ void __launch_bounds__(kPreThreads, OCC ? HITB200_PRE_MIN_BLOCKS : 2)
   for (int m = 0; m < S.n_drag; ++m)
     for (int k = 0; k < 4; ++k) sc[S_DRAG + 4 * m + k] = (-S.drag_coef / N) * red[R_FIXED + 4 * m + k];
   if (mode == PRE_STEP) step_control(S, red, sc);
+}
+
+
+template <typename T, int OCC>
+__global__ void __launch_bounds__(kPreThreads, OCC ? HITB200_PRE_MIN_BLOCKS : 2)
+    prepass_kernel(const SolveDev* __restrict__ solves, const Work* __restrict__ work, int buf,
+                   int mode, int enf, Bind bind) {
+  const Work w = work[blockIdx.x];
+  const SolveDev& S = solves[w.solve];
+  double* sc = S.scal;
+  if (mode == PRE_SENSOR && !bind.use && sc[S_HV_STEP] == 0.0) return;  // no hyperviscosity this step
+  if (mode == PRE_STAGE && !bind.use && sc[S_ACTIVE] == 0.0) return;
+  const int nslots = prepass_tile<T>(S, w, buf, mode, enf, bind);
+  if (!last_block(&S.counters[0], S.nblk_pre)) return;
+  // ---- last CTA of this solve: fixed-order final reduction + scalar logic ----
+  __shared__ double red[R_FIXED + 4 * kMaxDrag];
+  prepass_finalize(S, nslots, red);
+  if (threadIdx.x == 0) prepass_scalars(S, red, sc, mode, bind.use);
 }
 
 // Forward transform of the caller's white-noise field restricted to the

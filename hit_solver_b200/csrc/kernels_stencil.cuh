@@ -136,7 +136,15 @@ __device__ __forceinline__ int row_of(int idx, int w, float iw) {
 #ifndef HITB200_SENSOR_MIN_BLOCKS
 #define HITB200_SENSOR_MIN_BLOCKS 2
 #endif
-template <typename T, bool NEAR>
+// FUSED (one solve, cooperative launch with every tile resident): the CTA
+// first reduces its tile's prepass quantities, all CTAs meet at a grid
+// barrier, each then finalises the reductions itself (the same fixed order
+// as the prepass kernel, so results are bit-identical to the two-kernel
+// path), CTA 0 runs the prepass scalar logic, and the sensor proceeds with
+// its thresholds.  sel 0 then stands for the step's prepass (time step,
+// Mach control), sel 1, 2 for the stage prepasses and sel 3 for the
+// hyperviscosity sensor's.
+template <typename T, bool NEAR, bool FUSED>
 __global__ void __launch_bounds__(kSensorThreads, sizeof(T) == 8 ? 1 : HITB200_SENSOR_MIN_BLOCKS)
     sensor_kernel(const SolveDev* __restrict__ solves, const Work* __restrict__ work, int sel,
                   int enf, int want_visc, Bind bind, uint8_t* __restrict__ mask_out) {
@@ -146,8 +154,11 @@ __global__ void __launch_bounds__(kSensorThreads, sizeof(T) == 8 ? 1 : HITB200_S
   const double* sc = S.scal;
   if (!bind.use) {
     if (sel == 3 && sc[S_HV_STEP] == 0.0) return;
-    if (sel != 3 && sc[S_ACTIVE] == 0.0) return;
+    if (sel != 3 && sc[S_ACTIVE] == 0.0 && !(FUSED && sel == 0)) return;
   }
+  const int pre_mode = sel == 0 ? PRE_STEP : (sel == 3 ? PRE_SENSOR : PRE_STAGE);
+  int pre_slots = 0;
+  if constexpr (FUSED) pre_slots = prepass_tile<T>(S, wk, sel == 3 ? 1 : sel, pre_mode, sel == 3 ? 0 : 1, bind);
   const double* q = bind.use ? bind.qin : (sel == 3 ? S.q1 : stage_in(S, sel));
   uint8_t* mask = bind.use ? mask_out : S.mask;
   const int nx = S.nx, ny = S.ny, per = S.periodic;
@@ -208,9 +219,37 @@ __global__ void __launch_bounds__(kSensorThreads, sizeof(T) == 8 ? 1 : HITB200_S
   }
   __syncthreads();
 
-  const T eps_r = T(sc[S_EPS_RHO]), eps_p = T(sc[S_EPS_P]), eps_e = T(sc[S_EPS_E]);
+  double l_eps_r, l_eps_p, l_eps_e, l_comp, l_shear;
+  if constexpr (FUSED) {
+    // all tiles' partials are written: finalise them here (the same fixed
+    // order in every CTA), thresholds exactly as prepass_scalars forms them
+    grid_barrier(&S.counters[4], &S.counters[5], gridDim.x, &S.counters[6]);
+    __shared__ double fred[R_FIXED + 4 * kMaxDrag];
+    prepass_finalize(S, pre_slots, fred);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      prepass_scalars(S, fred, S.scal, pre_mode, false);
+      if (*(volatile unsigned*)&S.counters[6]) {
+        S.scal[S_STATUS] = (double)((int)S.scal[S_STATUS] | ST_BARRIER);
+        S.counters[6] = 0u;
+      }
+    }
+    const double N = (double)nx * (double)ny;
+    const double div_rms = sqrt(fred[R_DIV2] / N), vort_rms = sqrt(fred[R_VORT2] / N);
+    l_comp = div_rms > 1e-12 ? -S.comp_thr * div_rms : -INFINITY;
+    l_shear = (S.shear_on && vort_rms > 1e-12) ? S.shear_thr * vort_rms : INFINITY;
+    l_eps_r = 1e-14 + 1e-12 * fred[R_RHO];
+    l_eps_p = 1e-14 + 1e-12 * fred[R_P];
+    l_eps_e = 1e-14 + 1e-12 * fred[R_E];
+  } else {
+    l_eps_r = sc[S_EPS_RHO];
+    l_eps_p = sc[S_EPS_P];
+    l_eps_e = sc[S_EPS_E];
+    l_comp = sc[S_COMP_LIM];
+    l_shear = sc[S_SHEAR_LIM];
+  }
+  const T eps_r = T(l_eps_r), eps_p = T(l_eps_p), eps_e = T(l_eps_e);
   const T thr = T(S.jump_thr);
-  const T comp_lim = T(sc[S_COMP_LIM]), shear_lim = T(sc[S_SHEAR_LIM]);
+  const T comp_lim = T(l_comp), shear_lim = T(l_shear);
   const bool comp_on = isfinite(comp_lim), shear_on = isfinite(shear_lim);
   const T tdx = T(2.0 * S.dx), tdy = T(2.0 * S.dy), hx = T(S.dx), hy = T(S.dy);
   const T itdx = T(1.0 / (2.0 * S.dx)), itdy = T(1.0 / (2.0 * S.dy));

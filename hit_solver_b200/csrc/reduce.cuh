@@ -103,6 +103,37 @@ __device__ __forceinline__ void finalize_partials(const double* part, int nblk, 
   __syncthreads();
 }
 
+// Barrier over every CTA of a cooperative launch (which guarantees that all
+// of them are resident).  count and gen are zero-initialised words of the
+// solve's counters; the last CTA to arrive resets count and advances gen.
+// A CTA that waits longer than ~2 s of polling gives up: it sets *err and
+// continues, so that a failed launch cannot hang the GPU.
+__device__ __forceinline__ void grid_barrier(unsigned* count, unsigned* gen, unsigned nblocks,
+                                             unsigned* err) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile unsigned* vgen = gen;
+    const unsigned g0 = *vgen;
+    __threadfence();
+    if (atomicAdd(count, 1u) == nblocks - 1u) {
+      atomicExch(count, 0u);
+      __threadfence();
+      atomicAdd(gen, 1u);
+    } else {
+      unsigned long long it = 0;
+      while (*vgen == g0) {
+        __nanosleep(100);
+        if (++it > (1ull << 24)) {
+          atomicOr(err, 1u);
+          break;
+        }
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+}
+
 __device__ __forceinline__ int red_op(int slot) {
   switch (slot) {
     case R_AX: case R_AY: case R_RHO: case R_P: case R_E: case R_SR:

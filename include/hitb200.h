@@ -275,7 +275,13 @@ int hitb200_batch_run(hitb200_batch* batch, int32_t nsteps, void* stream);
 #define HITB200_TUNE_SWEEP_X 0
 #define HITB200_TUNE_SWEEP_Y 1
 #define HITB200_TUNE_PREPASS 2
-#define HITB200_TUNE_COUNT 3
+/* 1: a single plan whose sensor tiles all fit on the GPU at once fuses each
+ * prepass into the following sensor launch (one cooperative launch with a
+ * grid barrier instead of two launches); ignored where it cannot apply
+ * (batches, larger grids).  Off by default.  Results are bit-identical
+ * either way. */
+#define HITB200_TUNE_FUSED_SENSOR 3
+#define HITB200_TUNE_COUNT 4
 int hitb200_plan_set_tuning(hitb200_plan* plan, const int32_t* knobs, int32_t n);
 int hitb200_plan_get_tuning(const hitb200_plan* plan, int32_t* knobs, int32_t n);
 int hitb200_batch_set_tuning(hitb200_batch* batch, const int32_t* knobs, int32_t n);
