@@ -365,3 +365,23 @@ def test_riemann_golden_runs(tag):
     assert diag.density_max == pytest.approx(float(d["run_density_max"]), rel=1e-10)
     assert diag.max_abs_vorticity == pytest.approx(float(d["run_max_abs_vorticity"]), rel=1e-8)
     assert diag.final_sensor_fraction == pytest.approx(float(d["run_sensor_fraction"]), abs=1e-12)
+
+
+@pytest.mark.parametrize("nx,ny", [(1024, 64), (64, 1024), (768, 96)])
+def test_large_grid_steps_match_oracle(nx, ny):
+    """Lines of 768 and 1024 nodes (8 nodes per sweep thread, in x and in y):
+    2 FP64 steps of Riemann configuration 3 against the oracle, and the
+    FP32-bulk form against the FP64 one."""
+    from hit_solver_b200.problems.riemann import RiemannConfig3, RiemannSolver
+
+    out = {}
+    for precision in ("fp64", "fp32-bulk"):
+        cfg = RiemannConfig3(nx=nx, ny=ny, x_split=0.45, y_split=0.55, shear_threshold=None,
+                             precision=precision)
+        solver = RiemannSolver(cfg)
+        solver.advance(2)
+        out[precision] = host(solver.q)
+    prm = O.RiemannParams(number=3, nx=nx, ny=ny, x_split=0.45, y_split=0.55, shear_threshold=None)
+    want, _, _, _ = O.riemann_run(prm, max_steps=2)
+    assert rel_err(out["fp64"], want) < 1e-8
+    assert rel_err(out["fp32-bulk"], out["fp64"]) < 1e-5
