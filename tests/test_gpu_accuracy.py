@@ -1,4 +1,4 @@
-"""Accuracy of the FP32-bulk form over a long production HIT run.
+"""Accuracy over long production runs.
 
 The 512^2 production forced HIT (OU forcing on shell 3..5 with Mach control,
 viscosity, hyperviscosity every 5 steps, drag, cooling) runs 1000 steps in the
@@ -7,6 +7,11 @@ The FP64 form is itself held to the oracle step by step by the parity tests.
 Kinetic energy, enstrophy (mean vorticity^2, spectral as in the reference's
 diagnostics), turbulent Mach number and the injected forcing power of the
 FP32-bulk run must stay within 1e-4 relative of the FP64 run.
+
+The same physics at 64^2 runs 1000 steps against the oracle itself, with the
+reference's NumPy forcing-noise stream: the FP64 form's final state stays
+within 1e-9 relative (measured 8e-13) and the FP32-bulk form's within 1e-4
+(measured 5e-6).
 """
 
 import pytest
@@ -60,3 +65,54 @@ def test_fp32_bulk_long_riemann_stays_finite():
     assert int(sc[_lib.S_STATUS]) == 0
     assert bool(torch.isfinite(s.q).all())
     assert abs(float(s.q[0].min()) - 0.13659) < 2e-3
+
+
+@pytest.fixture(scope="module")
+def oracle_hit_64_1000():
+    """The oracle's production-physics HIT run at 64^2 for 1000 steps with the
+    reference's NumPy forcing-noise stream (about 25 s on one host core)."""
+    import numpy as np
+
+    from oracle import hit_oracle as O
+
+    prm = O.HITParams(nx=64, ny=64, tfinal=1e9, **_HIT64)
+    q, t, steps, info = O.hit_run(prm, max_steps=STEPS)
+    dx = prm.length / prm.nx
+    return np.asarray(q), t, steps, info, O.hit_diagnostics(q, dx, dx, prm.length, prm.gamma)
+
+
+_HIT64 = dict(cfl=0.05, target_mach=0.25, forcing_correlation_time=0.5, mach_control=True,
+              mach_control_target=0.25, viscosity=7.5e-4, large_scale_drag=0.1, cooling_time=5.0)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision,state_tol,diag_tol", [("fp64", 1e-9, 1e-11),
+                                                          ("fp32", 1e-4, 1e-6)])
+def test_hit_64_1000_steps_match_oracle(oracle_hit_64_1000, precision, state_tol, diag_tol):
+    """1000 production-physics steps (OU forcing with the reference's noise
+    stream, Mach control, viscosity, drag, cooling, hyperviscosity every 5
+    steps) against the oracle: the final state and the reference's scalar
+    diagnostics (kinetic energy, enstrophy, turbulent Mach number, rms
+    velocity, divergence, mass) and the injected forcing power."""
+    from hit_solver_b200.hit2d import HIT2DConfig
+    from oracle import hit_oracle as O
+    from tests.gpu_util import host, rel_err
+
+    want, t_w, steps_w, info_w, d_w = oracle_hit_64_1000
+    cfg = HIT2DConfig(nx=64, ny=64, tfinal=1e9, initial_kmin=3, initial_kmax=5, forcing_kmin=3.0,
+                      forcing_kmax=5.0, hyperviscosity_mn=0.002, precision=precision,
+                      max_steps=STEPS, **_HIT64)
+    s = HITSolver(cfg)
+    s.advance(STEPS)
+    sc = s.plan.scalars()
+    assert int(sc[_lib.S_STEP]) == steps_w == STEPS and int(sc[_lib.S_STATUS]) == 0
+    assert abs(sc[_lib.S_TIME] - t_w) <= diag_tol * t_w
+    q = host(s.q)
+    assert rel_err(q, want) < state_tol
+    length = 2.0 * 3.141592653589793
+    d = O.hit_diagnostics(q, length / 64, length / 64, length, 1.4)
+    for key in ("kinetic_energy", "enstrophy", "turbulent_mach", "rms_velocity", "mass"):
+        assert abs(d[key] - d_w[key]) <= diag_tol * abs(d_w[key]), (key, d[key], d_w[key])
+    # the divergence is a small difference of large terms: one decade looser
+    assert abs(d["divergence_rms"] - d_w["divergence_rms"]) <= 10 * diag_tol * d_w["divergence_rms"]
+    assert abs(sc[_lib.S_F_INJECTED] - info_w["injected_power"]) <= 10 * diag_tol * abs(info_w["injected_power"])
