@@ -20,9 +20,13 @@ hyperviscosity).  Metric: cell-updates/s (cells x steps / s).
               read back, the final state downloaded, all inside the timed
               region.
   roofline    the step's dominant kernel: algorithmic bytes per launch /
-              its CUDA-event launch time.
+              its CUDA-event launch time; ``step``: the whole step's
+              algorithmic 256 B per cell-update over the measured step time.
   cpu_baseline  the CPU oracle (NumPy FP64 restatement of the reference
               algorithm) on a bounded number of steps of the same workload.
+  spectra     shell spectra of 64 resident 512^2 snapshots per step (the
+              per-snapshot work of HIT2DSpectra.compute), snapshots/s, with
+              its phases against the HBM peak and the oracle on 3 snapshots.
 
 Launch:  python bench.py [--gpus N --steps K --warmup W]; for N > 1 under
 torchrun each rank runs its own replica (the solve does not shard).
@@ -54,6 +58,7 @@ WORKLOAD = {"workload": "riemann_config3_512x512_hybrid_hv1_cfl0.4", "nx": NX, "
             "hyperviscosity_mn": 0.001, "hyperviscosity_interval": 1, "cfl": 0.4,
             "guard_cells": 2, "precision": "fp32-bulk (fp64 state)"}
 FALLBACK_HBM_GBS = 6650.0
+STEP_BYTES_PER_CELL = 256  # 8 FP64 state vectors (4 components) per SSP-RK3 step
 
 
 def parse_args():
@@ -68,6 +73,8 @@ def parse_args():
     p.add_argument("--ref-procs", type=int, default=0,
                    help="reference arm: host processes (0: one per core, at most 32)")
     p.add_argument("--ensemble", type=int, default=64, help="solves in the ensemble leg (0: skip)")
+    p.add_argument("--spectra", type=int, default=64,
+                   help="snapshots per step in the shell-spectra leg (0: skip)")
     p.add_argument("--serve-requests", type=int, default=24,
                    help="requests in the serving measurement (0: skip)")
     p.add_argument("--serve-rate", type=float, default=20.0, help="mean arrivals per second")
@@ -381,6 +388,14 @@ def run_b200(args, world, rank, local):
     if ens is not None:
         ens["speedup_vs_plain_fp64_hit_512"] = ens["value"] / hit["plain_fp64"]["value"]
 
+    # ---- shell spectra of resident snapshots (HIT2DSpectra's per-snapshot work) ----
+    spectra = (spectra_run(K, W, flush, world, args.spectra,
+                           rank == 0 and world == 1 and not args.no_cpu_baseline)
+               if args.spectra > 0 else None)
+
+    # ---- initial states: host vs device construction at 1024^2 ----
+    init = initial_state_run() if rank == 0 else None
+
     # ---- serving: a seeded Poisson stream through the continuous-batching loop ----
     serve = serving_run(args) if args.serve_requests > 0 else None
 
@@ -439,6 +454,8 @@ def run_b200(args, world, rank, local):
         "batched_hit": hit,
         "ensemble": ens,
         "serving": serve,
+        "spectra": spectra,
+        "initial_states": init,
         "e2e": {"value": world * cells * K / te2e, "unit": "cell-updates/s",
                 "h2d_bytes_per_step": state_bytes / K,
                 "d2h_bytes_per_step": 8 * _lib.S_COUNT + state_bytes / K},
@@ -453,7 +470,14 @@ def run_b200(args, world, rank, local):
                                      "ms_per_launch": round(v["ms_per_launch"], 5),
                                      "gbs": round(v["bytes_per_launch"] / (v["ms_per_launch"] / 1e3) / 1e9, 1)
                                      if v["bytes_per_launch"] > 0 else None}
-                                 for k, v in sorted(per.items(), key=lambda kv: -kv[1]["ms_per_step"])}},
+                                 for k, v in sorted(per.items(), key=lambda kv: -kv[1]["ms_per_step"])},
+                     # the whole step against the same peak: 8 FP64 state
+                     # vectors of SSP-RK3 per cell-update (256 B)
+                     "step": {"bytes_per_cell_update": STEP_BYTES_PER_CELL,
+                              "single_gbs": STEP_BYTES_PER_CELL * cells * K / t32 / 1e9,
+                              "single_frac": STEP_BYTES_PER_CELL * cells * K / t32 / 1e9 / peak,
+                              "batched_gbs": STEP_BYTES_PER_CELL * B * cells * kb / tb / 1e9,
+                              "batched_frac": STEP_BYTES_PER_CELL * B * cells * kb / tb / 1e9 / peak}},
         "tuning": {"knobs": "sweep_x, sweep_y, prepass: 0 latency / 1 throughput variant "
                             "(hit_solver_b200.autotune)", **tuning},
         "gpu_launches": K * launches_per_step,
@@ -537,6 +561,126 @@ def ensemble_run(K: int, W: int, flush, world: int, count: int):
     return {"workload": f"{count} HIT solves, grids from {{128,256,384,512}}^2, Mach U[0.1,0.4]",
             "value": world * cells * k / t, "unit": "cell-updates/s", "ms_per_step": 1e3 * t / k,
             "cells": cells, "solves": count, "steps": k, "tuning": knobs, "status_bits": status}
+
+
+def spectra_run(K: int, W: int, flush, world: int, count: int, cpu: bool):
+    """Shell spectra (the per-snapshot work of HIT2DSpectra.compute) of `count`
+    device-resident 512^2 snapshots per step: fluctuation fields (CUDA),
+    rfft2 of the four fields (cuFFT, torch.fft), shell binning (CUDA).  Phase
+    times come from CUDA events around each call of a separate pass."""
+    import numpy as np
+    import torch
+
+    from hit_solver_b200 import _lib, core
+    from hit_solver_b200.postprocess import shell_spectra
+
+    gen = torch.Generator(device="cuda").manual_seed(5)
+    shape = (count, NY, NX)
+    rho = 1.0 + 0.3 * torch.rand(shape, generator=gen, device="cuda", dtype=torch.float64)
+    u = 0.2 * torch.randn(shape, generator=gen, device="cuda", dtype=torch.float64)
+    v = 0.2 * torch.randn(shape, generator=gen, device="cuda", dtype=torch.float64)
+    h = 2.0 * math.pi / NX
+    run = lambda: shell_spectra(rho, u, v, h, h, "reynolds")  # noqa: E731
+    for _ in range(W):
+        run()
+    k = max(K // 20, 5)
+    t = dist_max(timed_steps(run, k, flush), world)
+    # phase times: the same three calls with events between them
+    lib = _lib.load()
+    nh = NX // 2 + 1
+    ns = min(NX, NY) // 2 + 1
+    ws = torch.empty(int(lib.hitb200_spectra_workspace_bytes(count, NX, NY)), dtype=torch.uint8,
+                     device="cuda")
+    fields = torch.empty((count, 4, NY, NX), dtype=torch.float64, device="cuda")
+    e = torch.empty((count, ns), dtype=torch.float64, device="cuda")
+    z = torch.empty_like(e)
+    st = torch.cuda.current_stream()
+    ph = {"fields": 0.0, "rfft2": 0.0, "shells": 0.0}
+    for _ in range(k):
+        flush.zero_()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+        ev[0].record(st)
+        _lib.check(lib.hitb200_spectra_fields(rho.data_ptr(), u.data_ptr(), v.data_ptr(), count, NX,
+                                              NY, 0, fields.data_ptr(), ws.data_ptr(), ws.numel(),
+                                              core.stream_handle()))
+        ev[1].record(st)
+        spec = torch.fft.rfft2(fields)
+        ev[2].record(st)
+        _lib.check(lib.hitb200_spectra_shells(spec.data_ptr(), count, NX, NY, h, h, e.data_ptr(),
+                                              z.data_ptr(), ws.data_ptr(), ws.numel(),
+                                              core.stream_handle()))
+        ev[3].record(st)
+        torch.cuda.synchronize()
+        for i, name in enumerate(ph):
+            ph[name] += ev[i].elapsed_time(ev[i + 1]) / k
+        del spec
+    peak, _kind = measured_peak()
+    cells = count * NX * NY
+    # algorithmic bytes: fields = mean pass (read rho, u, v) + field pass (read
+    # rho, u, v, write 4 fields); shells = read the 4 half spectra (16 B a mode)
+    fbytes = cells * (24 + 24 + 32)
+    sbytes = count * 4 * NY * nh * 16
+    phases = {
+        "fields": {"ms": ph["fields"], "gbs": fbytes / (ph["fields"] / 1e3) / 1e9,
+                   "bytes": fbytes, "frac": fbytes / (ph["fields"] / 1e3) / 1e9 / peak},
+        "rfft2_cufft": {"ms": ph["rfft2"]},
+        "shells": {"ms": ph["shells"], "gbs": sbytes / (ph["shells"] / 1e3) / 1e9, "bytes": sbytes,
+                   "frac": sbytes / (ph["shells"] / 1e3) / 1e9 / peak},
+    }
+    out = {"workload": f"shell spectra of {count} resident {NX}x{NY} snapshots (Reynolds)",
+           "value": world * count * k / t, "unit": "snapshots/s", "ms_per_step": 1e3 * t / k,
+           "snapshots": count, "steps": k, "phases": phases,
+           "l2": "flushed (320 MB write) before every timed step"}
+    if cpu:
+        from oracle import spectra_oracle as SO
+
+        x = (np.arange(NX) + 0.5) * h
+        r0, u0, v0 = (a[0].cpu().numpy() for a in (rho, u, v))
+        SO.snapshot_shells(x, x, r0, u0, v0, "reynolds")
+        reps = 3
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            SO.snapshot_shells(x, x, r0, u0, v0, "reynolds")
+        tc = (time.perf_counter() - t0) / reps
+        out["cpu_baseline"] = {"value": 1.0 / tc, "unit": "snapshots/s", "cores": 1, "kind": "port",
+                               "sample": f"{reps} snapshots of {NX}x{NY} through the NumPy oracle"}
+    del rho, u, v, fields, ws
+    torch.cuda.synchronize()
+    return out
+
+
+def initial_state_run(n: int = 1024, reps: int = 5):
+    """Building one n^2 initial state, the host form (NumPy, the reference's
+    arithmetic) against the device form (CUDA kernels and cuFFT): the
+    admission cost of a solve."""
+    import numpy as np
+    import torch
+
+    from hit_solver_b200.hit2d import (HIT2DConfig, create_grid, initialize_hit_2d,
+                                       initialize_hit_2d_device)
+    from hit_solver_b200.equations import EulerEquation2D
+    from hit_solver_b200.problems.riemann import RiemannConfig3
+
+    cfg = HIT2DConfig(nx=n, ny=n, target_mach=0.25, initial_kmin=3, initial_kmax=5)
+    dom = create_grid(cfg)[0]
+    eq = EulerEquation2D(gamma=cfg.gamma)
+
+    def clock(fn):
+        fn()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            fn()
+        torch.cuda.synchronize()
+        return 1e3 * (time.perf_counter() - t0) / reps
+
+    rc = RiemannConfig3(nx=n, ny=n)
+    return {
+        "workload": f"one {n}x{n} initial state: wall time, host form incl. its upload",
+        "hit_host_ms": clock(lambda: initialize_hit_2d(cfg, dom, eq, np.random.default_rng(1))),
+        "hit_device_ms": clock(lambda: initialize_hit_2d_device(cfg, dom, eq, np.random.default_rng(1))),
+        "riemann_device_ms": clock(rc.initial_state),
+    }
 
 
 def serving_run(args):

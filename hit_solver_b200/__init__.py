@@ -15,7 +15,7 @@ machine without a GPU (the C library still loads; calls need a device).
 from __future__ import annotations
 
 __all__ = ["build", "core", "hit2d", "problems", "spatial_operator", "equations", "forcing",
-           "time_operator", "domain", "backend", "batch", "serving"]
+           "time_operator", "domain", "backend", "batch", "serving", "postprocess"]
 
 
 def __getattr__(name):

@@ -107,6 +107,28 @@ SIGNATURES = [
     ("hitb200_stable_time_step_noalloc", ctypes.c_int,
      [_DP, ctypes.c_int32, ctypes.c_int32, ctypes.c_double, ctypes.c_double, ctypes.c_double,
       ctypes.c_double, ctypes.c_double, _DP, _VP]),
+    ("hitb200_hit_streamfunction", ctypes.c_int,
+     [_DP, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_double, ctypes.c_double,
+      ctypes.c_double, ctypes.c_double, _DP, _VP]),
+    ("hitb200_hit_compose_workspace_bytes", ctypes.c_size_t, []),
+    ("hitb200_hit_compose", ctypes.c_int,
+     [_DP, _DP, ctypes.c_int32, ctypes.c_int32, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+      _DP, _DP, _VP, ctypes.c_size_t, _VP]),
+    ("hitb200_riemann_initial_state", ctypes.c_int,
+     [ctypes.POINTER(ctypes.c_double), ctypes.c_int32, ctypes.c_int32, ctypes.c_double,
+      ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+      ctypes.c_double, _DP, _VP]),
+    ("hitb200_spectra_workspace_bytes", ctypes.c_size_t,
+     [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32]),
+    ("hitb200_spectra_fields", ctypes.c_int,
+     [_DP, _DP, _DP, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _DP, _VP,
+      ctypes.c_size_t, _VP]),
+    ("hitb200_spectra_state_fields", ctypes.c_int,
+     [_DP, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _DP, _VP,
+      ctypes.c_size_t, _VP]),
+    ("hitb200_spectra_shells", ctypes.c_int,
+     [_VP, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_double, ctypes.c_double, _DP,
+      _DP, _VP, ctypes.c_size_t, _VP]),
     ("hitb200_forcing_update", ctypes.c_int,
      [_VP, _DP, _DP, ctypes.c_double, ctypes.c_double, _DP, _DP, _VP]),
     ("hitb200_step", ctypes.c_int, [_VP, _DP, _DP, _VP]),

@@ -19,7 +19,8 @@ ROOT = PKG.parent
 CSRC = PKG / "csrc"
 LIB = PKG / "libhitb200.so"
 SOURCES = ["api.cu"]
-HEADERS = ["common.cuh", "reduce.cuh", "weno.cuh", "kernels_reduce.cuh", "kernels_stencil.cuh"]
+HEADERS = ["common.cuh", "reduce.cuh", "weno.cuh", "kernels_reduce.cuh", "kernels_stencil.cuh",
+           "kernels_spectra.cuh", "kernels_init.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -17,7 +17,9 @@
 
 #include "../../include/hitb200.h"
 #include "common.cuh"
+#include "kernels_init.cuh"
 #include "kernels_reduce.cuh"
+#include "kernels_spectra.cuh"
 #include "kernels_stencil.cuh"
 
 using namespace hitb200;
@@ -1552,6 +1554,206 @@ extern "C" int hitb200_batch_get_tuning(const hitb200_batch* b, int32_t* knobs, 
   if (!b || !knobs) return invalid("NULL argument");
   if (n <= 0 || n > HITB200_TUNE_COUNT) return invalid("tuning knobs: 1..HITB200_TUNE_COUNT values");
   for (int i = 0; i < n; ++i) knobs[i] = b->tuning[i];
+  return HITB200_OK;
+}
+
+// =============================================================================
+// Initial states on the device (OOP/hit2d.py:158-204,
+// OOP/problems/riemann_config3.py:59-99).
+// =============================================================================
+namespace {
+
+int init_grid_check(int32_t nx, int32_t ny, double dx, double dy) {
+  if (nx <= 0 || ny <= 0) return invalid("initial state: nx and ny must be positive");
+  if (!(dx > 0.0) || !(dy > 0.0) || !std::isfinite(dx) || !std::isfinite(dy))
+    return invalid("initial state: dx and dy must be positive and finite");
+  return HITB200_OK;
+}
+
+int init_blocks(long long n) {
+  return (int)std::max(1LL, std::min((n + kInitThreads - 1) / kInitThreads, 8192LL));
+}
+
+}  // namespace
+
+extern "C" int hitb200_hit_streamfunction(const double* modes, int32_t n_modes, int32_t nx,
+                                          int32_t ny, double x_min, double dx, double y_min,
+                                          double dy, double* psi, void* stream) {
+  if (!psi || (n_modes > 0 && !modes)) return invalid("hit_streamfunction: NULL pointer");
+  if (n_modes < 0) return invalid("hit_streamfunction: n_modes must be >= 0");
+  const int r = init_grid_check(nx, ny, dx, dy);
+  if (r != HITB200_OK) return r;
+  const long long n = (long long)nx * ny;
+  hit_psi_kernel<<<init_blocks(n), kInitThreads, 0, static_cast<cudaStream_t>(stream)>>>(
+      modes, n_modes, nx, ny, x_min, dx, y_min, dy, psi);
+  HB_LAUNCHED("hit_psi_kernel");
+  return HITB200_OK;
+}
+
+extern "C" size_t hitb200_hit_compose_workspace_bytes(void) {
+  return (size_t)kInitSumBlocks * 3 * sizeof(double);
+}
+
+extern "C" int hitb200_hit_compose(const double* u, const double* v, int32_t nx, int32_t ny,
+                                   double gamma, double target_mach, double c_mean, double* q,
+                                   double* vrms_out, void* workspace, size_t workspace_bytes,
+                                   void* stream) {
+  if (!u || !v || !q || !vrms_out || !workspace) return invalid("hit_compose: NULL pointer");
+  if (nx <= 0 || ny <= 0) return invalid("hit_compose: nx and ny must be positive");
+  if (!(gamma > 1.0)) return invalid("hit_compose: gamma must be > 1");
+  if (workspace_bytes < hitb200_hit_compose_workspace_bytes())
+    return invalid("hit_compose: workspace smaller than hitb200_hit_compose_workspace_bytes");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const long long n = (long long)nx * ny;
+  double* part = static_cast<double*>(workspace);
+  hit_ic_sum_kernel<0><<<kInitSumBlocks, kInitThreads, 0, st>>>(u, v, n, part);
+  HB_LAUNCHED("hit_ic_sum_kernel<0>");
+  hit_ic_sum_kernel<1><<<kInitSumBlocks, kInitThreads, 0, st>>>(u, v, n, part);
+  HB_LAUNCHED("hit_ic_sum_kernel<1>");
+  hit_ic_compose_kernel<<<init_blocks(n), kInitThreads, 0, st>>>(u, v, n, part, gamma, target_mach,
+                                                                  c_mean, q, vrms_out);
+  HB_LAUNCHED("hit_ic_compose_kernel");
+  return HITB200_OK;
+}
+
+extern "C" int hitb200_riemann_initial_state(const double* states, int32_t nx, int32_t ny,
+                                             double x_min, double dx, double y_min, double dy,
+                                             double x_split, double y_split, double gamma,
+                                             double* q, void* stream) {
+  if (!states || !q) return invalid("riemann_initial_state: NULL pointer");
+  const int r = init_grid_check(nx, ny, dx, dy);
+  if (r != HITB200_OK) return r;
+  if (!(gamma > 1.0)) return invalid("riemann_initial_state: gamma must be > 1");
+  QuadStates s;
+  std::memcpy(s.s, states, sizeof(s.s));
+  const long long n = (long long)nx * ny;
+  quadrant_kernel<<<init_blocks(n), kInitThreads, 0, static_cast<cudaStream_t>(stream)>>>(
+      s, nx, ny, x_min, dx, y_min, dy, x_split, y_split, gamma, q);
+  HB_LAUNCHED("quadrant_kernel");
+  return HITB200_OK;
+}
+
+// =============================================================================
+// Shell spectra (HIT2DSpectra.compute, OOP/postprocess/spectra.py:48-149).
+// The caller owns every buffer, the transform between the two calls and the
+// workspace: [n_snap][kSpecMeanBlocks][3] mean partials, then
+// [n_snap][blocks][2][ns] shell partials, ns = min(nx, ny) / 2 + 1.
+// =============================================================================
+namespace {
+
+// Row blocks per snapshot of the shell kernel: about 8 CTAs per SM over the
+// whole batch, at least one row per warp.
+int spectra_row_blocks(int n_snap, int ny, int* rows_per_cta) {
+  int sms = 148;
+  int dev = 0;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int target = std::max(1, (8 * sms + n_snap - 1) / n_snap);
+  const int most = (ny + kSpecWarps - 1) / kSpecWarps;
+  const int want = std::min(target, most);
+  const int rows = (ny + want - 1) / want;
+  *rows_per_cta = rows;
+  return (ny + rows - 1) / rows;
+}
+
+size_t spectra_ws_bytes(int n_snap, int nx, int ny) {
+  int rows = 0;
+  const int nblk = spectra_row_blocks(n_snap, ny, &rows);
+  const size_t ns = (size_t)std::min(nx, ny) / 2 + 1;
+  return ((size_t)n_snap * kSpecMeanBlocks * 3 + (size_t)n_snap * nblk * 2 * ns) * sizeof(double);
+}
+
+int spectra_check(int32_t n_snap, int32_t nx, int32_t ny, const void* ws, size_t ws_bytes) {
+  if (n_snap <= 0) return invalid("spectra: n_snap must be positive");
+  if (nx < 2 || ny < 2) return invalid("spectra: nx and ny must be at least 2");
+  if ((size_t)std::min(nx, ny) / 2 + 1 > (size_t)kSpecMaxShells) {
+    g_last_error = "spectra: min(nx, ny) / 2 + 1 shells above the supported 1025 (grids up to 2048)";
+    return HITB200_ERR_UNSUPPORTED;
+  }
+  if (!ws) return invalid("spectra: workspace is NULL");
+  if (ws_bytes < spectra_ws_bytes(n_snap, nx, ny))
+    return invalid("spectra: workspace smaller than hitb200_spectra_workspace_bytes");
+  return HITB200_OK;
+}
+
+template <bool CONS>
+int spectra_fields_t(const double* a, const double* u, const double* v, int32_t n_snap, int32_t nx,
+                     int32_t ny, int32_t favre, double* out, void* ws, cudaStream_t st) {
+  const long long ncell = (long long)nx * ny;
+  double* part = static_cast<double*>(ws);
+  spectra_mean_kernel<CONS><<<dim3(kSpecMeanBlocks, n_snap), kSpecThreads, 0, st>>>(a, u, v, ncell,
+                                                                                    favre, part);
+  HB_LAUNCHED("spectra_mean_kernel");
+  const long long want = (ncell + 4LL * kSpecThreads - 1) / (4LL * kSpecThreads);
+  const int nb = (int)std::max(1LL, std::min(want, 4096LL));
+  spectra_fields_kernel<CONS><<<dim3(nb, n_snap), kSpecThreads, 0, st>>>(a, u, v, ncell, favre, part,
+                                                                         kSpecMeanBlocks, out);
+  HB_LAUNCHED("spectra_fields_kernel");
+  return HITB200_OK;
+}
+
+}  // namespace
+
+extern "C" size_t hitb200_spectra_workspace_bytes(int32_t n_snap, int32_t nx, int32_t ny) {
+  if (n_snap <= 0 || nx < 2 || ny < 2) return 0;
+  return spectra_ws_bytes(n_snap, nx, ny);
+}
+
+extern "C" int hitb200_spectra_fields(const double* rho, const double* u, const double* v,
+                                      int32_t n_snap, int32_t nx, int32_t ny, int32_t favre,
+                                      double* out, void* workspace, size_t workspace_bytes,
+                                      void* stream) {
+  if (!rho || !u || !v || !out) return invalid("spectra: NULL field pointer");
+  const int r = spectra_check(n_snap, nx, ny, workspace, workspace_bytes);
+  if (r != HITB200_OK) return r;
+  return spectra_fields_t<false>(rho, u, v, n_snap, nx, ny, favre ? 1 : 0, out, workspace,
+                                 static_cast<cudaStream_t>(stream));
+}
+
+extern "C" int hitb200_spectra_state_fields(const double* q, int32_t n_snap, int32_t nx, int32_t ny,
+                                            int32_t favre, double* out, void* workspace,
+                                            size_t workspace_bytes, void* stream) {
+  if (!q || !out) return invalid("spectra: NULL state pointer");
+  const int r = spectra_check(n_snap, nx, ny, workspace, workspace_bytes);
+  if (r != HITB200_OK) return r;
+  return spectra_fields_t<true>(q, nullptr, nullptr, n_snap, nx, ny, favre ? 1 : 0, out, workspace,
+                                static_cast<cudaStream_t>(stream));
+}
+
+extern "C" int hitb200_spectra_shells(const void* spec, int32_t n_snap, int32_t nx, int32_t ny,
+                                      double dx, double dy, double* energy, double* enstrophy,
+                                      void* workspace, size_t workspace_bytes, void* stream) {
+  if (!spec || !energy || !enstrophy) return invalid("spectra: NULL pointer");
+  if (!(dx > 0.0) || !(dy > 0.0) || !std::isfinite(dx) || !std::isfinite(dy))
+    return invalid("spectra: dx and dy must be positive and finite");
+  const int r = spectra_check(n_snap, nx, ny, workspace, workspace_bytes);
+  if (r != HITB200_OK) return r;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const int ns = std::min(nx, ny) / 2 + 1;
+  int rows = 0;
+  const int nblk = spectra_row_blocks(n_snap, ny, &rows);
+  // dk and 1 / (n d) as the reference's NumPy expressions round them
+  const double dk = std::min(2.0 * M_PI / (nx * dx), 2.0 * M_PI / (ny * dy));
+  const double inv_nxdx = 1.0 / ((double)nx * dx), inv_nydy = 1.0 / ((double)ny * dy);
+  const double norm = (double)nx * (double)ny;
+  const double inv_norm = 1.0 / (norm * norm);
+  double* part = static_cast<double*>(workspace) + (size_t)n_snap * kSpecMeanBlocks * 3;
+  const size_t smem = (size_t)kSpecWarps * 2 * ns * sizeof(double);
+  {
+    static size_t done[kMaxAttrDevices] = {};
+    const int dev = attr_device();
+    std::lock_guard<std::mutex> lock(g_attr_mu);
+    if (smem > 48 * 1024 && smem > done[dev]) {
+      HB_CUDA(cudaFuncSetAttribute(spectra_shell_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)smem));
+      done[dev] = smem;
+    }
+  }
+  spectra_shell_kernel<<<dim3(nblk, n_snap), kSpecThreads, smem, st>>>(
+      static_cast<const double2*>(spec), nx, ny, inv_nxdx, inv_nydy, dk, inv_norm, ns, rows, part);
+  HB_LAUNCHED("spectra_shell_kernel");
+  spectra_final_kernel<<<dim3((2 * ns + kSpecThreads - 1) / kSpecThreads, n_snap), kSpecThreads, 0,
+                         st>>>(part, nblk, ns, energy, enstrophy);
+  HB_LAUNCHED("spectra_final_kernel");
   return HITB200_OK;
 }
 

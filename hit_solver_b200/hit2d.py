@@ -35,8 +35,10 @@ class HIT2DConfig:
     """Fields and defaults of OOP/hit2d.py:36-80; ``backend`` defaults to
     "b200".  Additive fields: ``precision`` ("fp64" plain form or "fp32-bulk"),
     ``forcing_noise`` ("numpy": the reference's RNG stream, uploaded each
-    step; "device": drawn on the device) and ``max_steps`` (stop after this
-    many steps even before tfinal)."""
+    step; "device": drawn on the device), ``max_steps`` (stop after this
+    many steps even before tfinal) and ``initial_condition`` ("host": the
+    reference's NumPy arithmetic, bit for bit; "device": the same phases,
+    synthesised on the GPU, equal to roundoff)."""
 
     nx: int = 128
     ny: int = 128
@@ -84,6 +86,7 @@ class HIT2DConfig:
     precision: str = "fp64"
     forcing_noise: str = "numpy"
     max_steps: int | None = None
+    initial_condition: str = "host"
 
     @classmethod
     def isotropic_128(cls, output_dir: Path = DEFAULT_SNAPSHOT_DIR, backend: str = "b200"):
@@ -142,6 +145,60 @@ def initialize_hit_2d(config: HIT2DConfig, domain: Domain2D, equation, rng, xp=N
     q[2] = rho * v
     q[3] = p / (config.gamma - 1.0) + 0.5 * rho * (u ** 2 + v ** 2)
     return torch.from_numpy(q).cuda()
+
+
+def initial_modes(config: HIT2DConfig, rng) -> np.ndarray:
+    """(kx, ky, amplitude, phase) of every streamfunction mode of
+    initialize_hit_2d (OOP/hit2d.py:175-189), in the reference's loop order,
+    each phase drawn from ``rng`` as the reference draws it."""
+    rows = []
+    for kx in range(-config.initial_kmax, config.initial_kmax + 1):
+        for ky in range(-config.initial_kmax, config.initial_kmax + 1):
+            if ky < 0 or (ky == 0 and kx <= 0):
+                continue
+            magnitude = np.sqrt(kx ** 2 + ky ** 2)
+            if magnitude < config.initial_kmin or magnitude > config.initial_kmax:
+                continue
+            rows.append((float(kx), float(ky), 1.0 / max(kx ** 2 + ky ** 2, 1),
+                         rng.uniform(0.0, 2.0 * np.pi)))
+    return np.asarray(rows, dtype=np.float64).reshape(-1, 4)
+
+
+def initialize_hit_2d_device(config: HIT2DConfig, domain: Domain2D, equation, rng) -> torch.Tensor:
+    """initialize_hit_2d (OOP/hit2d.py:158-204) built on the device: the
+    phases come from ``rng`` on the host (a few dozen draws, the reference's
+    stream), the streamfunction sum over modes and cells runs in
+    ``hitb200_hit_streamfunction``, its spectral derivatives in cuFFT
+    (torch.fft, as the reference's fft2 / ifft2), and the mean removal,
+    Mach scaling and conservative state in ``hitb200_hit_compose``.  Equal to
+    the host form to roundoff (cos and the transforms are not NumPy's)."""
+    core.require_cuda()
+    lib = _lib.load()
+    nx, ny = domain.nx, domain.ny
+    modes = torch.from_numpy(initial_modes(config, rng)).cuda()
+    psi = torch.empty((ny, nx), dtype=torch.float64, device="cuda")
+    stream = core.stream_handle()
+    _lib.check(lib.hitb200_hit_streamfunction(modes.data_ptr(), modes.shape[0], nx, ny,
+                                              float(domain.x_min), float(domain.dx),
+                                              float(domain.y_min), float(domain.dy),
+                                              psi.data_ptr(), stream))
+    KX, KY = (torch.from_numpy(np.ascontiguousarray(k)).cuda() for k in _wavenumbers(domain))
+    ph = torch.fft.fft2(psi)
+    u = torch.fft.ifft2(1j * KY * ph).real.contiguous()
+    v = (-torch.fft.ifft2(1j * KX * ph).real).contiguous()
+    # mean sound speed of rho = 1, p = 1/gamma as NumPy forms it (a constant field)
+    p = np.full((ny, nx), 1.0 / config.gamma)
+    c_mean = float(np.mean(np.sqrt(equation.gamma * p / np.ones_like(p))))
+    q = torch.empty((4, ny, nx), dtype=torch.float64, device="cuda")
+    vrms = torch.empty(1, dtype=torch.float64, device="cuda")
+    ws = torch.empty(int(lib.hitb200_hit_compose_workspace_bytes()), dtype=torch.uint8,
+                     device="cuda")
+    _lib.check(lib.hitb200_hit_compose(u.data_ptr(), v.data_ptr(), nx, ny, float(config.gamma),
+                                       float(config.target_mach), c_mean, q.data_ptr(),
+                                       vrms.data_ptr(), ws.data_ptr(), ws.numel(), stream))
+    if float(vrms.item()) <= np.finfo(float).eps:
+        raise ValueError("initial streamfunction produced zero velocity")
+    return q
 
 
 def _source_plan(q, equation, domain: Domain2D | None = None, **kw) -> core.Plan:
@@ -461,13 +518,16 @@ class HITSolver:
         precision_code(config.precision)
         if config.forcing_noise not in ("numpy", "device"):
             raise ValueError("forcing_noise must be 'numpy' or 'device'")
+        if config.initial_condition not in ("host", "device"):
+            raise ValueError("initial_condition must be 'host' or 'device'")
         self.config = config
         self.domain = create_grid(config)[0]
         self.equation = _make_equation(config)
         self.plan = core.Plan(hit_descriptor(config, self.domain))
         rng = np.random.default_rng(config.forcing_seed)
         self.noise_rng = np.random.default_rng(config.forcing_seed + 1)
-        q = initialize_hit_2d(config, self.domain, self.equation, rng)
+        init = initialize_hit_2d_device if config.initial_condition == "device" else initialize_hit_2d
+        q = init(config, self.domain, self.equation, rng)
         self.q = self.equation.enforce_physical_state(q)
         self.plan.set_time(0.0, 0, 0.0, -1 if config.max_steps is None else config.max_steps)
         if config.forcing_noise == "numpy":

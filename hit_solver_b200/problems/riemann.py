@@ -9,6 +9,7 @@ guard clean, hyperviscosity every ``hyperviscosity_interval`` steps).
 
 from __future__ import annotations
 
+import ctypes
 import json
 import math
 from dataclasses import asdict, dataclass, field
@@ -75,22 +76,20 @@ class RiemannConfig3:
         "ul": (0.5323, 1.206, 0.0, 0.3), "ur": (1.5, 0.0, 0.0, 1.5)}
 
     def initial_state(self):
-        """Piecewise-constant quadrants; a cell is upper/right when its centre
-        is >= the split.  Built on the host, returned as a CUDA tensor."""
-        X, Y = self.domain.mesh()
-        top, right = Y >= self.y_split, X >= self.x_split
-        prim = np.zeros((4, self.ny, self.nx))
-        for key, sel in (("ll", ~top & ~right), ("lr", ~top & right), ("ul", top & ~right),
-                         ("ur", top & right)):
-            for c in range(4):
-                prim[c][sel] = self._STATES[key][c]
-        rho, u, v, p = prim
-        q = np.zeros_like(prim)
-        q[0] = np.maximum(rho, 1e-10)
-        q[1] = q[0] * u
-        q[2] = q[0] * v
-        q[3] = np.maximum(p, 1e-10) / (self.gamma - 1.0) + 0.5 * q[0] * (u ** 2 + v ** 2)
-        return torch.from_numpy(q).cuda()
+        """Piecewise-constant quadrants (riemann_config3.py:59-99); a cell is
+        upper/right when its centre is >= the split.  Filled on the device
+        (``hitb200_riemann_initial_state``), bit for bit the reference's
+        values."""
+        core.require_cuda()
+        dom = self.domain
+        states = (ctypes.c_double * 16)(*[float(c) for key in ("ll", "lr", "ul", "ur")
+                                          for c in self._STATES[key]])
+        q = torch.empty((4, self.ny, self.nx), dtype=torch.float64, device="cuda")
+        _lib.check(_lib.load().hitb200_riemann_initial_state(
+            states, self.nx, self.ny, float(dom.x_min), float(dom.dx), float(dom.y_min),
+            float(dom.dy), float(self.x_split), float(self.y_split), float(self.gamma),
+            q.data_ptr(), core.stream_handle()))
+        return q
 
 
 @dataclass(frozen=True)

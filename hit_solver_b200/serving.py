@@ -81,7 +81,8 @@ class Result:
 def hit_request_config(n: int, seed: int, mach: float, steps: int, precision: str) -> HIT2DConfig:
     """The production forced-HIT physics (OU shell 3..5, tau 0.5, Mach control,
     nu 7.5e-4, hyperviscosity every 5 steps, drag on |k| <= 2, cooling 5.0,
-    CFL 0.05) at size n, seed and Mach; device forcing noise; ``steps`` steps."""
+    CFL 0.05) at size n, seed and Mach; device forcing noise and initial
+    state; ``steps`` steps."""
     return HIT2DConfig(
         nx=n, ny=n, tfinal=math.inf, target_mach=mach, initial_kmin=3, initial_kmax=5,
         forcing_kmin=3.0, forcing_kmax=5.0, forcing_correlation_time=0.5,
@@ -89,7 +90,7 @@ def hit_request_config(n: int, seed: int, mach: float, steps: int, precision: st
         hyperviscosity_mn=0.002, hyperviscosity_interval=5, large_scale_drag=0.10,
         large_scale_drag_kmax=2.0, cooling_time=5.0, mach_control=True,
         mach_control_target=mach, forcing_seed=seed, cfl=0.05, precision=precision,
-        forcing_noise="device", max_steps=steps)
+        forcing_noise="device", max_steps=steps, initial_condition="device")
 
 
 def riemann_request_config(kind: str, n: int, split: float, precision: str) -> RiemannConfig3:

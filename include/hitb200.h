@@ -243,6 +243,69 @@ int hitb200_copy_scalars_async(hitb200_plan* plan, double* dst, int32_t n, void*
  * raw rho min, rho max, p min, p max.  Synchronises. */
 int hitb200_diagnostics(hitb200_plan* plan, const double* q, double* out, int32_t n);
 
+/* ---- initial states on the device ---------------------------------------------- */
+/* The streamfunction of initialize_hit_2d (OOP/hit2d.py:158-189):
+ * psi[j][i] = sum_m amplitude_m cos(kx_m x_i + ky_m y_j + phase_m) with
+ * x_i = x_min + dx (i + 1/2), y_j likewise, accumulated in mode order as the
+ * reference does.  modes: device double [n_modes][4] = (kx, ky, amplitude,
+ * phase), the phases drawn by the caller in the reference's order;
+ * psi: device double [ny][nx]. */
+int hitb200_hit_streamfunction(const double* modes, int32_t n_modes, int32_t nx, int32_t ny,
+                               double x_min, double dx, double y_min, double dy, double* psi,
+                               void* stream);
+/* The rest of initialize_hit_2d (OOP/hit2d.py:191-204) from the spectral
+ * velocity u = dpsi/dy, v = -dpsi/dx (device double [ny][nx]): removes the
+ * means, scales the velocity to target_mach * c_mean / rms (c_mean: the
+ * mean sound speed of rho = 1, p = 1/gamma, as the caller's NumPy forms it)
+ * and writes the conservative state q (device double [4][ny][nx]) and the rms
+ * before scaling to the device double *vrms_out (the reference raises when
+ * it is not above machine epsilon).  workspace: device memory of
+ * hitb200_hit_compose_workspace_bytes() bytes. */
+size_t hitb200_hit_compose_workspace_bytes(void);
+int hitb200_hit_compose(const double* u, const double* v, int32_t nx, int32_t ny, double gamma,
+                        double target_mach, double c_mean, double* q, double* vrms_out,
+                        void* workspace, size_t workspace_bytes, void* stream);
+/* Four-quadrant Riemann state (OOP/problems/riemann_config3.py:59-99;
+ * riemann_config6.py, riemann_config3_08.py): states = host double [4][4],
+ * the primitive (rho, u, v, p) of the lower-left, lower-right, upper-left and
+ * upper-right quadrants; a cell is upper when y_j >= y_split and right when
+ * x_i >= x_split (cell centres as above); q (device double [4][ny][nx]) =
+ * conservative_from_primitive with the density and pressure floors. */
+int hitb200_riemann_initial_state(const double* states, int32_t nx, int32_t ny, double x_min,
+                                  double dx, double y_min, double dy, double x_split,
+                                  double y_split, double gamma, double* q, void* stream);
+
+/* ---- shell spectra ------------------------------------------------------------ */
+/* The per-snapshot part of HIT2DSpectra.compute (OOP/postprocess/spectra.py:
+ * 48-149) for n_snap snapshots of one grid at once, in three steps on
+ * `stream`:
+ *   1. hitb200_spectra_fields (snapshot arrays) or hitb200_spectra_state_fields
+ *      (conservative states, primitives as primitive_from_conservative,
+ *      OOP/equations.py:136-145) writes out[s] = [sqrt(rho) u', sqrt(rho) v',
+ *      u', v'], device double [n_snap][4][ny][nx]; u' = u - mean(u) (favre 0,
+ *      spectra.py:206-209) or u - mean(rho u) / mean(rho) (favre 1, :202-205);
+ *   2. the caller's unnormalised forward real-to-complex 2-D FFT of `out` over
+ *      its last two axes: complex double [n_snap][4][ny][nx/2+1] (cuFFT /
+ *      numpy.fft.rfft2 layout and sign);
+ *   3. hitb200_spectra_shells bins 1/2 (|U|^2 + |V|^2) / (nx ny)^2 (energy) and
+ *      1/2 |kx V' - ky U'|^2 / (nx ny)^2 (enstrophy) of every mode into shell
+ *      rint(|k| / dk), dk = min(2 pi / (nx dx), 2 pi / (ny dy)), k from
+ *      2 pi fftfreq (spectra.py:84-121): energy, enstrophy: device double
+ *      [n_snap][min(nx, ny)/2 + 1]; modes beyond the last shell are dropped.
+ * The workspace is device memory of hitb200_spectra_workspace_bytes bytes
+ * (same n_snap, nx, ny and device) shared by steps 1 and 3.  Sums run in a
+ * fixed order.  Grids with min(nx, ny) above 2049 -> HITB200_ERR_UNSUPPORTED. */
+size_t hitb200_spectra_workspace_bytes(int32_t n_snap, int32_t nx, int32_t ny);
+int hitb200_spectra_fields(const double* rho, const double* u, const double* v, int32_t n_snap,
+                           int32_t nx, int32_t ny, int32_t favre, double* out, void* workspace,
+                           size_t workspace_bytes, void* stream);
+int hitb200_spectra_state_fields(const double* q, int32_t n_snap, int32_t nx, int32_t ny,
+                                 int32_t favre, double* out, void* workspace,
+                                 size_t workspace_bytes, void* stream);
+int hitb200_spectra_shells(const void* spec, int32_t n_snap, int32_t nx, int32_t ny, double dx,
+                           double dy, double* energy, double* enstrophy, void* workspace,
+                           size_t workspace_bytes, void* stream);
+
 /* ---- batched form ------------------------------------------------------------- */
 /* Many independent solves (any mix of grid sizes) advanced by one launch per
  * kernel of the step: the "ensemble" / serving form.  All descriptors must

@@ -190,12 +190,65 @@ def gen_riemann(R):
     return out
 
 
+SPECTRA_SETTINGS = (  # (name, fluctuation type, start_time, end_time, stride)
+    ("reynolds", "reynolds", None, None, 1),
+    ("favre", "favre", None, None, 1),
+    ("window", "reynolds", 0.02, 0.07, 2),
+)
+
+
+def gen_spectra(R):
+    """HIT2DSpectra.compute (OOP/postprocess/spectra.py:48-149) over snapshots
+    that the reference's run_simulation wrote: a non-square 32 x 24 grid (two
+    fundamental wavenumbers) and an odd 25 x 20 one, Reynolds and Favre
+    fluctuations, a time window with a stride.  The snapshot fields and the
+    results (with the warnings raised) are stored."""
+    import warnings
+
+    from OOP.postprocess.spectra import HIT2DSpectra
+
+    hit2d = R["hit2d"]
+    for tag, nx, ny in (("32x24", 32, 24), ("25x20", 25, 20)):
+        with tempfile.TemporaryDirectory() as tmp:
+            cfg = hit2d.HIT2DConfig(nx=nx, ny=ny, tfinal=0.08, cfl=0.05, target_mach=0.3,
+                                    initial_kmin=2, initial_kmax=6, forcing_kmin=3.0,
+                                    forcing_kmax=5.0, viscosity=7.5e-4, large_scale_drag=0.1,
+                                    cooling_time=5.0, diagnostics_every=1000, snapshot_every=2,
+                                    output_dir=Path(tmp), backend="numpy")
+            with contextlib.redirect_stdout(io.StringIO()):
+                hit2d.run_simulation(cfg)
+            paths = sorted(Path(tmp).glob("hit2d_step*.npz"))
+            snaps = [dict(np.load(p)) for p in paths]
+            out = {"time": np.array([float(d["time"]) for d in snaps]),
+                   "step": np.array([int(d["step"]) for d in snaps]),
+                   "x": snaps[0]["x"], "y": snaps[0]["y"],
+                   "rho": np.stack([d["rho"] for d in snaps]),
+                   "u": np.stack([d["u"] for d in snaps]),
+                   "v": np.stack([d["v"] for d in snaps])}
+            for name, kind, t0, t1, stride in SPECTRA_SETTINGS:
+                with warnings.catch_warnings(record=True) as caught:
+                    warnings.simplefilter("always")
+                    r = HIT2DSpectra(tmp, fluctuation_type=kind, start_time=t0, end_time=t1,
+                                     stride=stride).compute()
+                out.update({f"{name}_k": r.k, f"{name}_energy_mean": r.energy_mean,
+                            f"{name}_energy_std": r.energy_std,
+                            f"{name}_enstrophy_mean": r.enstrophy_mean,
+                            f"{name}_enstrophy_std": r.enstrophy_std,
+                            f"{name}_n": np.asarray(r.number_of_snapshots),
+                            f"{name}_interval": np.asarray(r.selected_time_interval),
+                            f"{name}_hk_energy": np.asarray(r.high_k_energy_ratio),
+                            f"{name}_hk_enstrophy": np.asarray(r.high_k_enstrophy_ratio),
+                            f"{name}_warnings": np.asarray([str(w.message) for w in caught] or [""])})
+        np.savez_compressed(HERE / f"spectra_{tag}.npz", **out)
+
+
 def main(root: str) -> None:
     R = _import_reference(root)
     for name, (cfg, domain, eq, q) in periodic_cases(R).items():
         gen_periodic(R, name, cfg, domain, eq, q)
     gen_hit_run(R)
     gen_riemann(R)
+    gen_spectra(R)
     print("golden vectors written to", HERE)
 
 

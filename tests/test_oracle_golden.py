@@ -159,3 +159,26 @@ def test_reference_initial_states():
     assert np.count_nonzero(rho == 0.138) == 64
     assert np.count_nonzero(rho == 0.5323) == 32
     assert np.count_nonzero(rho == 1.5) == 4
+
+
+SPECTRA_SETTINGS = (("reynolds", "reynolds", None, None, 1), ("favre", "favre", None, None, 1),
+                    ("window", "reynolds", 0.02, 0.07, 2))
+
+
+@pytest.mark.parametrize("tag", ["32x24", "25x20"])
+def test_spectra_summary(tag):
+    """HIT2DSpectra.compute over snapshots of the reference's own run."""
+    from oracle import spectra_oracle as SO
+
+    d = load(f"spectra_{tag}")
+    for name, kind, t0, t1, stride in SPECTRA_SETTINGS:
+        sel = [i for i, t in enumerate(d["time"])
+               if (t0 is None or t >= t0) and (t1 is None or t <= t1)][::stride]
+        r = SO.spectra_summary(((d["time"][i], d["x"], d["y"], d["rho"][i], d["u"][i], d["v"][i])
+                                for i in sel), kind)
+        assert r["number_of_snapshots"] == int(d[f"{name}_n"])
+        np.testing.assert_array_equal(r["selected_time_interval"], d[f"{name}_interval"])
+        for key in ("k", "energy_mean", "energy_std", "enstrophy_mean", "enstrophy_std"):
+            np.testing.assert_array_equal(r[key], d[f"{name}_{key}"], err_msg=f"{name} {key}")
+        assert r["high_k_energy_ratio"] == float(d[f"{name}_hk_energy"])
+        assert r["high_k_enstrophy_ratio"] == float(d[f"{name}_hk_enstrophy"])
