@@ -87,7 +87,7 @@ __global__ void __launch_bounds__(kSpecThreads)
 
 // grid (cell blocks, snapshots).  out[s] = [sqrt(rho) u', sqrt(rho) v', u', v']
 // ([4][ny][nx]); the means come from the nmb partial rows of the snapshot,
-// summed in a fixed order by every CTA.
+// summed in a fixed order by the first warp of every CTA.
 template <bool CONS>
 __global__ void __launch_bounds__(kSpecThreads)
     spectra_fields_kernel(const double* __restrict__ a, const double* __restrict__ u,
@@ -95,22 +95,28 @@ __global__ void __launch_bounds__(kSpecThreads)
                           const double* __restrict__ part, int nmb, double* __restrict__ out) {
   __shared__ double mean[2];
   const size_t s = blockIdx.y;
-  if (threadIdx.x == 0) {
+  if (threadIdx.x < 32) {
+    // warp 0: lane l sums partials l, l + 32, ...; then a fixed butterfly
     double sr = 0.0, su = 0.0, sv = 0.0;
     const double* p = part + s * nmb * 3;
-    for (int k = 0; k < nmb; ++k) {
+    for (int k = threadIdx.x; k < nmb; k += 32) {
       sr += p[3 * k];
       su += p[3 * k + 1];
       sv += p[3 * k + 2];
     }
-    const double n = (double)ncell;
-    if (favre) {
-      const double rm = sr / n;  // mean(rho); then mean(rho u) / mean(rho)
-      mean[0] = (su / n) / rm;
-      mean[1] = (sv / n) / rm;
-    } else {
-      mean[0] = su / n;
-      mean[1] = sv / n;
+    sr = warp_sum(sr);
+    su = warp_sum(su);
+    sv = warp_sum(sv);
+    if (threadIdx.x == 0) {
+      const double n = (double)ncell;
+      if (favre) {
+        const double rm = sr / n;  // mean(rho); then mean(rho u) / mean(rho)
+        mean[0] = (su / n) / rm;
+        mean[1] = (sv / n) / rm;
+      } else {
+        mean[0] = su / n;
+        mean[1] = sv / n;
+      }
     }
   }
   __syncthreads();
@@ -224,6 +230,7 @@ __global__ void __launch_bounds__(kSpecThreads)
   if (t >= 2 * ns) return;
   const double* p = part + s * nblk * 2 * (size_t)ns + t;
   double acc = 0.0;
+#pragma unroll 8
   for (int b = 0; b < nblk; ++b) acc += p[(size_t)b * 2 * ns];
   if (t < ns) energy[s * ns + t] = acc;
   else enstrophy[s * ns + t - ns] = acc;
