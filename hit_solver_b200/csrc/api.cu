@@ -154,8 +154,9 @@ struct hitb200_plan {
   Work* d_tiles32 = nullptr;
   Work* d_xlines = nullptr;
   Work* d_ylines = nullptr;
+  Work* d_srows = nullptr;  // forcing-synthesis row blocks
   int* d_partner = nullptr;
-  int n_tiles = 0, n_tiles32 = 0, n_x = 0, n_y = 0, Rx = 1, Ry = 1;
+  int n_tiles = 0, n_tiles32 = 0, n_x = 0, n_y = 0, Rx = 1, Ry = 1, n_srows = 0;
   int elem = 8;
   size_t smem_x = 0, smem_y = 0, smem_sensor = 0;
   // graph replay of hitb200_step
@@ -174,8 +175,10 @@ struct hitb200_batch {
   int tuning[HITB200_TUNE_COUNT] = {0, 0, 0, 0};
   SolveDev* d_solves = nullptr;
   Work *d_tiles = nullptr, *d_tiles32 = nullptr, *d_xlines = nullptr, *d_ylines = nullptr;
+  Work* d_srows = nullptr;
   int* d_partner = nullptr;
   int n_tiles = 0, n_tiles32 = 0, n_x = 0, n_y = 0, elem = 8, mch_x = 1, mch_y = 1, guard_blocks = 1;
+  int n_srows = 0;
   int rx_max = 1, ry_max = 1;
   size_t smem_x = 0, smem_y = 0, smem_sensor = 0;
   int any_outflow = 0, any_forcing = 0, any_hv = 0, any_noise_upload = 0;
@@ -189,9 +192,9 @@ namespace {
 struct LaunchSet {
   const SolveDev* solves;
   int nsolves;
-  const Work *tiles, *tiles32, *xl, *yl;
+  const Work *tiles, *tiles32, *xl, *yl, *srows;
   const int* partner;
-  int n_tiles, n_tiles32, n_x, n_y, elem, mch_x, mch_y, guard_blocks;
+  int n_tiles, n_tiles32, n_x, n_y, elem, mch_x, mch_y, guard_blocks, n_srows;
   int thr_x, thr_y;  // sweep CTA sizes: kLineThreads per line of the widest work item
   int occ_x, occ_y, occ_pre;  // kernel variants: 0 latency, 1 throughput (tuning knobs)
   int fused;                  // prepass fused into the sensor (single solves, tuning knob)
@@ -377,7 +380,7 @@ int launch_step_sequence(const LaunchSet& L, int any_forcing, int noise_upload, 
       noise_rng_kernel<<<L.nsolves, 128, 0, L.st>>>(L.solves, L.nsolves, L.partner);
     }
     PMARK("force_synth", 48 * L.cells_force);
-    force_synth_kernel<<<L.n_tiles32, kRedThreads, 0, L.st>>>(L.solves, L.tiles32, nb);
+    force_synth_kernel<<<L.n_srows, kRedThreads, 0, L.st>>>(L.solves, L.srows, nb);
   }
   for (int stage = 0; stage < 3; ++stage) {
     if (L.fused) {
@@ -447,6 +450,8 @@ LaunchSet plan_launch_set(hitb200_plan* p, cudaStream_t st) {
   L.tiles = p->d_tiles;
   L.tiles32 = p->d_tiles32;
   L.n_tiles32 = p->n_tiles32;
+  L.srows = p->d_srows;
+  L.n_srows = p->n_srows;
   L.guard_blocks = guard_blocks_for(p->desc);
   L.xl = p->d_xlines;
   L.yl = p->d_ylines;
@@ -625,12 +630,13 @@ size_t hitb200_plan_device_bytes(const hitb200_desc* d) {
   a.take(SCAL_SIZE * sizeof(double));
   a.take(ntile * (R_FIXED + 4 * mt.drag.size()) * sizeof(double));
   a.take(ntile * (2 * mt.force.size() + 1) * sizeof(double));
-  a.take(ntile * 4 * sizeof(double));
+  a.take(std::max(ntile, (size_t)d->ny) * 4 * sizeof(double));  // synthesis partials
   a.take(ntile * NDIAG * sizeof(double));
   a.take(8 * sizeof(unsigned) + sizeof(int) + NDIAG * sizeof(double));
   a.take(ntile * sizeof(Work));
   a.take((size_t)((d->nx + kSenTX - 1) / kSenTX) * ((d->ny + kSenTY - 1) / kSenTY) * sizeof(Work));
   a.take((size_t)(d->ny + d->nx) * sizeof(Work));
+  a.take((size_t)d->ny * sizeof(Work));  // synthesis row blocks (at most one per row)
   return a.off;
 }
 
@@ -694,7 +700,9 @@ int hitb200_plan_create(const hitb200_desc* d, hitb200_plan** out) {
   const size_t nred = R_FIXED + 4 * mt.drag.size();
   const size_t o_ppre = a.take(p->n_tiles * nred * sizeof(double));
   const size_t o_pnoise = a.take(p->n_tiles * (2 * mt.force.size() + 1) * sizeof(double));
-  const size_t o_psynth = a.take(p->n_tiles * 4 * sizeof(double));
+  const int srows = synth_rows(nx);
+  p->n_srows = (ny + srows - 1) / srows;
+  const size_t o_psynth = a.take((size_t)std::max(p->n_tiles, p->n_srows) * 4 * sizeof(double));
   const size_t o_pdiag = a.take(p->n_tiles * NDIAG * sizeof(double));
   const size_t o_cnt = a.take(8 * sizeof(unsigned) + sizeof(int) + NDIAG * sizeof(double));
   const size_t o_tiles = a.take(p->n_tiles * sizeof(Work));
@@ -703,6 +711,7 @@ int hitb200_plan_create(const hitb200_desc* d, hitb200_plan** out) {
   const size_t o_tiles32 = a.take(p->n_tiles32 * sizeof(Work));
   const size_t o_xl = a.take(p->n_x * sizeof(Work));
   const size_t o_yl = a.take(p->n_y * sizeof(Work));
+  const size_t o_sr = a.take(p->n_srows * sizeof(Work));
   p->arena_bytes = a.off;
   cudaError_t e = cudaMalloc(&p->arena, a.off);
   if (e != cudaSuccess) {
@@ -777,7 +786,8 @@ int hitb200_plan_create(const hitb200_desc* d, hitb200_plan** out) {
   s.fixed_dt = d->fixed_dt;
   s.noise_mode = d->noise_mode;
   s.seed = d->seed;
-  s.nblk_pre = s.nblk_noise = s.nblk_synth = s.nblk_diag = p->n_tiles32;
+  s.nblk_pre = s.nblk_noise = s.nblk_diag = p->n_tiles32;
+  s.nblk_synth = p->n_srows;
   s.nred = (int)nred;
   s.q = nullptr;
   s.q1 = reinterpret_cast<double*>(base + o_q1);
@@ -807,6 +817,7 @@ int hitb200_plan_create(const hitb200_desc* d, hitb200_plan** out) {
   p->d_tiles32 = reinterpret_cast<Work*>(base + o_tiles32);
   p->d_xlines = reinterpret_cast<Work*>(base + o_xl);
   p->d_ylines = reinterpret_cast<Work*>(base + o_yl);
+  p->d_srows = reinterpret_cast<Work*>(base + o_sr);
 
   // ---- host-built tables ----
   std::vector<double2> tw(nx + ny);
@@ -841,6 +852,8 @@ int hitb200_plan_create(const hitb200_desc* d, hitb200_plan** out) {
   std::vector<Work> xl, yl;
   for (int r = 0; r < ny; r += p->Rx) xl.push_back({0, r, std::min(p->Rx, ny - r), 0});
   for (int c = 0; c < nx; c += p->Ry) yl.push_back({0, c, std::min(p->Ry, nx - c), 0});
+  std::vector<Work> sr;
+  for (int r = 0; r < ny; r += srows) sr.push_back({0, 0, r, (int)sr.size()});
 
 #define HB_PUT(dst, src, bytes)                                                  \
   do {                                                                           \
@@ -860,6 +873,7 @@ int hitb200_plan_create(const hitb200_desc* d, hitb200_plan** out) {
   HB_PUT(p->d_tiles32, tiles32.data(), tiles32.size() * sizeof(Work));
   HB_PUT(p->d_xlines, xl.data(), xl.size() * sizeof(Work));
   HB_PUT(p->d_ylines, yl.data(), yl.size() * sizeof(Work));
+  HB_PUT(p->d_srows, sr.data(), sr.size() * sizeof(Work));
   HB_PUT(p->d_solve, &s, sizeof(SolveDev));
 #undef HB_PUT
   e = cudaMemset(s.counters, 0, 8 * sizeof(unsigned) + sizeof(int));
@@ -1093,7 +1107,7 @@ int hitb200_forcing_update(hitb200_plan* p, const double* q, const double* noise
   Bind b2{};
   b2.use = 1;
   b2.qin = q;
-  force_synth_kernel<<<L.n_tiles32, kRedThreads, 0, st>>>(L.solves, L.tiles32, b2);
+  force_synth_kernel<<<L.n_srows, kRedThreads, 0, st>>>(L.solves, L.srows, b2);
   const size_t plane = (size_t)p->desc.nx * p->desc.ny;
   const int nb = (int)std::min<size_t>((plane + 255) / 256, 4096);
   if (p->elem == 4) {
@@ -1225,7 +1239,7 @@ int hitb200_diagnostics(hitb200_plan* p, const double* q, double* out, int32_t n
 // Work lists, descriptor table and launch shape of a batch over b->plans.
 static int batch_build(hitb200_batch* b) {
   std::vector<SolveDev> hs;
-  std::vector<Work> tiles, tiles32, xl, yl;
+  std::vector<Work> tiles, tiles32, xl, yl, sr;
   std::vector<int> partner;
   const int n = (int)b->plans.size();
   // y panels of 4 columns (full 32-byte row segments of the FP64 state)
@@ -1259,6 +1273,8 @@ static int batch_build(hitb200_batch* b) {
     for (int r0 = 0; r0 < p->desc.ny; r0 += p->Rx) xl.push_back({i, r0, std::min(p->Rx, p->desc.ny - r0), 0});
     const int ry = ry4 ? 4 : p->Ry;
     for (int c0 = 0; c0 < p->desc.nx; c0 += ry) yl.push_back({i, c0, std::min(ry, p->desc.nx - c0), 0});
+    const int srows = synth_rows(p->desc.nx);
+    for (int r0 = 0, ks = 0; r0 < p->desc.ny; r0 += srows) sr.push_back({i, 0, r0, ks++});
     ModeTables mt = build_modes(p->desc);
     partner.insert(partner.end(), mt.partner.begin(), mt.partner.end());
     b->elem = p->elem;
@@ -1281,10 +1297,11 @@ static int batch_build(hitb200_batch* b) {
   b->n_tiles32 = (int)tiles32.size();
   b->n_x = (int)xl.size();
   b->n_y = (int)yl.size();
+  b->n_srows = (int)sr.size();
   default_tuning(b->n_x, b->n_y, b->n_tiles32, b->tuning);
   size_t bytes = hs.size() * sizeof(SolveDev) +
-                 (tiles.size() + tiles32.size() + xl.size() + yl.size()) * sizeof(Work) +
-                 partner.size() * sizeof(int) + 1024 + 6 * 256;
+                 (tiles.size() + tiles32.size() + xl.size() + yl.size() + sr.size()) * sizeof(Work) +
+                 partner.size() * sizeof(int) + 1024 + 7 * 256;
   unsigned char* buf = nullptr;
   cudaError_t e = cudaMalloc(&buf, bytes);
   if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(batch tables)");
@@ -1301,6 +1318,7 @@ static int batch_build(hitb200_batch* b) {
   b->d_tiles32 = reinterpret_cast<Work*>(put(tiles32.data(), tiles32.size() * sizeof(Work)));
   b->d_xlines = reinterpret_cast<Work*>(put(xl.data(), xl.size() * sizeof(Work)));
   b->d_ylines = reinterpret_cast<Work*>(put(yl.data(), yl.size() * sizeof(Work)));
+  b->d_srows = reinterpret_cast<Work*>(put(sr.data(), sr.size() * sizeof(Work)));
   b->d_partner = reinterpret_cast<int*>(put(partner.data(), partner.size() * sizeof(int)));
   if (ce != cudaSuccess) return cuda_fail(ce, "cudaMemcpy(batch tables)");
   prime_attributes(b->elem, b->mch_x, b->mch_y, b->smem_x, b->smem_y, b->smem_sensor);
@@ -1444,6 +1462,8 @@ static LaunchSet batch_launch_set(hitb200_batch* b, cudaStream_t st) {
   L.tiles = b->d_tiles;
   L.tiles32 = b->d_tiles32;
   L.n_tiles32 = b->n_tiles32;
+  L.srows = b->d_srows;
+  L.n_srows = b->n_srows;
   L.guard_blocks = b->guard_blocks;
   L.xl = b->d_xlines;
   L.yl = b->d_ylines;

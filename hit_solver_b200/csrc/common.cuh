@@ -23,6 +23,13 @@ constexpr int kHalo = 5;              // staged halo of the sweep lines
 constexpr int kMaxLine = 1024;        // longest supported grid line
 constexpr int kMaxDrag = 32;          // max drag modes (|k| <= kmax band)
 constexpr int kMaxForce = 128;        // max forcing shell modes
+// Forcing synthesis CTAs cover whole rows: about 1024 cells each, at most
+// kSynthMaxRows rows (the rows' mode table is built once per row).
+constexpr int kSynthMaxRows = 32;
+constexpr int kSynthTerms = 512;   // (row, mode) terms of one row-table chunk
+__host__ __device__ constexpr int synth_rows(int nx) {
+  return nx >= 1024 ? 1 : (1024 / nx > kSynthMaxRows ? kSynthMaxRows : 1024 / nx);
+}
 constexpr int kMaxWidth = 8;          // max sensor dilation width
 constexpr int kMaxKx = 16;            // max |x wavenumber bin| of drag / forcing modes
 constexpr int kMaxKyDrag = 4;         // max |y wavenumber bin| of drag modes

@@ -628,7 +628,8 @@ __global__ void noise_rng_kernel(const SolveDev* __restrict__ solves, int nsolve
 // Forcing synthesis: f_hat = (i ky phi, -i kx phi), fx = Re ifft2 (forcing.py:
 // 82-85) evaluated directly on the shell modes, plus the sums the rescaling
 // needs (forcing.py:87-118), then the scalar rescaling logic.  The synthesis
-// is separable: for each row y of the tile the modes are first folded into
+// is separable: each CTA covers whole rows (about 1024 cells, synth_rows),
+// and for each of its rows y the modes are first folded into
 // P_k(y) = sum over modes with |kx| = k of c_m e^{i ky y} (conjugated for
 // kx < 0), so that a cell needs only Re sum_k P_k(y) e^{i k x}, k = 0..max|kx|.
 __global__ void __launch_bounds__(kRedThreads)
@@ -645,47 +646,66 @@ __global__ void __launch_bounds__(kRedThreads)
   const int2* modes = S.modes + S.n_drag;
   const double invN = 1.0 / ((double)nx * (double)ny);
   __shared__ double2 ca[kMaxForce], cb[kMaxForce];
-  __shared__ double2 px[kTileY][kMaxKx + 1], py[kTileY][kMaxKx + 1];
+  __shared__ double2 px[kSynthMaxRows][kMaxKx + 1], py[kSynthMaxRows][kMaxKx + 1];
   __shared__ double sm[kRedWarps * 4];
   __shared__ double red[4];
-  for (int m = threadIdx.x; m < nf; m += blockDim.x) {
+  // the solve's mode tables in shared memory, read by every (row, mode) term
+  __shared__ int2 mk[kMaxForce];  // (x bin, y bin) of the modes in |x bin| order
+  __shared__ short kofs[kMaxKx + 2];
+  // ca, cb and mk are indexed by the position j in that order (mode f_order[j])
+  for (int j = threadIdx.x; j < nf; j += blockDim.x) {
+    const int m = S.f_order[j];
     const double pr = sc[S_PHI + 2 * m], pi = sc[S_PHI + 2 * m + 1];
     const double2 kv = S.kvec[m];
-    ca[m] = make_double2(-kv.y * pi * invN, kv.y * pr * invN);   // (i ky phi)/N
-    cb[m] = make_double2(kv.x * pi * invN, -kv.x * pr * invN);   // (-i kx phi)/N
+    ca[j] = make_double2(-kv.y * pi * invN, kv.y * pr * invN);   // (i ky phi)/N
+    cb[j] = make_double2(kv.x * pi * invN, -kv.x * pr * invN);   // (-i kx phi)/N
+    mk[j] = modes[m];
   }
+  for (int k = threadIdx.x; k < K + 2; k += blockDim.x) kofs[k] = S.f_kofs[k];
   __syncthreads();
-  for (int t = threadIdx.x; t < kTileY * (K + 1); t += blockDim.x) {
-    const int a = t / (K + 1), k = t - a * (K + 1);
-    const int gj = min(w.b + a, ny - 1);
-    double2 sx = make_double2(0.0, 0.0), sy = make_double2(0.0, 0.0);
-    for (int j = S.f_kofs[k]; j < S.f_kofs[k + 1]; ++j) {
-      const int m = S.f_order[j];
-      const int2 md = modes[m];
-      const double2 e = S.twy[mode_index(md.y, gj, ny)];  // e^{-i ky y}
-      const double er = e.x, ei = -e.y;                   // e^{+i ky y}
-      double ar = ca[m].x * er - ca[m].y * ei, ai = ca[m].x * ei + ca[m].y * er;
-      double br = cb[m].x * er - cb[m].y * ei, bi = cb[m].x * ei + cb[m].y * er;
+  const double2* __restrict__ twy = S.twy;
+  // this CTA: rows w.b .. w.b + rows - 1, every column
+  const int rows = min(synth_rows(nx), ny - w.b);
+  // row tables in chunks of rows: one thread per (row, mode) term into shared
+  // memory (the twiddle loads all in flight at once), then each (row, |kx|)
+  // sum over its modes in mode order
+  __shared__ double2 tmx[kSynthTerms], tmy[kSynthTerms];
+  const int rc = max(1, min(rows, kSynthTerms / max(nf, 1)));
+  for (int a0 = 0; a0 < rows; a0 += rc) {
+    const int na = min(rc, rows - a0);
+    for (int t = threadIdx.x; t < na * nf; t += blockDim.x) {
+      const int aa = t / nf, j = t - aa * nf;
+      const int2 md = mk[j];
+      const double2 e = twy[mode_index(md.y, w.b + a0 + aa, ny)];  // e^{-i ky y}
+      const double er = e.x, ei = -e.y;                             // e^{+i ky y}
+      double ar = ca[j].x * er - ca[j].y * ei, ai = ca[j].x * ei + ca[j].y * er;
+      double br = cb[j].x * er - cb[j].y * ei, bi = cb[j].x * ei + cb[j].y * er;
       if (md.x < 0) {
         ai = -ai;
         bi = -bi;
       }
-      sx.x += ar;
-      sx.y += ai;
-      sy.x += br;
-      sy.y += bi;
+      tmx[t] = make_double2(ar, ai);
+      tmy[t] = make_double2(br, bi);
     }
-    px[a][k] = sx;
-    py[a][k] = sy;
+    __syncthreads();
+    for (int t = threadIdx.x; t < na * (K + 1); t += blockDim.x) {
+      const int aa = t / (K + 1), k = t - aa * (K + 1);
+      double2 sx = make_double2(0.0, 0.0), sy = make_double2(0.0, 0.0);
+      for (int j = kofs[k]; j < kofs[k + 1]; ++j) {
+        const double2 u = tmx[aa * nf + j], v = tmy[aa * nf + j];
+        sx.x += u.x;
+        sx.y += u.y;
+        sy.x += v.x;
+        sy.y += v.y;
+      }
+      px[a0 + aa][k] = sx;
+      py[a0 + aa][k] = sy;
+    }
+    __syncthreads();
   }
-  __syncthreads();
-  const int tx = threadIdx.x & 31, ty0 = threadIdx.x >> 5;
-  const int gi = w.a + tx;
   double sxx = 0, syy = 0, sxy = 0, spow = 0;
-#pragma unroll
-  for (int kk = 0; kk < kCellsPerThread; ++kk) {
-    const int a = ty0 + kRedWarps * kk, gj = w.b + a;
-    if (gj >= ny || gi >= nx) continue;
+  for (int idx = threadIdx.x; idx < rows * nx; idx += blockDim.x) {
+    const int a = idx / nx, gi = idx - a * nx, gj = w.b + a;
     double fx = px[a][0].x, fy = py[a][0].x;
     int ix = 0;
     for (int k = 1; k <= K; ++k) {

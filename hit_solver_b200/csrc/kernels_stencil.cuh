@@ -447,12 +447,10 @@ constexpr double kSolveScale = 1.2037766123870306;  // -rho / a
 constexpr int kPowTab = 128;                         // rho^k below 1e-43 beyond this
 
 // rho^k, k in [0, kPowTab); filled once by the host (hitb200_plan_create).
+// Outflow sweeps copy it to shared memory while they stage their lines: read
+// from global memory at the end-row correction, every CTA of a launch asked
+// for the same few lines of L2 at once.
 __device__ double g_rho_pow[kPowTab];
-
-template <typename T>
-__device__ __forceinline__ T rho_pow(int k) {
-  return (k >= 0 && k < kPowTab) ? T(__ldg(&g_rho_pow[k])) : T(0);
-}
 
 constexpr int kSweepHalo = 8;  // staged nodes left of node 0 (WENO reads 5)
 
@@ -637,6 +635,10 @@ __global__ void __launch_bounds__(AXIS == 0 ? 256 : 512,
   T* WB = reinterpret_cast<T*>(smem + L.off_wb());
   uint8_t* MK = smem + L.off_mk();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+  __shared__ T rpow[kPowTab];  // rho^k for the outflow end rows
+  if (!per)
+    for (int t = threadIdx.x; t < kPowTab; t += blockDim.x) rpow[t] = T(__ldg(&g_rho_pow[t]));
+  auto rho_pow = [&](int k) -> T { return (k >= 0 && k < kPowTab) ? rpow[k] : T(0); };
 
   // ---- L: stage flux and enforced state of the lines ---------------------------
   // x lines: consecutive threads take consecutive nodes of a row; y lines:
@@ -955,7 +957,7 @@ __global__ void __launch_bounds__(AXIS == 0 ? 256 : 512,
         x[2][0] = ends[r][2][0];
         x[3][0] = ends[r][3][0];
       } else {
-        const T e = rho_pow<T>(n - 1);
+        const T e = rho_pow(n - 1);
         const T den = T(1) - e * e;
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
@@ -963,7 +965,7 @@ __global__ void __launch_bounds__(AXIS == 0 ? 256 : 512,
           const T ca = (r0 - e * r1) / den, cb = (r1 - e * r0) / den;
 #pragma unroll
           for (int k = 0; k < MN; ++k)
-            if (k < len) x[c][k] += ca * rho_pow<T>(i0 + k) + cb * rho_pow<T>(n - 1 - i0 - k);
+            if (k < len) x[c][k] += ca * rho_pow(i0 + k) + cb * rho_pow(n - 1 - i0 - k);
         }
       }
     }
