@@ -173,9 +173,12 @@ __device__ __forceinline__ EnfPrim<T> enforced_prim(double q0, double q1, double
 // into this CTA's row of partials (S.part_pre[w.c][*]); returns the number of
 // slots.  Runs on the first kPreThreads threads of the CTA; every thread of
 // the CTA must call it (it synchronises the CTA).
+// Returns the number of reduction slots, or -1 when `active` is false: an
+// inactive solve's tile stops after its loads (issued before the caller's flag
+// arrives, so that they do not wait for it) and writes nothing.
 template <typename T>
 __device__ int prepass_tile(const SolveDev& S, const Work& w, int buf, int mode, int enf,
-                            const Bind& bind) {
+                            const Bind& bind, bool active = true) {
   const bool act = threadIdx.x < kPreThreads;
   const double* q = bind.use ? bind.qin : stage_in(S, buf);
   const int nx = S.nx, ny = S.ny, per = S.periodic;
@@ -295,6 +298,7 @@ __device__ int prepass_tile(const SolveDev& S, const Work& w, int buf, int mode,
       sv[ra][rb] = e.v;
     }
     __syncthreads();
+    if (!active) return -1;
 #pragma unroll
     for (int k = 0; k < kPreRows; ++k) {
       const int a0 = warp + kPreWarps * k, gj = y0 + a0;
@@ -332,6 +336,7 @@ __device__ int prepass_tile(const SolveDev& S, const Work& w, int buf, int mode,
     }
   } else {
     __syncthreads();  // tw table
+    if (!active) return -1;
   }
   if (act) {
   warp_to_smem4<OP_MAX>(ax, ay, mr, mp, sm, make_int4(R_AX, R_AY, R_RHO, R_P), nslots);
@@ -486,8 +491,9 @@ __global__ void __launch_bounds__(kPreThreads, OCC ? HITB200_PRE_MIN_BLOCKS : 2)
   const SolveDev& S = solves[w.solve];
   double* sc = S.scal;
   if (mode == PRE_SENSOR && !bind.use && sc[S_HV_STEP] == 0.0) return;  // no hyperviscosity this step
-  if (mode == PRE_STAGE && !bind.use && sc[S_ACTIVE] == 0.0) return;
-  const int nslots = prepass_tile<T>(S, w, buf, mode, enf, bind);
+  const bool active = !(mode == PRE_STAGE && !bind.use && sc[S_ACTIVE] == 0.0);
+  const int nslots = prepass_tile<T>(S, w, buf, mode, enf, bind, active);
+  if (nslots < 0) return;
   if (!last_block(&S.counters[0], S.nblk_pre)) return;
   // ---- last CTA of this solve: fixed-order final reduction + scalar logic ----
   __shared__ double red[R_FIXED + 4 * kMaxDrag];

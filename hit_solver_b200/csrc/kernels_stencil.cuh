@@ -152,9 +152,18 @@ __global__ void __launch_bounds__(kSensorThreads, sizeof(T) == 8 ? 1 : HITB200_S
   const Work wk = work[blockIdx.x];
   const SolveDev& S = solves[wk.solve];
   const double* sc = S.scal;
+  // a finished solve's launch is a no-op; outside the fused form its flag is
+  // tested once the staging loads are in flight
+  bool active = true;
   if (!bind.use) {
     if (sel == 3 && sc[S_HV_STEP] == 0.0) return;
-    if (sel != 3 && sc[S_ACTIVE] == 0.0 && !(FUSED && sel == 0)) return;
+    if (sel != 3 && !(FUSED && sel == 0)) {
+      if constexpr (FUSED) {
+        if (sc[S_ACTIVE] == 0.0) return;
+      } else {
+        active = sc[S_ACTIVE] != 0.0;
+      }
+    }
   }
   const int pre_mode = sel == 0 ? PRE_STEP : (sel == 3 ? PRE_SENSOR : PRE_STAGE);
   int pre_slots = 0;
@@ -218,6 +227,7 @@ __global__ void __launch_bounds__(kSensorThreads, sizeof(T) == 8 ? 1 : HITB200_S
     }
   }
   __syncthreads();
+  if (!active) return;
 
   double l_eps_r, l_eps_p, l_eps_e, l_comp, l_shear;
   if constexpr (FUSED) {
@@ -617,7 +627,9 @@ __global__ void __launch_bounds__(AXIS == 0 ? 256 : 512,
   const Work wk = work[blockIdx.x];
   const SolveDev& S = solves[wk.solve];
   const double* sc = S.scal;
-  if (!bind.use && sc[S_ACTIVE] == 0.0) return;
+  // a finished solve's launch is a no-op; its flag is tested once the staging
+  // loads are in flight, so that they do not wait for the scalar block
+  const bool active = bind.use || sc[S_ACTIVE] != 0.0;
   const int nx = S.nx, ny = S.ny, per = S.periodic;
   const int n = AXIS == 0 ? nx : ny;
   const size_t plane = (size_t)nx * ny;
@@ -700,6 +712,7 @@ __global__ void __launch_bounds__(AXIS == 0 ? 256 : 512,
     MK[r * (n + 2) + p] = weno_all ? 1 : mask[o];
   }
   __syncthreads();
+  if (!active) return;
 
   // face il + 1/2 (il in [-1, n-1]) is flagged when node il or il + 1 is
   auto flagged = [&](const uint8_t* mk, int f) -> bool {
