@@ -204,6 +204,15 @@ __device__ __forceinline__ void enforce_node_rcp(T& q0, T& q1, T& q2, T& q3, T g
   q3 = p > T(kPFloor) ? q3 : T(kPFloor) / (gamma - T(1)) + kin;
 }
 
+// Programmatic dependent launch.  A kernel launched with programmatic stream
+// serialization may start while the previous kernel of the stream finishes:
+// pdl_wait() blocks until that kernel has completed and its writes are
+// visible, so everything that reads what it wrote comes after pdl_wait().
+// pdl_release() lets the next kernel start its prologue.  Both are no-ops in
+// a launch without the attribute.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_release() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 template <typename T>
 __device__ __forceinline__ T warp_sum(T v) {
 #pragma unroll

@@ -490,10 +490,12 @@ __global__ void __launch_bounds__(kPreThreads, OCC ? HITB200_PRE_MIN_BLOCKS : 2)
   const Work w = work[blockIdx.x];
   const SolveDev& S = solves[w.solve];
   double* sc = S.scal;
+  pdl_wait();  // below: the state and scalars of the previous kernels
   if (mode == PRE_SENSOR && !bind.use && sc[S_HV_STEP] == 0.0) return;  // no hyperviscosity this step
   const bool active = !(mode == PRE_STAGE && !bind.use && sc[S_ACTIVE] == 0.0);
   const int nslots = prepass_tile<T>(S, w, buf, mode, enf, bind, active);
   if (nslots < 0) return;
+  pdl_release();
   if (!last_block(&S.counters[0], S.nblk_pre)) return;
   // ---- last CTA of this solve: fixed-order final reduction + scalar logic ----
   __shared__ double red[R_FIXED + 4 * kMaxDrag];

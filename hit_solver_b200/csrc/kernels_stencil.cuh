@@ -152,6 +152,7 @@ __global__ void __launch_bounds__(kSensorThreads, sizeof(T) == 8 ? 1 : HITB200_S
   const Work wk = work[blockIdx.x];
   const SolveDev& S = solves[wk.solve];
   const double* sc = S.scal;
+  pdl_wait();  // below: the state and scalars of the previous kernels
   // a finished solve's launch is a no-op; outside the fused form its flag is
   // tested once the staging loads are in flight
   bool active = true;
@@ -228,6 +229,7 @@ __global__ void __launch_bounds__(kSensorThreads, sizeof(T) == 8 ? 1 : HITB200_S
   }
   __syncthreads();
   if (!active) return;
+  pdl_release();
 
   double l_eps_r, l_eps_p, l_eps_e, l_comp, l_shear;
   if constexpr (FUSED) {
@@ -627,9 +629,6 @@ __global__ void __launch_bounds__(AXIS == 0 ? 256 : 512,
   const Work wk = work[blockIdx.x];
   const SolveDev& S = solves[wk.solve];
   const double* sc = S.scal;
-  // a finished solve's launch is a no-op; its flag is tested once the staging
-  // loads are in flight, so that they do not wait for the scalar block
-  const bool active = bind.use || sc[S_ACTIVE] != 0.0;
   const int nx = S.nx, ny = S.ny, per = S.periodic;
   const int n = AXIS == 0 ? nx : ny;
   const size_t plane = (size_t)nx * ny;
@@ -642,7 +641,6 @@ __global__ void __launch_bounds__(AXIS == 0 ? 256 : 512,
   const double h = AXIS == 0 ? S.dx : S.dy;
   const double* qin = bind.use ? bind.qin : stage_in(S, stage);
   const uint8_t* mask = bind.use ? bind.mask : S.mask;
-  const T alpha = T(AXIS == 0 ? sc[S_ALPHA_X] : sc[S_ALPHA_Y]);
   T* FQ = reinterpret_cast<T*>(smem);
   T* WB = reinterpret_cast<T*>(smem + L.off_wb());
   uint8_t* MK = smem + L.off_mk();
@@ -651,6 +649,11 @@ __global__ void __launch_bounds__(AXIS == 0 ? 256 : 512,
   if (!per)
     for (int t = threadIdx.x; t < kPowTab; t += blockDim.x) rpow[t] = T(__ldg(&g_rho_pow[t]));
   auto rho_pow = [&](int k) -> T { return (k >= 0 && k < kPowTab) ? rpow[k] : T(0); };
+  pdl_wait();  // below: the state, mask and scalars of the previous kernels
+  // a finished solve's launch is a no-op; its flag is tested once the staging
+  // loads are in flight, so that they do not wait for the scalar block
+  const bool active = bind.use || sc[S_ACTIVE] != 0.0;
+  const T alpha = T(AXIS == 0 ? sc[S_ALPHA_X] : sc[S_ALPHA_Y]);
 
   // ---- L: stage flux and enforced state of the lines ---------------------------
   // x lines: consecutive threads take consecutive nodes of a row; y lines:
@@ -985,6 +988,7 @@ __global__ void __launch_bounds__(AXIS == 0 ? 256 : 512,
   }
 
   // ---- E: epilogue ----------------------------------------------------------------------
+  pdl_release();
   const int terms = bind.use ? bind.terms : fused_terms(S);
   if (AXIS == 1) {
     // y sweep: partial rhs -dG/dy (or the bare derivative for the API),
@@ -1193,6 +1197,7 @@ __global__ void __launch_bounds__(kStencilThreads)
   __shared__ T Ls[4][LY][LX];
   const Work wk = work[blockIdx.x];
   const SolveDev& S = solves[wk.solve];
+  pdl_wait();  // below: the state, mask and scalars of the previous kernels
   if (!bind.use && S.scal[S_HV_STEP] == 0.0) return;
   const double* q = bind.use ? bind.qin : S.q1;
   double* out = bind.use ? bind.qout : S.q;
@@ -1235,6 +1240,7 @@ __global__ void __launch_bounds__(kStencilThreads)
     }
   }
   __syncthreads();
+  pdl_release();
   // solve fields in registers: the stores below cannot force reloads
   const double gam = S.gamma;
   const int gcell = (!bind.use && !per) ? S.guard : 0;  // fused outflow guard of the step
