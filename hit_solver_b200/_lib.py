@@ -28,6 +28,8 @@ S_ALPHA_X, S_ALPHA_Y, S_DIV_RMS, S_VORT_RMS, S_DT, S_TIME, S_STEP, S_ACTIVE, S_M
  S_F_FXX, S_F_FYY, S_F_FXY, S_F_AF, S_F_DECAY, S_F_SCALE, S_MAX_STEPS, S_STATUS,
  S_NEAR_THRESHOLD, S_HV_APPLIED) = range(9, 25)
 S_COUNT = 32
+# bits of the S_STATUS slot (HITB200_ST_*)
+ST_NONFINITE, ST_NONPOS_RHO, ST_NONPOS_P, ST_BARRIER = 1, 2, 4, 8
 TUNE_SWEEP_X, TUNE_SWEEP_Y, TUNE_PREPASS, TUNE_FUSED_SENSOR, TUNE_COUNT = 0, 1, 2, 3, 4
 
 NAN = float("nan")
@@ -183,6 +185,18 @@ def load(path: Path | str | None = None) -> ctypes.CDLL:
     if path is None:
         _lib = lib
     return lib
+
+
+def check_step_status(bits: int, label: str) -> None:
+    """Raise for the status bits a run loop must not continue past: a grid
+    barrier that timed out (RuntimeError: the step's results are invalid)
+    and a non-finite state (FloatingPointError, as the reference's loops
+    raise).  The validation bits are left to the Riemann validation."""
+    bits = int(bits)
+    if bits & ST_BARRIER:
+        raise RuntimeError(f"{label}: a grid barrier of the fused prepass/sensor timed out")
+    if bits & ST_NONFINITE:
+        raise FloatingPointError(f"NaN or infinite value detected in {label}")
 
 
 def check(status: int) -> None:

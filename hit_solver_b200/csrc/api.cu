@@ -24,6 +24,10 @@
 
 using namespace hitb200;
 
+static_assert(ST_NONFINITE == HITB200_ST_NONFINITE && ST_NONPOS_RHO == HITB200_ST_NONPOS_RHO &&
+                  ST_NONPOS_P == HITB200_ST_NONPOS_P && ST_BARRIER == HITB200_ST_BARRIER,
+              "status bits of the device code and of the C ABI must agree");
+
 namespace {
 
 thread_local std::string g_last_error;

@@ -579,8 +579,7 @@ def run_simulation(config: HIT2DConfig):
     while True:
         solver.advance(chunk)
         s = solver.scalars()
-        if int(s[_lib.S_STATUS]) & 1:
-            raise FloatingPointError("NaN or infinite value detected in HIT2D state")
+        _lib.check_step_status(s[_lib.S_STATUS], "HIT2D state")
         new_step, time, dt = int(s[_lib.S_STEP]), s[_lib.S_TIME], s[_lib.S_DT]
         progressed = new_step > step
         step = new_step

@@ -361,6 +361,7 @@ def run_riemann(config: RiemannConfig3):
         solver.advance(chunk)
         done += chunk
         if done % config.progress_every == 0 or done == solver.n_steps:
+            _lib.check_step_status(solver.plan.scalars()[_lib.S_STATUS], f"state at step {done}")
             validate_raw_physical_state(solver.q, config.equation, f"state at step {done}")
             print(f"step={done:6d}, time={done * solver.dt:.6f}")
     s = solver.plan.scalars()

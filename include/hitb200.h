@@ -123,6 +123,12 @@ enum hitb200_scalar {
   HITB200_S_HV_APPLIED = 24,     /* hyperviscosity applications so far */
   HITB200_S_COUNT = 32
 };
+/* Bits of HITB200_S_STATUS. */
+#define HITB200_ST_NONFINITE 1    /* NaN/Inf in a state the step read            */
+#define HITB200_ST_NONPOS_RHO 2   /* raw density <= 0 (validation)               */
+#define HITB200_ST_NONPOS_P 4     /* raw pressure <= 0 (validation)              */
+#define HITB200_ST_BARRIER 8      /* a fused prepass/sensor grid barrier timed out
+                                     (about 2 s); that step's results are invalid */
 
 /* ---- plan ---------------------------------------------------------------- */
 /* Defaults of HIT2DConfig (OOP/hit2d.py:36-80) on a 2*pi periodic square. */

@@ -105,3 +105,20 @@ def test_null_arguments_are_rejected(lib):
     assert lib.hitb200_enforce_state(None, None, 10, 1.4, None) == _lib.ERR_INVALID
     assert lib.hitb200_step(None, None, None, None) == _lib.ERR_INVALID
     assert lib.hitb200_plan_destroy(None) == _lib.OK
+
+
+def test_step_status_bits_map_to_exceptions():
+    """The run loops' host check of the S_STATUS bits: a timed-out grid
+    barrier is a RuntimeError (the step's results are invalid), a non-finite
+    state a FloatingPointError; the validation bits are left to the Riemann
+    validation and pass."""
+    import pytest
+
+    from hit_solver_b200 import _lib
+
+    _lib.check_step_status(0, "x")
+    _lib.check_step_status(float(_lib.ST_NONPOS_RHO | _lib.ST_NONPOS_P), "x")
+    with pytest.raises(RuntimeError, match="barrier"):
+        _lib.check_step_status(_lib.ST_BARRIER | _lib.ST_NONFINITE, "x")
+    with pytest.raises(FloatingPointError, match="NaN"):
+        _lib.check_step_status(float(_lib.ST_NONFINITE), "HIT2D state")
