@@ -425,10 +425,20 @@ __device__ void prepass_finalize(const SolveDev& S, int nslots, double* red) {
   const int op = pre_op(t);
   double acc = op == OP_SUM ? 0.0 : -INFINITY;
   if (threadIdx.x < kPreThreads && j < C) {
-#pragma unroll 8
-    for (int b = j; b < S.nblk_pre; b += C) {
-      const double x = __ldcg(S.part_pre + (size_t)b * nslots + t);
-      acc = op == OP_SUM ? acc + x : fmax(acc, x);
+    // 16 loads in flight per round (the partials come from every SM's
+    // recent stores), combined in block order
+    const double* base = S.part_pre + t;
+    const int nb = S.nblk_pre;
+    for (int b0 = j; b0 < nb; b0 += 16 * C) {
+      double x[16];
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        const int b = b0 + i * C;
+        x[i] = b < nb ? __ldcg(base + (size_t)b * nslots) : 0.0;
+      }
+#pragma unroll
+      for (int i = 0; i < 16; ++i)
+        if (b0 + i * C < nb) acc = op == OP_SUM ? acc + x[i] : fmax(acc, x[i]);
     }
     chunk[j * nslots + t] = acc;
   }

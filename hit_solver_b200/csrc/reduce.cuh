@@ -86,23 +86,6 @@ __device__ __forceinline__ bool last_block(unsigned* counter, int nblk) {
   return is_last;
 }
 
-// Final fixed-order reduction of partials[nblk][nslots] into out[nslots].
-__device__ __forceinline__ void finalize_partials(const double* part, int nblk, int nslots,
-                                                  const int* ops, double* out) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int t = warp; t < nslots; t += kRedWarps) {
-    const int op = ops ? ops[t] : OP_SUM;
-    double acc = op == OP_SUM ? 0.0 : -INFINITY;
-    for (int b = lane; b < nblk; b += 32) {
-      double x = __ldcg(part + (size_t)b * nslots + t);
-      acc = op == OP_SUM ? acc + x : fmax(acc, x);
-    }
-    acc = op == OP_SUM ? warp_sum(acc) : warp_max(acc);
-    if (lane == 0) out[t] = acc;
-  }
-  __syncthreads();
-}
-
 // Barrier over every CTA of a cooperative launch (which guarantees that all
 // of them are resident).  count and gen are zero-initialised words of the
 // solve's counters; the last CTA to arrive resets count and advances gen.
