@@ -1112,7 +1112,38 @@ __global__ void __launch_bounds__(AXIS == 0 ? 256 : 512,
       rhs[2] += double(visp[plane + o]);
       rhs[3] += double(visp[2 * plane + o]);
     }
-    if (terms & (4 | 8)) {
+    if constexpr (sizeof(T) == 4) {
+      // FP32-bulk form: the forcing and drag sources in FP32 (they are rhs
+      // terms; FP64 stays in the stage combine below)
+      if (terms & (4 | 8)) {
+        const float prho = fmaxf(float(qa[0]), float(kRhoFloor));
+        const float prinv = __frcp_rn(prho);
+        const float pu = float(qa[1]) * prinv, pv = float(qa[2]) * prinv;
+        if (terms & 4) {
+          const float ffs = float(fs);
+          const float tfx = bind.use ? float(bfx[o]) : ffs * float(sfx[o]);
+          const float tfy = bind.use ? float(bfy[o]) : ffs * float(sfy[o]);
+          rhs[1] += double(prho * tfx);
+          rhs[2] += double(prho * tfy);
+          rhs[3] += double(prho * (pu * tfx + pv * tfy));
+        }
+        if (drag) {
+          float lx = float(dpx[rr][0].x), ly = float(dpy[rr][0].x);
+          int ix = 0;
+          for (int kk = 1; kk <= kxd; ++kk) {
+            ix += col;
+            if (ix >= nx) ix -= nx;  // (k x) mod nx
+            const double2 e = twx[ix];
+            const float er = float(e.x), ei = -float(e.y);  // e^{+i k x}
+            lx += float(dpx[rr][kk].x) * er - float(dpx[rr][kk].y) * ei;
+            ly += float(dpy[rr][kk].x) * er - float(dpy[rr][kk].y) * ei;
+          }
+          rhs[1] += double(lx);
+          rhs[2] += double(ly);
+          rhs[3] += double(pu * lx + pv * ly);
+        }
+      }
+    } else if (terms & (4 | 8)) {
       // rho, u, v of primitive_from_conservative (one reciprocal)
       const double prho = qa[0] > kRhoFloor ? qa[0] : kRhoFloor;
       const double prinv = 1.0 / prho;
