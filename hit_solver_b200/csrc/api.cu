@@ -501,10 +501,9 @@ LaunchSet plan_launch_set(hitb200_plan* p, cudaStream_t st) {
   L.smem_sensor = p->smem_sensor;
   L.st = st;
   L.cells = (double)p->desc.nx * p->desc.ny;
-  // one solve's launches are single waves: the next kernel's CTAs can take
-  // free SM slots and run their prologue while the previous one finishes
-  // (512^2 FP32 step 0.280 -> 0.275 ms)
-  L.pdl = 1;
+  // programmatic dependent launch only in the step sequence (set by its
+  // callers), whose kernel order makes each kernel's early loads safe
+  L.pdl = 0;
   L.cells_visc = p->desc.viscosity > 0.0 ? L.cells : 0.0;
   L.cells_force = p->desc.forcing_on ? L.cells : 0.0;
   return L;
@@ -1166,6 +1165,8 @@ int hitb200_step(hitb200_plan* p, double* q, const double* noise, void* stream) 
     HB_CUDA(cudaMemcpyAsync((void*)p->hs.noise, noise, (size_t)p->desc.nx * p->desc.ny * sizeof(double),
                             cudaMemcpyDefault, st));
   LaunchSet L = plan_launch_set(p, st);
+  L.pdl = 1;  // one solve's launches are single waves: the next kernel's CTAs
+              // stage their inputs while the previous kernel finishes
   return launch_step_sequence(L, p->desc.forcing_on, upload, !p->desc.periodic, p->hs.hv_interval > 0);
 }
 
@@ -1184,6 +1185,8 @@ int hitb200_run(hitb200_plan* p, double* q, int32_t nsteps, void* stream) {
     cudaStream_t cap;
     HB_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
     LaunchSet L = plan_launch_set(p, cap);
+    L.pdl = 1;  // one solve's launches are single waves: the next kernel's CTAs
+                // stage their inputs while the previous kernel finishes
     // make every kernel's shared-memory attribute final before capture
     HB_CUDA(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
     r = launch_step_sequence(L, p->desc.forcing_on, 0, !p->desc.periodic, p->hs.hv_interval > 0);
@@ -1469,6 +1472,8 @@ int hitb200_step_profile(hitb200_plan* p, double* q, const double* noise, float*
   Prof pr;
   pr.st = st;
   LaunchSet L = plan_launch_set(p, st);
+  L.pdl = 1;  // one solve's launches are single waves: the next kernel's CTAs
+              // stage their inputs while the previous kernel finishes
   r = launch_step_sequence(L, p->desc.forcing_on, upload, !p->desc.periodic, p->hs.hv_interval > 0, &pr);
   if (r != HITB200_OK) return r;
   return finish_profile(pr, ms, bytes, cap, count, names, names_size);

@@ -152,19 +152,16 @@ __global__ void __launch_bounds__(kSensorThreads, sizeof(T) == 8 ? 1 : HITB200_S
   const Work wk = work[blockIdx.x];
   const SolveDev& S = solves[wk.solve];
   const double* sc = S.scal;
-  pdl_wait();  // below: the state and scalars of the previous kernels
-  // a finished solve's launch is a no-op; outside the fused form its flag is
-  // tested once the staging loads are in flight
-  bool active = true;
-  if (!bind.use) {
-    if (sel == 3 && sc[S_HV_STEP] == 0.0) return;
-    if (sel != 3 && !(FUSED && sel == 0)) {
-      if constexpr (FUSED) {
-        if (sc[S_ACTIVE] == 0.0) return;
-      } else {
-        active = sc[S_ACTIVE] != 0.0;
-      }
-    }
+  // Launched after the prepass of its state, the unfused sensor stages that
+  // state (written two or more kernels earlier, so complete when this CTA
+  // starts: the prepass releases its dependents only after its own wait) and
+  // waits for the prepass only before it reads the thresholds.  The fused
+  // form computes the prepass itself and waits first.
+  if constexpr (FUSED) pdl_wait();
+  // the hyperviscosity flag is written by the step's first kernel
+  if (!bind.use && sel == 3 && sc[S_HV_STEP] == 0.0) return;
+  if constexpr (FUSED) {
+    if (!bind.use && sel != 3 && sel != 0 && sc[S_ACTIVE] == 0.0) return;
   }
   const int pre_mode = sel == 0 ? PRE_STEP : (sel == 3 ? PRE_SENSOR : PRE_STAGE);
   int pre_slots = 0;
@@ -196,7 +193,8 @@ __global__ void __launch_bounds__(kSensorThreads, sizeof(T) == 8 ? 1 : HITB200_S
     const int a = row_of(idx, SX, isx), b = idx - a * SX;
     const int gj = fold_node(y0 - HW + a, ny, per), gi = fold_node(x0 - HW + b, nx, per);
     const size_t o = (size_t)gj * nx + gi;
-    T q0 = T(q[o]), q1 = T(q[o + plane]), q2 = T(q[o + 2 * plane]), q3 = T(q[o + 3 * plane]);
+    T q0 = T(__ldcg(q + o)), q1 = T(__ldcg(q + o + plane)), q2 = T(__ldcg(q + o + 2 * plane)),
+      q3 = T(__ldcg(q + o + 3 * plane));
     if constexpr (sizeof(T) == 8) {
       if (enf) enforce_node(q0, q1, q2, q3, g);
       const Prim<T> p = primitives(q0, q1, q2, q3, g);
@@ -228,7 +226,11 @@ __global__ void __launch_bounds__(kSensorThreads, sizeof(T) == 8 ? 1 : HITB200_S
     }
   }
   __syncthreads();
-  if (!active) return;
+  if constexpr (!FUSED) {
+    pdl_wait();  // below: the prepass's thresholds and the solve's flags
+    // a finished solve's launch is a no-op
+    if (!bind.use && sel != 3 && sc[S_ACTIVE] == 0.0) return;
+  }
   pdl_release();
 
   double l_eps_r, l_eps_p, l_eps_e, l_comp, l_shear;
@@ -649,11 +651,6 @@ __global__ void __launch_bounds__(AXIS == 0 ? 256 : 512,
   if (!per)
     for (int t = threadIdx.x; t < kPowTab; t += blockDim.x) rpow[t] = T(__ldg(&g_rho_pow[t]));
   auto rho_pow = [&](int k) -> T { return (k >= 0 && k < kPowTab) ? rpow[k] : T(0); };
-  pdl_wait();  // below: the state, mask and scalars of the previous kernels
-  // a finished solve's launch is a no-op; its flag is tested once the staging
-  // loads are in flight, so that they do not wait for the scalar block
-  const bool active = bind.use || sc[S_ACTIVE] != 0.0;
-  const T alpha = T(AXIS == 0 ? sc[S_ALPHA_X] : sc[S_ALPHA_Y]);
 
   // ---- L: stage flux and enforced state of the lines ---------------------------
   // x lines: consecutive threads take consecutive nodes of a row; y lines:
@@ -672,7 +669,8 @@ __global__ void __launch_bounds__(AXIS == 0 ? 256 : 512,
     }
     const int gp = fold_node(p - kSweepHalo, n, per);
     const size_t o = AXIS == 0 ? (size_t)(line0 + r) * nx + gp : (size_t)gp * nx + line0 + r;
-    T a0 = T(qin[o]), a1 = T(qin[o + plane]), a2 = T(qin[o + 2 * plane]), a3 = T(qin[o + 3 * plane]);
+    T a0 = T(__ldcg(qin + o)), a1 = T(__ldcg(qin + o + plane)), a2 = T(__ldcg(qin + o + 2 * plane)),
+      a3 = T(__ldcg(qin + o + 3 * plane));
     // enforce_physical_state, then primitive_from_conservative of the result
     const T rho = a0 > T(kRhoFloor) ? a0 : T(kRhoFloor);
     const T rinv = T(1) / rho;
@@ -697,6 +695,15 @@ __global__ void __launch_bounds__(AXIS == 0 ? 256 : 512,
     f[6 * LS] = a2;
     f[7 * LS] = a3;
   }
+  // The stage input was written two or more kernels earlier (complete when
+  // this CTA starts: the previous kernel releases its dependents only after
+  // its own wait); the mask, the partial rhs and the scalars come from the
+  // kernels just before, so the wait sits here.
+  pdl_wait();
+  // a finished solve's launch is a no-op; its flag is tested once the staging
+  // loads are in flight, so that they do not wait for the scalar block
+  const bool active = bind.use || sc[S_ACTIVE] != 0.0;
+  const T alpha = T(AXIS == 0 ? sc[S_ALPHA_X] : sc[S_ALPHA_Y]);
   const int weno_all = S.scheme == 1;
   const int nm = AXIS == 0 ? R * (n + 2) : ((n + 2) << rsh);
 #pragma unroll 4
@@ -1228,7 +1235,7 @@ __global__ void __launch_bounds__(kStencilThreads)
   __shared__ T Ls[4][LY][LX];
   const Work wk = work[blockIdx.x];
   const SolveDev& S = solves[wk.solve];
-  pdl_wait();  // below: the state, mask and scalars of the previous kernels
+  // the hyperviscosity flag is written by the step's first kernel
   if (!bind.use && S.scal[S_HV_STEP] == 0.0) return;
   const double* q = bind.use ? bind.qin : S.q1;
   double* out = bind.use ? bind.qout : S.q;
@@ -1242,8 +1249,11 @@ __global__ void __launch_bounds__(kStencilThreads)
     const int gj = fold_node(y0 - 2 + a, ny, per), gi = fold_node(x0 - 2 + b, nx, per);
     const size_t o = (size_t)gj * nx + gi;
 #pragma unroll
-    for (int c = 0; c < 4; ++c) Qs[c][a][b] = T(q[c * plane + o]);
+    for (int c = 0; c < 4; ++c) Qs[c][a][b] = T(__ldcg(q + c * plane + o));
   }
+  // the input state was written two or more kernels earlier (complete when
+  // this CTA starts); the mask comes from the sensor just before
+  pdl_wait();
   __syncthreads();
   const T dx2 = T(S.dx * S.dx), dy2 = T(S.dy * S.dy);
   const T idx2 = T(1.0 / (S.dx * S.dx)), idy2 = T(1.0 / (S.dy * S.dy));
