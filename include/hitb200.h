@@ -332,6 +332,10 @@ hitb200_plan* hitb200_batch_plan(hitb200_batch* batch, int32_t i);
 /* Bind the state array of every solve (device pointers, kept until rebound). */
 int hitb200_batch_bind(hitb200_batch* batch, double* const* q);
 int hitb200_batch_step(hitb200_batch* batch, void* stream);
+/* nsteps steps replayed from a graph captured at the first call on a stream:
+ * the members in two halves (balanced by cells) on two branches of the graph,
+ * so that one half's kernels fill the other's tails.  Results are the same
+ * as hitb200_batch_step's. */
 int hitb200_batch_run(hitb200_batch* batch, int32_t nsteps, void* stream);
 /* ---- kernel variants (autotuner knobs; no counterpart in the reference) -------- */
 /* Each knob picks the variant of one kernel family: 0 = latency variant
