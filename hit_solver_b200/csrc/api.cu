@@ -52,6 +52,57 @@ int invalid(const std::string& msg) {
   return HITB200_ERR_INVALID;
 }
 
+// Streams and fork / join events of one graph capture, released on every
+// exit path.
+struct CaptureRes {
+  cudaStream_t st[2] = {nullptr, nullptr};
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  ~CaptureRes() {
+    for (cudaStream_t s : st)
+      if (s) cudaStreamDestroy(s);
+    for (cudaEvent_t e : ev)
+      if (e) cudaEventDestroy(e);
+  }
+};
+
+// Captures `launch(streams)` into an executable graph on private streams:
+// one, or two forked from the first and joined back (`branches` = 2), so
+// that the graph holds two independent chains of kernels.  Every stream and
+// event is created before the capture begins and released after it ends.
+template <class F>
+int capture_graph(int branches, F&& launch, cudaGraphExec_t* out) {
+  *out = nullptr;
+  CaptureRes c;
+  for (int i = 0; i < branches; ++i) HB_CUDA(cudaStreamCreateWithFlags(&c.st[i], cudaStreamNonBlocking));
+  if (branches > 1)
+    for (cudaEvent_t& e : c.ev) HB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  HB_CUDA(cudaStreamBeginCapture(c.st[0], cudaStreamCaptureModeThreadLocal));
+  cudaError_t e = cudaSuccess;
+  if (branches > 1) {
+    e = cudaEventRecord(c.ev[0], c.st[0]);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(c.st[1], c.ev[0], 0);
+  }
+  const int r = e == cudaSuccess ? launch(c.st) : HITB200_OK;
+  if (e == cudaSuccess && branches > 1) {
+    e = cudaEventRecord(c.ev[1], c.st[1]);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(c.st[0], c.ev[1], 0);
+  }
+  cudaGraph_t gr = nullptr;
+  const cudaError_t ee = cudaStreamEndCapture(c.st[0], &gr);
+  if (e != cudaSuccess || r != HITB200_OK || ee != cudaSuccess) {
+    if (gr) cudaGraphDestroy(gr);
+    if (r != HITB200_OK) return r;
+    return cuda_fail(e != cudaSuccess ? e : ee, "graph capture");
+  }
+  e = cudaGraphInstantiate(out, gr, 0);
+  cudaGraphDestroy(gr);
+  if (e != cudaSuccess) {
+    *out = nullptr;
+    return cuda_fail(e, "cudaGraphInstantiate");
+  }
+  return HITB200_OK;
+}
+
 bool is_none(double v) { return std::isnan(v); }
 
 // numpy.fft.fftfreq integer bins of an n-point transform.
@@ -1187,22 +1238,14 @@ int hitb200_run(hitb200_plan* p, double* q, int32_t nsteps, void* stream) {
   if (!p->graph || p->graph_stream != st) {
     if (p->graph) cudaGraphExecDestroy(p->graph);
     p->graph = nullptr;
-    cudaStream_t cap;
-    HB_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
-    LaunchSet L = plan_launch_set(p, cap);
+    LaunchSet L = plan_launch_set(p, nullptr);
     L.pdl = 1;  // one solve's launches are single waves: the next kernel's CTAs
                 // stage their inputs while the previous kernel finishes
-    // make every kernel's shared-memory attribute final before capture
-    HB_CUDA(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
-    r = launch_step_sequence(L, p->desc.forcing_on, 0, !p->desc.periodic, p->hs.hv_interval > 0);
-    cudaGraph_t gr;
-    cudaError_t e = cudaStreamEndCapture(cap, &gr);
-    cudaStreamDestroy(cap);
+    r = capture_graph(1, [&](cudaStream_t* cs) {
+      L.st = cs[0];
+      return launch_step_sequence(L, p->desc.forcing_on, 0, !p->desc.periodic, p->hs.hv_interval > 0);
+    }, &p->graph);
     if (r != HITB200_OK) return r;
-    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
-    e = cudaGraphInstantiate(&p->graph, gr, 0);
-    cudaGraphDestroy(gr);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaGraphInstantiate");
     p->graph_stream = st;
   }
   for (int i = 0; i < nsteps; ++i) HB_CUDA(cudaGraphLaunch(p->graph, st));
@@ -1592,65 +1635,35 @@ int hitb200_batch_run(hitb200_batch* b, int32_t nsteps, void* stream) {
   if (!b->graph || b->graph_stream != st) {
     if (b->graph) cudaGraphExecDestroy(b->graph);
     b->graph = nullptr;
-    cudaStream_t cap;
-    HB_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
-    HB_CUDA(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
-    int r = HITB200_OK;
-    // The members in K = 2 groups (contiguous, balanced by cells), one branch
+    // The members in two groups (contiguous, balanced by cells), one branch
     // of the graph each, so that one group's kernels fill the other's tails:
     // 8 x 512^2 HIT step 1.300 -> 1.173 ms, 64-solve ensemble 5.31 -> 5.21 ms
     // (3, 4 and 8 groups measured no better).  Results do not depend on it:
     // every kernel works on one member at a time.
     const int n = (int)b->plans.size();
-    const int K = std::min(n, 2);
-    std::vector<cudaStream_t> side;
-    std::vector<cudaEvent_t> evs;
-    if (K > 1) {
-      double tot = 0.0;
+    int cut = n;
+    if (n > 1) {
+      double tot = 0.0, acc = 0.0;
       for (hitb200_plan* p : b->plans) tot += (double)p->desc.nx * p->desc.ny;
-      std::vector<int> cut(1, 0);
-      double acc = 0.0;
-      for (int i = 0; i < n && (int)cut.size() < K; ++i) {
-        acc += (double)b->plans[i]->desc.nx * b->plans[i]->desc.ny;
-        if (acc >= tot * (double)cut.size() / K && i + 1 < n) cut.push_back(i + 1);
+      for (cut = 1; cut < n - 1; ++cut) {
+        acc += (double)b->plans[cut - 1]->desc.nx * b->plans[cut - 1]->desc.ny;
+        if (acc >= 0.5 * tot) break;
       }
-      cut.push_back(n);
-      cudaEvent_t fork;
-      HB_CUDA(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
-      evs.push_back(fork);
-      cudaEventRecord(fork, cap);
-      for (size_t g = 0; g + 1 < cut.size(); ++g) {
-        cudaStream_t sg = cap;
-        if (g > 0) {
-          HB_CUDA(cudaStreamCreateWithFlags(&sg, cudaStreamNonBlocking));
-          side.push_back(sg);
-          cudaStreamWaitEvent(sg, fork, 0);
-        }
-        LaunchSet Lg = batch_sub_set(b, sg, cut[g], cut[g + 1]);
-        const int rg = launch_step_sequence(Lg, b->any_forcing, 0, b->any_outflow, b->any_hv);
-        if (r == HITB200_OK) r = rg;
-      }
-      for (cudaStream_t sg : side) {
-        cudaEvent_t join;
-        HB_CUDA(cudaEventCreateWithFlags(&join, cudaEventDisableTiming));
-        evs.push_back(join);
-        cudaEventRecord(join, sg);
-        cudaStreamWaitEvent(cap, join, 0);
-      }
-    } else {
-      LaunchSet L = batch_launch_set(b, cap);
-      r = launch_step_sequence(L, b->any_forcing, 0, b->any_outflow, b->any_hv);
     }
-    cudaGraph_t gr;
-    cudaError_t e = cudaStreamEndCapture(cap, &gr);
-    cudaStreamDestroy(cap);
-    for (cudaStream_t sg : side) cudaStreamDestroy(sg);
-    for (cudaEvent_t ev : evs) cudaEventDestroy(ev);
+    const int r = capture_graph(n > 1 ? 2 : 1, [&](cudaStream_t* cs) {
+      if (n == 1) {
+        LaunchSet L = batch_launch_set(b, cs[0]);
+        return launch_step_sequence(L, b->any_forcing, 0, b->any_outflow, b->any_hv);
+      }
+      int rr = HITB200_OK;
+      for (int g = 0; g < 2; ++g) {
+        LaunchSet Lg = g == 0 ? batch_sub_set(b, cs[0], 0, cut) : batch_sub_set(b, cs[1], cut, n);
+        const int rg = launch_step_sequence(Lg, b->any_forcing, 0, b->any_outflow, b->any_hv);
+        if (rr == HITB200_OK) rr = rg;
+      }
+      return rr;
+    }, &b->graph);
     if (r != HITB200_OK) return r;
-    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
-    e = cudaGraphInstantiate(&b->graph, gr, 0);
-    cudaGraphDestroy(gr);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaGraphInstantiate");
     b->graph_stream = st;
   }
   for (int i = 0; i < nsteps; ++i) HB_CUDA(cudaGraphLaunch(b->graph, st));
