@@ -94,6 +94,8 @@ SIGNATURES = [
     ("hitb200_plan_create", ctypes.c_int, [ctypes.POINTER(Desc), ctypes.POINTER(_VP)]),
     ("hitb200_plan_destroy", ctypes.c_int, [_VP]),
     ("hitb200_plan_device_bytes", ctypes.c_size_t, [ctypes.POINTER(Desc)]),
+    ("hitb200_release_cached_blocks", ctypes.c_int, []),
+    ("hitb200_cached_block_bytes", ctypes.c_size_t, []),
     ("hitb200_enforce", ctypes.c_int, [_VP, _DP, _DP, _VP]),
     ("hitb200_enforce_state", ctypes.c_int,
      [_DP, _DP, ctypes.c_int64, ctypes.c_double, _VP]),

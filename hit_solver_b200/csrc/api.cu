@@ -11,6 +11,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -104,6 +105,97 @@ int capture_graph(int branches, F&& launch, cudaGraphExec_t* out) {
 }
 
 bool is_none(double v) { return std::isnan(v); }
+
+// ---- device block cache -----------------------------------------------------------
+// Plan arenas and batch tables are device blocks in 2 MiB granules.  A
+// destroyed plan or batch returns its block here instead of to cudaFree:
+// on the B200 a cudaFree of a plan arena or of a batch table took 10 ms to
+// 0.7 s even on an idle device, and a cudaMalloc 10-40 ms, which stalled a
+// serving loop that retires and admits solves every few rounds.  A request
+// takes the smallest cached block of its device that fits, if that wastes
+// at most half of it.  The cache holds at most kBlockCacheMax bytes;
+// hitb200_release_cached_blocks() frees them, and an allocation that fails
+// frees this device's blocks and retries.
+struct DevBlock {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+  int dev = 0;
+};
+constexpr size_t kBlockGranule = size_t(2) << 20;
+constexpr size_t kBlockCacheMax = size_t(8) << 30;
+std::mutex g_blocks_mu;
+std::multimap<std::pair<int, size_t>, void*> g_blocks;  // (device, bytes) -> block
+size_t g_blocks_bytes = 0;
+
+// Frees the cached blocks of device `dev` (every device for dev < 0); the
+// caller holds g_blocks_mu.
+void release_blocks_locked(int dev) {
+  if (g_blocks.empty()) return;
+  int cur = 0, set = -1;
+  cudaGetDevice(&cur);
+  for (auto it = g_blocks.begin(); it != g_blocks.end();) {
+    if (dev >= 0 && it->first.first != dev) {
+      ++it;
+      continue;
+    }
+    if (it->first.first != (set < 0 ? cur : set)) {
+      set = it->first.first;
+      cudaSetDevice(set);
+    }
+    cudaFree(it->second);
+    g_blocks_bytes -= it->first.second;
+    it = g_blocks.erase(it);
+  }
+  if (set >= 0 && set != cur) cudaSetDevice(cur);
+}
+
+cudaError_t block_alloc(size_t bytes, DevBlock* out) {
+  const size_t want = (bytes + kBlockGranule - 1) / kBlockGranule * kBlockGranule;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  {
+    std::lock_guard<std::mutex> lk(g_blocks_mu);
+    auto it = g_blocks.lower_bound({dev, want});
+    if (it != g_blocks.end() && it->first.first == dev && it->first.second <= 2 * want) {
+      *out = {it->second, it->first.second, dev};
+      g_blocks_bytes -= it->first.second;
+      g_blocks.erase(it);
+      return cudaSuccess;
+    }
+  }
+  void* ptr = nullptr;
+  e = cudaMalloc(&ptr, want);
+  if (e == cudaErrorMemoryAllocation) {
+    cudaGetLastError();
+    {
+      std::lock_guard<std::mutex> lk(g_blocks_mu);
+      release_blocks_locked(dev);
+    }
+    e = cudaMalloc(&ptr, want);
+  }
+  if (e != cudaSuccess) return e;
+  *out = {ptr, want, dev};
+  return cudaSuccess;
+}
+
+// Returns a block to the cache (or to cudaFree when the cache is full).  No
+// queued work may use it any more: the caller synchronised its device.
+void block_free(DevBlock& b) {
+  if (!b.ptr) return;
+  std::lock_guard<std::mutex> lk(g_blocks_mu);
+  if (g_blocks_bytes + b.bytes <= kBlockCacheMax) {
+    g_blocks.insert({{b.dev, b.bytes}, b.ptr});
+    g_blocks_bytes += b.bytes;
+  } else {
+    int cur = 0;
+    cudaGetDevice(&cur);
+    if (b.dev != cur) cudaSetDevice(b.dev);
+    cudaFree(b.ptr);
+    if (b.dev != cur) cudaSetDevice(cur);
+  }
+  b = DevBlock{};
+}
 
 // numpy.fft.fftfreq integer bins of an n-point transform.
 int fft_bin(int j, int n) {
@@ -205,6 +297,7 @@ struct hitb200_plan {
   SolveDev* d_solve = nullptr;
   unsigned char* arena = nullptr;
   size_t arena_bytes = 0;
+  DevBlock arena_block;     // the arena's cached device block
   Work* d_tiles = nullptr;
   Work* d_tiles32 = nullptr;
   Work* d_xlines = nullptr;
@@ -228,7 +321,8 @@ struct hitb200_batch {
   std::vector<hitb200_plan*> plans;
   bool owns_plans = true;  // false for hitb200_batch_from_plans
   int tuning[HITB200_TUNE_COUNT] = {0, 0, 0, 0};
-  SolveDev* d_solves = nullptr;
+  SolveDev* d_solves = nullptr;  // start of the tables' device block
+  DevBlock tables;
   Work *d_tiles = nullptr, *d_tiles32 = nullptr, *d_xlines = nullptr, *d_ylines = nullptr;
   Work* d_srows = nullptr;
   int* d_partner = nullptr;
@@ -695,6 +789,17 @@ int hitb200_desc_init(hitb200_desc* d) {
   return HITB200_OK;
 }
 
+int hitb200_release_cached_blocks(void) {
+  std::lock_guard<std::mutex> lk(g_blocks_mu);
+  release_blocks_locked(-1);
+  return HITB200_OK;
+}
+
+size_t hitb200_cached_block_bytes(void) {
+  std::lock_guard<std::mutex> lk(g_blocks_mu);
+  return g_blocks_bytes;
+}
+
 size_t hitb200_plan_device_bytes(const hitb200_desc* d) {
   if (validate_desc(d) != HITB200_OK) return 0;
   const size_t N = (size_t)d->nx * d->ny;
@@ -800,11 +905,12 @@ int hitb200_plan_create(const hitb200_desc* d, hitb200_plan** out) {
   const size_t o_yl = a.take(p->n_y * sizeof(Work));
   const size_t o_sr = a.take(p->n_srows * sizeof(Work));
   p->arena_bytes = a.off;
-  cudaError_t e = cudaMalloc(&p->arena, a.off);
+  cudaError_t e = block_alloc(a.off, &p->arena_block);
   if (e != cudaSuccess) {
     delete p;
     return cuda_fail(e, "cudaMalloc(plan arena)");
   }
+  p->arena = static_cast<unsigned char*>(p->arena_block.ptr);
   unsigned char* base = p->arena;
   SolveDev& s = p->hs;
   std::memset(&s, 0, sizeof(s));
@@ -946,7 +1052,7 @@ int hitb200_plan_create(const hitb200_desc* d, hitb200_plan** out) {
   do {                                                                           \
     e = cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice);                     \
     if (e != cudaSuccess) {                                                      \
-      cudaFree(p->arena);                                                        \
+      block_free(p->arena_block);                                                \
       delete p;                                                                  \
       return cuda_fail(e, "cudaMemcpy(plan tables)");                            \
     }                                                                            \
@@ -965,7 +1071,7 @@ int hitb200_plan_create(const hitb200_desc* d, hitb200_plan** out) {
 #undef HB_PUT
   e = cudaMemset(s.counters, 0, 8 * sizeof(unsigned) + sizeof(int));
   if (e != cudaSuccess) {
-    cudaFree(p->arena);
+    block_free(p->arena_block);
     delete p;
     return cuda_fail(e, "cudaMemset(counters)");
   }
@@ -1002,7 +1108,15 @@ int hitb200_plan_create(const hitb200_desc* d, hitb200_plan** out) {
 int hitb200_plan_destroy(hitb200_plan* p) {
   if (!p) return HITB200_OK;
   if (p->graph) cudaGraphExecDestroy(p->graph);
-  if (p->arena) cudaFree(p->arena);
+  if (p->arena_block.ptr) {
+    // queued launches of this plan may still use the arena
+    int cur = 0;
+    cudaGetDevice(&cur);
+    if (cur != p->arena_block.dev) cudaSetDevice(p->arena_block.dev);
+    cudaDeviceSynchronize();
+    if (cur != p->arena_block.dev) cudaSetDevice(cur);
+    block_free(p->arena_block);
+  }
   delete p;
   return HITB200_OK;
 }
@@ -1395,9 +1509,9 @@ static int batch_build(hitb200_batch* b) {
   size_t bytes = hs.size() * sizeof(SolveDev) +
                  (tiles.size() + tiles32.size() + xl.size() + yl.size() + sr.size()) * sizeof(Work) +
                  partner.size() * sizeof(int) + 1024 + 7 * 256;
-  unsigned char* buf = nullptr;
-  cudaError_t e = cudaMalloc(&buf, bytes);
+  cudaError_t e = block_alloc(bytes, &b->tables);
   if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(batch tables)");
+  unsigned char* buf = static_cast<unsigned char*>(b->tables.ptr);
   size_t off = 0;
   cudaError_t ce = cudaSuccess;
   auto put = [&](const void* src, size_t nbytes) -> unsigned char* {
@@ -1474,11 +1588,11 @@ int hitb200_batch_destroy(hitb200_batch* b) {
   if (!b) return HITB200_OK;
   int status = HITB200_OK;
   if (b->graph) cudaGraphExecDestroy(b->graph);
-  if (b->d_solves) {
+  if (b->tables.ptr) {
     // the tables may still be read by queued launches of this batch
     const cudaError_t e = cudaDeviceSynchronize();
     if (e != cudaSuccess) status = cuda_fail(e, "cudaDeviceSynchronize(batch destroy)");
-    cudaFree(b->d_solves);
+    block_free(b->tables);
   }
   for (hitb200_plan* p : b->plans) {
     if (b->owns_plans) {

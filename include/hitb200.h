@@ -13,7 +13,9 @@
  *     (HITB200_OK = 0).  Only calls documented as "synchronises" wait for the
  *     device.
  *   - The caller owns every array it passes.  A plan owns its scratch, which
- *     it allocates in hitb200_plan_create and frees in hitb200_plan_destroy.
+ *     it allocates in hitb200_plan_create and releases in
+ *     hitb200_plan_destroy (to the library's block cache; see
+ *     hitb200_release_cached_blocks).
  *   - Plans are not thread-safe; distinct plans may be used concurrently.
  *
  * Each entry point names the reference interface it replaces (file:line
@@ -136,9 +138,18 @@ int hitb200_desc_init(hitb200_desc* desc);
 /* Replaces constructing the sensor/operator/hyperviscosity/forcing objects
  * (OOP/hit2d.py:773-803, OOP/problems/riemann_config3.py:689-707). */
 int hitb200_plan_create(const hitb200_desc* desc, hitb200_plan** plan);
+/* Synchronises the plan's device, then returns its arena to the block cache. */
 int hitb200_plan_destroy(hitb200_plan* plan);
 /* Device bytes a plan of this descriptor allocates (admission control). */
 size_t hitb200_plan_device_bytes(const hitb200_desc* desc);
+/* Block cache: destroyed plans' arenas and batches' tables stay allocated
+ * (at most 8 GiB, 2 MiB granules) and serve later plans and batches of the
+ * same device, since a cudaFree / cudaMalloc pair per retired and admitted
+ * solve stalls a serving loop.  An allocation that fails first frees its
+ * device's cached blocks.  hitb200_release_cached_blocks frees them all
+ * (every device); hitb200_cached_block_bytes is the total held. */
+int hitb200_release_cached_blocks(void);
+size_t hitb200_cached_block_bytes(void);
 const char* hitb200_status_string(int status);
 /* Library build identifier, for logs. */
 const char* hitb200_version(void);
