@@ -1373,8 +1373,8 @@ __global__ void __launch_bounds__(kStencilThreads)
     for (int c = 0; c < 4; ++c) Qs[c][a][b] = T(__ldcg(q + c * plane + o));
   }
   // the input state was written two or more kernels earlier (complete when
-  // this CTA starts); the mask comes from the sensor just before
-  pdl_wait();
+  // this CTA starts); the mask comes from the sensor just before and is
+  // read only by the final update, so the first Laplacian precedes the wait
   __syncthreads();
   const T dx2 = T(S.dx * S.dx), dy2 = T(S.dy * S.dy);
   const T idx2 = T(1.0 / (S.dx * S.dx)), idy2 = T(1.0 / (S.dy * S.dy));
@@ -1402,6 +1402,7 @@ __global__ void __launch_bounds__(kStencilThreads)
     }
   }
   __syncthreads();
+  pdl_wait();  // below: the sensor's mask
   pdl_release();
   // solve fields in registers: the stores below cannot force reloads
   const double gam = S.gamma;
