@@ -179,6 +179,18 @@ cudaError_t block_alloc(size_t bytes, DevBlock* out) {
   return cudaSuccess;
 }
 
+// Waits for every queued launch of the block's device (whichever device is
+// current).
+cudaError_t sync_block_device(const DevBlock& b) {
+  int cur = 0;
+  cudaError_t e = cudaGetDevice(&cur);
+  if (e != cudaSuccess) return e;
+  if (cur != b.dev) cudaSetDevice(b.dev);
+  e = cudaDeviceSynchronize();
+  if (cur != b.dev) cudaSetDevice(cur);
+  return e;
+}
+
 // Returns a block to the cache (or to cudaFree when the cache is full).  No
 // queued work may use it any more: the caller synchronised its device.
 void block_free(DevBlock& b) {
@@ -1110,11 +1122,7 @@ int hitb200_plan_destroy(hitb200_plan* p) {
   if (p->graph) cudaGraphExecDestroy(p->graph);
   if (p->arena_block.ptr) {
     // queued launches of this plan may still use the arena
-    int cur = 0;
-    cudaGetDevice(&cur);
-    if (cur != p->arena_block.dev) cudaSetDevice(p->arena_block.dev);
-    cudaDeviceSynchronize();
-    if (cur != p->arena_block.dev) cudaSetDevice(cur);
+    sync_block_device(p->arena_block);
     block_free(p->arena_block);
   }
   delete p;
@@ -1590,7 +1598,7 @@ int hitb200_batch_destroy(hitb200_batch* b) {
   if (b->graph) cudaGraphExecDestroy(b->graph);
   if (b->tables.ptr) {
     // the tables may still be read by queued launches of this batch
-    const cudaError_t e = cudaDeviceSynchronize();
+    const cudaError_t e = sync_block_device(b->tables);
     if (e != cudaSuccess) status = cuda_fail(e, "cudaDeviceSynchronize(batch destroy)");
     block_free(b->tables);
   }
