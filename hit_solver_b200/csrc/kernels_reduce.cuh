@@ -211,8 +211,10 @@ __device__ int prepass_tile(const SolveDev& S, const Work& w, int buf, int mode,
     tw[a][k] = S.twy[mode_index(k, gj, ny)];
   }
 
-  double ax = 0, ay = 0, div2 = 0, vort2 = 0, mr = 0, mp = 0, me = 0, ps = 0, sr = 0, vel2 = 0,
-         cs = 0;
+  double div2 = 0, vort2 = 0, ps = 0, sr = 0, vel2 = 0, cs = 0;
+  // maxima in the bulk type: exact, so widening once at the end gives the
+  // same doubles as widening every value
+  T axT = T(0), ayT = T(0), mrT = T(0), mpT = T(0), meT = T(0);
   int bad = 0;  // validation flags: 1 non-finite, 2 rho <= 0, 4 p <= 0
   const int gi = x0 + lane;
   // one-node ring for the central differences (corners are not used), loaded
@@ -259,11 +261,11 @@ __device__ int prepass_tile(const SolveDev& S, const Work& w, int buf, int mode,
       su[a + 1][lane + 1] = e.u;
       sv[a + 1][lane + 1] = e.v;
       const T c = sqrt(gT * e.p * e.rinv);
-      ax = fmax(ax, double(fabs(e.u) + c));
-      ay = fmax(ay, double(fabs(e.v) + c));
-      mr = fmax(mr, double(e.rho));
-      mp = fmax(mp, double(e.p));
-      me = fmax(me, double(e.p * e.rinv * igm1));
+      axT = fmax(axT, fabs(e.u) + c);
+      ayT = fmax(ayT, fabs(e.v) + c);
+      mrT = fmax(mrT, e.rho);
+      mpT = fmax(mpT, e.p);
+      meT = fmax(meT, e.p * e.rinv * igm1);
     }
     // cooling's mean pressure: the FP32-bulk form takes it from its enforced
     // pressure (equal to the floored raw pressure up to rounding)
@@ -338,6 +340,7 @@ __device__ int prepass_tile(const SolveDev& S, const Work& w, int buf, int mode,
     __syncthreads();  // tw table
     if (!active) return -1;
   }
+  const double ax = double(axT), ay = double(ayT), mr = double(mrT), mp = double(mpT), me = double(meT);
   if (act) {
   warp_to_smem4<OP_MAX>(ax, ay, mr, mp, sm, make_int4(R_AX, R_AY, R_RHO, R_P), nslots);
   warp_to_smem4<OP_MAX>(me, sr, 0.0, 0.0, sm, make_int4(R_E, R_SR, -1, -1), nslots);
