@@ -2078,7 +2078,10 @@ unsigned char* g_dt_scratch_addr[kMaxScratchDevices] = {};
 // Device address of g_dt_scratch on the current device.  In host code the
 // name g_dt_scratch is only a host-side stand-in, so the address is looked up
 // once per device with that device current (the first call on a device may
-// also load the module there) and then passed to the kernel.
+// also load the module there) and then passed to the kernel.  The address
+// belongs to the device's context: after cudaDeviceReset the module is loaded
+// again elsewhere, so a process that resets a device must not call the entry
+// point on it again (the cached address would be stale).
 int dt_scratch_address(unsigned char** out) {
   int dev = 0;
   HB_CUDA(cudaGetDevice(&dev));
@@ -2108,6 +2111,9 @@ __global__ void __launch_bounds__(kRedThreads)
   const int tx = threadIdx.x & 31, ty0 = threadIdx.x >> 5;
   const size_t plane = (size_t)nx * ny;
   const double idx_ = 1.0 / dx, idy_ = 1.0 / dy;
+  // NaN-propagating maximum, as the reference's np.max: a non-finite cell
+  // makes dt NaN instead of being skipped by fmax
+  auto nan_max = [](double m, double x) { return (x != x || x > m) ? x : m; };
   double sr = 0.0;
   for (int a = ty0; a < kTileY; a += kRedWarps) {
     const int gj = y0 + a, gi = x0 + tx;
@@ -2121,22 +2127,24 @@ __global__ void __launch_bounds__(kRedThreads)
     const double p_raw = (g - 1.0) * (q3 - kin);
     const double pr = p_raw > kPFloor ? p_raw : kPFloor;
     const double cr = sqrt(g * pr * rinv);
-    sr = fmax(sr, (fabs(ur) + cr) * idx_ + (fabs(vr) + cr) * idy_);
+    sr = nan_max(sr, (fabs(ur) + cr) * idx_ + (fabs(vr) + cr) * idy_);
   }
   __shared__ double sm[kRedWarps];
-  sr = warp_max(sr);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) sr = nan_max(sr, __shfl_xor_sync(0xffffffffu, sr, o));
   if (tx == 0) sm[ty0] = sr;
   __syncthreads();
   if (threadIdx.x == 0) {
     double m = sm[0];
-    for (int w = 1; w < kRedWarps; ++w) m = fmax(m, sm[w]);
+    for (int w = 1; w < kRedWarps; ++w) m = nan_max(m, sm[w]);
     part[blockIdx.x] = m;
   }
   if (!last_block(ticket, gridDim.x)) return;
   if (threadIdx.x >= 32) return;
   double m = 0.0;
-  for (int b = tx; b < (int)gridDim.x; b += 32) m = fmax(m, __ldcg(part + b));
-  m = warp_max(m);
+  for (int b = tx; b < (int)gridDim.x; b += 32) m = nan_max(m, __ldcg(part + b));
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = nan_max(m, __shfl_xor_sync(0xffffffffu, m, o));
   if (tx == 0) {
     double dt = cfl / m;
     if (!isnan(remaining)) dt = fmin(dt, remaining);
@@ -2155,7 +2163,7 @@ extern "C" int hitb200_stable_time_step_noalloc(const double* q, int32_t nx, int
   if (!(dx > 0.0) || !(dy > 0.0)) return invalid("dx and dy must be positive");
   if (!(gamma > 1.0)) return invalid("gamma must exceed 1");
   if (!(cfl > 0.0)) return invalid("cfl must be positive");
-  const long long tiles = (long long)((nx + kTileX - 1) / kTileX) * ((ny + kTileY - 1) / kTileY);
+  const long long tiles = (((long long)nx + kTileX - 1) / kTileX) * (((long long)ny + kTileY - 1) / kTileY);
   if (tiles > kDtScratchTiles) {
     g_last_error = "grid of " + std::to_string(nx) + " x " + std::to_string(ny) + " cells needs " +
                    std::to_string(tiles) + " tiles of 32 x 32 cells; the static scratch of "

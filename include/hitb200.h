@@ -208,8 +208,11 @@ int hitb200_validate(hitb200_plan* plan, const double* q);
  * ticket counter must be zero when a call starts; it is zero at module load
  * and each call leaves it zero.  The first call on a device looks up the
  * scratch address (and may load the module): make it before any stream
- * capture.  All calls on a device share the scratch, so calls that may
- * overlap on the GPU (other streams or threads) race. */
+ * capture.  That address is kept for the life of the process, so after a
+ * cudaDeviceReset the entry point must not be called on that device again.
+ * All calls on a device share the scratch, so calls that may overlap on the
+ * GPU (other streams or threads) race.  A NaN in any cell makes dt NaN, as
+ * the reference's np.max does. */
 int hitb200_stable_time_step_noalloc(const double* q, int32_t nx, int32_t ny, double dx,
                                      double dy, double gamma, double cfl,
                                      double remaining_time, double* dt_out, void* stream);

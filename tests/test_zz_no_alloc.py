@@ -53,6 +53,10 @@ def test_noalloc_rejects_before_any_device_work():
     assert lib.hitb200_stable_time_step_noalloc(None, 8, 8, 1.0, 1.0, G, 0.4, nan, addr, None) == _lib.ERR_INVALID
     assert lib.hitb200_stable_time_step_noalloc(addr, 0, 8, 1.0, 1.0, G, 0.4, nan, addr, None) == _lib.ERR_INVALID
     assert lib.hitb200_stable_time_step_noalloc(addr, 8, 8, 1.0, 1.0, G, -1.0, nan, addr, None) == _lib.ERR_INVALID
+    # tile counts formed in 64 bits: near INT32_MAX cells per line is rejected, not overflowed
+    big = 2**31 - 1
+    assert lib.hitb200_stable_time_step_noalloc(addr, big, big, 1.0, 1.0, G, 0.4, nan, addr, None) == _lib.ERR_UNSUPPORTED
+    assert lib.hitb200_stable_time_step_noalloc(addr, big, 1, 1.0, 1.0, G, 0.4, nan, addr, None) == _lib.ERR_UNSUPPORTED
 
 
 @pytest.mark.gpu
@@ -88,3 +92,47 @@ def test_noalloc_largest_grid_twice():
     out = torch.empty(1, dtype=torch.float64, device="cuda")
     assert _close(_noalloc(q, dom, 0.4, None, out), ref)
     assert _close(_noalloc(q, dom, 0.4, None, out), ref)
+
+
+def _random_state(nx, ny, seed):
+    gen = torch.Generator(device="cuda").manual_seed(seed)
+    shape = (ny, nx)
+    rho = 1.0 + 0.5 * torch.rand(shape, generator=gen, device="cuda", dtype=torch.float64)
+    u = torch.randn(shape, generator=gen, device="cuda", dtype=torch.float64)
+    v = torch.randn(shape, generator=gen, device="cuda", dtype=torch.float64)
+    p = 0.5 + torch.rand(shape, generator=gen, device="cuda", dtype=torch.float64)
+    return torch.stack([rho, rho * u, rho * v, p / (G - 1.0) + 0.5 * rho * (u * u + v * v)]).contiguous()
+
+
+@pytest.mark.gpu
+def test_noalloc_queued_calls_without_sync():
+    # Calls queued back to back on one stream, each with its own state and
+    # output slot and no host synchronisation between them: the ticket counter
+    # each call leaves at zero serves the next one.  The 33 x 1000 grid has a
+    # ragged last tile in both directions (2 x 32 tiles).
+    lib = _lib.load()
+    dom = Domain2D(0.0, 1.0, 0.0, 2.0, 33, 1000)
+    states = [_random_state(33, 1000, seed) for seed in (1, 2, 3)]
+    out = torch.full((len(states),), -1.0, dtype=torch.float64, device="cuda")
+    for k, q in enumerate(states):
+        _lib.check(lib.hitb200_stable_time_step_noalloc(
+            q.data_ptr(), dom.nx, dom.ny, dom.dx, dom.dy, G, 0.4, math.nan,
+            out.data_ptr() + 8 * k, core.stream_handle()))
+    torch.cuda.synchronize()
+    plan = _plan(dom, False)
+    for k, q in enumerate(states):
+        ref = plan.stable_time_step(q, 0.4, None)
+        assert _close(float(out[k]), ref), (k, float(out[k]), ref)
+
+
+@pytest.mark.gpu
+def test_noalloc_nan_cell_gives_nan():
+    # np.max propagates NaN, so the reference's time step of a state with a
+    # NaN cell is NaN; the maximum here carries it the same way.
+    dom = Domain2D(0.0, 1.0, 0.0, 1.0, 96, 80)
+    q = _random_state(96, 80, 5)
+    q[1, 41, 17] = float("nan")
+    out = torch.empty(1, dtype=torch.float64, device="cuda")
+    assert math.isnan(_noalloc(q, dom, 0.4, None, out))
+    q[1, 41, 17] = 0.0
+    assert math.isfinite(_noalloc(q, dom, 0.4, None, out))
