@@ -2,7 +2,7 @@
 
 Run once, in a container where the reference source tree is available:
 
-    python tests/golden/make_golden.py /root/reference
+    python tests/golden/make_golden.py <reference-root>
 
 It imports the reference package ``OOP`` (with a placeholder ``matplotlib``
 from ``_stubs/``, since plotting is never exercised), evaluates the reference's
@@ -253,4 +253,6 @@ def main(root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        raise SystemExit("usage: python tests/golden/make_golden.py <reference-root>")
+    main(sys.argv[1])

@@ -385,3 +385,34 @@ def test_large_grid_steps_match_oracle(nx, ny):
     want, _, _, _ = O.riemann_run(prm, max_steps=2)
     assert rel_err(out["fp64"], want) < 1e-8
     assert rel_err(out["fp32-bulk"], out["fp64"]) < 1e-5
+
+
+_DIAG_FROM_STATE = ("kinetic_energy", "Kx", "Ky", "A_K", "C_uv", "rms_velocity", "turbulent_mach",
+                    "mean_density", "mean_pressure", "divergence_rms", "vorticity_rms", "mass",
+                    "mass_error")
+
+
+@pytest.mark.parametrize("name", ["periodic_hit_32x24", "periodic_blob_40x36"])
+def test_golden_periodic_diagnostics(name):
+    """compute_diagnostics (OOP/hit2d.py:471-548) of the fixture state: the
+    native moment reduction plus the spectral divergence and vorticity,
+    against the values the reference computed for the same state.  Values
+    that are roundoff in the reference (A_K, C_uv and the divergence of the
+    solenoidal initial state, about 1e-16) are compared on the scale of the
+    quantity they are a difference of."""
+    from pathlib import Path
+
+    from hit_solver_b200.equations import EulerEquation2D
+    from hit_solver_b200.hit2d import compute_diagnostics
+
+    d = np.load(Path(__file__).parent / "golden" / f"{name}.npz")
+    q = d["q"]
+    ny, nx = q.shape[1:]
+    dom = Domain2D(0.0, 2 * np.pi, 0.0, 2 * np.pi, nx, ny)
+    got = compute_diagnostics(dev(q), EulerEquation2D(gamma=G), dom)
+    scale = {"A_K": 1.0, "C_uv": 1.0, "divergence_rms": float(d["diag_vorticity_rms"]),
+             "mass_error": 1.0}
+    for key in _DIAG_FROM_STATE:
+        want = float(d[f"diag_{key}"])
+        ref = max(abs(want), scale.get(key, 0.0))
+        assert abs(got[key] - want) <= 1e-12 * ref, (key, got[key], want)
