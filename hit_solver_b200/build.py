@@ -20,7 +20,7 @@ CSRC = PKG / "csrc"
 LIB = PKG / "libhitb200.so"
 SOURCES = ["api.cu"]
 HEADERS = ["common.cuh", "reduce.cuh", "weno.cuh", "kernels_reduce.cuh", "kernels_stencil.cuh",
-           "kernels_spectra.cuh", "kernels_init.cuh"]
+           "kernels_spectra.cuh", "kernels_init.cuh", "sensor_step.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -22,6 +22,7 @@
 #include "kernels_reduce.cuh"
 #include "kernels_spectra.cuh"
 #include "kernels_stencil.cuh"
+#include "sensor_step.cuh"
 
 using namespace hitb200;
 
@@ -327,6 +328,8 @@ struct hitb200_plan {
   SolveDev* own_solve = nullptr;  // the arena's descriptor (d_solve points into a batch table while batched)
   int tuning[HITB200_TUNE_COUNT] = {0, 0, 0, 0};  // kernel variants (tuning knobs)
   bool fuse_ok = false;  // all of the fused sensor's CTAs fit on the GPU at once
+  int sensor_w = -1;          // width of the step sensor instantiation (-1: generic sensor)
+  size_t smem_sensor_step = 0;
 };
 
 struct hitb200_batch {
@@ -345,6 +348,8 @@ struct hitb200_batch {
   std::vector<int> off_tiles, off_tiles32, off_xl, off_yl, off_srows;
   int rx_max = 1, ry_max = 1;
   size_t smem_x = 0, smem_y = 0, smem_sensor = 0;
+  int sensor_w = -1;  // shared width of the members' step sensor (-1: generic sensor)
+  size_t smem_sensor_step = 0;
   int any_outflow = 0, any_forcing = 0, any_hv = 0, any_noise_upload = 0;
   cudaGraphExec_t graph = nullptr;
   cudaStream_t graph_stream = nullptr;
@@ -363,6 +368,8 @@ struct LaunchSet {
   int occ_x, occ_y, occ_pre;  // kernel variants: 0 latency, 1 throughput (tuning knobs)
   int fused;                  // prepass fused into the sensor (single solves, tuning knob)
   size_t smem_x, smem_y, smem_sensor;
+  int sensor_w;             // step sensor instantiation shared by the solves (-1: generic)
+  size_t smem_sensor_step;
   cudaStream_t st;
   // cells of all solves, and of the solves carrying viscous / forcing terms
   double cells = 0, cells_visc = 0, cells_force = 0;
@@ -458,6 +465,23 @@ void set_sensor_attr(size_t bytes) {
   }
 }
 
+// Widths with a step-sensor instantiation (sensor_step_kernel); others use
+// the generic sensor_kernel.
+inline int step_sensor_width(int w) { return (w == 3 || w == 4) ? w : -1; }
+inline size_t step_sensor_bytes(int w, int elem, bool visc) {
+  return w == 3 ? step_sensor_smem_bytes<3>(elem, visc) : w == 4 ? step_sensor_smem_bytes<4>(elem, visc) : 0;
+}
+template <typename T, int W>
+void set_step_sensor_attr(size_t bytes) {
+  static size_t done[kMaxAttrDevices] = {};
+  const int dev = attr_device();
+  std::lock_guard<std::mutex> lock(g_attr_mu);
+  if (bytes > done[dev]) {
+    cudaFuncSetAttribute(sensor_step_kernel<T, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    done[dev] = bytes;
+  }
+}
+
 template <typename T, int AXIS>
 void launch_sweep_t(const LaunchSet& L, int stage, int mode, const Bind& b) {
   const int mch = AXIS == 0 ? L.mch_x : L.mch_y;
@@ -497,6 +521,12 @@ void launch_sensor_t(const LaunchSet& L, int sel, int enf, int visc, const Bind&
   if (b.use)
     launch_k(sensor_kernel<T, true, false>, L.n_tiles32, kSensorThreads, L.smem_sensor, L, L.solves,
              L.tiles32, sel, enf, visc, b, mo);
+  else if (L.sensor_w == 4)
+    launch_k(sensor_step_kernel<T, 4>, L.n_tiles32, kSensorThreads, L.smem_sensor_step, L, L.solves,
+             L.tiles32, sel, enf, visc);
+  else if (L.sensor_w == 3)
+    launch_k(sensor_step_kernel<T, 3>, L.n_tiles32, kSensorThreads, L.smem_sensor_step, L, L.solves,
+             L.tiles32, sel, enf, visc);
   else
     launch_k(sensor_kernel<T, false, false>, L.n_tiles32, kSensorThreads, L.smem_sensor, L, L.solves,
              L.tiles32, sel, enf, visc, b, mo);
@@ -661,6 +691,8 @@ LaunchSet plan_launch_set(hitb200_plan* p, cudaStream_t st) {
   L.smem_x = p->smem_x;
   L.smem_y = p->smem_y;
   L.smem_sensor = p->smem_sensor;
+  L.sensor_w = p->sensor_w;
+  L.smem_sensor_step = p->smem_sensor_step;
   L.st = st;
   L.cells = (double)p->desc.nx * p->desc.ny;
   // programmatic dependent launch only in the step sequence (set by its
@@ -674,7 +706,7 @@ LaunchSet plan_launch_set(hitb200_plan* p, cudaStream_t st) {
 // Shared-memory opt-in of every kernel a launch set may use; called at plan /
 // batch creation so that no attribute call happens during graph capture.
 void prime_attributes(int elem, int mch_x, int mch_y, size_t smem_x, size_t smem_y,
-                      size_t smem_sensor) {
+                      size_t smem_sensor, int sensor_w, size_t smem_sensor_step) {
   auto sweep = [&](auto tag, int axis, int mch, size_t bytes) {
     using T = decltype(tag);
 #define HB_ATTR(M)                                                    \
@@ -694,10 +726,14 @@ void prime_attributes(int elem, int mch_x, int mch_y, size_t smem_x, size_t smem
     sweep(float{}, 0, mch_x, smem_x);
     sweep(float{}, 1, mch_y, smem_y);
     set_sensor_attr<float>(smem_sensor);
+    if (sensor_w == 4) set_step_sensor_attr<float, 4>(smem_sensor_step);
+    if (sensor_w == 3) set_step_sensor_attr<float, 3>(smem_sensor_step);
   } else {
     sweep(double{}, 0, mch_x, smem_x);
     sweep(double{}, 1, mch_y, smem_y);
     set_sensor_attr<double>(smem_sensor);
+    if (sensor_w == 4) set_step_sensor_attr<double, 4>(smem_sensor_step);
+    if (sensor_w == 3) set_step_sensor_attr<double, 3>(smem_sensor_step);
   }
 }
 
@@ -880,6 +916,8 @@ int hitb200_plan_create(const hitb200_desc* d, hitb200_plan** out) {
   p->smem_x = p->elem == 4 ? SweepLayout<float>(nx, p->Rx).bytes() : SweepLayout<double>(nx, p->Rx).bytes();
   p->smem_y = p->elem == 4 ? SweepLayout<float>(ny, p->Ry).bytes() : SweepLayout<double>(ny, p->Ry).bytes();
   p->smem_sensor = sensor_smem_bytes(d->sensor_width, p->elem, d->viscosity > 0.0);
+  p->sensor_w = step_sensor_width(d->sensor_width);
+  p->smem_sensor_step = step_sensor_bytes(p->sensor_w, p->elem, d->viscosity > 0.0);
   if (p->smem_x > kSweepSmemMax || p->smem_y > kSweepSmemMax) {
     delete p;
     return (g_last_error = "grid lines too long for the sweep's shared memory", HITB200_ERR_UNSUPPORTED);
@@ -1087,7 +1125,8 @@ int hitb200_plan_create(const hitb200_desc* d, hitb200_plan** out) {
     delete p;
     return cuda_fail(e, "cudaMemset(counters)");
   }
-  prime_attributes(p->elem, mch_for(nx), mch_for(ny), p->smem_x, p->smem_y, p->smem_sensor);
+  prime_attributes(p->elem, mch_for(nx), mch_for(ny), p->smem_x, p->smem_y, p->smem_sensor, p->sensor_w,
+                   p->smem_sensor_step);
   {
     // the fused sensor needs every tile's CTA resident at once (grid barrier)
     int dev = 0, sms = 0, per_sm = 0;
@@ -1501,6 +1540,8 @@ static int batch_build(hitb200_batch* b) {
                                                          : SweepLayout<double>(p->desc.ny, 4).bytes())
                                          : p->smem_y);
     b->smem_sensor = std::max(b->smem_sensor, p->smem_sensor);
+    b->sensor_w = i == 0 ? p->sensor_w : (b->sensor_w == p->sensor_w ? b->sensor_w : -1);
+    b->smem_sensor_step = std::max(b->smem_sensor_step, p->smem_sensor_step);
     b->any_outflow |= !p->desc.periodic;
     b->any_forcing |= p->desc.forcing_on;
     b->any_hv |= p->hs.hv_interval > 0;
@@ -1536,7 +1577,9 @@ static int batch_build(hitb200_batch* b) {
   b->d_srows = reinterpret_cast<Work*>(put(sr.data(), sr.size() * sizeof(Work)));
   b->d_partner = reinterpret_cast<int*>(put(partner.data(), partner.size() * sizeof(int)));
   if (ce != cudaSuccess) return cuda_fail(ce, "cudaMemcpy(batch tables)");
-  prime_attributes(b->elem, b->mch_x, b->mch_y, b->smem_x, b->smem_y, b->smem_sensor);
+  if (b->sensor_w < 0) b->smem_sensor_step = 0;
+  prime_attributes(b->elem, b->mch_x, b->mch_y, b->smem_x, b->smem_y, b->smem_sensor, b->sensor_w,
+                   b->smem_sensor_step);
   // member plans use the batch's copy of their descriptor while batched
   for (int i = 0; i < n; ++i) {
     b->plans[i]->d_solve = b->d_solves + i;
@@ -1702,6 +1745,8 @@ static LaunchSet batch_launch_set(hitb200_batch* b, cudaStream_t st) {
   L.smem_x = b->smem_x;
   L.smem_y = b->smem_y;
   L.smem_sensor = b->smem_sensor;
+  L.sensor_w = b->sensor_w;
+  L.smem_sensor_step = b->smem_sensor_step;
   L.st = st;
   for (hitb200_plan* p : b->plans) {
     const double n = (double)p->desc.nx * p->desc.ny;

@@ -499,7 +499,13 @@ __global__ void __launch_bounds__(kSensorThreads, sizeof(T) == 8 ? 1 : HITB200_S
   T* QX = TXY + kVisX * kVisY;
   T* QY = QX + kVisX * kVisY;
   __syncthreads();  // E (internal energy) is free: the mask is complete
-  for (int idx = threadIdx.x; idx < SX * SY; idx += blockDim.x) E[idx] = P[idx] / (RHO[idx] * rgas);
+  // temperature p / (rho R): FP64 divides as the reference; FP32 forms
+  // (p * (1 / rho)) / R with the staging's reciprocal, as the step sensor does
+  const T irg = T(1.0 / S.gas_r);
+  for (int idx = threadIdx.x; idx < SX * SY; idx += blockDim.x) {
+    if constexpr (sizeof(T) == 8) E[idx] = P[idx] / (RHO[idx] * rgas);
+    else E[idx] = (P[idx] * __frcp_rn(RHO[idx])) * irg;
+  }
   __syncthreads();
   const float ivx = 1.0f / (float)kVisX;
   for (int idx = threadIdx.x; idx < kVisX * kVisY; idx += blockDim.x) {
