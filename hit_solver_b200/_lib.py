@@ -147,6 +147,10 @@ SIGNATURES = [
      [_VP, ctypes.c_double, ctypes.c_int64, ctypes.c_double, ctypes.c_int64]),
     ("hitb200_read_scalars", ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_double), ctypes.c_int32]),
     ("hitb200_copy_scalars_async", ctypes.c_int, [_VP, _DP, ctypes.c_int32, _VP]),
+    ("hitb200_state_block_size", ctypes.c_size_t, []),
+    ("hitb200_save_state_block", ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_double), ctypes.c_size_t]),
+    ("hitb200_load_state_block", ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_double), ctypes.c_size_t]),
+    ("hitb200_set_barrier_test", ctypes.c_int, [ctypes.c_int32, ctypes.c_double]),
     ("hitb200_diagnostics", ctypes.c_int,
      [_VP, _DP, ctypes.POINTER(ctypes.c_double), ctypes.c_int32]),
     ("hitb200_batch_create", ctypes.c_int,

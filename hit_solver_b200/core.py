@@ -167,6 +167,26 @@ class Plan:
         _lib.check(self.lib.hitb200_read_scalars(self.handle, buf, n))
         return list(buf)
 
+    def save_state_block(self):
+        """The whole device scalar block (time, step, controller and forcing
+        state, OU potential): with the state q, a checkpoint of the solve."""
+        import numpy as np
+
+        n = int(self.lib.hitb200_state_block_size())
+        buf = (ctypes.c_double * n)()
+        _lib.check(self.lib.hitb200_save_state_block(self.handle, buf, n))
+        return np.array(buf, dtype=np.float64)
+
+    def load_state_block(self, block) -> None:
+        import numpy as np
+
+        block = np.ascontiguousarray(block, dtype=np.float64)
+        n = int(self.lib.hitb200_state_block_size())
+        if block.shape != (n,):
+            raise ValueError(f"state block must hold {n} doubles")
+        _lib.check(self.lib.hitb200_load_state_block(
+            self.handle, block.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), n))
+
     @property
     def tuning(self) -> list[int]:
         """Kernel variant knobs (see hit_solver_b200.autotune)."""

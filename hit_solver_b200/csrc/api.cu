@@ -1440,6 +1440,35 @@ int hitb200_copy_scalars_async(hitb200_plan* p, double* dst, int32_t n, void* st
   return HITB200_OK;
 }
 
+size_t hitb200_state_block_size(void) { return (size_t)SCAL_SIZE; }
+
+int hitb200_save_state_block(hitb200_plan* p, double* out, size_t n) {
+  if (!p || !out) return invalid("NULL argument");
+  if (n != (size_t)SCAL_SIZE) return invalid("the state block holds hitb200_state_block_size() doubles");
+  HB_CUDA(cudaDeviceSynchronize());
+  HB_CUDA(cudaMemcpy(out, p->hs.scal, n * sizeof(double), cudaMemcpyDeviceToHost));
+  return HITB200_OK;
+}
+
+int hitb200_load_state_block(hitb200_plan* p, const double* in, size_t n) {
+  if (!p || !in) return invalid("NULL argument");
+  if (n != (size_t)SCAL_SIZE) return invalid("the state block holds hitb200_state_block_size() doubles");
+  HB_CUDA(cudaDeviceSynchronize());
+  HB_CUDA(cudaMemcpy(p->hs.scal, in, n * sizeof(double), cudaMemcpyHostToDevice));
+  return HITB200_OK;
+}
+
+int hitb200_set_barrier_test(int32_t extra_arrivals, double limit_seconds) {
+  if (extra_arrivals < 0 || extra_arrivals > 1) return invalid("extra_arrivals must be 0 or 1");
+  if (!(limit_seconds > 0.0) || limit_seconds > 10.0) return invalid("limit_seconds must be in (0, 10]");
+  const unsigned extra = (unsigned)extra_arrivals;
+  const unsigned long long ns = (unsigned long long)(limit_seconds * 1e9);
+  HB_CUDA(cudaDeviceSynchronize());
+  HB_CUDA(cudaMemcpyToSymbol(g_barrier_extra, &extra, sizeof(extra)));
+  HB_CUDA(cudaMemcpyToSymbol(g_barrier_limit_ns, &ns, sizeof(ns)));
+  return HITB200_OK;
+}
+
 int hitb200_diagnostics(hitb200_plan* p, const double* q, double* out, int32_t n) {
   if (!p || !q || !out) return invalid("NULL argument");
   LaunchSet L = plan_launch_set(p, 0);

@@ -335,11 +335,16 @@ __global__ void __launch_bounds__(kSensorThreads, sizeof(T) == 8 ? 1 : HITB200_S
     grid_barrier(&S.counters[4], &S.counters[5], gridDim.x, &S.counters[6]);
     __shared__ double fred[R_FIXED + 4 * kMaxDrag];
     prepass_finalize(S, pre_slots, fred);
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-      prepass_scalars(S, fred, S.scal, pre_mode, false);
-      if (*(volatile unsigned*)&S.counters[6]) {
-        S.scal[S_STATUS] = (double)((int)S.scal[S_STATUS] | ST_BARRIER);
-        S.counters[6] = 0u;
+    // The last CTA past the barrier writes the scalar block (every CTA holds
+    // the same reductions) and reports a wait that ran out: by then every
+    // CTA that gave up has set the flag.
+    if (threadIdx.x == 0) {
+      __threadfence();
+      if (atomicAdd(&S.counters[7], 1u) == gridDim.x - 1u) {
+        S.counters[7] = 0u;
+        prepass_scalars(S, fred, S.scal, pre_mode, false);
+        if (atomicExch(&S.counters[6], 0u))
+          S.scal[S_STATUS] = (double)((int)S.scal[S_STATUS] | ST_BARRIER);
       }
     }
     const double N = (double)nx * (double)ny;

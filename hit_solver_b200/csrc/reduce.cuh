@@ -86,27 +86,44 @@ __device__ __forceinline__ bool last_block(unsigned* counter, int nblk) {
   return is_last;
 }
 
+// Test hook of the grid barrier (set by hitb200_set_barrier_test): the number
+// of arrivals the barrier waits for beyond its launch's CTAs (0 in normal use;
+// 1 makes every wait run out) and the wait limit in nanoseconds.
+__device__ unsigned g_barrier_extra = 0u;
+__device__ unsigned long long g_barrier_limit_ns = 2000000000ull;
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
 // Barrier over every CTA of a cooperative launch (which guarantees that all
 // of them are resident).  count and gen are zero-initialised words of the
 // solve's counters; the last CTA to arrive resets count and advances gen.
-// A CTA that waits longer than ~2 s of polling gives up: it sets *err and
-// continues, so that a failed launch cannot hang the GPU.
+// A CTA that waits longer than the limit (about 2 s of the global timer, or
+// 2^26 polls) gives up: it withdraws its arrival, sets *err and continues, so
+// that a failed launch cannot hang the GPU.
 __device__ __forceinline__ void grid_barrier(unsigned* count, unsigned* gen, unsigned nblocks,
                                              unsigned* err) {
   __syncthreads();
   if (threadIdx.x == 0) {
     volatile unsigned* vgen = gen;
+    const unsigned target = nblocks - 1u + *(volatile unsigned*)&g_barrier_extra;
+    const unsigned long long limit = *(volatile unsigned long long*)&g_barrier_limit_ns;
     const unsigned g0 = *vgen;
     __threadfence();
-    if (atomicAdd(count, 1u) == nblocks - 1u) {
+    if (atomicAdd(count, 1u) == target) {
       atomicExch(count, 0u);
       __threadfence();
       atomicAdd(gen, 1u);
     } else {
+      const unsigned long long t0 = global_ns();
       unsigned long long it = 0;
       while (*vgen == g0) {
         __nanosleep(100);
-        if (++it > (1ull << 24)) {
+        if (++it > (1ull << 26) || ((it & 31) == 0 && global_ns() - t0 > limit)) {
+          atomicSub(count, 1u);
           atomicOr(err, 1u);
           break;
         }

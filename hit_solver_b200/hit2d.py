@@ -549,6 +549,26 @@ class HITSolver:
     def scalars(self) -> list[float]:
         return self.plan.scalars()
 
+    def checkpoint(self) -> dict:
+        """Everything the solve carries from one step to the next: the state,
+        the plan's scalar block (time, step, Mach-control and forcing state,
+        OU potential) and, with the reference's noise stream, that stream's
+        position.  ``restore`` on a solver of the same configuration resumes
+        the run bit for bit."""
+        torch.cuda.synchronize()
+        ck = {"q": self.q.detach().cpu().clone(), "block": self.plan.save_state_block()}
+        if self.config.forcing_noise == "numpy":
+            ck["noise_rng"] = self.noise_rng.bit_generator.state
+        return ck
+
+    def restore(self, ck: dict) -> None:
+        if tuple(ck["q"].shape) != tuple(self.q.shape):
+            raise ValueError("checkpoint state does not match the solver's grid")
+        self.q.copy_(ck["q"])
+        self.plan.load_state_block(ck["block"])
+        if "noise_rng" in ck:
+            self.noise_rng.bit_generator.state = ck["noise_rng"]
+
 
 def run_simulation(config: HIT2DConfig):
     """Driver of OOP/hit2d.py:764-918 on the B200 backend.  Returns (q, t, steps)."""

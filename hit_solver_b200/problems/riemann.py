@@ -328,6 +328,18 @@ class RiemannSolver:
     def advance(self, nsteps: int) -> None:
         self.plan.run(self.q, nsteps)
 
+    def checkpoint(self) -> dict:
+        """The state and the plan's scalar block (time, step, dt,
+        hyperviscosity count): ``restore`` resumes the run bit for bit."""
+        torch.cuda.synchronize()
+        return {"q": self.q.detach().cpu().clone(), "block": self.plan.save_state_block()}
+
+    def restore(self, ck: dict) -> None:
+        if tuple(ck["q"].shape) != tuple(self.q.shape):
+            raise ValueError("checkpoint state does not match the solver's grid")
+        self.q.copy_(ck["q"])
+        self.plan.load_state_block(ck["block"])
+
 
 def print_diagnostic_summary(d: RiemannDiagnostics) -> None:
     print("Diagnostic summary:")

@@ -48,6 +48,10 @@ class Request:
     split    Riemann quadrant intersection x0 = y0
     seed     HIT initial-condition and forcing seed
     mach     HIT turbulent Mach number (initial and Mach-control target)
+    initial_state
+             optional conservative state [4, n, n] (host or device) that
+             replaces the generated initial condition at admission: a
+             restart, or a caller's own initial field
     """
 
     rid: int
@@ -58,6 +62,7 @@ class Request:
     seed: int = 0
     mach: float = 0.25
     steps: int = 200
+    initial_state: torch.Tensor | None = field(default=None, repr=False)
 
 
 @dataclass
@@ -72,6 +77,10 @@ class Result:
     time: float
     status: int
     state: torch.Tensor | None = field(default=None, repr=False)
+    # set when the solve was evicted: the exception type the reference's loops
+    # raise for its state (FloatingPointError / RuntimeError) and the message
+    error: str | None = None
+    error_type: str | None = None
 
     @property
     def latency(self) -> float:
@@ -106,8 +115,32 @@ def make_solver(req: Request, precision: str):
     if req.n <= 0:
         raise ValueError("grid size must be positive")
     if req.kind == "hit":
-        return HITSolver(hit_request_config(req.n, req.seed, req.mach, req.steps, precision))
-    return RiemannSolver(riemann_request_config(req.kind, req.n, req.split, precision))
+        solver = HITSolver(hit_request_config(req.n, req.seed, req.mach, req.steps, precision))
+    else:
+        solver = RiemannSolver(riemann_request_config(req.kind, req.n, req.split, precision))
+    if req.initial_state is not None:
+        if tuple(req.initial_state.shape) != tuple(solver.q.shape):
+            raise ValueError(f"request {req.rid}: initial_state must have shape {tuple(solver.q.shape)}")
+        solver.q.copy_(req.initial_state)
+    return solver
+
+
+def member_error(kind: str, bits: int) -> tuple[str, str] | None:
+    """The exception a solve's status bits call for, as the reference's loops
+    raise it: FloatingPointError for a non-finite state (OOP/hit2d.py:716-717)
+    and, for Riemann solves, a non-positive raw density or pressure
+    (OOP/problems/riemann_config3.py:442-452); RuntimeError for a fused grid
+    barrier that timed out.  None while the solve is sound."""
+    bits = int(bits)
+    if bits & _lib.ST_BARRIER:
+        return "RuntimeError", "a grid barrier of the fused prepass/sensor timed out"
+    if bits & _lib.ST_NONFINITE:
+        return "FloatingPointError", "NaN or infinite value detected in the state"
+    if kind != "hit" and bits & _lib.ST_NONPOS_RHO:
+        return "FloatingPointError", "state contains non-positive density"
+    if kind != "hit" and bits & _lib.ST_NONPOS_P:
+        return "FloatingPointError", "state contains non-positive pressure"
+    return None
 
 
 def footprint(req: Request, precision: str) -> int:
@@ -209,8 +242,11 @@ class SolveServer:
             for i, m in enumerate(active):
                 s = scal[i]
                 # S_ACTIVE turns 0 at the first step past the end; a member
-                # whose step count reached max_steps is done already
-                done = s[_lib.S_ACTIVE] == 0.0 or (
+                # whose step count reached max_steps is done already; a member
+                # whose state went bad is evicted (its companions are unaffected:
+                # every kernel works on one solve's data)
+                err = member_error(m.req.kind, s[_lib.S_STATUS])
+                done = err is not None or s[_lib.S_ACTIVE] == 0.0 or (
                     s[_lib.S_MAX_STEPS] >= 0.0 and s[_lib.S_STEP] >= s[_lib.S_MAX_STEPS])
                 if not done:
                     keep.append(m)
@@ -220,7 +256,9 @@ class SolveServer:
                 results.append(Result(m.req.rid, m.req.kind, m.req.n, m.req.arrival, m.admitted,
                                       done_at, steps, float(s[_lib.S_TIME]),
                                       int(s[_lib.S_STATUS]),
-                                      m.solver.q if self.keep_states else None))
+                                      m.solver.q if self.keep_states else None,
+                                      error=None if err is None else err[1],
+                                      error_type=None if err is None else err[0]))
                 used -= m.bytes
             if len(keep) != len(active):
                 batch.close()  # hands the plans back before finished ones are freed
@@ -236,6 +274,7 @@ class SolveServer:
             "cell_updates_per_s": cell_steps / makespan if makespan > 0 else 0.0,
             "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
             "steps_per_round": self.steps_per_round, "hbm_budget": self.hbm_budget,
+            "failed": sum(1 for r in results if r.error is not None),
         }
         return results
 
@@ -277,4 +316,5 @@ def run_alone(req: Request, precision: str = "fp32-bulk") -> torch.Tensor:
 
 
 __all__ = ["Request", "Result", "SolveServer", "footprint", "hit_request_config",
-           "make_solver", "poisson_requests", "riemann_request_config", "run_alone"]
+           "make_solver", "member_error", "poisson_requests", "riemann_request_config",
+           "run_alone"]

@@ -255,6 +255,25 @@ int hitb200_read_scalars(hitb200_plan* plan, double* out, int32_t n);
 /* Copy the device scalar slots asynchronously into caller memory
  * (host-pinned or device), n doubles. */
 int hitb200_copy_scalars_async(hitb200_plan* plan, double* dst, int32_t n, void* stream);
+/* The plan's whole device scalar block: the slots above plus the sensor
+ * limits, the drag and forcing coefficients and the OU potential of every
+ * forced mode.  A solve's state q and this block are all it carries from one
+ * step to the next (the device forcing noise is keyed by seed and step), so
+ * saving both and loading them into a plan of the same descriptor resumes the
+ * solve bit for bit: the serving loop's checkpoint and restore.  No
+ * reference counterpart (its loops keep these values in Python objects).
+ * n must equal hitb200_state_block_size(); both calls synchronise. */
+size_t hitb200_state_block_size(void);
+int hitb200_save_state_block(hitb200_plan* plan, double* out, size_t n);
+int hitb200_load_state_block(hitb200_plan* plan, const double* in, size_t n);
+/* Failure injection for the fused prepass/sensor's grid barrier, a test hook
+ * with no reference counterpart: the barrier waits for extra_arrivals (0 or
+ * 1) CTAs beyond its launch and gives up after limit_seconds of the global
+ * timer (default 2 s), each CTA withdrawing its arrival; the step then sets
+ * HITB200_ST_BARRIER (its results are invalid) and the GPU stays usable.
+ * extra_arrivals = 1 makes every fused step's wait run out; 0 restores
+ * normal use.  Applies to the current device; synchronises. */
+int hitb200_set_barrier_test(int32_t extra_arrivals, double limit_seconds);
 /* Scalar diagnostics of compute_diagnostics (OOP/hit2d.py:471-548), without
  * the spectral divergence/vorticity, plus conservation sums and extrema:
  * out[0..16] = kinetic_energy, Kx, Ky, A_K, C_uv, rms_velocity,

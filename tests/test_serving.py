@@ -66,3 +66,64 @@ def test_mixed_stream_matches_solo_runs():
             assert res.steps == req.steps
         solo = serving.run_alone(req, "fp32-bulk")
         assert torch.equal(res.state, solo), f"request {res.rid} differs from its solo run"
+
+
+def test_member_error_mapping():
+    from hit_solver_b200 import _lib
+
+    assert serving.member_error("hit", 0) is None
+    assert serving.member_error("riemann3", 0) is None
+    assert serving.member_error("hit", _lib.ST_NONFINITE)[0] == "FloatingPointError"
+    assert serving.member_error("hit", _lib.ST_BARRIER)[0] == "RuntimeError"
+    # the reference validates positivity only in its Riemann loop
+    assert serving.member_error("hit", _lib.ST_NONPOS_RHO) is None
+    assert serving.member_error("riemann6", _lib.ST_NONPOS_P)[0] == "FloatingPointError"
+
+
+@pytest.mark.gpu
+def test_nan_request_is_evicted_and_others_unaffected():
+    """A request whose initial state holds a NaN (injected on the host) is
+    evicted at the end of its first round with the reference's
+    FloatingPointError, while its batch companions run to their end and
+    equal their solo runs bit for bit (OOP/hit2d.py:716-717;
+    OOP/problems/riemann_config3.py:442-452)."""
+    good = serving.make_solver(serving.Request(9, "riemann3", 48, split=0.55), "fp32-bulk")
+    bad_state = good.q.clone()
+    bad_state[2, 20, 31] = float("nan")
+    reqs = [
+        serving.Request(0, "hit", 48, 0.0, seed=3, mach=0.25, steps=30),
+        serving.Request(1, "riemann3", 48, 0.0, split=0.55, initial_state=bad_state),
+        serving.Request(2, "riemann6", 40, 0.0, split=0.45),
+    ]
+    server = serving.SolveServer("fp32-bulk", steps_per_round=8, keep_states=True)
+    results = {r.rid: r for r in server.serve(reqs)}
+    assert set(results) == {0, 1, 2}
+    bad = results[1]
+    assert bad.error_type == "FloatingPointError" and "NaN" in bad.error
+    assert bad.steps <= 8  # evicted at the first round boundary
+    assert server.stats["failed"] == 1
+    for rid in (0, 2):
+        res = results[rid]
+        assert res.error is None and res.status == 0
+        assert torch.equal(res.state, serving.run_alone(reqs[rid], "fp32-bulk"))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kind", ["hit", "riemann3"])
+def test_checkpoint_restore_resumes_bit_for_bit(kind):
+    """q plus the plan's scalar block (time, step, controller and forcing
+    state, OU potential; the device noise is keyed by seed and step) resume a
+    solve exactly: 7 + 9 steps through a checkpoint equal 16 straight steps."""
+    req = serving.Request(0, kind, 64, split=0.6, seed=8, mach=0.3, steps=10 ** 6)
+    straight = serving.make_solver(req, "fp32-bulk")
+    straight.advance(16)
+    first = serving.make_solver(req, "fp32-bulk")
+    first.advance(7)
+    ck = first.checkpoint()
+    del first
+    resumed = serving.make_solver(req, "fp32-bulk")
+    resumed.restore(ck)
+    resumed.advance(9)
+    torch.cuda.synchronize()
+    assert torch.equal(resumed.q, straight.q)
+    assert resumed.plan.scalars() == straight.plan.scalars()
