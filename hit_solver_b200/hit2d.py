@@ -570,8 +570,22 @@ class HITSolver:
             self.noise_rng.bit_generator.state = ck["noise_rng"]
 
 
+def as_config(config) -> HIT2DConfig:
+    """The mirror's HIT2DConfig for a configuration object of the reference
+    (``OOP.hit2d.HIT2DConfig`` with ``backend="b200"``, handed over by the
+    reference's run_simulation): its fields copied, the mirror's own fields at
+    their defaults."""
+    if isinstance(config, HIT2DConfig):
+        return config
+    from dataclasses import fields
+
+    names = {f.name for f in fields(HIT2DConfig)}
+    return HIT2DConfig(**{k: getattr(config, k) for k in names if hasattr(config, k)})
+
+
 def run_simulation(config: HIT2DConfig):
     """Driver of OOP/hit2d.py:764-918 on the B200 backend.  Returns (q, t, steps)."""
+    config = as_config(config)
     select_array_module(config.backend)
     print("Using array backend: b200")
     if config.hyperviscosity_interval <= 0 and config.hyperviscosity_mn > 0.0:

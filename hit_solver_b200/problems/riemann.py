@@ -355,8 +355,23 @@ def print_diagnostic_summary(d: RiemannDiagnostics) -> None:
     print(f"  hyperviscosity       : {d.hyperviscosity_enabled} ({d.hyperviscosity_applications} applications)")
 
 
+def as_config(config) -> RiemannConfig3:
+    """The mirror's configuration for a configuration object of the reference
+    (its RiemannConfig3 / RiemannConfig3Offset08 / RiemannConfig6 with
+    ``backend="b200"``): the class of the same name, its fields copied."""
+    if isinstance(config, RiemannConfig3):
+        return config
+    from dataclasses import fields
+
+    cls = {"RiemannConfig3Offset08": RiemannConfig3Offset08,
+           "RiemannConfig6": RiemannConfig6}.get(type(config).__name__, RiemannConfig3)
+    names = {f.name for f in fields(cls)}
+    return cls(**{k: getattr(config, k) for k in names if hasattr(config, k)})
+
+
 def run_riemann(config: RiemannConfig3):
     """Driver of riemann_config3.py:681-749 on the B200 backend; returns (q, diagnostics)."""
+    config = as_config(config)
     print("Using array backend: b200")
     solver = RiemannSolver(config)
     label = getattr(config, "configuration_label", f"Config {config.configuration_number}")

@@ -242,6 +242,54 @@ def gen_spectra(R):
         np.savez_compressed(HERE / f"spectra_{tag}.npz", **out)
 
 
+def _collect(tmp: Path) -> dict:
+    """Every file a run wrote, flattened into arrays: '<file>::<key>' for each
+    .npz member (dtype and shape kept) and '<file>' for each .json (its text)."""
+    out = {}
+    for path in sorted(tmp.rglob("*")):
+        if path.is_dir():
+            continue
+        rel = path.relative_to(tmp).as_posix()
+        if path.suffix == ".npz":
+            with np.load(path, allow_pickle=False) as d:
+                for k in d.files:
+                    out[f"{rel}::{k}"] = d[k]
+        elif path.suffix == ".json":
+            out[rel] = np.asarray(path.read_text())
+    return out
+
+
+def gen_formats(R):
+    """Output files of the reference's own writers: run_simulation's
+    config.json, diagnostic_history.npz and snapshots (OOP/hit2d.py:551-694,
+    764-918) for a short 24^2 HIT run, and run_riemann plus save_run_outputs
+    (OOP/problems/riemann_config3.py:486-519, 681-809; no figure) for a
+    24^2 configuration-3 run."""
+    hit2d, rc3 = R["hit2d"], R["rc3"]
+    with tempfile.TemporaryDirectory() as t:
+        tmp = Path(t)
+        cfg = hit2d.HIT2DConfig(nx=24, ny=24, tfinal=0.006, cfl=0.05, target_mach=0.25,
+                                initial_kmin=3, initial_kmax=5, forcing_kmin=3.0,
+                                forcing_kmax=5.0, forcing_correlation_time=0.5,
+                                mach_control=True, mach_control_target=0.25, viscosity=7.5e-4,
+                                large_scale_drag=0.1, cooling_time=5.0, hyperviscosity_mn=0.002,
+                                diagnostics_every=2, snapshot_every=3, output_dir=tmp / "hit",
+                                backend="numpy")
+        with contextlib.redirect_stdout(io.StringIO()):
+            hit2d.run_simulation(cfg)
+        out = _collect(tmp / "hit")
+    np.savez_compressed(HERE / "formats_hit_24.npz", **out)
+    with tempfile.TemporaryDirectory() as t:
+        tmp = Path(t)
+        cfg = rc3.RiemannConfig3(nx=24, ny=24, tfinal=0.02, backend="numpy", shear_threshold=None,
+                                 progress_every=10**6)
+        with contextlib.redirect_stdout(io.StringIO()):
+            q, diag = rc3.run_riemann(cfg)
+            rc3.save_run_outputs(q, cfg, diag, tmp, run_id="fixture", plot=False)
+        out = _collect(tmp)
+    np.savez_compressed(HERE / "formats_riemann_24.npz", **out)
+
+
 def main(root: str) -> None:
     R = _import_reference(root)
     for name, (cfg, domain, eq, q) in periodic_cases(R).items():
@@ -249,6 +297,7 @@ def main(root: str) -> None:
     gen_hit_run(R)
     gen_riemann(R)
     gen_spectra(R)
+    gen_formats(R)
     print("golden vectors written to", HERE)
 
 
