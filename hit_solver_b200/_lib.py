@@ -151,6 +151,16 @@ SIGNATURES = [
     ("hitb200_save_state_block", ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_double), ctypes.c_size_t]),
     ("hitb200_load_state_block", ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_double), ctypes.c_size_t]),
     ("hitb200_set_barrier_test", ctypes.c_int, [ctypes.c_int32, ctypes.c_double]),
+    ("hitb200_spectral_workspace_bytes", ctypes.c_size_t, [ctypes.c_int32, ctypes.c_int32]),
+    ("hitb200_spectral_diagnostics", ctypes.c_int,
+     [_VP, _DP, ctypes.c_double, ctypes.POINTER(ctypes.c_double), _DP, _DP, _DP, ctypes.c_size_t, _VP]),
+    ("hitb200_hit_velocity_workspace_bytes", ctypes.c_size_t, [ctypes.c_int32, ctypes.c_int32]),
+    ("hitb200_hit_velocity", ctypes.c_int,
+     [_DP, ctypes.c_int32, ctypes.c_int32, ctypes.c_double, ctypes.c_double, _DP, _DP, _DP,
+      ctypes.c_size_t, _VP]),
+    ("hitb200_rfft2_workspace_bytes", ctypes.c_size_t, [ctypes.c_int32, ctypes.c_int32]),
+    ("hitb200_rfft2", ctypes.c_int,
+     [_DP, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _DP, _DP, ctypes.c_size_t, _VP]),
     ("hitb200_diagnostics", ctypes.c_int,
      [_VP, _DP, ctypes.POINTER(ctypes.c_double), ctypes.c_int32]),
     ("hitb200_batch_create", ctypes.c_int,

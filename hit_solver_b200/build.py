@@ -20,7 +20,8 @@ CSRC = PKG / "csrc"
 LIB = PKG / "libhitb200.so"
 SOURCES = ["api.cu"]
 HEADERS = ["common.cuh", "reduce.cuh", "weno.cuh", "kernels_reduce.cuh", "kernels_stencil.cuh",
-           "kernels_spectra.cuh", "kernels_init.cuh", "sensor_step.cuh"]
+           "kernels_spectra.cuh", "kernels_init.cuh", "sensor_step.cuh",
+           "kernels_fft.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -18,6 +18,7 @@
 
 #include "../../include/hitb200.h"
 #include "common.cuh"
+#include "kernels_fft.cuh"
 #include "kernels_init.cuh"
 #include "kernels_reduce.cuh"
 #include "kernels_spectra.cuh"
@@ -2252,3 +2253,197 @@ extern "C" int hitb200_stable_time_step_noalloc(const double* q, int32_t nx, int
   HB_LAUNCHED("dt_scratch_kernel");
   return HITB200_OK;
 }
+
+// =============================================================================
+// Line transforms: spectral diagnostics, the initial condition's spectral
+// derivatives and the real 2-D transform of the shell spectra
+// (kernels_fft.cuh).  Grid lines up to kFftMaxN points.
+// =============================================================================
+namespace {
+
+// e^{-2 pi i j / n}, j in [0, n), as the plan's twiddle tables are formed.
+std::vector<double2> fft_roots(int n) {
+  std::vector<double2> w(n);
+  for (int j = 0; j < n; ++j) {
+    const double th = 2.0 * M_PI * (double)j / (double)n;
+    w[j] = make_double2(std::cos(th), -std::sin(th));
+  }
+  return w;
+}
+
+template <bool IN_REAL, bool OUT_REAL, int C>
+void fft_attr(size_t bytes) {
+  static size_t done[kMaxAttrDevices] = {};
+  const int dev = attr_device();
+  std::lock_guard<std::mutex> lock(g_attr_mu);
+  if (bytes > done[dev]) {
+    cudaFuncSetAttribute(fft_lines_kernel<IN_REAL, OUT_REAL, C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)bytes);
+    done[dev] = bytes;
+  }
+}
+
+// `fields` batches of `lines` lines of n points (see FftLines).
+template <bool IN_REAL, bool OUT_REAL, int C>
+void fft_launch(const void* in, void* out, int n, int lines, int fields, FftLines li, FftLines lo,
+                int out_count, int sign, const double2* W, double scale, cudaStream_t st) {
+  const size_t smem = fft_smem_bytes(n, C);
+  fft_attr<IN_REAL, OUT_REAL, C>(smem);
+  const long long grid = (long long)fields * ((lines + C - 1) / C);
+  fft_lines_kernel<IN_REAL, OUT_REAL, C><<<(unsigned)grid, kFftThreads, smem, st>>>(
+      in, out, n, lines, li, lo, out_count, sign, W, fft_radices(n), scale);
+}
+
+// Column transforms (in place, complex) of `fields` arrays [ny][w] (w columns).
+void fft_columns(double2* a, int ny, int w, int fields, int sign, const double2* W, double scale,
+                 cudaStream_t st) {
+  const FftLines l{(long long)ny * w, 1, w};
+  if (fft_smem_bytes(ny, 4) <= 160 * 1024)
+    fft_launch<false, false, 4>(a, a, ny, w, fields, l, l, ny, sign, W, scale, st);
+  else
+    fft_launch<false, false, 2>(a, a, ny, w, fields, l, l, ny, sign, W, scale, st);
+}
+
+int fft_grid_check(int32_t nx, int32_t ny) {
+  if (nx <= 0 || ny <= 0) return invalid("transform: nx and ny must be positive");
+  if (nx > kFftMaxN || ny > kFftMaxN)
+    return (g_last_error = "transform: grid lines longer than 1024 points are not supported",
+            HITB200_ERR_UNSUPPORTED);
+  return HITB200_OK;
+}
+
+constexpr int kSpecReduceBlocks = 512;
+
+// Workspace of the spectral diagnostics: rho, u, v [3][n] and the four real
+// results [4][n] (doubles), then (16-byte aligned) the transforms of u, v
+// [2][n] and of the four products [4][n], the reduction partials, totals and
+// ticket.
+size_t spectral_c1_off(size_t n) { return (7 * n * sizeof(double) + 255) & ~(size_t)255; }
+size_t spectral_ws(int nx, int ny) {
+  const size_t n = (size_t)nx * ny;
+  return spectral_c1_off(n) + 6 * n * sizeof(double2) + kSpecReduceBlocks * 4 * sizeof(double) +
+         8 * sizeof(double) + 256;
+}
+
+}  // namespace
+
+extern "C" size_t hitb200_spectral_workspace_bytes(int32_t nx, int32_t ny) {
+  if (nx <= 0 || ny <= 0) return 0;
+  return spectral_ws(nx, ny);
+}
+
+extern "C" int hitb200_spectral_diagnostics(hitb200_plan* p, const double* q, double kmax, double* out,
+                                            double* div, double* vort, void* workspace,
+                                            size_t workspace_bytes, void* stream) {
+  if (!p || !q || !out) return invalid("NULL argument");
+  if (!p->desc.periodic) return invalid("spectral diagnostics need a periodic grid");
+  const int nx = p->desc.nx, ny = p->desc.ny;
+  int r = fft_grid_check(nx, ny);
+  if (r != HITB200_OK) return r;
+  if (!workspace || workspace_bytes < spectral_ws(nx, ny))
+    return invalid("workspace smaller than hitb200_spectral_workspace_bytes");
+  cudaStream_t st = (cudaStream_t)stream;
+  const long long n = (long long)nx * ny;
+  double* ruv = static_cast<double*>(workspace);  // [3][n] rho, u, v
+  double* dwb = ruv + 3 * n;                       // [4][n] div, vort, u_low, v_low
+  double2* c1 = reinterpret_cast<double2*>(static_cast<unsigned char*>(workspace) + spectral_c1_off(n));
+  double2* c2 = c1 + 2 * n;                               // [4][n]
+  double* part = reinterpret_cast<double*>(c2 + 4 * n);
+  double* res = part + kSpecReduceBlocks * 4;
+  unsigned* ticket = reinterpret_cast<unsigned*>(res + 4);
+  HB_CUDA(cudaMemsetAsync(ticket, 0, sizeof(unsigned), st));
+  const int blocks = (int)std::min<long long>(kSpecReduceBlocks, (n + 255) / 256);
+  spec_prims_kernel<<<blocks, 256, 0, st>>>(q, ruv, n, p->desc.gamma);
+  // fft2 of u and v: rows (real input), then columns
+  fft_launch<true, false, 1>(ruv + n, c1, nx, ny, 2, FftLines{n, nx, 1}, FftLines{n, nx, 1}, nx, -1,
+                             p->hs.twx, 1.0, st);
+  fft_columns(c1, ny, nx, 2, -1, p->hs.twy, 1.0, st);
+  spec_multiply_kernel<<<blocks, 256, 0, st>>>(c1, c2, nx, ny, p->hs.dx, p->hs.dy,
+                                               kmax > 0.0 ? kmax : -1.0);
+  // ifft2 (real parts) of the four products
+  fft_columns(c2, ny, nx, 4, +1, p->hs.twy, 1.0 / ny, st);
+  fft_launch<false, true, 1>(c2, dwb, nx, ny, 4, FftLines{n, nx, 1}, FftLines{n, nx, 1}, nx, +1,
+                             p->hs.twx, 1.0 / nx, st);
+  spec_reduce_kernel<<<blocks, 256, 0, st>>>(ruv, dwb, c1, n, part, ticket, res, div, vort);
+  HB_LAUNCHED("spectral diagnostics");
+  double h[4];
+  HB_CUDA(cudaMemcpyAsync(h, res, sizeof(h), cudaMemcpyDeviceToHost, st));
+  HB_CUDA(cudaStreamSynchronize(st));
+  const double N = (double)n;
+  out[0] = std::sqrt(h[0] / N);
+  out[1] = std::sqrt(h[1] / N);
+  // large_scale_kinetic_fraction (OOP/hit2d.py:429-449)
+  const double total = h[3] / N;
+  out[2] = (kmax <= 0.0 || total <= DBL_EPSILON) ? 0.0 : (h[2] / N) / total;
+  return HITB200_OK;
+}
+
+extern "C" size_t hitb200_hit_velocity_workspace_bytes(int32_t nx, int32_t ny) {
+  if (nx <= 0 || ny <= 0) return 0;
+  return 3 * (size_t)nx * ny * sizeof(double2) + (size_t)(nx + ny) * sizeof(double2) + 256;
+}
+
+extern "C" int hitb200_hit_velocity(const double* psi, int32_t nx, int32_t ny, double dx, double dy,
+                                    double* u, double* v, void* workspace, size_t workspace_bytes,
+                                    void* stream) {
+  if (!psi || !u || !v) return invalid("NULL argument");
+  int r = fft_grid_check(nx, ny);
+  if (r != HITB200_OK) return r;
+  if (!(dx > 0.0) || !(dy > 0.0)) return invalid("dx and dy must be positive");
+  if (!workspace || workspace_bytes < hitb200_hit_velocity_workspace_bytes(nx, ny))
+    return invalid("workspace smaller than hitb200_hit_velocity_workspace_bytes");
+  cudaStream_t st = (cudaStream_t)stream;
+  const long long n = (long long)nx * ny;
+  double2* ph = static_cast<double2*>(workspace);
+  double2* uv = ph + n;
+  double2* wx = uv + 2 * n;
+  double2* wy = wx + nx;
+  const std::vector<double2> rx = fft_roots(nx), ry = fft_roots(ny);
+  HB_CUDA(cudaMemcpyAsync(wx, rx.data(), nx * sizeof(double2), cudaMemcpyHostToDevice, st));
+  HB_CUDA(cudaMemcpyAsync(wy, ry.data(), ny * sizeof(double2), cudaMemcpyHostToDevice, st));
+  fft_launch<true, false, 1>(psi, ph, nx, ny, 1, FftLines{n, nx, 1}, FftLines{n, nx, 1}, nx, -1, wx, 1.0,
+                             st);
+  fft_columns(ph, ny, nx, 1, -1, wy, 1.0, st);
+  const int blocks = (int)std::min<long long>(1024, (n + 255) / 256);
+  spec_velocity_kernel<<<blocks, 256, 0, st>>>(ph, uv, nx, ny, dx, dy);
+  fft_columns(uv, ny, nx, 2, +1, wy, 1.0 / ny, st);
+  fft_launch<false, true, 1>(uv, u, nx, ny, 1, FftLines{n, nx, 1}, FftLines{n, nx, 1}, nx, +1, wx,
+                             1.0 / nx, st);
+  fft_launch<false, true, 1>(uv + n, v, nx, ny, 1, FftLines{n, nx, 1}, FftLines{n, nx, 1}, nx, +1, wx,
+                             1.0 / nx, st);
+  HB_LAUNCHED("hit velocity transforms");
+  // the host tables must outlive their (staged) copies
+  HB_CUDA(cudaStreamSynchronize(st));
+  return HITB200_OK;
+}
+
+extern "C" size_t hitb200_rfft2_workspace_bytes(int32_t nx, int32_t ny) {
+  if (nx <= 0 || ny <= 0) return 0;
+  return (size_t)(nx + ny) * sizeof(double2) + 256;
+}
+
+extern "C" int hitb200_rfft2(const double* in, int32_t n_fields, int32_t nx, int32_t ny, void* out,
+                             void* workspace, size_t workspace_bytes, void* stream) {
+  if (!in || !out) return invalid("NULL argument");
+  if (n_fields <= 0) return invalid("n_fields must be positive");
+  int r = fft_grid_check(nx, ny);
+  if (r != HITB200_OK) return r;
+  if (!workspace || workspace_bytes < hitb200_rfft2_workspace_bytes(nx, ny))
+    return invalid("workspace smaller than hitb200_rfft2_workspace_bytes");
+  cudaStream_t st = (cudaStream_t)stream;
+  double2* wx = static_cast<double2*>(workspace);
+  double2* wy = wx + nx;
+  const std::vector<double2> rx = fft_roots(nx), ry = fft_roots(ny);
+  HB_CUDA(cudaMemcpyAsync(wx, rx.data(), nx * sizeof(double2), cudaMemcpyHostToDevice, st));
+  HB_CUDA(cudaMemcpyAsync(wy, ry.data(), ny * sizeof(double2), cudaMemcpyHostToDevice, st));
+  const int nh = nx / 2 + 1;
+  const long long n = (long long)nx * ny;
+  double2* o = static_cast<double2*>(out);
+  fft_launch<true, false, 1>(in, o, nx, ny, n_fields, FftLines{n, nx, 1}, FftLines{(long long)ny * nh, nh, 1},
+                             nh, -1, wx, 1.0, st);
+  fft_columns(o, ny, nh, n_fields, -1, wy, 1.0, st);
+  HB_LAUNCHED("rfft2 transforms");
+  HB_CUDA(cudaStreamSynchronize(st));
+  return HITB200_OK;
+}
+

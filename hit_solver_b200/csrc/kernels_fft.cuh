@@ -1,0 +1,240 @@
+// Discrete Fourier transforms of grid lines, for the spectral parts of the
+// diagnostics (OOP/hit2d.py:146-155, 429-468), the initial condition's
+// spectral derivatives (OOP/hit2d.py:186-188) and the shell spectra's real
+// transform (OOP/postprocess/spectra.py:84-121); NumPy's fft conventions:
+// forward sum_m x_m e^{-2 pi i j m / n}, inverse with +i and the 1/n scale.
+//
+// Each line (n <= 1024 complex doubles) is transformed inside shared memory
+// by a self-sorting (Stockham) mixed-radix algorithm: n = R_0 R_1 ... with
+// radices 4, 2, 3, 5, 7 and then any remaining prime; the stage of radix R
+// with Ns points already combined maps output o = t m + j (m = n / R,
+// k = j mod Ns) to
+//     b[(j / Ns) Ns R + k + t Ns] = sum_r a[j + r m] W^{r (k n / (Ns R) + t m)},
+// W = e^{-2 pi i / n} (forward) read from a table of the n roots, staged in
+// shared memory.  A CTA transforms C adjacent lines at once (C > 1 for
+// columns, so that every row access covers C consecutive elements).  The
+// work per stage is n R complex multiply-adds per line (a prime n falls back
+// to the n^2 transform), negligible next to the line's memory traffic.
+#pragma once
+
+#include "common.cuh"
+
+namespace hitb200 {
+
+constexpr int kFftMaxN = 1024;
+constexpr int kFftThreads = 256;
+
+struct FftRadices {
+  int count;
+  int r[16];
+};
+
+// Radices of n: 4s, then 2, 3, 5, 7, then the remaining primes.
+inline FftRadices fft_radices(int n) {
+  FftRadices f{};
+  for (int p : {4, 2, 3, 5, 7})
+    while (n % p == 0 && f.count < 16) {
+      f.r[f.count++] = p;
+      n /= p;
+    }
+  for (int q = 11; n > 1 && f.count < 16; q += 2)
+    while (n % q == 0) {
+      f.r[f.count++] = q;
+      n /= q;
+    }
+  return f;
+}
+
+// Lines: element e of line l of field f sits at
+//   base + f * field + l * line + e * elem.
+struct FftLines {
+  long long field, line, elem;
+};
+
+// Transform C lines per CTA (grid: fields * ceil(lines / C)).  IN_REAL: the
+// input holds doubles (imaginary part zero).  sign -1 forward, +1 inverse
+// (unscaled; the output is multiplied by `scale`).  Only the first out_count
+// outputs of each line are stored (n, or n / 2 + 1 for a half spectrum).
+// OUT_REAL: only the real parts are stored (doubles).  W: the n roots
+// e^{-2 pi i m / n}.
+template <bool IN_REAL, bool OUT_REAL, int C>
+__global__ void __launch_bounds__(kFftThreads)
+    fft_lines_kernel(const void* __restrict__ in, void* __restrict__ out, int n, int lines,
+                     FftLines li, FftLines lo, int out_count, int sign,
+                     const double2* __restrict__ W, FftRadices rad, double scale) {
+  extern __shared__ __align__(16) double2 fbuf[];
+  double2* a = fbuf;
+  double2* b = fbuf + (size_t)n * C;
+  double2* w = fbuf + (size_t)2 * n * C;
+  const int groups = (lines + C - 1) / C;
+  const int f = blockIdx.x / groups, l0 = (blockIdx.x - f * groups) * C;
+  const int nc = min(C, lines - l0);
+  for (int m = threadIdx.x; m < n; m += blockDim.x) {
+    double2 v = W[m];
+    if (sign > 0) v.y = -v.y;
+    w[m] = v;
+  }
+  // element e of line l0 + c at a[e C + c]: consecutive threads take the C
+  // lines of one element (adjacent in memory for columns)
+  for (int idx = threadIdx.x; idx < n * C; idx += blockDim.x) {
+    const int e = idx / C, c = idx - e * C;
+    double2 v = make_double2(0.0, 0.0);
+    if (c < nc) {
+      const long long o = f * li.field + (long long)(l0 + c) * li.line + (long long)e * li.elem;
+      if constexpr (IN_REAL) v.x = static_cast<const double*>(in)[o];
+      else v = static_cast<const double2*>(in)[o];
+    }
+    a[idx] = v;
+  }
+  __syncthreads();
+  int Ns = 1;
+  for (int s = 0; s < rad.count; ++s) {
+    const int R = rad.r[s], m = n / R, step = n / (Ns * R);
+    for (int idx = threadIdx.x; idx < n * C; idx += blockDim.x) {
+      const int o = idx / C, c = idx - o * C;
+      const int j = o % m, t = o / m;
+      const int k = j % Ns;
+      const int e1 = k * step + t * m;  // < n
+      double re = 0.0, im = 0.0;
+      int e = 0;
+      for (int r = 0; r < R; ++r) {
+        const double2 x = a[(j + r * m) * C + c];
+        const double2 tw = w[e];
+        re = fma(x.x, tw.x, fma(-x.y, tw.y, re));
+        im = fma(x.x, tw.y, fma(x.y, tw.x, im));
+        e += e1;
+        if (e >= n) e -= n;
+      }
+      b[((j / Ns) * Ns * R + k + t * Ns) * C + c] = make_double2(re, im);
+    }
+    __syncthreads();
+    double2* tmp = a;
+    a = b;
+    b = tmp;
+    Ns *= R;
+  }
+  for (int idx = threadIdx.x; idx < out_count * C; idx += blockDim.x) {
+    const int e = idx / C, c = idx - e * C;
+    if (c >= nc) continue;
+    const double2 v = a[e * C + c];
+    const long long o = f * lo.field + (long long)(l0 + c) * lo.line + (long long)e * lo.elem;
+    if constexpr (OUT_REAL) static_cast<double*>(out)[o] = v.x * scale;
+    else static_cast<double2*>(out)[o] = make_double2(v.x * scale, v.y * scale);
+  }
+}
+
+inline size_t fft_smem_bytes(int n, int C) { return (size_t)(2 * C + 1) * n * sizeof(double2); }
+
+// 2 pi fftfreq(n, d)[j] as NumPy forms it: bin * (1 / (n d)), times 2 pi.
+__device__ __forceinline__ double fft_wavenumber(int j, int n, double d) {
+  const int bin = j < (n + 1) / 2 ? j : j - n;
+  return 2.0 * 3.141592653589793 * ((double)bin * (1.0 / ((double)n * d)));
+}
+
+// ---- spectral diagnostics (OOP/hit2d.py:146-155, 429-468) -------------------
+// rho, u, v of primitive_from_conservative (OOP/equations.py:136-145):
+// fields [3][ny][nx].
+__global__ void spec_prims_kernel(const double* __restrict__ q, double* __restrict__ ruv, long long n,
+                                  double gamma) {
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n;
+       c += (long long)gridDim.x * blockDim.x) {
+    const Prim<double> p = primitives(q[c], q[n + c], q[2 * n + c], q[3 * n + c], gamma);
+    ruv[c] = p.rho;
+    ruv[n + c] = p.u;
+    ruv[2 * n + c] = p.v;
+  }
+}
+
+// From the transforms U, V [2][ny][nx]: i (KX U + KY V) (divergence),
+// i (KX V - KY U) (vorticity) and U, V restricted to 0 < |k| <= kmax (the
+// low-k band of the kinetic fraction) -> out [4][ny][nx].
+__global__ void spec_multiply_kernel(const double2* __restrict__ uv, double2* __restrict__ out, int nx,
+                                     int ny, double dx, double dy, double kmax) {
+  const long long n = (long long)nx * ny;
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n;
+       c += (long long)gridDim.x * blockDim.x) {
+    const int j = (int)(c / nx), i = (int)(c - (long long)j * nx);
+    const double kx = fft_wavenumber(i, nx, dx), ky = fft_wavenumber(j, ny, dy);
+    const double2 U = uv[c], V = uv[n + c];
+    // i z = (-z.y, z.x)
+    const double dre = kx * U.x + ky * V.x, dim = kx * U.y + ky * V.y;
+    const double wre = kx * V.x - ky * U.x, wim = kx * V.y - ky * U.y;
+    out[c] = make_double2(-dim, dre);
+    out[n + c] = make_double2(-wim, wre);
+    const double k2 = kx * kx + ky * ky;
+    const double mag = sqrt(k2);
+    const bool keep = k2 > 0.0 && mag <= kmax;
+    out[2 * n + c] = keep ? U : make_double2(0.0, 0.0);
+    out[3 * n + c] = keep ? V : make_double2(0.0, 0.0);
+  }
+}
+
+// Sums of div^2, vort^2, rho (ul^2 + vl^2) and rho (u'^2 + v'^2) (u' = u -
+// mean u, the mean from the transform's zero mode) into per-CTA partials;
+// the last CTA (ticket in part_n[0]) writes the four totals to res.
+// div / vort fields are copied out when the pointers are given.
+__global__ void __launch_bounds__(256)
+    spec_reduce_kernel(const double* __restrict__ ruv, const double* __restrict__ dwb,
+                       const double2* __restrict__ uv, long long n, double* __restrict__ part,
+                       unsigned* ticket, double* __restrict__ res, double* __restrict__ div_out,
+                       double* __restrict__ vort_out) {
+  const double mu = uv[0].x / (double)n, mv = uv[n].x / (double)n;
+  double s[4] = {0.0, 0.0, 0.0, 0.0};
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n;
+       c += (long long)gridDim.x * blockDim.x) {
+    const double d = dwb[c], w = dwb[n + c], ul = dwb[2 * n + c], vl = dwb[3 * n + c];
+    const double rho = ruv[c], uf = ruv[n + c] - mu, vf = ruv[2 * n + c] - mv;
+    s[0] += d * d;
+    s[1] += w * w;
+    s[2] += rho * (ul * ul + vl * vl);
+    s[3] += rho * (uf * uf + vf * vf);
+    if (div_out) div_out[c] = d;
+    if (vort_out) vort_out[c] = w;
+  }
+  __shared__ double sm[8][4];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const double v = warp_sum(s[k]);
+    if (lane == 0) sm[warp][k] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < 4) {
+    double acc = 0.0;
+    for (int w = 0; w < 8; ++w) acc += sm[w][threadIdx.x];
+    part[blockIdx.x * 4 + threadIdx.x] = acc;
+  }
+  __shared__ bool last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const unsigned t = atomicAdd(ticket, 1u);
+    last = t == gridDim.x - 1u;
+    if (last) *ticket = 0u;
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  if (threadIdx.x < 4) {
+    double acc = 0.0;
+    for (unsigned b = 0; b < gridDim.x; ++b) acc += __ldcg(part + b * 4 + threadIdx.x);
+    res[threadIdx.x] = acc;
+  }
+}
+
+// i KY P and -i KX P (the initial condition's u = d psi / dy, v = -d psi / dx,
+// OOP/hit2d.py:186-188) -> out [2][ny][nx].
+__global__ void spec_velocity_kernel(const double2* __restrict__ ph, double2* __restrict__ out, int nx,
+                                     int ny, double dx, double dy) {
+  const long long n = (long long)nx * ny;
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n;
+       c += (long long)gridDim.x * blockDim.x) {
+    const int j = (int)(c / nx), i = (int)(c - (long long)j * nx);
+    const double kx = fft_wavenumber(i, nx, dx), ky = fft_wavenumber(j, ny, dy);
+    const double2 P = ph[c];
+    out[c] = make_double2(-ky * P.y, ky * P.x);
+    out[n + c] = make_double2(kx * P.y, -kx * P.x);
+  }
+}
+
+}  // namespace hitb200

@@ -11,6 +11,7 @@ snapshots or checks for the end of the run.
 from __future__ import annotations
 
 import argparse
+import ctypes
 import math
 import sys
 from dataclasses import dataclass, field
@@ -168,8 +169,9 @@ def initialize_hit_2d_device(config: HIT2DConfig, domain: Domain2D, equation, rn
     """initialize_hit_2d (OOP/hit2d.py:158-204) built on the device: the
     phases come from ``rng`` on the host (a few dozen draws, the reference's
     stream), the streamfunction sum over modes and cells runs in
-    ``hitb200_hit_streamfunction``, its spectral derivatives in cuFFT
-    (torch.fft, as the reference's fft2 / ifft2), and the mean removal,
+    ``hitb200_hit_streamfunction``, its spectral derivatives in the library's
+    line transforms (``hitb200_hit_velocity``, the reference's fft2 / ifft2),
+    and the mean removal,
     Mach scaling and conservative state in ``hitb200_hit_compose``.  Equal to
     the host form to roundoff (cos and the transforms are not NumPy's)."""
     core.require_cuda()
@@ -182,10 +184,13 @@ def initialize_hit_2d_device(config: HIT2DConfig, domain: Domain2D, equation, rn
                                               float(domain.x_min), float(domain.dx),
                                               float(domain.y_min), float(domain.dy),
                                               psi.data_ptr(), stream))
-    KX, KY = (torch.from_numpy(np.ascontiguousarray(k)).cuda() for k in _wavenumbers(domain))
-    ph = torch.fft.fft2(psi)
-    u = torch.fft.ifft2(1j * KY * ph).real.contiguous()
-    v = (-torch.fft.ifft2(1j * KX * ph).real).contiguous()
+    u = torch.empty_like(psi)
+    v = torch.empty_like(psi)
+    wsv = torch.empty(int(lib.hitb200_hit_velocity_workspace_bytes(nx, ny)), dtype=torch.uint8,
+                      device="cuda")
+    _lib.check(lib.hitb200_hit_velocity(psi.data_ptr(), nx, ny, float(domain.dx), float(domain.dy),
+                                        u.data_ptr(), v.data_ptr(), wsv.data_ptr(), wsv.numel(),
+                                        stream))
     # mean sound speed of rho = 1, p = 1/gamma as NumPy forms it (a constant field)
     p = np.full((ny, nx), 1.0 / config.gamma)
     c_mean = float(np.mean(np.sqrt(equation.gamma * p / np.ones_like(p))))
@@ -272,42 +277,49 @@ def update_mach_controlled_power(config, current_power, rho, u, v, pressure):
     return next_power, info
 
 
-def _spectral_band(values, domain: Domain2D, k_min=0.0, k_max=None):
-    KX, KY = _wavenumbers(domain)
-    k2 = KX ** 2 + KY ** 2
-    mag = np.sqrt(k2)
-    keep = (mag >= float(k_min)) & (k2 > 0.0)
-    if k_max is not None:
-        keep &= mag <= float(k_max)
-    keep_t = torch.from_numpy(keep).to(values.device)
-    return torch.fft.ifft2(torch.where(keep_t, torch.fft.fft2(values), 0.0)).real
-
-
-def _spectral_derivatives(values, domain: Domain2D):
-    KX, KY = _wavenumbers(domain)
-    kx = torch.from_numpy(KX).to(values.device)
-    ky = torch.from_numpy(KY).to(values.device)
-    vh = torch.fft.fft2(values)
-    return torch.fft.ifft2(1j * kx * vh).real, torch.fft.ifft2(1j * ky * vh).real
+def spectral_diagnostics(q, equation, domain: Domain2D, kmax: float = 0.0, fields: bool = False,
+                         plan: core.Plan | None = None):
+    """Spectral divergence and vorticity rms (OOP/hit2d.py:146-155, 459-468)
+    and the low-k kinetic fraction for 0 < |k| <= kmax (:429-449) of the
+    state q, by the library's own line transforms
+    (hitb200_spectral_diagnostics).  Returns (div_rms, vort_rms, k_low) and,
+    with ``fields``, the divergence and vorticity fields."""
+    q = core.as_state(q)
+    ny, nx = q.shape[1:]
+    if plan is None:
+        plan = core.plan_for(grid_desc(domain, equation.gamma, True))
+    lib = plan.lib
+    ws = torch.empty(int(lib.hitb200_spectral_workspace_bytes(nx, ny)), dtype=torch.uint8,
+                     device=q.device)
+    div = vort = None
+    if fields:
+        div = torch.empty((ny, nx), dtype=torch.float64, device=q.device)
+        vort = torch.empty_like(div)
+    out = (ctypes.c_double * 3)()
+    _lib.check(lib.hitb200_spectral_diagnostics(
+        plan.handle, q.data_ptr(), float(kmax), out, core.ptr(div), core.ptr(vort), ws.data_ptr(),
+        ws.numel(), core.stream_handle()))
+    res = (out[0], out[1], out[2])
+    return (res, div, vort) if fields else res
 
 
 def divergence_and_vorticity(u, v, domain: Domain2D):
-    """Spectral divergence and vorticity (OOP/hit2d.py:459-468)."""
-    du_dx, du_dy = _spectral_derivatives(u, domain)
-    dv_dx, dv_dy = _spectral_derivatives(v, domain)
-    return du_dx + dv_dy, dv_dx - du_dy
+    """Spectral divergence and vorticity fields (OOP/hit2d.py:459-468) of the
+    velocity (u, v): the state [1, u, v, 1] through spectral_diagnostics
+    (its velocity is u, v exactly)."""
+    u = core.as_field(u, (domain.ny, domain.nx), "u")
+    v = core.as_field(v, (domain.ny, domain.nx), "v")
+    q = torch.stack([torch.ones_like(u), u, v, torch.ones_like(u)]).contiguous()
+    _, div, vort = spectral_diagnostics(q, EulerEquation2D(gamma=1.4), domain, fields=True)
+    return div, vort
 
 
 def large_scale_kinetic_fraction(q, equation, domain: Domain2D, kmax: float) -> float:
+    """Fraction of the kinetic energy of the velocity fluctuations in the band
+    0 < |k| <= kmax (OOP/hit2d.py:429-449)."""
     if kmax <= 0.0:
         return 0.0
-    rho, u, v, _ = equation.primitive_from_conservative(q)
-    uf, vf = u - torch.mean(u), v - torch.mean(v)
-    total = float(torch.mean(rho * (uf ** 2 + vf ** 2)))
-    if total <= np.finfo(float).eps:
-        return 0.0
-    ul, vl = _spectral_band(uf, domain, 0.0, kmax), _spectral_band(vf, domain, 0.0, kmax)
-    return float(torch.mean(rho * (ul ** 2 + vl ** 2))) / total
+    return spectral_diagnostics(q, equation, domain, kmax)[2]
 
 
 def source_power(source) -> float:
@@ -330,15 +342,14 @@ def compute_diagnostics(q, equation, domain: Domain2D, initial_mass=None, forcin
     vals = plan.diagnostics(q)
     d = dict(zip(_DIAG_KEYS, vals[:10]))
     d["mass"] = vals[9]
-    _, u, v, _ = equation.primitive_from_conservative(q)
-    div, vort = divergence_and_vorticity(u, v, domain)
+    div_rms, vort_rms, _ = spectral_diagnostics(q, equation, domain, plan=plan)
     diagnostics = {
         "kinetic_energy": d["kinetic_energy"], "Kx": d["Kx"], "Ky": d["Ky"], "A_K": d["A_K"],
         "C_uv": d["C_uv"], "rms_velocity": d["rms_velocity"],
         "turbulent_mach": d["turbulent_mach"], "mean_density": d["mean_density"],
         "mean_pressure": d["mean_pressure"],
-        "divergence_rms": float(torch.sqrt(torch.mean(div ** 2))),
-        "vorticity_rms": float(torch.sqrt(torch.mean(vort ** 2))),
+        "divergence_rms": div_rms,
+        "vorticity_rms": vort_rms,
         "mass": d["mass"],
         "mass_error": 0.0 if initial_mass is None else d["mass"] - initial_mass,
         "large_scale_kinetic_fraction": large_scale_fraction,
@@ -371,8 +382,9 @@ def save_run_config(output_dir: Path, config: HIT2DConfig) -> Path:
 
 
 def save_snapshot(output_dir: Path, step: int, time: float, q, equation, domain: Domain2D) -> Path:
+    q = core.as_state(q)
     rho, u, v, p = equation.primitive_from_conservative(q)
-    div, vort = divergence_and_vorticity(u, v, domain)
+    _, div, vort = spectral_diagnostics(q, equation, domain, fields=True)
     output_dir = Path(output_dir)
     output_dir.mkdir(parents=True, exist_ok=True)
     path = output_dir / f"hit2d_step{step:07d}.npz"

@@ -8,8 +8,8 @@ snapshots at once on the GPU:
 
 * ``hitb200_spectra_fields`` / ``hitb200_spectra_state_fields`` (CUDA) form
   sqrt(rho) u', sqrt(rho) v', u', v' of every snapshot;
-* ``torch.fft.rfft2`` (cuFFT) transforms them, the half spectrum being enough
-  for real fields;
+* ``hitb200_rfft2`` (the library's mixed-radix line transforms) gives their
+  half spectra, enough for real fields;
 * ``hitb200_spectra_shells`` (CUDA) bins the modes into shells in a fixed
   order.
 
@@ -60,7 +60,12 @@ def _fields3(t: torch.Tensor, name: str) -> torch.Tensor:
 def _shells(fields: torch.Tensor, nx: int, ny: int, dx: float, dy: float, ws: torch.Tensor):
     lib = _lib.load()
     n = fields.shape[0]
-    spec = torch.fft.rfft2(fields).contiguous()  # [n, 4, ny, nx // 2 + 1] complex128
+    # [n, 4, ny, nx // 2 + 1] complex128: the library's line transforms
+    spec = torch.empty((n, 4, ny, nx // 2 + 1), dtype=torch.complex128, device=fields.device)
+    fws = torch.empty(int(lib.hitb200_rfft2_workspace_bytes(nx, ny)), dtype=torch.uint8,
+                      device=fields.device)
+    _lib.check(lib.hitb200_rfft2(fields.data_ptr(), 4 * n, nx, ny, spec.data_ptr(), fws.data_ptr(),
+                                 fws.numel(), core.stream_handle()))
     ns = min(nx, ny) // 2 + 1
     energy = torch.empty((n, ns), dtype=torch.float64, device=fields.device)
     enstrophy = torch.empty_like(energy)

@@ -345,6 +345,35 @@ int hitb200_spectra_shells(const void* spec, int32_t n_snap, int32_t nx, int32_t
                            double dy, double* energy, double* enstrophy, void* workspace,
                            size_t workspace_bytes, void* stream);
 
+/* ---- line transforms ------------------------------------------------------------ */
+/* Hand-written mixed-radix transforms of grid lines (any length up to 1024)
+ * with NumPy's fft conventions; the workspaces are caller device memory of
+ * the stated size.
+ *
+ * The spectral diagnostics of a periodic plan's state q: out[0] =
+ * divergence_rms and out[1] = vorticity_rms of the spectral derivatives
+ * (divergence_and_vorticity, OOP/hit2d.py:146-155, 459-468, in
+ * compute_diagnostics :471-548), out[2] = large_scale_kinetic_fraction
+ * (:429-449) for the band 0 < |k| <= kmax (0 when kmax <= 0); div and vort
+ * (device double [ny][nx], may be NULL) receive the fields themselves (the
+ * snapshot's, :571-597).  Synchronises. */
+size_t hitb200_spectral_workspace_bytes(int32_t nx, int32_t ny);
+int hitb200_spectral_diagnostics(hitb200_plan* plan, const double* q, double kmax, double* out,
+                                 double* div, double* vort, void* workspace, size_t workspace_bytes,
+                                 void* stream);
+/* u = d psi / dy, v = -d psi / dx by spectral derivatives (the initial
+ * condition's, OOP/hit2d.py:186-188): psi, u, v device double [ny][nx].
+ * Synchronises (its root tables are copied from host memory). */
+size_t hitb200_hit_velocity_workspace_bytes(int32_t nx, int32_t ny);
+int hitb200_hit_velocity(const double* psi, int32_t nx, int32_t ny, double dx, double dy, double* u,
+                         double* v, void* workspace, size_t workspace_bytes, void* stream);
+/* numpy.fft.rfft2 of n_fields real arrays [ny][nx] (device doubles) into
+ * out, complex double [n_fields][ny][nx/2+1] (the shell spectra's transform,
+ * OOP/postprocess/spectra.py:84-121).  Synchronises. */
+size_t hitb200_rfft2_workspace_bytes(int32_t nx, int32_t ny);
+int hitb200_rfft2(const double* in, int32_t n_fields, int32_t nx, int32_t ny, void* out, void* workspace,
+                  size_t workspace_bytes, void* stream);
+
 /* ---- batched form ------------------------------------------------------------- */
 /* Many independent solves (any mix of grid sizes) advanced by one launch per
  * kernel of the step: the "ensemble" / serving form.  All descriptors must

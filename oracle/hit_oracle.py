@@ -472,6 +472,20 @@ def band_filter(a, dx, dy, kmin, kmax):
     return np.fft.ifft2(np.where(keep, np.fft.fft2(a), 0.0)).real
 
 
+def large_scale_kinetic_fraction(q, dx, dy, gamma, kmax):
+    """Kinetic-energy fraction of the velocity fluctuations in 0 < |k| <= kmax
+    (``OOP/hit2d.py:429-449``)."""
+    if kmax <= 0.0:
+        return 0.0
+    rho, u, v, _ = primitives(q, gamma)
+    uf, vf = u - np.mean(u), v - np.mean(v)
+    total = float(np.mean(rho * (uf ** 2 + vf ** 2)))
+    if total <= np.finfo(float).eps:
+        return 0.0
+    ul, vl = band_filter(uf, dx, dy, 0.0, kmax), band_filter(vf, dx, dy, 0.0, kmax)
+    return float(np.mean(rho * (ul ** 2 + vl ** 2))) / total
+
+
 def drag_source(q, dx, dy, gamma, coef, kmax):
     """Linear drag on the low-k momentum fluctuations (``OOP/hit2d.py:370-399``)."""
     out = np.zeros_like(q)

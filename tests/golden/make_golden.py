@@ -112,12 +112,14 @@ def gen_periodic(R, name, cfg, domain, eq, q):
         for key, val in info.items():
             f_out[f"forcing{k}_info_{key}"] = np.asarray(val)
     diag = hit2d.compute_diagnostics(q, eq, domain)
+    klow = {f"klow_{k:g}": np.asarray(hit2d.large_scale_kinetic_fraction(q, eq, domain, k))
+            for k in (1.0, 2.0, 3.5)}
     np.savez_compressed(
         HERE / f"periodic_{name}.npz",
         q=q, mask=mask, mask_shear=sensor_shear.detect(qs), d_x=d_x, d_y=d_y, rhs=op.rhs(q),
         dt=np.asarray(dt), fx=fx, fy=fy, viscous=visc, drag=drag, cooling=cool, forcing_src=fsrc,
         step=step, hv=hvq, dx=np.asarray(domain.dx), dy=np.asarray(domain.dy),
-        **f_out, **{f"diag_{k}": np.asarray(v) for k, v in diag.items()})
+        **f_out, **klow, **{f"diag_{k}": np.asarray(v) for k, v in diag.items()})
 
 
 def gen_hit_run(R):

@@ -416,3 +416,61 @@ def test_golden_periodic_diagnostics(name):
         want = float(d[f"diag_{key}"])
         ref = max(abs(want), scale.get(key, 0.0))
         assert abs(got[key] - want) <= 1e-12 * ref, (key, got[key], want)
+
+
+@pytest.mark.parametrize("name", ["periodic_hit_32x24", "periodic_blob_40x36"])
+def test_golden_large_scale_kinetic_fraction(name):
+    """large_scale_kinetic_fraction (OOP/hit2d.py:429-449) through the
+    library's line transforms, against the reference's values for the
+    fixture state (the 1 and 2 bands hold only roundoff of this state)."""
+    from pathlib import Path
+
+    from hit_solver_b200.equations import EulerEquation2D
+    from hit_solver_b200.hit2d import large_scale_kinetic_fraction
+
+    d = np.load(Path(__file__).parent / "golden" / f"{name}.npz")
+    q = d["q"]
+    ny, nx = q.shape[1:]
+    dom = Domain2D(0.0, 2 * np.pi, 0.0, 2 * np.pi, nx, ny)
+    for k in (1.0, 2.0, 3.5):
+        got = large_scale_kinetic_fraction(dev(q), EulerEquation2D(gamma=G), dom, k)
+        want = float(d[f"klow_{k:g}"])
+        assert abs(got - want) <= 1e-12 * max(abs(want), 1.0), (k, got, want)
+
+
+@pytest.mark.parametrize("shape", [(24, 32), (20, 25), (97, 64), (63, 50), (1024, 6), (7, 1021), (384, 384)])
+def test_rfft2_matches_numpy(shape):
+    """The library's mixed-radix line transforms (hitb200_rfft2) against
+    numpy.fft.rfft2: radices 4, 2, 3, 5, 7 and prime lengths."""
+    ny, nx = shape
+    lib = _lib.load()
+    rng = np.random.default_rng(ny * 7 + nx)
+    a = rng.standard_normal((3, ny, nx))
+    out = torch.empty((3, ny, nx // 2 + 1), dtype=torch.complex128, device="cuda")
+    ws = torch.empty(int(lib.hitb200_rfft2_workspace_bytes(nx, ny)), dtype=torch.uint8, device="cuda")
+    _lib.check(lib.hitb200_rfft2(dev(a).data_ptr(), 3, nx, ny, out.data_ptr(), ws.data_ptr(), ws.numel(),
+                                 core.stream_handle()))
+    want = np.fft.rfft2(a)
+    assert rel_err(out.cpu().numpy(), want) < 1e-13
+
+
+def test_spectral_divergence_vorticity_fields():
+    """divergence_and_vorticity (OOP/hit2d.py:146-155, 459-468) against the
+    oracle's NumPy spectral derivatives on a non-square grid with a Nyquist
+    row (even ny) and an odd nx."""
+    from hit_solver_b200.hit2d import divergence_and_vorticity
+
+    ny, nx = 40, 27
+    dom = Domain2D(0.0, 2 * np.pi, 0.0, 3.0, nx, ny)
+    rng = np.random.default_rng(3)
+    u, v = rng.standard_normal((ny, nx)), rng.standard_normal((ny, nx))
+    kx, ky = O.wavenumbers(nx, ny, dom.dx, dom.dy)
+
+    def d(a, k):
+        return np.fft.ifft2(1j * k * np.fft.fft2(a)).real
+
+    want_div = d(u, kx) + d(v, ky)
+    want_vort = d(v, kx) - d(u, ky)
+    div, vort = divergence_and_vorticity(dev(u), dev(v), dom)
+    assert rel_err(host(div), want_div) < 1e-12
+    assert rel_err(host(vort), want_vort) < 1e-12

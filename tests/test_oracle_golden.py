@@ -45,6 +45,14 @@ def test_periodic_sensor_rhs_sources(name):
 
 
 @pytest.mark.parametrize("name", PERIODIC)
+def test_large_scale_kinetic_fraction(name):
+    d = load(name)
+    q, dx, dy = d["q"], float(d["dx"]), float(d["dy"])
+    for k in (1.0, 2.0, 3.5):
+        assert O.large_scale_kinetic_fraction(q, dx, dy, GAMMA, k) == float(d[f"klow_{k:g}"])
+
+
+@pytest.mark.parametrize("name", PERIODIC)
 def test_periodic_rk3_step(name):
     d = load(name)
     q, dx, dy = d["q"], float(d["dx"]), float(d["dy"])
