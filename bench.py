@@ -383,6 +383,7 @@ def run_b200(args, world, rank, local):
 
     # ---- 512^2 production HIT: plain FP64 single solve vs FP32-bulk batch ----
     hit = hit_forms(K, W, B, flush, world)
+    dropin = dropin_hit_run() if rank == 0 else None
     hit["tuning"] = hit.pop("_tuning")
     ens = ensemble_run(K, W, flush, world, args.ensemble) if args.ensemble > 0 else None
     if ens is not None:
@@ -452,6 +453,17 @@ def run_b200(args, world, rank, local):
                     "solves": B, "dtype": "fp32 (fp64 state)",
                     "speedup_vs_plain_fp64": (B * cells * kb / tb) / (cells * K / t64)},
         "batched_hit": hit,
+        "dropin_hit": dropin,
+        # the headline's companions in one place: the batched FP32 form against
+        # the plain FP64 single solve on 512^2 production HIT (the north-star
+        # ratio), the plain FP64 Riemann solve, and the drop-in HIT path
+        "north_star": {
+            "batched_fp32_hit_cell_updates_per_s": hit["batched_fp32"]["value"],
+            "plain_fp64_hit_cell_updates_per_s": hit["plain_fp64"]["value"],
+            "batched_vs_plain_fp64_hit": hit["speedup_batched_vs_plain"],
+            "plain_fp64_riemann_cell_updates_per_s": world * cells * K / t64,
+            "dropin_hit_ms_per_step": None if dropin is None else dropin["numpy"]["ms_per_step"],
+        },
         "ensemble": ens,
         "serving": serve,
         "spectra": spectra,
@@ -473,7 +485,15 @@ def run_b200(args, world, rank, local):
                                  for k, v in sorted(per.items(), key=lambda kv: -kv[1]["ms_per_step"])},
                      # the whole step against the same peak: 8 FP64 state
                      # vectors of SSP-RK3 per cell-update (256 B)
+                     "kernels_mode": "each kernel timed alone: one uncaptured step with CUDA "
+                                     "events between launches (no programmatic-launch overlap); "
+                                     "their sum is kernels_sum_ms_per_step, the graph-replayed "
+                                     "step is ms_per_step",
+                     "kernels_sum_ms_per_step": round(sum(v["ms_per_step"] for v in per.values()), 5),
                      "step": {"bytes_per_cell_update": STEP_BYTES_PER_CELL,
+                              "plain_fp64_hit_gbs": STEP_BYTES_PER_CELL * hit["plain_fp64"]["value"] / 1e9,
+                              "batched_fp32_hit_gbs": STEP_BYTES_PER_CELL * hit["batched_fp32"]["value"] / 1e9,
+                              "batched_vs_plain_fp64_hit": hit["speedup_batched_vs_plain"],
                               "single_gbs": STEP_BYTES_PER_CELL * cells * K / t32 / 1e9,
                               "single_frac": STEP_BYTES_PER_CELL * cells * K / t32 / 1e9 / peak,
                               "batched_gbs": STEP_BYTES_PER_CELL * B * cells * kb / tb / 1e9,
@@ -566,8 +586,10 @@ def ensemble_run(K: int, W: int, flush, world: int, count: int):
 def spectra_run(K: int, W: int, flush, world: int, count: int, cpu: bool):
     """Shell spectra (the per-snapshot work of HIT2DSpectra.compute) of `count`
     device-resident 512^2 snapshots per step: fluctuation fields (CUDA),
-    rfft2 of the four fields (cuFFT, torch.fft), shell binning (CUDA).  Phase
-    times come from CUDA events around each call of a separate pass."""
+    rfft2 of the four fields (the library's own line transforms), shell
+    binning (CUDA).  Phase times come from CUDA events around each call of a
+    separate pass; cuFFT's rfft2 of the same fields is timed beside it as a
+    comparison."""
     import numpy as np
     import torch
 
@@ -596,6 +618,9 @@ def spectra_run(K: int, W: int, flush, world: int, count: int, cpu: bool):
     z = torch.empty_like(e)
     st = torch.cuda.current_stream()
     ph = {"fields": 0.0, "rfft2": 0.0, "shells": 0.0}
+    spec = torch.empty((count, 4, NY, nh), dtype=torch.complex128, device="cuda")
+    fws = torch.empty(int(lib.hitb200_rfft2_workspace_bytes(NX, NY)), dtype=torch.uint8, device="cuda")
+    cufft_ms = 0.0
     for _ in range(k):
         flush.zero_()
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
@@ -604,7 +629,8 @@ def spectra_run(K: int, W: int, flush, world: int, count: int, cpu: bool):
                                               NY, 0, fields.data_ptr(), ws.data_ptr(), ws.numel(),
                                               core.stream_handle()))
         ev[1].record(st)
-        spec = torch.fft.rfft2(fields)
+        _lib.check(lib.hitb200_rfft2(fields.data_ptr(), 4 * count, NX, NY, spec.data_ptr(),
+                                     fws.data_ptr(), fws.numel(), core.stream_handle()))
         ev[2].record(st)
         _lib.check(lib.hitb200_spectra_shells(spec.data_ptr(), count, NX, NY, h, h, e.data_ptr(),
                                               z.data_ptr(), ws.data_ptr(), ws.numel(),
@@ -613,7 +639,15 @@ def spectra_run(K: int, W: int, flush, world: int, count: int, cpu: bool):
         torch.cuda.synchronize()
         for i, name in enumerate(ph):
             ph[name] += ev[i].elapsed_time(ev[i + 1]) / k
-        del spec
+        # comparison: the library FFT (cuFFT) on the same fields
+        flush.zero_()
+        c0, c1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        c0.record(st)
+        ref = torch.fft.rfft2(fields)
+        c1.record(st)
+        torch.cuda.synchronize()
+        cufft_ms += c0.elapsed_time(c1) / k
+        del ref
     peak, _kind = measured_peak()
     cells = count * NX * NY
     # algorithmic bytes: fields = mean pass (read rho, u, v) + field pass (read
@@ -623,7 +657,8 @@ def spectra_run(K: int, W: int, flush, world: int, count: int, cpu: bool):
     phases = {
         "fields": {"ms": ph["fields"], "gbs": fbytes / (ph["fields"] / 1e3) / 1e9,
                    "bytes": fbytes, "frac": fbytes / (ph["fields"] / 1e3) / 1e9 / peak},
-        "rfft2_cufft": {"ms": ph["rfft2"]},
+        "rfft2": {"ms": ph["rfft2"], "impl": "hitb200_rfft2 (mixed-radix line transforms)",
+                  "cufft_ms": cufft_ms},
         "shells": {"ms": ph["shells"], "gbs": sbytes / (ph["shells"] / 1e3) / 1e9, "bytes": sbytes,
                    "frac": sbytes / (ph["shells"] / 1e3) / 1e9 / peak},
     }
@@ -651,7 +686,7 @@ def spectra_run(K: int, W: int, flush, world: int, count: int, cpu: bool):
 
 def initial_state_run(n: int = 1024, reps: int = 5):
     """Building one n^2 initial state, the host form (NumPy, the reference's
-    arithmetic) against the device form (CUDA kernels and cuFFT): the
+    arithmetic) against the device form (CUDA kernels, own line transforms): the
     admission cost of a solve."""
     import numpy as np
     import torch
@@ -681,6 +716,54 @@ def initial_state_run(n: int = 1024, reps: int = 5):
         "hit_device_ms": clock(lambda: initialize_hit_2d_device(cfg, dom, eq, np.random.default_rng(1))),
         "riemann_device_ms": clock(rc.initial_state),
     }
+
+
+def dropin_hit_run(steps: int = 50):
+    """The drop-in HIT path (what ``run_hit2d.py --backend b200`` runs): the
+    mirror's HITSolver on the 512^2 production physics with the reference's
+    NumPy forcing-noise stream, continued on the device (``numpy``, graph
+    replay) and drawn by NumPy on the host and uploaded each step
+    (``numpy-host``); device-timed per step.  Plus the mirror's
+    run_simulation for the same physics end to end (60 steps, diagnostics and
+    snapshots only at the ends, host wall clock including its setup)."""
+    import tempfile
+
+    import torch
+
+    from hit_solver_b200.hit2d import HIT2DConfig, HITSolver, run_simulation
+
+    kw = dict(nx=NX, ny=NY, tfinal=1e9, cfl=0.05, target_mach=0.25, initial_kmin=3,
+              initial_kmax=5, forcing_kmin=3.0, forcing_kmax=5.0, forcing_correlation_time=0.5,
+              mach_control=True, mach_control_target=0.25, viscosity=7.5e-4,
+              hyperviscosity_mn=0.002, large_scale_drag=0.10, cooling_time=5.0, precision="fp64")
+    out = {"workload": "hit_production_512x512, reference NumPy noise stream, FP64"}
+    st = torch.cuda.current_stream()
+    for mode, k in (("numpy", steps), ("numpy-host", max(steps // 5, 5))):
+        s = HITSolver(HIT2DConfig(forcing_noise=mode, **kw))
+        s.advance(3)
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(st)
+        s.advance(k)
+        b.record(st)
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(b) / k
+        out[mode] = {"ms_per_step": ms, "value": NX * NY / (ms / 1e3), "unit": "cell-updates/s",
+                     "steps": k}
+        del s
+    out["speedup_device_stream"] = out["numpy-host"]["ms_per_step"] / out["numpy"]["ms_per_step"]
+    with tempfile.TemporaryDirectory() as tmp:
+        cfg = HIT2DConfig(forcing_noise="numpy", max_steps=60, diagnostics_every=10 ** 6,
+                          snapshot_every=10 ** 6, output_dir=Path(tmp), **kw)
+        import contextlib
+        import io
+
+        t0 = time.perf_counter()
+        with contextlib.redirect_stdout(io.StringIO()):
+            run_simulation(cfg)
+        torch.cuda.synchronize()
+        out["run_simulation_60_steps_s"] = time.perf_counter() - t0
+    return out
 
 
 def serving_run(args):

@@ -29,7 +29,7 @@ S_ALPHA_X, S_ALPHA_Y, S_DIV_RMS, S_VORT_RMS, S_DT, S_TIME, S_STEP, S_ACTIVE, S_M
  S_NEAR_THRESHOLD, S_HV_APPLIED) = range(9, 25)
 S_COUNT = 32
 # bits of the S_STATUS slot (HITB200_ST_*)
-ST_NONFINITE, ST_NONPOS_RHO, ST_NONPOS_P, ST_BARRIER = 1, 2, 4, 8
+ST_NONFINITE, ST_NONPOS_RHO, ST_NONPOS_P, ST_BARRIER, ST_NOISE = 1, 2, 4, 8, 16
 TUNE_SWEEP_X, TUNE_SWEEP_Y, TUNE_PREPASS, TUNE_FUSED_SENSOR, TUNE_COUNT = 0, 1, 2, 3, 4
 
 NAN = float("nan")
@@ -151,6 +151,9 @@ SIGNATURES = [
     ("hitb200_save_state_block", ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_double), ctypes.c_size_t]),
     ("hitb200_load_state_block", ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_double), ctypes.c_size_t]),
     ("hitb200_set_barrier_test", ctypes.c_int, [ctypes.c_int32, ctypes.c_double]),
+    ("hitb200_set_noise_stream", ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_uint64)]),
+    ("hitb200_get_noise_stream", ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_uint64)]),
+    ("hitb200_noise_field", ctypes.c_int, [_VP, _DP, _VP]),
     ("hitb200_spectral_workspace_bytes", ctypes.c_size_t, [ctypes.c_int32, ctypes.c_int32]),
     ("hitb200_spectral_diagnostics", ctypes.c_int,
      [_VP, _DP, ctypes.c_double, ctypes.POINTER(ctypes.c_double), _DP, _DP, _DP, ctypes.c_size_t, _VP]),
@@ -211,6 +214,8 @@ def check_step_status(bits: int, label: str) -> None:
     bits = int(bits)
     if bits & ST_BARRIER:
         raise RuntimeError(f"{label}: a grid barrier of the fused prepass/sensor timed out")
+    if bits & ST_NOISE:
+        raise RuntimeError(f"{label}: the device forcing-noise stream ran short of draws")
     if bits & ST_NONFINITE:
         raise FloatingPointError(f"NaN or infinite value detected in {label}")
 

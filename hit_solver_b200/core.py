@@ -167,6 +167,23 @@ class Plan:
         _lib.check(self.lib.hitb200_read_scalars(self.handle, buf, n))
         return list(buf)
 
+    def set_noise_stream(self, pcg64_state: dict) -> None:
+        """Continue a NumPy PCG64 stream (``bit_generator.state``) on the device
+        (noise_mode 2 plans)."""
+        st = pcg64_state["state"]
+        mask = (1 << 64) - 1
+        words = (ctypes.c_uint64 * 4)(st["state"] & mask, st["state"] >> 64, st["inc"] & mask,
+                                      st["inc"] >> 64)
+        _lib.check(self.lib.hitb200_set_noise_stream(self.handle, words))
+
+    def noise_stream(self) -> dict:
+        """The device noise stream's position as a NumPy PCG64 state dict."""
+        words = (ctypes.c_uint64 * 4)()
+        _lib.check(self.lib.hitb200_get_noise_stream(self.handle, words))
+        return {"bit_generator": "PCG64",
+                "state": {"state": words[0] | (words[1] << 64), "inc": words[2] | (words[3] << 64)},
+                "has_uint32": 0, "uinteger": 0}
+
     def save_state_block(self):
         """The whole device scalar block (time, step, controller and forcing
         state, OU potential): with the state q, a checkpoint of the solve."""

@@ -20,6 +20,7 @@
 #include "common.cuh"
 #include "kernels_fft.cuh"
 #include "kernels_init.cuh"
+#include "kernels_npnoise.cuh"
 #include "kernels_reduce.cuh"
 #include "kernels_spectra.cuh"
 #include "kernels_stencil.cuh"
@@ -28,7 +29,8 @@
 using namespace hitb200;
 
 static_assert(ST_NONFINITE == HITB200_ST_NONFINITE && ST_NONPOS_RHO == HITB200_ST_NONPOS_RHO &&
-                  ST_NONPOS_P == HITB200_ST_NONPOS_P && ST_BARRIER == HITB200_ST_BARRIER,
+                  ST_NONPOS_P == HITB200_ST_NONPOS_P && ST_BARRIER == HITB200_ST_BARRIER &&
+                  ST_NOISE == HITB200_ST_NOISE,
               "status bits of the device code and of the C ABI must agree");
 
 namespace {
@@ -331,6 +333,8 @@ struct hitb200_plan {
   bool fuse_ok = false;  // all of the fused sensor's CTAs fit on the GPU at once
   int sensor_w = -1;          // width of the step sensor instantiation (-1: generic sensor)
   size_t smem_sensor_step = 0;
+  bool has_gen = false;       // the reference's noise stream generated on the device (noise_mode 2)
+  NoiseBufs gen{};
 };
 
 struct hitb200_batch {
@@ -371,6 +375,8 @@ struct LaunchSet {
   size_t smem_x, smem_y, smem_sensor;
   int sensor_w;             // step sensor instantiation shared by the solves (-1: generic)
   size_t smem_sensor_step;
+  const NoiseBufs* gen = nullptr;  // single plans of noise_mode 2: the noise stream's buffers
+  double* gen_out = nullptr;       // ... and the noise field they fill
   cudaStream_t st;
   // cells of all solves, and of the solves carrying viscous / forcing terms
   double cells = 0, cells_visc = 0, cells_force = 0;
@@ -579,6 +585,20 @@ void launch_prepass(const LaunchSet& L, int buf, int mode, int enf, const Bind& 
 #undef HB_PRE
 }
 
+// The reference's forcing-noise field of the step from its PCG64 stream
+// (kernels_npnoise.cuh), into the solve's noise buffer.
+void launch_noise_gen(const LaunchSet& L) {
+  const NoiseBufs& b = *L.gen;
+  const int per = kNoiseThreads * kNoiseChunk;
+  const int nblk = (int)((b.P + per - 1) / per);
+  npnoise_classify_kernel<<<nblk, kNoiseThreads, 0, L.st>>>(L.solves, b, S_PCG);
+  npnoise_scan_kernel<<<1, 1024, 0, L.st>>>(L.solves, b, nblk);
+  npnoise_compact_kernel<<<nblk, kNoiseThreads, 0, L.st>>>(L.solves, b);
+  npnoise_resolve_kernel<<<1, kNoiseResolveThreads, 0, L.st>>>(L.solves, b);
+  npnoise_scatter_kernel<<<nblk, kNoiseThreads, 0, L.st>>>(L.solves, b, L.gen_out, (long long)L.cells,
+                                                           S_PCG);
+}
+
 // The reference's loop body (OOP/hit2d.py:828-879; riemann_config3.py:728-740).
 int launch_step_sequence(const LaunchSet& L, int any_forcing, int noise_upload, int any_outflow,
                          int any_hv, Prof* prof = nullptr) {
@@ -592,7 +612,11 @@ int launch_step_sequence(const LaunchSet& L, int any_forcing, int noise_upload, 
     launch_prepass(L, 0, PRE_STEP, 1, nb);
   }
   if (any_forcing) {
-    if (noise_upload) {
+    if (L.gen) {
+      PMARK("noise_gen", 8 * L.cells_force);
+      launch_noise_gen(L);
+    }
+    if (noise_upload || L.gen) {
       PMARK("noise_dft", 8 * L.cells_force);
       noise_dft_kernel<<<L.n_tiles32, kRedThreads, 0, L.st>>>(L.solves, L.tiles32, nb);
     } else {
@@ -692,6 +716,8 @@ LaunchSet plan_launch_set(hitb200_plan* p, cudaStream_t st) {
   L.smem_x = p->smem_x;
   L.smem_y = p->smem_y;
   L.smem_sensor = p->smem_sensor;
+  L.gen = p->has_gen ? &p->gen : nullptr;
+  L.gen_out = p->has_gen ? const_cast<double*>(p->hs.noise) : nullptr;
   L.sensor_w = p->sensor_w;
   L.smem_sensor_step = p->smem_sensor_step;
   L.st = st;
@@ -749,6 +775,7 @@ int validate_desc(const hitb200_desc* d) {
   if (d->sensor_width < 0 || d->sensor_width > kMaxWidth)
     return (g_last_error = "sensor width must be in [0, 8]", HITB200_ERR_UNSUPPORTED);
   if (d->hv_interval < 0) return invalid("hyperviscosity_interval must be >= 0");
+  if (d->noise_mode < 0 || d->noise_mode > 2) return invalid("noise_mode must be 0, 1 or 2");
   if (!d->periodic && (d->guard_cells < 0)) return invalid("guard_cells must be >= 0");
   if (!d->periodic && d->guard_cells > 0 && (d->nx <= 2 * d->guard_cells || d->ny <= 2 * d->guard_cells))
     return invalid("state is too small for the requested guard cells");
@@ -849,6 +876,57 @@ size_t hitb200_cached_block_bytes(void) {
   return g_blocks_bytes;
 }
 
+}  // extern "C"
+
+namespace {
+// Buffers of the device noise stream for N normals (kernels_npnoise.cuh).
+long long noise_gen_positions(size_t N) { return (long long)N + (long long)N / 8 + 4096; }
+size_t noise_gen_bytes(size_t N) {
+  const size_t P = (size_t)noise_gen_positions(N);
+  const size_t nblk = (P + kNoiseThreads * kNoiseChunk - 1) / (kNoiseThreads * kNoiseChunk);
+  // val, deficit (8 B), slow, reach (4 B), cons, outf, visited (1 B), counts, offsets
+  return 8 * P * 2 + 4 * P * 2 + 3 * P + 4 * (2 * nblk + 1) + 4 + 64 * 8;
+}
+NoiseBufs noise_gen_layout(unsigned char* base, size_t N) {
+  NoiseBufs b{};
+  const size_t P = (size_t)noise_gen_positions(N);
+  const size_t nblk = (P + kNoiseThreads * kNoiseChunk - 1) / (kNoiseThreads * kNoiseChunk);
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    unsigned char* q = base + off;
+    off = (off + bytes + 7) & ~(size_t)7;
+    return q;
+  };
+  b.val = reinterpret_cast<double*>(take(8 * P));
+  b.deficit = reinterpret_cast<long long*>(take(8 * P));
+  b.slow = reinterpret_cast<unsigned*>(take(4 * P));
+  b.reach = reinterpret_cast<unsigned*>(take(4 * P));
+  b.cons = take(P);
+  b.outf = take(P);
+  b.visited = take(P);
+  b.cta_count = reinterpret_cast<unsigned*>(take(4 * nblk));
+  b.cta_off = reinterpret_cast<unsigned*>(take(4 * (nblk + 1)));
+  b.nslow = reinterpret_cast<unsigned*>(take(4));
+  b.P = (long long)P;
+  return b;
+}
+
+// The ziggurat table of the device noise stream, once per device.
+cudaError_t upload_zig_tables() {
+  static bool done[kMaxAttrDevices] = {};
+  const int dev = attr_device();
+  std::lock_guard<std::mutex> lock(g_attr_mu);
+  if (done[dev]) return cudaSuccess;
+  cudaError_t e = cudaMemcpyToSymbol(g_zig_w, zig::kZigW, sizeof(zig::kZigW));
+  if (e == cudaSuccess) e = cudaMemcpyToSymbol(g_zig_k, zig::kZigK, sizeof(zig::kZigK));
+  if (e == cudaSuccess) e = cudaMemcpyToSymbol(g_zig_f, zig::kZigF, sizeof(zig::kZigF));
+  if (e == cudaSuccess) done[dev] = true;
+  return e;
+}
+}  // namespace
+
+extern "C" {
+
 size_t hitb200_plan_device_bytes(const hitb200_desc* d) {
   if (validate_desc(d) != HITB200_OK) return 0;
   const size_t N = (size_t)d->nx * d->ny;
@@ -863,7 +941,8 @@ size_t hitb200_plan_device_bytes(const hitb200_desc* d) {
   if (d->viscosity > 0.0) a.take(3 * N * elem);              // vis
   a.take(N);                                                 // mask
   if (d->forcing_on) a.take(2 * N * sizeof(double));         // fx, fy
-  if (d->forcing_on && d->noise_mode == 0) a.take(N * sizeof(double));
+  if (d->forcing_on && d->noise_mode != 1) a.take(N * sizeof(double));
+  if (d->forcing_on && d->noise_mode == 2) a.take(noise_gen_bytes(N));
   a.take((d->nx + d->ny) * sizeof(double2));
   a.take((mt.drag.size() + mt.force.size() + 1) * sizeof(int2));
   a.take((mt.force.size() + 1) * sizeof(double2));
@@ -934,7 +1013,8 @@ int hitb200_plan_create(const hitb200_desc* d, hitb200_plan** out) {
   const size_t o_mask = a.take(N);
   const size_t o_fx = d->forcing_on ? a.take(N * p->elem) : 0;
   const size_t o_fy = d->forcing_on ? a.take(N * p->elem) : 0;
-  const size_t o_noise = (d->forcing_on && d->noise_mode == 0) ? a.take(N * sizeof(double)) : 0;
+  const size_t o_noise = (d->forcing_on && d->noise_mode != 1) ? a.take(N * sizeof(double)) : 0;
+  const size_t o_gen = (d->forcing_on && d->noise_mode == 2) ? a.take(noise_gen_bytes(N)) : 0;
   const size_t o_tw = a.take((nx + ny) * sizeof(double2));
   const size_t o_modes = a.take((mt.drag.size() + mt.force.size() + 1) * sizeof(int2));
   const size_t o_kvec = a.take((mt.force.size() + 1) * sizeof(double2));
@@ -1042,6 +1122,16 @@ int hitb200_plan_create(const hitb200_desc* d, hitb200_plan** out) {
   s.fx = d->forcing_on ? reinterpret_cast<void*>(base + o_fx) : nullptr;
   s.fy = d->forcing_on ? reinterpret_cast<void*>(base + o_fy) : nullptr;
   s.noise = o_noise ? reinterpret_cast<double*>(base + o_noise) : nullptr;
+  if (o_gen) {
+    p->has_gen = true;
+    p->gen = noise_gen_layout(base + o_gen, N);
+    const cudaError_t ze = upload_zig_tables();
+    if (ze != cudaSuccess) {
+      block_free(p->arena_block);
+      delete p;
+      return cuda_fail(ze, "cudaMemcpyToSymbol(ziggurat tables)");
+    }
+  }
   s.twx = reinterpret_cast<double2*>(base + o_tw);
   s.twy = s.twx + nx;
   s.modes = reinterpret_cast<int2*>(base + o_modes);
@@ -1393,7 +1483,7 @@ int hitb200_run(hitb200_plan* p, double* q, int32_t nsteps, void* stream) {
   if (p->in_batch) return invalid("plan belongs to a batch; use hitb200_batch_run");
   if (nsteps < 0) return invalid("nsteps must be >= 0");
   if (p->desc.forcing_on && p->desc.noise_mode == 0)
-    return invalid("hitb200_run needs noise_mode 1 (device noise) when forcing is on");
+    return invalid("hitb200_run needs noise_mode 1 or 2 (device noise) when forcing is on");
   cudaStream_t st = (cudaStream_t)stream;
   int r = bind_state(p, q, st);
   if (r != HITB200_OK) return r;
@@ -1442,6 +1532,38 @@ int hitb200_copy_scalars_async(hitb200_plan* p, double* dst, int32_t n, void* st
 }
 
 size_t hitb200_state_block_size(void) { return (size_t)SCAL_SIZE; }
+
+int hitb200_set_noise_stream(hitb200_plan* p, const uint64_t* stream_state) {
+  if (!p || !stream_state) return invalid("NULL argument");
+  if (!p->has_gen) return invalid("the plan has no device noise stream (noise_mode 2 with forcing)");
+  double v[4];
+  static_assert(sizeof(double) == sizeof(uint64_t), "64-bit slots");
+  std::memcpy(v, stream_state, sizeof(v));
+  HB_CUDA(cudaDeviceSynchronize());
+  HB_CUDA(cudaMemcpy(p->hs.scal + S_PCG, v, sizeof(v), cudaMemcpyHostToDevice));
+  return HITB200_OK;
+}
+
+int hitb200_noise_field(hitb200_plan* p, double* out, void* stream) {
+  if (!p || !out) return invalid("NULL argument");
+  if (!p->has_gen) return invalid("the plan has no device noise stream (noise_mode 2 with forcing)");
+  if (p->in_batch) return invalid("plan belongs to a batch");
+  LaunchSet L = plan_launch_set(p, (cudaStream_t)stream);
+  L.gen_out = out;
+  launch_noise_gen(L);
+  HB_LAUNCHED("noise stream");
+  return HITB200_OK;
+}
+
+int hitb200_get_noise_stream(hitb200_plan* p, uint64_t* stream_state) {
+  if (!p || !stream_state) return invalid("NULL argument");
+  if (!p->has_gen) return invalid("the plan has no device noise stream (noise_mode 2 with forcing)");
+  double v[4];
+  HB_CUDA(cudaDeviceSynchronize());
+  HB_CUDA(cudaMemcpy(v, p->hs.scal + S_PCG, sizeof(v), cudaMemcpyDeviceToHost));
+  std::memcpy(stream_state, v, sizeof(v));
+  return HITB200_OK;
+}
 
 int hitb200_save_state_block(hitb200_plan* p, double* out, size_t n) {
   if (!p || !out) return invalid("NULL argument");
@@ -1575,10 +1697,10 @@ static int batch_build(hitb200_batch* b) {
     b->any_outflow |= !p->desc.periodic;
     b->any_forcing |= p->desc.forcing_on;
     b->any_hv |= p->hs.hv_interval > 0;
-    b->any_noise_upload |= (p->desc.forcing_on && p->desc.noise_mode == 0);
+    b->any_noise_upload |= (p->desc.forcing_on && p->desc.noise_mode != 1);
   }
   mark();
-  if (b->any_noise_upload) return invalid("batched solves draw forcing noise on the device (noise_mode 1)");
+  if (b->any_noise_upload) return invalid("batched solves draw forcing noise with the device RNG (noise_mode 1)");
   b->n_tiles = (int)tiles.size();
   b->n_tiles32 = (int)tiles32.size();
   b->n_x = (int)xl.size();

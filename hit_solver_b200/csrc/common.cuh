@@ -70,11 +70,14 @@ enum Scal : int {
   S_DRAG = 64,       // 4 per drag mode: c * Re/Im of the rho*u and rho*v mode sums
   S_PHI = S_DRAG + 4 * kMaxDrag,          // OU potential: 2 per forcing mode
   S_XI = S_PHI + 2 * kMaxForce,           // noise DFT of the step: 2 per mode
-  SCAL_SIZE = S_XI + 2 * kMaxForce,
+  // PCG64 stream of the reference's forcing noise (noise_mode 2): the bit
+  // patterns of state.lo, state.hi, inc.lo, inc.hi
+  S_PCG = S_XI + 2 * kMaxForce,
+  SCAL_SIZE = S_PCG + 4,
 };
 
 // Status bits accumulated in S_STATUS.
-enum StatusBits : int { ST_NONFINITE = 1, ST_NONPOS_RHO = 2, ST_NONPOS_P = 4, ST_BARRIER = 8 };
+enum StatusBits : int { ST_NONFINITE = 1, ST_NONPOS_RHO = 2, ST_NONPOS_P = 4, ST_BARRIER = 8, ST_NOISE = 16 };
 
 // ---- per-solve descriptor (device resident, read-only in kernels) -------------
 struct SolveDev {

@@ -23,6 +23,7 @@ namespace hitb200 {
 
 constexpr int kFftMaxN = 1024;
 constexpr int kFftThreads = 256;
+constexpr int kFftMaxButterfly = 7;  // radices up to this are whole butterflies per thread
 
 struct FftRadices {
   int count;
@@ -90,22 +91,72 @@ __global__ void __launch_bounds__(kFftThreads)
   int Ns = 1;
   for (int s = 0; s < rad.count; ++s) {
     const int R = rad.r[s], m = n / R, step = n / (Ns * R);
-    for (int idx = threadIdx.x; idx < n * C; idx += blockDim.x) {
-      const int o = idx / C, c = idx - o * C;
-      const int j = o % m, t = o / m;
-      const int k = j % Ns;
-      const int e1 = k * step + t * m;  // < n
-      double re = 0.0, im = 0.0;
-      int e = 0;
-      for (int r = 0; r < R; ++r) {
-        const double2 x = a[(j + r * m) * C + c];
-        const double2 tw = w[e];
-        re = fma(x.x, tw.x, fma(-x.y, tw.y, re));
-        im = fma(x.x, tw.y, fma(x.y, tw.x, im));
-        e += e1;
-        if (e >= n) e -= n;
+    if (R <= kFftMaxButterfly) {
+      // one butterfly per thread: the R inputs j + r m, twiddled by
+      // W^{r k step}, transformed together, written to the R outputs
+      for (int idx = threadIdx.x; idx < m * C; idx += blockDim.x) {
+        const int j = idx / C, c = idx - j * C;
+        const int k = j % Ns;
+        const int out0 = (j - k) * R + k;  // (j / Ns) Ns R + k
+        double2 v[kFftMaxButterfly];
+        v[0] = a[j * C + c];
+        const int tk = k * step;  // r tk < n for r < R
+#pragma unroll
+        for (int r = 1; r < kFftMaxButterfly; ++r) {
+          if (r >= R) break;
+          const double2 x = a[(j + r * m) * C + c];
+          const double2 tw = w[r * tk];
+          v[r] = make_double2(fma(x.x, tw.x, -x.y * tw.y), fma(x.x, tw.y, x.y * tw.x));
+        }
+        if (R == 2) {
+          b[out0 * C + c] = make_double2(v[0].x + v[1].x, v[0].y + v[1].y);
+          b[(out0 + Ns) * C + c] = make_double2(v[0].x - v[1].x, v[0].y - v[1].y);
+        } else if (R == 4) {
+          // W_4 = -i (forward) / +i (inverse), applied exactly
+          const double2 s0 = make_double2(v[0].x + v[2].x, v[0].y + v[2].y);
+          const double2 s1 = make_double2(v[0].x - v[2].x, v[0].y - v[2].y);
+          const double2 s2 = make_double2(v[1].x + v[3].x, v[1].y + v[3].y);
+          const double2 d = make_double2(v[1].x - v[3].x, v[1].y - v[3].y);
+          const double2 s3 = sign < 0 ? make_double2(d.y, -d.x) : make_double2(-d.y, d.x);
+          b[out0 * C + c] = make_double2(s0.x + s2.x, s0.y + s2.y);
+          b[(out0 + Ns) * C + c] = make_double2(s1.x + s3.x, s1.y + s3.y);
+          b[(out0 + 2 * Ns) * C + c] = make_double2(s0.x - s2.x, s0.y - s2.y);
+          b[(out0 + 3 * Ns) * C + c] = make_double2(s1.x - s3.x, s1.y - s3.y);
+        } else {
+          // small odd radix: y_t = sum_r v_r W^{r t m}
+          for (int t = 0; t < R; ++t) {
+            double re = 0.0, im = 0.0;
+            int e = 0;
+            for (int r = 0; r < R; ++r) {
+              const double2 tw = w[e];
+              re = fma(v[r].x, tw.x, fma(-v[r].y, tw.y, re));
+              im = fma(v[r].x, tw.y, fma(v[r].y, tw.x, im));
+              e += t * m;
+              if (e >= n) e -= n;
+            }
+            b[(out0 + t * Ns) * C + c] = make_double2(re, im);
+          }
+        }
       }
-      b[((j / Ns) * Ns * R + k + t * Ns) * C + c] = make_double2(re, im);
+    } else {
+      // a large prime radix: one output per thread, R terms each
+      for (int idx = threadIdx.x; idx < n * C; idx += blockDim.x) {
+        const int o = idx / C, c = idx - o * C;
+        const int j = o % m, t = o / m;
+        const int k = j % Ns;
+        const int e1 = k * step + t * m;  // < n
+        double re = 0.0, im = 0.0;
+        int e = 0;
+        for (int r = 0; r < R; ++r) {
+          const double2 x = a[(j + r * m) * C + c];
+          const double2 tw = w[e];
+          re = fma(x.x, tw.x, fma(-x.y, tw.y, re));
+          im = fma(x.x, tw.y, fma(x.y, tw.x, im));
+          e += e1;
+          if (e >= n) e -= n;
+        }
+        b[((j / Ns) * Ns * R + k + t * Ns) * C + c] = make_double2(re, im);
+      }
     }
     __syncthreads();
     double2* tmp = a;

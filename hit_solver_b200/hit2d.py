@@ -29,14 +29,17 @@ from .run_utils import dataclass_to_json_dict, write_json
 from .spatial_operator import PeriodicEulerShockSensor2D
 
 DEFAULT_SNAPSHOT_DIR = Path("2D") / "hit2d_snapshots"
+NOISE_MODES = ("numpy", "numpy-host", "device")
 
 
 @dataclass(frozen=True)
 class HIT2DConfig:
     """Fields and defaults of OOP/hit2d.py:36-80; ``backend`` defaults to
     "b200".  Additive fields: ``precision`` ("fp64" plain form or "fp32-bulk"),
-    ``forcing_noise`` ("numpy": the reference's RNG stream, uploaded each
-    step; "device": drawn on the device), ``max_steps`` (stop after this
+    ``forcing_noise`` ("numpy": the reference's NumPy stream, continued on
+    the device draw for draw; "numpy-host": the same stream drawn by NumPy on
+    the host and uploaded each step; "device": shell noise drawn with a
+    counter-based RNG on the device), ``max_steps`` (stop after this
     many steps even before tfinal) and ``initial_condition`` ("host": the
     reference's NumPy arithmetic, bit for bit; "device": the same phases,
     synthesised on the GPU, equal to roundoff)."""
@@ -462,7 +465,7 @@ def hit_descriptor(config: HIT2DConfig, domain: Domain2D) -> _lib.Desc:
     d.mach_max_power = _lib.none_to_nan(config.mach_control_max_power)
     d.cfl, d.tfinal = config.cfl, config.tfinal
     d.fixed_dt = 0
-    d.noise_mode = 0 if config.forcing_noise == "numpy" else 1
+    d.noise_mode = {"numpy": 2, "numpy-host": 0, "device": 1}[config.forcing_noise]
     d.seed = int(config.forcing_seed) + 1
     return d
 
@@ -528,8 +531,8 @@ class HITSolver:
             raise ValueError("hyperviscosity_interval must be positive when mn > 0")
         select_array_module(config.backend)
         precision_code(config.precision)
-        if config.forcing_noise not in ("numpy", "device"):
-            raise ValueError("forcing_noise must be 'numpy' or 'device'")
+        if config.forcing_noise not in NOISE_MODES:
+            raise ValueError(f"forcing_noise must be one of {NOISE_MODES}")
         if config.initial_condition not in ("host", "device"):
             raise ValueError("initial_condition must be 'host' or 'device'")
         self.config = config
@@ -543,12 +546,16 @@ class HITSolver:
         self.q = self.equation.enforce_physical_state(q)
         self.plan.set_time(0.0, 0, 0.0, -1 if config.max_steps is None else config.max_steps)
         if config.forcing_noise == "numpy":
+            # the reference's stream (default_rng(seed + 1), OOP/hit2d.py:791-803),
+            # continued on the device draw for draw
+            self.plan.set_noise_stream(self.noise_rng.bit_generator.state)
+        if config.forcing_noise == "numpy-host":
             self._noise_dev = torch.empty((config.ny, config.nx), dtype=torch.float64, device="cuda")
             self._noise_host = torch.empty((config.ny, config.nx), dtype=torch.float64).pin_memory()
 
     def advance(self, nsteps: int) -> None:
         """Issue nsteps steps; steps past tfinal / max_steps are device no-ops."""
-        if self.config.forcing_noise == "numpy":
+        if self.config.forcing_noise == "numpy-host":
             for _ in range(nsteps):
                 self._noise_host.numpy()[...] = self.noise_rng.standard_normal(
                     (self.config.ny, self.config.nx))
@@ -569,7 +576,7 @@ class HITSolver:
         the run bit for bit."""
         torch.cuda.synchronize()
         ck = {"q": self.q.detach().cpu().clone(), "block": self.plan.save_state_block()}
-        if self.config.forcing_noise == "numpy":
+        if self.config.forcing_noise == "numpy-host":
             ck["noise_rng"] = self.noise_rng.bit_generator.state
         return ck
 
@@ -691,7 +698,7 @@ def parse_args(argv=None) -> argparse.Namespace:
     p.add_argument("--backend", choices=("auto", "numpy", "cupy", "b200"), default="b200")
     p.add_argument("--no-forcing", action="store_true")
     p.add_argument("--precision", choices=("fp64", "fp32-bulk"), default="fp64")
-    p.add_argument("--forcing-noise", choices=("numpy", "device"), default="numpy")
+    p.add_argument("--forcing-noise", choices=NOISE_MODES, default="numpy")
     p.add_argument("--max-steps", type=int, default=None)
     return p.parse_args(argv)
 

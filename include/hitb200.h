@@ -90,7 +90,9 @@ typedef struct hitb200_desc {
   /* time stepping */
   double cfl, tfinal;
   int32_t fixed_dt;   /* 1: dt fixed by hitb200_set_time (Riemann); 0: CFL dt each step (HIT) */
-  int32_t noise_mode; /* 0: forcing noise fields uploaded by the caller; 1: device RNG */
+  int32_t noise_mode; /* 0: forcing noise fields uploaded by the caller; 1: device RNG;
+                         2: the reference's NumPy stream (PCG64 + ziggurat normals) generated
+                         on the device from a state set by hitb200_set_noise_stream */
   uint64_t seed;      /* device RNG seed (noise_mode 1) */
 } hitb200_desc;
 
@@ -131,6 +133,8 @@ enum hitb200_scalar {
 #define HITB200_ST_NONPOS_P 4     /* raw pressure <= 0 (validation)              */
 #define HITB200_ST_BARRIER 8      /* a fused prepass/sensor grid barrier timed out
                                      (about 2 s); that step's results are invalid */
+#define HITB200_ST_NOISE 16       /* the device noise stream ran short of draws
+                                     (noise_mode 2; never expected) */
 
 /* ---- plan ---------------------------------------------------------------- */
 /* Defaults of HIT2DConfig (OOP/hit2d.py:36-80) on a 2*pi periodic square. */
@@ -266,6 +270,18 @@ int hitb200_copy_scalars_async(hitb200_plan* plan, double* dst, int32_t n, void*
 size_t hitb200_state_block_size(void);
 int hitb200_save_state_block(hitb200_plan* plan, double* out, size_t n);
 int hitb200_load_state_block(hitb200_plan* plan, const double* in, size_t n);
+/* The PCG64 state of a noise_mode 2 plan's forcing-noise stream: {state low
+ * 64 bits, state high, increment low, increment high}, as NumPy's
+ * PCG64.state holds them.  Each step then draws standard_normal((ny, nx))
+ * from it draw for draw as numpy.random.Generator.standard_normal does
+ * (OOP/forcing.py:66,77) and advances it past the draws used.  Both
+ * synchronise. */
+int hitb200_set_noise_stream(hitb200_plan* plan, const uint64_t* stream_state);
+int hitb200_get_noise_stream(hitb200_plan* plan, uint64_t* stream_state);
+/* One standard_normal((ny, nx)) field of that stream into out (device
+ * double [ny][nx]), advancing it: the field the next step would draw.
+ * Stream ordered.  A no-op while the plan's solve is inactive (past its end). */
+int hitb200_noise_field(hitb200_plan* plan, double* out, void* stream);
 /* Failure injection for the fused prepass/sensor's grid barrier, a test hook
  * with no reference counterpart: the barrier waits for extra_arrivals (0 or
  * 1) CTAs beyond its launch and gives up after limit_seconds of the global

@@ -19,7 +19,10 @@ import numpy as np
 import pytest
 
 GOLD = Path(__file__).resolve().parent / "golden"
-RTOL = 1e-9
+# the FP64 tolerance of the parity tests for states after short runs (relative
+# to the largest magnitude of the compared array); derived fields (vorticity)
+# carry the state's roundoff differences divided by the mesh width
+RTOL = 1e-8
 
 
 def _collect(tmp: Path) -> dict:
