@@ -206,6 +206,27 @@ __device__ __forceinline__ void enforce_node_rcp(T& q0, T& q1, T& q2, T& q3, T g
   q2 = rho * v;
   q3 = p > T(kPFloor) ? q3 : T(kPFloor) / (gamma - T(1)) + kin;
 }
+// 1 / x correctly rounded: the same value as the division, in fewer
+// instructions for FP32
+template <typename T>
+__device__ __forceinline__ T rcp_rn(T x) {
+  if constexpr (sizeof(T) == 4) return __frcp_rn(x);
+  else return 1.0 / x;
+}
+
+// the same with the floor energy kPFloor / (gamma - 1) computed by the caller
+template <typename T>
+__device__ __forceinline__ void enforce_node_rcp(T& q0, T& q1, T& q2, T& q3, T gamma, T pfl) {
+  const T rho = q0 > T(kRhoFloor) ? q0 : T(kRhoFloor);
+  const T rinv = T(1) / rho;
+  const T u = q1 * rinv, v = q2 * rinv;
+  const T kin = T(0.5) * rho * (u * u + v * v);
+  const T p = (gamma - T(1)) * (q3 - kin);
+  q0 = rho;
+  q1 = rho * u;
+  q2 = rho * v;
+  q3 = p > T(kPFloor) ? q3 : pfl + kin;
+}
 
 // Programmatic dependent launch.  A kernel launched with programmatic stream
 // serialization may start while the previous kernel of the stream finishes:

@@ -738,6 +738,44 @@ __device__ __forceinline__ void gload_run(const T* p, int len, T (&v)[N]) {
 //   stage 2:      clean(1/3 q + 2/3 (q2 + dt L))     (OOP/time_operator.py:21-26)
 // with L = -dF/dx - dG/dy + viscous + forcing + drag + cooling and clean the
 // enforce filter plus, on outflow grids, the guard cells.
+// V consecutive elements (V = 1 or 2) in one access; V = 2 needs a pointer
+// aligned to 2 elements.
+template <int V>
+struct VecWidth {
+  static constexpr int value = V;
+};
+template <typename E>
+struct Vec2Of;
+template <>
+struct Vec2Of<double> {
+  using type = double2;
+};
+template <>
+struct Vec2Of<float> {
+  using type = float2;
+};
+template <int V, typename E>
+__device__ __forceinline__ void vld(const E* p, E (&v)[V]) {
+  if constexpr (V == 2) {
+    const typename Vec2Of<E>::type t = *reinterpret_cast<const typename Vec2Of<E>::type*>(p);
+    v[0] = t.x;
+    v[1] = t.y;
+  } else {
+    v[0] = *p;
+  }
+}
+template <int V, typename E>
+__device__ __forceinline__ void vst(E* p, const E (&v)[V]) {
+  if constexpr (V == 2) {
+    typename Vec2Of<E>::type t;
+    t.x = v[0];
+    t.y = v[1];
+    *reinterpret_cast<typename Vec2Of<E>::type*>(p) = t;
+  } else {
+    *p = v[0];
+  }
+}
+
 template <typename T, int AXIS, int MN, int OCC>
 __global__ void __launch_bounds__(AXIS == 0 ? 256 : 512,
                                   AXIS == 0 ? (OCC ? kSweepMinBlocksX : 2) : (OCC ? kSweepMinBlocksY : 1))
@@ -774,6 +812,7 @@ __global__ void __launch_bounds__(AXIS == 0 ? 256 : 512,
   // x lines: consecutive threads take consecutive nodes of a row; y lines:
   // consecutive threads take the R columns of a row, then the next row.
   const int nl = AXIS == 0 ? R * LS : (LS << rsh);
+  const T pfl = T(kPFloor) / (g - T(1));  // floor energy of enforce_physical_state
 #pragma unroll 4
   for (int idx = threadIdx.x; idx < nl; idx += blockDim.x) {
     int r, p;
@@ -791,13 +830,13 @@ __global__ void __launch_bounds__(AXIS == 0 ? 256 : 512,
       a3 = T(__ldcg(qin + o + 3 * plane));
     // enforce_physical_state, then primitive_from_conservative of the result
     const T rho = a0 > T(kRhoFloor) ? a0 : T(kRhoFloor);
-    const T rinv = T(1) / rho;
+    const T rinv = rcp_rn(rho);
     T u = a1 * rinv, v = a2 * rinv;
     const T kin = T(0.5) * rho * (u * u + v * v);
     T pr = (g - T(1)) * (a3 - kin);
     a1 = rho * u;
     a2 = rho * v;
-    a3 = pr > T(kPFloor) ? a3 : T(kPFloor) / (g - T(1)) + kin;
+    a3 = pr > T(kPFloor) ? a3 : pfl + kin;
     u = a1 * rinv;
     v = a2 * rinv;
     pr = (g - T(1)) * (a3 - T(0.5) * rho * (u * u + v * v));
@@ -871,9 +910,18 @@ __global__ void __launch_bounds__(AXIS == 0 ? 256 : 512,
     }
     const uint8_t* mk = MK + r * (n + 2) + 1;  // mk[i] = node i, i in [-1, n]
     const int il0 = ch * 32 - 2;
-    const int il = il0 + lane;
-    const bool need = il <= n && (flagged(mk, il - 1) || flagged(mk, il) || flagged(mk, il + 1));
-    const unsigned bal = __ballot_sync(kFull, need);
+    // Face il needs W when a flagged face lies among il - 1 .. il + 1, that
+    // is when one of the nodes il - 1 .. il + 2 is flagged (nodes outside
+    // [-1, n] count as unflagged; faces run over [-1, n - 1]).  Bit t of
+    // the 35-bit word nb is node il0 - 1 + t; bit `lane` of the OR of its
+    // four shifts is face il0 + lane's need.
+    const int j0 = il0 - 1 + lane, j1 = il0 + 31 + lane;
+    const unsigned b0 = __ballot_sync(kFull, j0 >= -1 && j0 <= n && mk[j0]);
+    const unsigned b1 = __ballot_sync(kFull, lane < 3 && j1 <= n && mk[j1]);
+    const unsigned long long nb = (unsigned long long)b0 | ((unsigned long long)b1 << 32);
+    const int nvalid = n - il0 + 1;  // faces il0 .. n
+    const unsigned valid = nvalid >= 32 ? kFull : (nvalid <= 0 ? 0u : (1u << nvalid) - 1u);
+    const unsigned bal = (unsigned)(nb | (nb >> 1) | (nb >> 2) | (nb >> 3)) & valid;
     const int items = 4 * __popc(bal);
     for (int k = lane; k < items; k += 32) {
       const int c = k & 3, f = il0 + nth_set_bit(bal, k >> 2);
@@ -995,10 +1043,11 @@ __global__ void __launch_bounds__(AXIS == 0 ? 256 : 512,
       for (int c = 0; c < 4; ++c) tot.a[c] = wj.m * tot.a[c] + wj.a[c];
       tot.m *= wj.m;
     }
+    // periodic: y_{-1} = y_{n-1} closes the cycle exactly
+    const T icyc = per ? T(1) / (T(1) - tot.m) : T(0);
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
-      // periodic: y_{-1} = y_{n-1} closes the cycle exactly
-      const T ybnd = per ? tot.a[c] / (T(1) - tot.m) : T(0);
+      const T ybnd = per ? tot.a[c] * icyc : T(0);
       const T yin = fe.m * (pre.m * ybnd + pre.a[c]) + fe.a[c];
       T pw = rho;
 #pragma unroll
@@ -1066,9 +1115,10 @@ __global__ void __launch_bounds__(AXIS == 0 ? 256 : 512,
       for (int c = 0; c < 4; ++c) tot.a[c] = wj.m * tot.a[c] + wj.a[c];
       tot.m *= wj.m;
     }
+    const T icyc = per ? T(1) / (T(1) - tot.m) : T(0);
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
-      const T zbnd = per ? tot.a[c] / (T(1) - tot.m) : T(0);
+      const T zbnd = per ? tot.a[c] * icyc : T(0);
       const T zin = be.m * (post.m * zbnd + post.a[c]) + be.a[c];
       T pw = rho;
 #pragma unroll
@@ -1237,104 +1287,174 @@ __global__ void __launch_bounds__(AXIS == 0 ? 256 : 512,
   const double2* __restrict__ twx = S.twx;
   const double* __restrict__ qinr = qin;
   const T* __restrict__ ryr = ry;
-  for (int idx = threadIdx.x; idx < R * n; idx += blockDim.x) {
-    const int rr = idx >= n ? 1 : 0, col = idx - rr * n, row = line0 + rr;
-    const size_t o = (size_t)row * nx + col;
-    double qa[4], rhs[4];
+  // Two consecutive nodes per thread with 16-byte (FP64) and 8-byte (FP32)
+  // vector accesses when the row length is even and every caller pointer is
+  // 16-byte aligned (arena buffers always are): half the load instructions
+  // and twice the bytes in flight per load.
+  const uintptr_t al = (uintptr_t)qinr | (uintptr_t)q0 | (uintptr_t)qo |
+                       (bind.use ? ((uintptr_t)bfx | (uintptr_t)bfy | (uintptr_t)bind.out) : 0);
+  const bool vec = (nx & 1) == 0 && (al & 15) == 0;
+  const double pfl64 = kPFloor / (gam - 1.0);
+  // The rhs terms are summed in the bulk type T (in the FP32-bulk form the
+  // sum is FP32, as every term is); FP64 takes over in the stage combine.
+  auto epilogue = [&](auto vt) {
+    constexpr int V = decltype(vt)::value;
+    const int pl = (int)plane;
+    // pass 1: the full rhs of every node in T, back into XS (the same thread
+    // reads it in pass 2); the FP64 stage combine runs as a separate pass so
+    // that neither pass holds the other's inputs in registers
+    for (int idx = threadIdx.x * V; idx < R * n; idx += blockDim.x * V) {
+      const int rr = idx >= n ? 1 : 0, col = idx - rr * n;
+      const int o = (line0 + rr) * nx + col;
+      T acc[4][V];
 #pragma unroll
-    for (int c = 0; c < 4; ++c) {
-      qa[c] = qinr[c * plane + o];
-      rhs[c] = double(ryr[c * plane + o]) - ((terms & 1) ? double(XS[(rr * 4 + c) * LW + col]) : 0.0);
-    }
-    if (visc) {
-      rhs[1] += double(visp[o]);
-      rhs[2] += double(visp[plane + o]);
-      rhs[3] += double(visp[2 * plane + o]);
-    }
-    if constexpr (sizeof(T) == 4) {
-      // FP32-bulk form: the forcing and drag sources in FP32 (they are rhs
-      // terms; FP64 stays in the stage combine below)
+      for (int c = 0; c < 4; ++c) {
+        vld<V>(ryr + c * pl + o, acc[c]);
+        if (terms & 1) {
+          T xs[V];
+          vld<V>(XS + (rr * 4 + c) * LW + col, xs);
+#pragma unroll
+          for (int v = 0; v < V; ++v) acc[c][v] -= xs[v];
+        }
+      }
+      if (visc) {
+#pragma unroll
+        for (int c = 1; c < 4; ++c) {
+          T vs[V];
+          vld<V>(visp + (c - 1) * pl + o, vs);
+#pragma unroll
+          for (int v = 0; v < V; ++v) acc[c][v] += vs[v];
+        }
+      }
       if (terms & (4 | 8)) {
-        const float prho = fmaxf(float(qa[0]), float(kRhoFloor));
-        const float prinv = __frcp_rn(prho);
-        const float pu = float(qa[1]) * prinv, pv = float(qa[2]) * prinv;
+        double q3[3][V];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) vld<V>(qinr + c * pl + o, q3[c]);
+        T tfx[V], tfy[V];
         if (terms & 4) {
-          const float ffs = float(fs);
-          const float tfx = bind.use ? float(bfx[o]) : ffs * float(sfx[o]);
-          const float tfy = bind.use ? float(bfy[o]) : ffs * float(sfy[o]);
-          rhs[1] += double(prho * tfx);
-          rhs[2] += double(prho * tfy);
-          rhs[3] += double(prho * (pu * tfx + pv * tfy));
-        }
-        if (drag) {
-          float lx = float(dpx[rr][0].x), ly = float(dpy[rr][0].x);
-          int ix = 0;
-          for (int kk = 1; kk <= kxd; ++kk) {
-            ix += col;
-            if (ix >= nx) ix -= nx;  // (k x) mod nx
-            const double2 e = twx[ix];
-            const float er = float(e.x), ei = -float(e.y);  // e^{+i k x}
-            lx += float(dpx[rr][kk].x) * er - float(dpx[rr][kk].y) * ei;
-            ly += float(dpy[rr][kk].x) * er - float(dpy[rr][kk].y) * ei;
+          if (bind.use) {
+            double fx2[V], fy2[V];
+            vld<V>(bfx + o, fx2);
+            vld<V>(bfy + o, fy2);
+#pragma unroll
+            for (int v = 0; v < V; ++v) {
+              tfx[v] = T(fx2[v]);
+              tfy[v] = T(fy2[v]);
+            }
+          } else {
+            vld<V>(sfx + o, tfx);
+            vld<V>(sfy + o, tfy);
+#pragma unroll
+            for (int v = 0; v < V; ++v) {
+              if constexpr (sizeof(T) == 4) {
+                tfx[v] = float(fs) * tfx[v];
+                tfy[v] = float(fs) * tfy[v];
+              } else {
+                tfx[v] = fs * tfx[v];
+                tfy[v] = fs * tfy[v];
+              }
+            }
           }
-          rhs[1] += double(lx);
-          rhs[2] += double(ly);
-          rhs[3] += double(pu * lx + pv * ly);
+        }
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+          // rho, u, v of primitive_from_conservative (one reciprocal)
+          T prho, pu, pv;
+          if constexpr (sizeof(T) == 4) {
+            prho = fmaxf(float(q3[0][v]), float(kRhoFloor));
+            const float prinv = __frcp_rn(prho);
+            pu = float(q3[1][v]) * prinv;
+            pv = float(q3[2][v]) * prinv;
+          } else {
+            prho = q3[0][v] > kRhoFloor ? q3[0][v] : kRhoFloor;
+            const double prinv = 1.0 / prho;
+            pu = q3[1][v] * prinv;
+            pv = q3[2][v] * prinv;
+          }
+          if (terms & 4) {
+            acc[1][v] += prho * tfx[v];
+            acc[2][v] += prho * tfy[v];
+            acc[3][v] += prho * (pu * tfx[v] + pv * tfy[v]);
+          }
+          if (drag) {
+            // Re sum_k P_k(row) e^{i k x}: the drag band synthesised per row
+            T lx = T(dpx[rr][0].x), ly = T(dpy[rr][0].x);
+            int ix = 0;
+            for (int kk = 1; kk <= kxd; ++kk) {
+              ix += col + v;
+              if (ix >= nx) ix -= nx;  // (k x) mod nx
+              const double2 e = twx[ix];
+              const T er = T(e.x), ei = -T(e.y);  // e^{+i k x}
+              lx += T(dpx[rr][kk].x) * er - T(dpx[rr][kk].y) * ei;
+              ly += T(dpy[rr][kk].x) * er - T(dpy[rr][kk].y) * ei;
+            }
+            acc[1][v] += lx;
+            acc[2][v] += ly;
+            acc[3][v] += pu * lx + pv * ly;
+          }
         }
       }
-    } else if (terms & (4 | 8)) {
-      // rho, u, v of primitive_from_conservative (one reciprocal)
-      const double prho = qa[0] > kRhoFloor ? qa[0] : kRhoFloor;
-      const double prinv = 1.0 / prho;
-      const Prim<double> pr{prho, qa[1] * prinv, qa[2] * prinv, 0.0};
-      if (terms & 4) {
-        const double fxv = bind.use ? bfx[o] : fs * double(sfx[o]);
-        const double fyv = bind.use ? bfy[o] : fs * double(sfy[o]);
-        const T rho_ = T(pr.rho), u = T(pr.u), vv = T(pr.v), tfx = T(fxv), tfy = T(fyv);
-        rhs[1] += double(rho_ * tfx);
-        rhs[2] += double(rho_ * tfy);
-        rhs[3] += double(rho_ * (u * tfx + vv * tfy));
+      if (terms & 16) {
+#pragma unroll
+        for (int v = 0; v < V; ++v) acc[3][v] += T(cool);
       }
-      if (drag) {
-        // Re sum_k P_k(row) e^{i k x}: the drag band synthesised per row
-        double lx = dpx[rr][0].x, ly = dpy[rr][0].x;
-        int ix = 0;
-        for (int kk = 1; kk <= kxd; ++kk) {
-          ix += col;
-          if (ix >= nx) ix -= nx;  // (k x) mod nx
-          const double2 e = twx[ix];
-          const double er = e.x, ei = -e.y;  // e^{+i k x}
-          lx += dpx[rr][kk].x * er - dpx[rr][kk].y * ei;
-          ly += dpy[rr][kk].x * er - dpy[rr][kk].y * ei;
+      if (mode == SW_RHS) {
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+          double r[V];
+#pragma unroll
+          for (int v = 0; v < V; ++v) r[v] = double(acc[c][v]);
+          vst<V>(bind.out + c * pl + o, r);
         }
-        rhs[1] += lx;
-        rhs[2] += ly;
-        rhs[3] += pr.u * lx + pr.v * ly;
+      } else {
+#pragma unroll
+        for (int c = 0; c < 4; ++c) vst<V>(XS + (rr * 4 + c) * LW + col, acc[c]);
       }
     }
-    if (terms & 16) rhs[3] += cool;
-    if (mode == SW_RHS) {
+    if (mode == SW_RHS) return;
+    // pass 2: stage combine in FP64 and the clean filter
+    for (int idx = threadIdx.x * V; idx < R * n; idx += blockDim.x * V) {
+      const int rr = idx >= n ? 1 : 0, col = idx - rr * n;
+      const int o = (line0 + rr) * nx + col;
+      double sv[4][V];
 #pragma unroll
-      for (int c = 0; c < 4; ++c) bind.out[c * plane + o] = rhs[c];
-      continue;
+      for (int c = 0; c < 4; ++c) {
+        double qa[V];
+        T r[V];
+        vld<V>(qinr + c * pl + o, qa);
+        vld<V>(XS + (rr * 4 + c) * LW + col, r);
+#pragma unroll
+        for (int v = 0; v < V; ++v) sv[c][v] = __fma_rn(dt, double(r[v]), qa[v]);
+      }
+      if (stage != 0) {
+        const double wa = stage == 1 ? 0.75 : 1.0 / 3.0, wb = stage == 1 ? 0.25 : 2.0 / 3.0;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+          double b[V];
+          vld<V>(q0 + c * pl + o, b);
+#pragma unroll
+          for (int v = 0; v < V; ++v) sv[c][v] = __fma_rn(wa, b[v], __dmul_rn(wb, sv[c][v]));
+        }
+      }
+#pragma unroll
+      for (int v = 0; v < V; ++v) enforce_node_rcp(sv[0][v], sv[1][v], sv[2][v], sv[3][v], gam, pfl64);
+      if (gc == 0) {
+#pragma unroll
+        for (int c = 0; c < 4; ++c) vst<V>(qo + c * pl + o, sv[c]);
+      } else {
+#pragma unroll
+        for (int c = 0; c < 4; ++c)
+#pragma unroll
+          for (int v = 0; v < V; ++v) ST[(rr * 4 + c) * n + col + v] = sv[c][v];
+      }
     }
-    double sv[4];
-#pragma unroll
-    for (int c = 0; c < 4; ++c) {
-      const double t = qa[c] + dt * rhs[c];
-      if (stage == 0) sv[c] = t;
-      else if (stage == 1) sv[c] = 0.75 * q0[c * plane + o] + 0.25 * t;
-      else sv[c] = (1.0 / 3.0) * q0[c * plane + o] + (2.0 / 3.0) * t;
-    }
-    enforce_node_rcp(sv[0], sv[1], sv[2], sv[3], gam);
-    if (gc == 0) {
-#pragma unroll
-      for (int c = 0; c < 4; ++c) qo[c * plane + o] = sv[c];
-    } else {
-#pragma unroll
-      for (int c = 0; c < 4; ++c) ST[(size_t)(rr * 4 + c) * n + col] = sv[c];
-    }
-  }
+  };
+#ifndef HITB200_NO_VEC_EPILOGUE
+  if (vec) epilogue(VecWidth<2>{});
+#else
+  if (false) epilogue(VecWidth<2>{});
+#endif
+  else epilogue(VecWidth<1>{});
   if (gc == 0 || mode != SW_STAGE) return;
   // Outflow guard fused: every row j takes row J(j) = clamp(j, g, ny-g-1) and
   // every column i column I(i); the CTA owning row J(j) writes row j.

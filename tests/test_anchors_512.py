@@ -38,13 +38,32 @@ PUBLISHED = json.loads((GOLD / "published_riemann_512.json").read_text())
 CLASSES = {3: R.RiemannConfig3, 6: R.RiemannConfig6}
 
 BLOCK = 16
-# Measured errors of the FP64 and FP32-bulk runs against the reference's NumPy
-# reruns, with margin (the larger of the two forms); see the test's docstring.
+# Errors against the reference's NumPy reruns.  The problems amplify roundoff
+# (see test_rerun_distance_is_the_problems_own_spread), so each limit is about
+# 2.5x the largest error measured on a B200 over ten runs per configuration:
+# both precision forms, each from the initial state and from four 1e-14
+# perturbations of its density.  Largest measured (c3 / c308 / c6):
+#   block_rms  rms over the 16 x 16 block means of (mirror - NumPy), relative
+#              to the rms of NumPy's: 2.1e-3 / 5.1e-3 / 2.0e-3
+#   block_means  largest block difference relative to the largest block
+#              mean: 1.7e-2 / 3.5e-2 / 2.0e-2
+#   density_min 2.3e-4 / 2.6e-4 / 8.7e-2; density_max 1.4e-3 / 2.4e-3 / 1.5e-3
+#   pressure_max 1.8e-3 / 4.7e-3 / 1.2e-2; max_abs_vorticity 7.7e-3 / 1.7e-2 /
+#   4.4e-2; sensor_fraction_abs 1.8e-4 / 2.2e-4 / 1.2e-3
 RERUN_TOL = {
-    "c3_mn0015": dict(block_means=1e-2, sensor_fraction_abs=2e-2, density_min=1e-2, density_max=1e-2),
-    "c308_t03": dict(block_means=1e-2, sensor_fraction_abs=2e-2, density_min=1e-2, density_max=1e-2),
-    "c6_t025": dict(block_means=1e-2, sensor_fraction_abs=2e-2, density_min=1e-1, density_max=1e-2),
+    "c3_mn0015": dict(block_rms=5e-3, block_means=4e-2, density_min=6e-4, density_max=4e-3,
+                      pressure_max=5e-3, max_abs_vorticity=2e-2, sensor_fraction_abs=1e-3),
+    "c308_t03": dict(block_rms=1.2e-2, block_means=8e-2, density_min=1e-3, density_max=6e-3,
+                     pressure_max=1.2e-2, max_abs_vorticity=4e-2, sensor_fraction_abs=1e-3),
+    "c6_t025": dict(block_rms=5e-3, block_means=5e-2, density_min=0.2, density_max=4e-3,
+                    pressure_max=3e-2, max_abs_vorticity=0.1, sensor_fraction_abs=3e-3),
 }
+# a 1e-14 relative perturbation of the initial density alone moves the final
+# block means of the mirror's own FP64 run by 1.0e-3 (c308), 1.6e-3 (c3),
+# 1.0e-3 (c6) in block_rms; the distance to the NumPy run is 3.4x, 1.3x, 1.2x
+# that spread
+PERTURBATION = 1e-14
+SPREAD_FACTOR = 8.0
 
 
 def _config(tag, precision):
@@ -77,6 +96,10 @@ def _rel(a, b):
     return abs(a - b) / abs(b)
 
 
+def _rms_rel(a, b):
+    return float(np.sqrt(np.mean((a - b) ** 2)) / np.sqrt(np.mean(b ** 2)))
+
+
 def _errors(got, q, want_diag, want_blocks=None):
     e = {k: _rel(getattr(got, k), float(want_diag[k]))
          for k in ("density_min", "density_max", "pressure_max", "max_abs_vorticity")}
@@ -84,6 +107,7 @@ def _errors(got, q, want_diag, want_blocks=None):
     if want_blocks is not None:
         bm = _block_means(q)
         e["block_means"] = float(np.max(np.abs(bm - want_blocks)) / np.max(np.abs(want_blocks)))
+        e["block_rms"] = _rms_rel(bm, want_blocks)
     return e
 
 
@@ -121,8 +145,10 @@ def test_numpy_rerun_riemann_512(riemann_runs, tag, precision):
     within the tolerances of RERUN_TOL.  The slip lines of these problems
     are Kelvin-Helmholtz unstable, so roundoff-level differences between two
     FP64 implementations grow over a thousand steps into visible differences
-    of local extrema (measured: density minimum of configuration 6 within 5 %
-    of the NumPy run's); smooth functionals of the field stay close."""
+    of local extrema (measured: density minimum of configuration 6 within 9 %
+    of the NumPy run's); smooth functionals of the field stay close, and
+    test_rerun_distance_is_the_problems_own_spread shows the distance is
+    of the size a 1e-14 perturbation of the initial state produces."""
     ref = np.load(GOLD / f"rerun_riemann_{tag}.npz")
     q, got = riemann_runs[tag, precision]
     want = {k[5:]: ref[k] for k in ref.files if k.startswith("diag_")}
@@ -133,6 +159,30 @@ def test_numpy_rerun_riemann_512(riemann_runs, tag, precision):
     tol = RERUN_TOL[tag]
     for key, lim in tol.items():
         assert e[key] <= lim, (key, e[key], lim)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("tag", RERUNS)
+def test_rerun_distance_is_the_problems_own_spread(riemann_runs, tag):
+    """The mirror's FP64 run restarted from its initial state with the density
+    multiplied by 1 + 1e-14 u (u uniform in [-1/2, 1/2), seeded) ends this far
+    (block_rms) from the unperturbed run; the NumPy rerun must lie within
+    SPREAD_FACTOR times that spread, and the spread itself must be far above
+    the perturbation (the problem amplifies roundoff: two correct FP64
+    implementations cannot agree more closely than this)."""
+    cfg = _config(tag, "fp64")
+    s = R.RiemannSolver(cfg)
+    g = torch.Generator(device="cpu").manual_seed(1)
+    u = (torch.rand(s.q.shape[1:], generator=g, dtype=torch.float64) - 0.5).to(s.q.device)
+    s.q[0] *= 1 + PERTURBATION * u
+    s.advance(s.n_steps)
+    torch.cuda.synchronize()
+    base = _block_means(riemann_runs[tag, "fp64"][0])
+    spread = _rms_rel(_block_means(s.q.double().cpu().numpy()), base)
+    dist = _rms_rel(base, np.load(GOLD / f"rerun_riemann_{tag}.npz")["block_means"])
+    print(f"\n[measured] spread {tag}: perturbed {spread:.2e} NumPy {dist:.2e} ratio {dist / spread:.2f}")
+    assert spread > 1e6 * PERTURBATION
+    assert dist <= SPREAD_FACTOR * spread
 
 
 # ---- 512^2 production HIT, 1000 steps, the reference's own noise stream ---------------------
