@@ -12,12 +12,18 @@ each variant with per-launch CUDA events, keeps the faster variant of every
 family, and applies it to the real batch.  The choice only changes speed, not
 results, and is cached per batch signature (precision and each member's grid
 and physics switches), so a serving loop that meets the same mix again pays
-nothing.
+nothing.  The cache is also kept on disk (``HITB200_TUNE_CACHE``, default
+``~/.cache/hit_solver_b200/tuning.json``; ``off`` disables it), keyed by the
+signature, the GPU's name and the library build, so a later process on the
+same GPU and build starts from the measured choice.
 """
 
 from __future__ import annotations
 
+import json
+import os
 import threading
+from pathlib import Path
 
 import torch
 
@@ -42,6 +48,82 @@ def signature(descs) -> tuple:
          int(d.forcing_on), int(d.drag_coefficient > 0.0), d.hv_interval)
         for d in descs)
     return (descs[0].precision, tuple(members))
+
+
+def cache_path() -> Path | None:
+    """The on-disk cache file, or None when disabled."""
+    v = os.environ.get("HITB200_TUNE_CACHE", "")
+    if v.lower() == "off":
+        return None
+    return Path(v) if v else Path.home() / ".cache" / "hit_solver_b200" / "tuning.json"
+
+
+def _disk_key(key) -> str:
+    """Signature plus what a measured choice depends on besides it: the GPU
+    model and the library build (size and modification time of the .so)."""
+    try:
+        st = os.stat(_lib.LIB_PATH)
+        build = f"{st.st_size}-{int(st.st_mtime)}"
+    except OSError:
+        build = "unknown"
+    dev = torch.cuda.get_device_name() if torch.cuda.is_available() else "cpu"
+    return json.dumps([dev, build, key], separators=(",", ":"))
+
+
+def _disk_load(dkey: str):
+    path = cache_path()
+    if path is None:
+        return None
+    try:
+        data = json.loads(path.read_text())
+    except (OSError, ValueError):
+        return None
+    v = data.get(dkey) if isinstance(data, dict) else None
+    if isinstance(v, list) and len(v) == _lib.TUNE_COUNT and all(x in (0, 1) for x in v):
+        return [int(x) for x in v]
+    return None
+
+
+def _disk_store(dkey: str, best) -> None:
+    """Merge one entry into the cache file (written whole to a temporary file
+    and renamed into place, so readers never see a partial file)."""
+    path = cache_path()
+    if path is None:
+        return
+    try:
+        path.parent.mkdir(parents=True, exist_ok=True)
+        try:
+            data = json.loads(path.read_text())
+            if not isinstance(data, dict):
+                data = {}
+        except (OSError, ValueError):
+            data = {}
+        data[dkey] = [int(x) for x in best]
+        tmp = path.with_name(f"{path.name}.{os.getpid()}.tmp")
+        tmp.write_text(json.dumps(data, indent=0, sort_keys=True))
+        os.replace(tmp, path)
+    except OSError:
+        pass  # a read-only home: the in-memory cache still holds the choice
+
+
+def _lookup(key, use_cache: bool):
+    if not use_cache:
+        return None
+    with _lock:
+        best = _cache.get(key)
+    if best is None:
+        best = _disk_load(_disk_key(key))
+        if best is not None:
+            with _lock:
+                _cache[key] = best
+    return best
+
+
+def _remember(key, best, use_cache: bool) -> None:
+    with _lock:
+        _cache[key] = best
+    if use_cache:
+        _disk_store(_disk_key(key), best)
 
 
 def _profile_ms(profile_fn, trials: int):
@@ -96,8 +178,7 @@ def tune_batch(batch, trials: int = 3, use_cache: bool = True) -> list[int]:
     from .batch import Batch
 
     key = signature(batch.descs)
-    with _lock:
-        best = _cache.get(key) if use_cache else None
+    best = _lookup(key, use_cache)
     if best is None:
         plans = [core.Plan(d) for d in batch.descs]
         states = [s.clone() for s in batch.states]
@@ -111,8 +192,7 @@ def tune_batch(batch, trials: int = 3, use_cache: bool = True) -> list[int]:
             scratch.close()
             del scratch, plans, states
             torch.cuda.synchronize()
-        with _lock:
-            _cache[key] = best
+        _remember(key, best, use_cache)
     batch.set_tuning(best)
     return best
 
@@ -123,8 +203,7 @@ def tune_plan(plan, q, trials: int = 3, use_cache: bool = True) -> list[int]:
     if plan.desc.forcing_on and plan.desc.noise_mode == 0:
         return plan.tuning
     key = signature([plan.desc]) + ("single",)
-    with _lock:
-        best = _cache.get(key) if use_cache else None
+    best = _lookup(key, use_cache)
     if best is None:
         scratch = core.Plan(plan.desc)
         qc = q.clone()
@@ -136,8 +215,7 @@ def tune_plan(plan, q, trials: int = 3, use_cache: bool = True) -> list[int]:
         best = _choose(lambda: scratch.step_profile(qc), scratch.set_tuning, trials, run)
         del scratch, qc
         torch.cuda.synchronize()
-        with _lock:
-            _cache[key] = best
+        _remember(key, best, use_cache)
     plan.set_tuning(best)
     return best
 

@@ -513,7 +513,11 @@ __global__ void __launch_bounds__(kPreThreads, OCC ? HITB200_PRE_MIN_BLOCKS : 2)
   // ---- last CTA of this solve: fixed-order final reduction + scalar logic ----
   __shared__ double red[R_FIXED + 4 * kMaxDrag];
   prepass_finalize(S, nslots, red);
-  if (threadIdx.x == 0) prepass_scalars(S, red, sc, mode, bind.use);
+  if (threadIdx.x == 0) {
+    prepass_scalars(S, red, sc, mode, bind.use);
+    // a bounded wait of an earlier kernel of this solve that ran out
+    if (atomicExch(&S.counters[6], 0u)) sc[S_STATUS] = (double)((int)sc[S_STATUS] | ST_BARRIER);
+  }
 }
 
 // Forward transform of the caller's white-noise field restricted to the

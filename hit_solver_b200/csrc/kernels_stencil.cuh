@@ -585,6 +585,16 @@ constexpr int kPowTab = 128;                         // rho^k below 1e-43 beyond
 __device__ double g_rho_pow[kPowTab];
 
 constexpr int kSweepHalo = 8;  // staged nodes left of node 0 (WENO reads 5)
+#ifndef HITB200_SWEEP_X_BULK
+#define HITB200_SWEEP_X_BULK 1
+#endif
+// The x sweep of the FP32-bulk form stages its rows by bulk copies (the
+// TMA unit) into shared memory.  Bit-identical to the load path; measured
+// on a B200, 8 x 512^2 batched HIT step 1.063 -> 1.053 ms, sweep_x 66.1 ->
+// 64.7 us per launch (with separate landing rows, costing two resident
+// CTAs per SM: 1.067 -> 1.202 ms).
+constexpr bool kSweepXBulk = HITB200_SWEEP_X_BULK != 0;
+constexpr unsigned long long kBulkWaitNs = 2000000000ull;  // bound of a copy wait
 
 // Shared memory of one sweep CTA holding R lines of n nodes:
 //   FQ  [R][8][LS]  flux F_c (c < 4) and enforced state Q_c (c >= 4) of nodes
@@ -813,22 +823,9 @@ __global__ void __launch_bounds__(AXIS == 0 ? 256 : 512,
   // consecutive threads take the R columns of a row, then the next row.
   const int nl = AXIS == 0 ? R * LS : (LS << rsh);
   const T pfl = T(kPFloor) / (g - T(1));  // floor energy of enforce_physical_state
-#pragma unroll 4
-  for (int idx = threadIdx.x; idx < nl; idx += blockDim.x) {
-    int r, p;
-    if (AXIS == 0) {
-      r = idx >= LS ? 1 : 0;
-      p = idx - r * LS;
-    } else {
-      r = idx & (RL - 1);
-      p = idx >> rsh;
-      if (r >= R) continue;
-    }
-    const int gp = fold_node(p - kSweepHalo, n, per);
-    const size_t o = AXIS == 0 ? (size_t)(line0 + r) * nx + gp : (size_t)gp * nx + line0 + r;
-    T a0 = T(__ldcg(qin + o)), a1 = T(__ldcg(qin + o + plane)), a2 = T(__ldcg(qin + o + 2 * plane)),
-      a3 = T(__ldcg(qin + o + 3 * plane));
-    // enforce_physical_state, then primitive_from_conservative of the result
+  // one node: enforce_physical_state, then primitive_from_conservative of the
+  // result, and the node's flux and enforced state into FQ
+  auto stage_node = [&](int r, int p, T a0, T a1, T a2, T a3) {
     const T rho = a0 > T(kRhoFloor) ? a0 : T(kRhoFloor);
     const T rinv = rcp_rn(rho);
     T u = a1 * rinv, v = a2 * rinv;
@@ -842,7 +839,7 @@ __global__ void __launch_bounds__(AXIS == 0 ? 256 : 512,
     pr = (g - T(1)) * (a3 - T(0.5) * rho * (u * u + v * v));
     pr = pr > T(kPFloor) ? pr : T(kPFloor);
     const T un = AXIS == 0 ? u : v;
-    T* f = FQ + (size_t)r * 8 * LS + p;
+    T* f = FQ + r * 8 * LS + p;
     f[0 * LS] = AXIS == 0 ? a1 : a2;
     f[1 * LS] = a1 * un + (AXIS == 0 ? pr : T(0));
     f[2 * LS] = a2 * un + (AXIS == 0 ? T(0) : pr);
@@ -851,6 +848,90 @@ __global__ void __launch_bounds__(AXIS == 0 ? 256 : 512,
     f[5 * LS] = a1;
     f[6 * LS] = a2;
     f[7 * LS] = a3;
+  };
+  bool bulk = false;
+  if constexpr (AXIS == 0 && sizeof(T) == 4 && kSweepXBulk) {
+    // x lines by bulk copies: the R rows' n interior nodes of each of the four
+    // planes land as FP64 in shared memory through the copy engine; the
+    // threads fetch the few halo nodes meanwhile
+    bulk = !bind.use && (nx & 1) == 0 && (reinterpret_cast<uintptr_t>(qin) & 15) == 0;
+  }
+  if (bulk) {
+    __shared__ unsigned long long tbar;
+    // The FP64 landing rows [R][4][LS] take the place of FQ ([R][8][LS] of
+    // T): each thread moves its nodes' values into registers before the
+    // flux staging overwrites them.
+    double* SQ = reinterpret_cast<double*>(smem);
+    if (threadIdx.x == 0) mbar_init(&tbar, 1);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      mbar_expect_tx(&tbar, (unsigned)(R * 4 * n * sizeof(double)));
+      for (int rr = 0; rr < R; ++rr)
+        for (int c = 0; c < 4; ++c)
+          bulk_g2s(SQ + (rr * 4 + c) * LS + kSweepHalo, qin + c * plane + (size_t)(line0 + rr) * nx,
+                   (unsigned)(n * sizeof(double)), &tbar);
+    }
+    const int nh = LS - n;  // halo slots of a line: p < kSweepHalo or p >= kSweepHalo + n
+    for (int idx = threadIdx.x; idx < R * 4 * nh; idx += blockDim.x) {
+      const int rc = idx / nh, h = idx - rc * nh;
+      const int pp = h < kSweepHalo ? h : h + n;
+      const int gp = fold_node(pp - kSweepHalo, n, per);
+      SQ[rc * LS + pp] = __ldcg(qin + (rc & 3) * plane + (size_t)(line0 + (rc >> 2)) * nx + gp);
+    }
+    // bounded wait for the copies; a CTA whose copies do not land in time
+    // reports it (ST_BARRIER at the next prepass) and skips its lines
+    const unsigned long long t0 = global_ns();
+    unsigned it = 0;
+    bool done = mbar_try_wait(&tbar, 0);
+    while (!done) {
+      if ((++it & 63) == 0 && global_ns() - t0 > kBulkWaitNs) break;
+      done = mbar_try_wait(&tbar, 0);
+    }
+    if (__syncthreads_or(!done)) {
+      if (threadIdx.x == 0) atomicOr(&S.counters[6], 1u);
+      const unsigned long long t1 = global_ns();
+      while (!mbar_try_wait(&tbar, 0) && global_ns() - t1 < kBulkWaitNs) {
+      }
+      return;
+    }
+    // a line's LS nodes over its 128 threads: at most MN + 1 nodes a thread
+    T held[4][MN + 1];
+#pragma unroll
+    for (int j = 0; j <= MN; ++j) {
+      const int idx = threadIdx.x + j * blockDim.x;
+      if (idx < nl) {
+        const int r = idx >= LS ? 1 : 0, pp = idx - r * LS;
+        const double* sq = SQ + r * 4 * LS + pp;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) held[c][j] = T(sq[c * LS]);
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j <= MN; ++j) {
+      const int idx = threadIdx.x + j * blockDim.x;
+      if (idx < nl) {
+        const int r = idx >= LS ? 1 : 0, pp = idx - r * LS;
+        stage_node(r, pp, held[0][j], held[1][j], held[2][j], held[3][j]);
+      }
+    }
+  } else {
+#pragma unroll 4
+    for (int idx = threadIdx.x; idx < nl; idx += blockDim.x) {
+      int r, p;
+      if (AXIS == 0) {
+        r = idx >= LS ? 1 : 0;
+        p = idx - r * LS;
+      } else {
+        r = idx & (RL - 1);
+        p = idx >> rsh;
+        if (r >= R) continue;
+      }
+      const int gp = fold_node(p - kSweepHalo, n, per);
+      const size_t o = AXIS == 0 ? (size_t)(line0 + r) * nx + gp : (size_t)gp * nx + line0 + r;
+      stage_node(r, p, T(__ldcg(qin + o)), T(__ldcg(qin + o + plane)), T(__ldcg(qin + o + 2 * plane)),
+                 T(__ldcg(qin + o + 3 * plane)));
+    }
   }
   // The stage input was written two or more kernels earlier (complete when
   // this CTA starts: the previous kernel releases its dependents only after

@@ -205,6 +205,9 @@ class SolveServer:
         stream = torch.cuda.current_stream()
         rounds = 0
         cell_steps = 0.0
+        # host time by phase: admission (plan and initial state), batch
+        # rebuilds, rounds (launch, graph capture after a rebuild, the wait)
+        phase = {"admit_s": 0.0, "rebuild_s": 0.0, "round_s": 0.0, "rebuilds": 0}
         t0 = clock()
         while pending or active:
             now = clock() - t0
@@ -214,7 +217,9 @@ class SolveServer:
                 if used + fp > self.hbm_budget:
                     break
                 req = pending.pop(0)
-                active.append(_Member(req, make_solver(req, self.precision), fp, clock() - t0))
+                ta = clock()
+                active.append(_Member(req, make_solver(req, self.precision), fp, ta - t0))
+                phase["admit_s"] += clock() - ta
                 used += fp
                 dirty = True
             if not active:
@@ -223,6 +228,8 @@ class SolveServer:
                     time.sleep(wait)
                 continue
             if dirty:
+                tr = clock()
+                phase["rebuilds"] += 1
                 if batch is not None:
                     batch.close()
                 batch = Batch.from_plans([m.solver.plan for m in active],
@@ -231,12 +238,15 @@ class SolveServer:
                     scal = torch.empty((2 * len(active), _lib.S_COUNT),
                                        dtype=torch.float64).pin_memory()
                 dirty = False
+                phase["rebuild_s"] += clock() - tr
+            tq = clock()
             batch.run(self.steps_per_round)
             rounds += 1
             for i, m in enumerate(active):
                 m.solver.plan.lib.hitb200_copy_scalars_async(
                     m.solver.plan.handle, scal[i].data_ptr(), _lib.S_COUNT, stream.cuda_stream)
             stream.synchronize()
+            phase["round_s"] += clock() - tq
             done_at = clock() - t0
             keep = []
             for i, m in enumerate(active):
@@ -275,6 +285,7 @@ class SolveServer:
             "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
             "steps_per_round": self.steps_per_round, "hbm_budget": self.hbm_budget,
             "failed": sum(1 for r in results if r.error is not None),
+            **phase,
         }
         return results
 

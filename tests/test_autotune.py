@@ -78,6 +78,26 @@ def test_autotune_batch_and_plan():
 
 
 @pytest.mark.gpu
+def test_autotune_choice_read_back_from_disk(tmp_path, monkeypatch):
+    """A later process (here: an emptied in-memory cache) takes the measured
+    choice from the disk cache without timing again."""
+    monkeypatch.setenv("HITB200_TUNE_CACHE", str(tmp_path / "tuning.json"))
+    autotune.clear_cache()
+    s = serving.make_solver(serving.Request(3, "riemann6", 96, split=0.4), "fp32-bulk")
+    k = autotune.tune_plan(s.plan, s.q, trials=1)
+    autotune.clear_cache()
+
+    def no_timing(*a, **kw):
+        raise AssertionError("tuned again instead of reading the disk cache")
+
+    monkeypatch.setattr(autotune, "_choose", no_timing)
+    s.plan.set_tuning([-1, -1, -1, -1])
+    assert autotune.tune_plan(s.plan, s.q) == k
+    assert s.plan.tuning == k
+    autotune.clear_cache()
+
+
+@pytest.mark.gpu
 def test_tuning_knob_validation():
     s = serving.make_solver(serving.Request(0, "riemann3", 32), "fp32-bulk")
     with pytest.raises(ValueError):
