@@ -659,7 +659,7 @@ def spectra_run(K: int, W: int, flush, world: int, count: int, cpu: bool):
     phases = {
         "fields": {"ms": ph["fields"], "gbs": fbytes / (ph["fields"] / 1e3) / 1e9,
                    "bytes": fbytes, "frac": fbytes / (ph["fields"] / 1e3) / 1e9 / peak},
-        "rfft2": {"ms": ph["rfft2"], "impl": "hitb200_rfft2 (mixed-radix line transforms)",
+        "rfft2": {"ms": ph["rfft2"], "impl": "hitb200_rfft2 (the library's line transforms: radix-8 in registers for power-of-two lengths)",
                   "cufft_ms": cufft_ms},
         "shells": {"ms": ph["shells"], "gbs": sbytes / (ph["shells"] / 1e3) / 1e9, "bytes": sbytes,
                    "frac": sbytes / (ph["shells"] / 1e3) / 1e9 / peak},

@@ -2405,10 +2405,36 @@ void fft_attr(size_t bytes) {
   }
 }
 
-// `fields` batches of `lines` lines of n points (see FftLines).
+template <bool IN_REAL, bool OUT_REAL, bool COLS>
+void fft_p2_attr(size_t bytes) {
+  static size_t done[kMaxAttrDevices] = {};
+  const int dev = attr_device();
+  std::lock_guard<std::mutex> lock(g_attr_mu);
+  if (bytes > done[dev]) {
+    cudaFuncSetAttribute(fft_p2_kernel<IN_REAL, OUT_REAL, COLS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)bytes);
+    done[dev] = bytes;
+  }
+}
+
+// `fields` batches of `lines` lines of n points (see FftLines); C > 1:
+// the lines are adjacent columns.  Power-of-two lengths take the radix-8
+// register kernel, others the mixed-radix one.
 template <bool IN_REAL, bool OUT_REAL, int C>
 void fft_launch(const void* in, void* out, int n, int lines, int fields, FftLines li, FftLines lo,
                 int out_count, int sign, const double2* W, double scale, cudaStream_t st) {
+  if (fft_pow2_ok(n) && !(IN_REAL && C > 1)) {
+    int logn = 0;
+    while ((1 << logn) < n) ++logn;
+    const int L = kFftP2Points >> logn;
+    const int clines = IN_REAL ? (lines + 1) / 2 : lines;
+    const size_t smem = fft_p2_smem_bytes(n);
+    fft_p2_attr<IN_REAL, OUT_REAL, (C > 1)>(smem);
+    const long long grid = (long long)fields * ((clines + L - 1) / L);
+    fft_p2_kernel<IN_REAL, OUT_REAL, (C > 1)><<<(unsigned)grid, kFftThreads, smem, st>>>(
+        in, out, n, logn, lines, li, lo, out_count, sign, W, scale);
+    return;
+  }
   const size_t smem = fft_smem_bytes(n, C);
   fft_attr<IN_REAL, OUT_REAL, C>(smem);
   const long long grid = (long long)fields * ((lines + C - 1) / C);

@@ -438,10 +438,13 @@ def test_golden_large_scale_kinetic_fraction(name):
         assert abs(got - want) <= 1e-12 * max(abs(want), 1.0), (k, got, want)
 
 
-@pytest.mark.parametrize("shape", [(24, 32), (20, 25), (97, 64), (63, 50), (1024, 6), (7, 1021), (384, 384)])
+@pytest.mark.parametrize("shape", [(24, 32), (20, 25), (97, 64), (63, 50), (1024, 6), (7, 1021), (384, 384),
+                                   (512, 512), (33, 64), (256, 16), (8, 1024), (1024, 32), (128, 8)])
 def test_rfft2_matches_numpy(shape):
-    """The library's mixed-radix line transforms (hitb200_rfft2) against
-    numpy.fft.rfft2: radices 4, 2, 3, 5, 7 and prime lengths."""
+    """The library's line transforms (hitb200_rfft2) against
+    numpy.fft.rfft2: mixed radices 4, 2, 3, 5, 7 and prime lengths, and the
+    radix-8 kernel of power-of-two lengths (rows packed in pairs, an odd
+    row count included)."""
     ny, nx = shape
     lib = _lib.load()
     rng = np.random.default_rng(ny * 7 + nx)
@@ -454,13 +457,30 @@ def test_rfft2_matches_numpy(shape):
     assert rel_err(out.cpu().numpy(), want) < 1e-13
 
 
-def test_spectral_divergence_vorticity_fields():
+def test_rfft2_unaligned_input_matches_numpy():
+    """Rows that start 8 bytes past a 16-byte boundary take the radix-8
+    kernel's one-value loads instead of its paired ones."""
+    ny, nx = 64, 128
+    lib = _lib.load()
+    a = np.random.default_rng(11).standard_normal((2, ny, nx))
+    buf = torch.empty(a.size + 1, dtype=torch.float64, device="cuda")
+    src = buf[1:].view(2, ny, nx)
+    src.copy_(dev(a))
+    assert src.data_ptr() % 16 == 8
+    out = torch.empty((2, ny, nx // 2 + 1), dtype=torch.complex128, device="cuda")
+    ws = torch.empty(int(lib.hitb200_rfft2_workspace_bytes(nx, ny)), dtype=torch.uint8, device="cuda")
+    _lib.check(lib.hitb200_rfft2(src.data_ptr(), 2, nx, ny, out.data_ptr(), ws.data_ptr(), ws.numel(),
+                                 core.stream_handle()))
+    assert rel_err(out.cpu().numpy(), np.fft.rfft2(a)) < 1e-13
+
+
+@pytest.mark.parametrize("ny,nx", [(40, 27), (64, 128)])
+def test_spectral_divergence_vorticity_fields(ny, nx):
     """divergence_and_vorticity (OOP/hit2d.py:146-155, 459-468) against the
-    oracle's NumPy spectral derivatives on a non-square grid with a Nyquist
-    row (even ny) and an odd nx."""
+    oracle's NumPy spectral derivatives on non-square grids with a Nyquist
+    row (even ny): an odd nx (mixed radix) and power-of-two lengths."""
     from hit_solver_b200.hit2d import divergence_and_vorticity
 
-    ny, nx = 40, 27
     dom = Domain2D(0.0, 2 * np.pi, 0.0, 3.0, nx, ny)
     rng = np.random.default_rng(3)
     u, v = rng.standard_normal((ny, nx)), rng.standard_normal((ny, nx))
