@@ -30,7 +30,7 @@ S_ALPHA_X, S_ALPHA_Y, S_DIV_RMS, S_VORT_RMS, S_DT, S_TIME, S_STEP, S_ACTIVE, S_M
 S_COUNT = 32
 # bits of the S_STATUS slot (HITB200_ST_*)
 ST_NONFINITE, ST_NONPOS_RHO, ST_NONPOS_P, ST_BARRIER, ST_NOISE = 1, 2, 4, 8, 16
-TUNE_SWEEP_X, TUNE_SWEEP_Y, TUNE_PREPASS, TUNE_FUSED_SENSOR, TUNE_COUNT = 0, 1, 2, 3, 4
+TUNE_SWEEP_X, TUNE_SWEEP_Y, TUNE_PREPASS, TUNE_FUSED_SENSOR, TUNE_Y_PANEL, TUNE_COUNT = 0, 1, 2, 3, 4, 5
 
 NAN = float("nan")
 

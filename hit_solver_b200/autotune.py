@@ -2,7 +2,9 @@
 
 Three kernel families have two compiled variants each: the x sweep, the y
 sweep and the prepass; a fourth knob fuses each prepass into the following
-sensor launch (single solves whose tiles all fit on the GPU at once).  The latency variant keeps more registers per thread
+sensor launch (single solves whose tiles all fit on the GPU at once), and a
+fifth picks the y sweep's tile shape (panels of 2 or 4 columns per CTA).
+The latency variant keeps more registers per thread
 and suits launches that cannot fill the GPU (one 512^2 solve); the
 throughput variant fits more CTAs per SM and suits launches over many solves.
 Plans and batches start from a default picked by launch size.  The tuner
@@ -154,19 +156,28 @@ def _graph_ms(run_fn, steps: int) -> float:
 
 def _choose(profile_fn, set_fn, trials: int, run_fn=None) -> list[int]:
     """Variant knobs: each family's faster variant by per-launch times (fused
-    sensor off); then, where run_fn can replay the plan's steps and the plan
-    can fuse its prepasses into the sensors, whichever of fused / unfused
-    gives the shorter graph-replayed step (launch gaps matter there)."""
+    sensor off, default y panels); then the y sweep's tile shape (the other
+    panel width) by the y sweep's time; then, where run_fn can replay the
+    plan's steps and the plan can fuse its prepasses into the sensors,
+    whichever of fused / unfused gives the shorter graph-replayed step
+    (launch gaps matter there)."""
     ms = {}
     for variant in (0, 1):
-        set_fn([variant, variant, variant, 0])
+        set_fn([variant, variant, variant, 0, 0])
         profile_fn()  # warm-up step of this variant
         ms[variant] = _profile_ms(profile_fn, trials)[0]
-    best = [0 if ms[0][k] <= ms[1][k] else 1 for k in _VARIANT_KNOBS] + [0]
+    best = [0 if ms[0][k] <= ms[1][k] else 1 for k in _VARIANT_KNOBS] + [0, 0]
+    ym = {}
+    for panel in (0, 1):
+        set_fn(best[:4] + [panel])
+        profile_fn()
+        ym[panel] = _profile_ms(profile_fn, trials)[0][_lib.TUNE_SWEEP_Y]
+    best[_lib.TUNE_Y_PANEL] = 0 if ym[0] <= ym[1] else 1
     if run_fn is not None:
         step = {}
         for fused in (0, 1):
-            set_fn(best[:3] + [fused])
+            best[_lib.TUNE_FUSED_SENSOR] = fused
+            set_fn(best)
             step[fused] = _graph_ms(run_fn, max(4, 2 * trials))
         best[_lib.TUNE_FUSED_SENSOR] = 0 if step[0] <= step[1] else 1
     set_fn(best)

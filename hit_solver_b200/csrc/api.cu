@@ -303,6 +303,7 @@ void default_tuning(int n_x, int n_y, int n_tiles32, int* t) {
   t[HITB200_TUNE_SWEEP_Y] = n_y >= 4 * sms;
   t[HITB200_TUNE_PREPASS] = n_tiles32 >= 4 * sms;
   t[HITB200_TUNE_FUSED_SENSOR] = 0;  // measured slower at 512^2; the autotuner decides
+  t[HITB200_TUNE_Y_PANEL] = 0;
 }
 
 }  // namespace
@@ -323,13 +324,18 @@ struct hitb200_plan {
   int n_tiles = 0, n_tiles32 = 0, n_x = 0, n_y = 0, Rx = 1, Ry = 1, n_srows = 0;
   int elem = 8;
   size_t smem_x = 0, smem_y = 0, smem_sensor = 0;
+  // the other y-panel width (tuning knob HITB200_TUNE_Y_PANEL; Ry2 == Ry
+  // when there is none) and its line list
+  int Ry2 = 1, n_y2 = 0;
+  size_t smem_y2 = 0;
+  Work* d_ylines2 = nullptr;
   // graph replay of hitb200_step
   cudaGraphExec_t graph = nullptr;
   cudaStream_t graph_stream = nullptr;
   const double* graph_q = nullptr;
   bool in_batch = false;
   SolveDev* own_solve = nullptr;  // the arena's descriptor (d_solve points into a batch table while batched)
-  int tuning[HITB200_TUNE_COUNT] = {0, 0, 0, 0};  // kernel variants (tuning knobs)
+  int tuning[HITB200_TUNE_COUNT] = {};  // kernel variants (tuning knobs)
   bool fuse_ok = false;  // all of the fused sensor's CTAs fit on the GPU at once
   int sensor_w = -1;          // width of the step sensor instantiation (-1: generic sensor)
   size_t smem_sensor_step = 0;
@@ -340,7 +346,7 @@ struct hitb200_plan {
 struct hitb200_batch {
   std::vector<hitb200_plan*> plans;
   bool owns_plans = true;  // false for hitb200_batch_from_plans
-  int tuning[HITB200_TUNE_COUNT] = {0, 0, 0, 0};
+  int tuning[HITB200_TUNE_COUNT] = {};
   SolveDev* d_solves = nullptr;  // start of the tables' device block
   DevBlock tables;
   Work *d_tiles = nullptr, *d_tiles32 = nullptr, *d_xlines = nullptr, *d_ylines = nullptr;
@@ -353,6 +359,13 @@ struct hitb200_batch {
   std::vector<int> off_tiles, off_tiles32, off_xl, off_yl, off_srows;
   int rx_max = 1, ry_max = 1;
   size_t smem_x = 0, smem_y = 0, smem_sensor = 0;
+  // the other y-panel width's line list (tuning knob HITB200_TUNE_Y_PANEL;
+  // has_y2 false when there is none)
+  bool has_y2 = false;
+  Work* d_ylines2 = nullptr;
+  int n_y2 = 0, ry_max2 = 1;
+  size_t smem_y2 = 0;
+  std::vector<int> off_yl2;
   int sensor_w = -1;  // shared width of the members' step sensor (-1: generic sensor)
   size_t smem_sensor_step = 0;
   int any_outflow = 0, any_forcing = 0, any_hv = 0, any_noise_upload = 0;
@@ -709,12 +722,17 @@ LaunchSet plan_launch_set(hitb200_plan* p, cudaStream_t st) {
   L.mch_y = mch_for(p->desc.ny);
   L.thr_x = kLineThreads * p->Rx;
   L.thr_y = kLineThreads * p->Ry;
+  if (p->tuning[HITB200_TUNE_Y_PANEL] && p->Ry2 != p->Ry) {
+    L.yl = p->d_ylines2;
+    L.n_y = p->n_y2;
+    L.thr_y = kLineThreads * p->Ry2;
+  }
   L.occ_x = p->tuning[HITB200_TUNE_SWEEP_X];
   L.occ_y = p->tuning[HITB200_TUNE_SWEEP_Y];
   L.occ_pre = p->tuning[HITB200_TUNE_PREPASS];
   L.fused = p->tuning[HITB200_TUNE_FUSED_SENSOR] && p->fuse_ok;
   L.smem_x = p->smem_x;
-  L.smem_y = p->smem_y;
+  L.smem_y = p->tuning[HITB200_TUNE_Y_PANEL] && p->Ry2 != p->Ry ? p->smem_y2 : p->smem_y;
   L.smem_sensor = p->smem_sensor;
   L.gen = p->has_gen ? &p->gen : nullptr;
   L.gen_out = p->has_gen ? const_cast<double*>(p->hs.noise) : nullptr;
@@ -956,6 +974,7 @@ size_t hitb200_plan_device_bytes(const hitb200_desc* d) {
   a.take(ntile * sizeof(Work));
   a.take((size_t)((d->nx + kSenTX - 1) / kSenTX) * ((d->ny + kSenTY - 1) / kSenTY) * sizeof(Work));
   a.take((size_t)(d->ny + d->nx) * sizeof(Work));
+  a.take((size_t)d->nx * sizeof(Work));  // the other y-panel width's lines
   a.take((size_t)d->ny * sizeof(Work));  // synthesis row blocks (at most one per row)
   return a.off;
 }
@@ -995,6 +1014,13 @@ int hitb200_plan_create(const hitb200_desc* d, hitb200_plan** out) {
   default_tuning(p->n_x, p->n_y, ((nx + kSenTX - 1) / kSenTX) * ((ny + kSenTY - 1) / kSenTY), p->tuning);
   p->smem_x = p->elem == 4 ? SweepLayout<float>(nx, p->Rx).bytes() : SweepLayout<double>(nx, p->Rx).bytes();
   p->smem_y = p->elem == 4 ? SweepLayout<float>(ny, p->Ry).bytes() : SweepLayout<double>(ny, p->Ry).bytes();
+  {
+    const int alt = p->Ry == 4 ? 2 : 4;
+    const size_t b2 = p->elem == 4 ? SweepLayout<float>(ny, alt).bytes() : SweepLayout<double>(ny, alt).bytes();
+    p->Ry2 = (nx >= alt && b2 <= 110 * 1024) ? alt : p->Ry;
+    p->n_y2 = (nx + p->Ry2 - 1) / p->Ry2;
+    p->smem_y2 = p->elem == 4 ? SweepLayout<float>(ny, p->Ry2).bytes() : SweepLayout<double>(ny, p->Ry2).bytes();
+  }
   p->smem_sensor = sensor_smem_bytes(d->sensor_width, p->elem, d->viscosity > 0.0);
   p->sensor_w = step_sensor_width(d->sensor_width);
   p->smem_sensor_step = step_sensor_bytes(p->sensor_w, p->elem, d->viscosity > 0.0);
@@ -1034,6 +1060,7 @@ int hitb200_plan_create(const hitb200_desc* d, hitb200_plan** out) {
   const size_t o_tiles32 = a.take(p->n_tiles32 * sizeof(Work));
   const size_t o_xl = a.take(p->n_x * sizeof(Work));
   const size_t o_yl = a.take(p->n_y * sizeof(Work));
+  const size_t o_yl2 = a.take(p->n_y2 * sizeof(Work));
   const size_t o_sr = a.take(p->n_srows * sizeof(Work));
   p->arena_bytes = a.off;
   cudaError_t e = block_alloc(a.off, &p->arena_block);
@@ -1151,6 +1178,7 @@ int hitb200_plan_create(const hitb200_desc* d, hitb200_plan** out) {
   p->d_tiles32 = reinterpret_cast<Work*>(base + o_tiles32);
   p->d_xlines = reinterpret_cast<Work*>(base + o_xl);
   p->d_ylines = reinterpret_cast<Work*>(base + o_yl);
+  p->d_ylines2 = reinterpret_cast<Work*>(base + o_yl2);
   p->d_srows = reinterpret_cast<Work*>(base + o_sr);
 
   // ---- host-built tables ----
@@ -1186,6 +1214,8 @@ int hitb200_plan_create(const hitb200_desc* d, hitb200_plan** out) {
   std::vector<Work> xl, yl;
   for (int r = 0; r < ny; r += p->Rx) xl.push_back({0, r, std::min(p->Rx, ny - r), 0});
   for (int c = 0; c < nx; c += p->Ry) yl.push_back({0, c, std::min(p->Ry, nx - c), 0});
+  std::vector<Work> yl2;
+  for (int c = 0; c < nx; c += p->Ry2) yl2.push_back({0, c, std::min(p->Ry2, nx - c), 0});
   std::vector<Work> sr;
   for (int r = 0; r < ny; r += srows) sr.push_back({0, 0, r, (int)sr.size()});
 
@@ -1207,6 +1237,7 @@ int hitb200_plan_create(const hitb200_desc* d, hitb200_plan** out) {
   HB_PUT(p->d_tiles32, tiles32.data(), tiles32.size() * sizeof(Work));
   HB_PUT(p->d_xlines, xl.data(), xl.size() * sizeof(Work));
   HB_PUT(p->d_ylines, yl.data(), yl.size() * sizeof(Work));
+  HB_PUT(p->d_ylines2, yl2.data(), yl2.size() * sizeof(Work));
   HB_PUT(p->d_srows, sr.data(), sr.size() * sizeof(Work));
   HB_PUT(p->d_solve, &s, sizeof(SolveDev));
 #undef HB_PUT
@@ -1216,7 +1247,7 @@ int hitb200_plan_create(const hitb200_desc* d, hitb200_plan** out) {
     delete p;
     return cuda_fail(e, "cudaMemset(counters)");
   }
-  prime_attributes(p->elem, mch_for(nx), mch_for(ny), p->smem_x, p->smem_y, p->smem_sensor, p->sensor_w,
+  prime_attributes(p->elem, mch_for(nx), mch_for(ny), p->smem_x, std::max(p->smem_y, p->smem_y2), p->smem_sensor, p->sensor_w,
                    p->smem_sensor_step);
   {
     // the fused sensor needs every tile's CTA resident at once (grid barrier)
@@ -1654,6 +1685,19 @@ static int batch_build(hitb200_batch* b) {
     }
     if (cols < 4L * sms) ry4 = 0;
   }
+  // the other panel width: each plan's own where the default is 4, else 4
+  // where every member's 4-column panel fits
+  bool has_y2 = true;
+  if (!ry4)
+    for (hitb200_plan* p : b->plans) {
+      const size_t by = p->elem == 4 ? SweepLayout<float>(p->desc.ny, 4).bytes()
+                                     : SweepLayout<double>(p->desc.ny, 4).bytes();
+      if (by > 110 * 1024 || p->desc.nx < 4) has_y2 = false;
+    }
+  std::vector<Work> yl2;
+  b->off_yl2.clear();
+  b->ry_max2 = 1;
+  b->smem_y2 = 0;
   auto mark = [&]() {
     b->off_tiles.push_back((int)tiles.size());
     b->off_tiles32.push_back((int)tiles32.size());
@@ -1678,6 +1722,14 @@ static int batch_build(hitb200_batch* b) {
     for (int r0 = 0; r0 < p->desc.ny; r0 += p->Rx) xl.push_back({i, r0, std::min(p->Rx, p->desc.ny - r0), 0});
     const int ry = ry4 ? 4 : p->Ry;
     for (int c0 = 0; c0 < p->desc.nx; c0 += ry) yl.push_back({i, c0, std::min(ry, p->desc.nx - c0), 0});
+    b->off_yl2.push_back((int)yl2.size());
+    if (has_y2) {
+      const int ry2 = ry4 ? p->Ry : 4;
+      for (int c0 = 0; c0 < p->desc.nx; c0 += ry2) yl2.push_back({i, c0, std::min(ry2, p->desc.nx - c0), 0});
+      b->ry_max2 = std::max(b->ry_max2, ry2);
+      b->smem_y2 = std::max(b->smem_y2, p->elem == 4 ? SweepLayout<float>(p->desc.ny, ry2).bytes()
+                                                       : SweepLayout<double>(p->desc.ny, ry2).bytes());
+    }
     const int srows = synth_rows(p->desc.nx);
     for (int r0 = 0, ks = 0; r0 < p->desc.ny; r0 += srows) sr.push_back({i, 0, r0, ks++});
     ModeTables mt = build_modes(p->desc);
@@ -1700,6 +1752,9 @@ static int batch_build(hitb200_batch* b) {
     b->any_noise_upload |= (p->desc.forcing_on && p->desc.noise_mode != 1);
   }
   mark();
+  b->off_yl2.push_back((int)yl2.size());
+  b->has_y2 = has_y2;
+  b->n_y2 = (int)yl2.size();
   if (b->any_noise_upload) return invalid("batched solves draw forcing noise with the device RNG (noise_mode 1)");
   b->n_tiles = (int)tiles.size();
   b->n_tiles32 = (int)tiles32.size();
@@ -1708,8 +1763,8 @@ static int batch_build(hitb200_batch* b) {
   b->n_srows = (int)sr.size();
   default_tuning(b->n_x, b->n_y, b->n_tiles32, b->tuning);
   size_t bytes = hs.size() * sizeof(SolveDev) +
-                 (tiles.size() + tiles32.size() + xl.size() + yl.size() + sr.size()) * sizeof(Work) +
-                 partner.size() * sizeof(int) + 1024 + 7 * 256;
+                 (tiles.size() + tiles32.size() + xl.size() + yl.size() + yl2.size() + sr.size()) * sizeof(Work) +
+                 partner.size() * sizeof(int) + 1024 + 8 * 256;
   cudaError_t e = block_alloc(bytes, &b->tables);
   if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(batch tables)");
   unsigned char* buf = static_cast<unsigned char*>(b->tables.ptr);
@@ -1726,11 +1781,12 @@ static int batch_build(hitb200_batch* b) {
   b->d_tiles32 = reinterpret_cast<Work*>(put(tiles32.data(), tiles32.size() * sizeof(Work)));
   b->d_xlines = reinterpret_cast<Work*>(put(xl.data(), xl.size() * sizeof(Work)));
   b->d_ylines = reinterpret_cast<Work*>(put(yl.data(), yl.size() * sizeof(Work)));
+  b->d_ylines2 = yl2.empty() ? nullptr : reinterpret_cast<Work*>(put(yl2.data(), yl2.size() * sizeof(Work)));
   b->d_srows = reinterpret_cast<Work*>(put(sr.data(), sr.size() * sizeof(Work)));
   b->d_partner = reinterpret_cast<int*>(put(partner.data(), partner.size() * sizeof(int)));
   if (ce != cudaSuccess) return cuda_fail(ce, "cudaMemcpy(batch tables)");
   if (b->sensor_w < 0) b->smem_sensor_step = 0;
-  prime_attributes(b->elem, b->mch_x, b->mch_y, b->smem_x, b->smem_y, b->smem_sensor, b->sensor_w,
+  prime_attributes(b->elem, b->mch_x, b->mch_y, b->smem_x, std::max(b->smem_y, b->smem_y2), b->smem_sensor, b->sensor_w,
                    b->smem_sensor_step);
   // member plans use the batch's copy of their descriptor while batched
   for (int i = 0; i < n; ++i) {
@@ -1888,6 +1944,12 @@ static LaunchSet batch_launch_set(hitb200_batch* b, cudaStream_t st) {
   L.mch_y = b->mch_y;
   L.thr_x = kLineThreads * b->rx_max;
   L.thr_y = kLineThreads * b->ry_max;
+  const bool y2 = b->tuning[HITB200_TUNE_Y_PANEL] && b->has_y2;
+  if (y2) {
+    L.yl = b->d_ylines2;
+    L.n_y = b->n_y2;
+    L.thr_y = kLineThreads * b->ry_max2;
+  }
   L.occ_x = b->tuning[HITB200_TUNE_SWEEP_X];
   L.occ_y = b->tuning[HITB200_TUNE_SWEEP_Y];
   L.occ_pre = b->tuning[HITB200_TUNE_PREPASS];
@@ -1895,7 +1957,7 @@ static LaunchSet batch_launch_set(hitb200_batch* b, cudaStream_t st) {
   L.pdl = 0;    // many waves per launch: early CTAs of the next kernel would hold slots
                 // the current one still needs (8 x 512^2 HIT step 1.352 -> 1.364 ms with it)
   L.smem_x = b->smem_x;
-  L.smem_y = b->smem_y;
+  L.smem_y = y2 ? b->smem_y2 : b->smem_y;
   L.smem_sensor = b->smem_sensor;
   L.sensor_w = b->sensor_w;
   L.smem_sensor_step = b->smem_sensor_step;
@@ -1927,8 +1989,13 @@ static LaunchSet batch_sub_set(hitb200_batch* b, cudaStream_t st, int s0, int s1
   L.n_tiles32 = b->off_tiles32[s1] - b->off_tiles32[s0];
   L.xl = b->d_xlines + b->off_xl[s0];
   L.n_x = b->off_xl[s1] - b->off_xl[s0];
-  L.yl = b->d_ylines + b->off_yl[s0];
-  L.n_y = b->off_yl[s1] - b->off_yl[s0];
+  if (b->tuning[HITB200_TUNE_Y_PANEL] && b->has_y2) {
+    L.yl = b->d_ylines2 + b->off_yl2[s0];
+    L.n_y = b->off_yl2[s1] - b->off_yl2[s0];
+  } else {
+    L.yl = b->d_ylines + b->off_yl[s0];
+    L.n_y = b->off_yl[s1] - b->off_yl[s0];
+  }
   L.srows = b->d_srows + b->off_srows[s0];
   L.n_srows = b->off_srows[s1] - b->off_srows[s0];
   // work items name members by their index in the whole batch (L.solves stays

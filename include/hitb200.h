@@ -432,7 +432,12 @@ int hitb200_batch_run(hitb200_batch* batch, int32_t nsteps, void* stream);
  * (batches, larger grids).  Off by default.  Results are bit-identical
  * either way. */
 #define HITB200_TUNE_FUSED_SENSOR 3
-#define HITB200_TUNE_COUNT 4
+/* Tile shape of the y sweep: 0 = the default panel width (columns per CTA:
+ * 2 for single plans, 4 for batches with many columns), 1 = the other width
+ * (4 or 2) where every member's panel fits in shared memory; ignored
+ * otherwise.  Results are bit-identical either way. */
+#define HITB200_TUNE_Y_PANEL 4
+#define HITB200_TUNE_COUNT 5
 int hitb200_plan_set_tuning(hitb200_plan* plan, const int32_t* knobs, int32_t n);
 int hitb200_plan_get_tuning(const hitb200_plan* plan, int32_t* knobs, int32_t n);
 int hitb200_batch_set_tuning(hitb200_batch* batch, const int32_t* knobs, int32_t n);

@@ -23,7 +23,7 @@ def _mixed(n_hit=48, n_riem=40):
 @pytest.mark.parametrize("precision", ["fp32-bulk", "fp64"])
 def test_variants_give_identical_states(precision):
     finals = []
-    for knobs in ([0, 0, 0, 0], [1, 1, 1, 0], [1, 0, 1, 0]):
+    for knobs in ([0, 0, 0, 0, 0], [1, 1, 1, 0, 1], [1, 0, 1, 0, 0], [0, 1, 0, 0, 1]):
         sv = [serving.make_solver(serving.Request(0, "hit", 48, seed=3, mach=0.3, steps=10 ** 6), precision),
               serving.make_solver(serving.Request(1, "riemann3", 40, split=0.45), precision)]
         b = Batch.from_plans([s.plan for s in sv], [s.q for s in sv])
@@ -42,9 +42,10 @@ def test_variants_give_identical_states(precision):
 @pytest.mark.parametrize("kind,n", [("riemann6", 64), ("riemann3", 96), ("hit", 64)])
 def test_single_plan_variants_identical(kind, n):
     # includes the fused prepass + sensor (knob 3), whose grid-barrier path
-    # must reproduce the two-kernel path bit for bit
+    # must reproduce the two-kernel path bit for bit, and the y sweep's other
+    # panel width (knob 4)
     out = []
-    for knobs in ([0, 0, 0, 0], [1, 1, 1, 0], [0, 0, 0, 1], [1, 1, 1, 1]):
+    for knobs in ([0, 0, 0, 0, 0], [1, 1, 1, 0, 0], [0, 0, 0, 1, 1], [1, 1, 1, 1, 1], [0, 1, 0, 0, 1]):
         s = serving.make_solver(serving.Request(0, kind, n, split=0.5, seed=4, steps=10 ** 6),
                                 "fp32-bulk")
         s.plan.set_tuning(knobs)
@@ -91,7 +92,7 @@ def test_autotune_choice_read_back_from_disk(tmp_path, monkeypatch):
         raise AssertionError("tuned again instead of reading the disk cache")
 
     monkeypatch.setattr(autotune, "_choose", no_timing)
-    s.plan.set_tuning([-1, -1, -1, -1])
+    s.plan.set_tuning([-1] * _lib.TUNE_COUNT)
     assert autotune.tune_plan(s.plan, s.q) == k
     assert s.plan.tuning == k
     autotune.clear_cache()
@@ -103,6 +104,6 @@ def test_tuning_knob_validation():
     with pytest.raises(ValueError):
         s.plan.set_tuning([2, 0, 0])
     with pytest.raises(ValueError):
-        s.plan.set_tuning([0, 0, 0, 0, 0])
-    s.plan.set_tuning([-1, -1, -1, -1])  # back to the launch-size default
+        s.plan.set_tuning([0] * (_lib.TUNE_COUNT + 1))
+    s.plan.set_tuning([-1] * _lib.TUNE_COUNT)  # back to the launch-size default
     assert set(s.plan.tuning) <= {0, 1}
