@@ -2336,28 +2336,19 @@ constexpr int kMaxScratchDevices = 64;
 
 static __device__ __align__(256) unsigned char g_dt_scratch[kDtScratchHead + 8 * kDtScratchTiles];
 
-std::mutex g_dt_scratch_mu;
-unsigned char* g_dt_scratch_addr[kMaxScratchDevices] = {};
-
 // Device address of g_dt_scratch on the current device.  In host code the
 // name g_dt_scratch is only a host-side stand-in, so the address is looked up
-// once per device with that device current (the first call on a device may
-// also load the module there) and then passed to the kernel.  The address
-// belongs to the device's context: after cudaDeviceReset the module is loaded
-// again elsewhere, so a process that resets a device must not call the entry
-// point on it again (the cached address would be stale).
+// with that device current on every call (the first call on a device may
+// also load the module there); it is not cached, so that a context created
+// again after cudaDeviceReset gets its own module's address.
 int dt_scratch_address(unsigned char** out) {
   int dev = 0;
   HB_CUDA(cudaGetDevice(&dev));
   if (dev < 0 || dev >= kMaxScratchDevices)
     return invalid("device ordinal out of range for the static time-step scratch");
-  std::lock_guard<std::mutex> lock(g_dt_scratch_mu);
-  if (!g_dt_scratch_addr[dev]) {
-    void* p = nullptr;
-    HB_CUDA(cudaGetSymbolAddress(&p, g_dt_scratch));
-    g_dt_scratch_addr[dev] = static_cast<unsigned char*>(p);
-  }
-  *out = g_dt_scratch_addr[dev];
+  void* p = nullptr;
+  HB_CUDA(cudaGetSymbolAddress(&p, g_dt_scratch));
+  *out = static_cast<unsigned char*>(p);
   return HITB200_OK;
 }
 

@@ -210,11 +210,10 @@ int hitb200_validate(hitb200_plan* plan, const double* q);
  * (held by every GPU that loads the library until exit): grids of more than
  * 1024 tiles of 32 x 32 cells are rejected with HITB200_ERR_UNSUPPORTED.  Its
  * ticket counter must be zero when a call starts; it is zero at module load
- * and each call leaves it zero.  The first call on a device looks up the
- * scratch address (and may load the module): make it before any stream
- * capture.  That address is kept for the life of the process, so after a
- * cudaDeviceReset the entry point must not be called on that device again.
- * All calls on a device share the scratch, so calls that may overlap on the
+ * and each call leaves it zero.  Each call looks up the scratch address of
+ * the current device's context (the first call on a device may load the
+ * module: make it before any stream capture), so the entry point stays valid
+ * after a cudaDeviceReset.  All calls on a device share the scratch, so calls that may overlap on the
  * GPU (other streams or threads) race.  A NaN in any cell makes dt NaN, as
  * the reference's np.max does. */
 int hitb200_stable_time_step_noalloc(const double* q, int32_t nx, int32_t ny, double dx,
