@@ -952,6 +952,7 @@ __global__ void __launch_bounds__(AXIS == 0 ? 256 : 512,
   const T alpha = T(AXIS == 0 ? __ldcg(&sc[S_ALPHA_X]) : sc[S_ALPHA_Y]);
   const int weno_all = S.scheme == 1;
   const int nm = AXIS == 0 ? R * (n + 2) : ((n + 2) << rsh);
+  unsigned anyf = 0;  // a flagged node among this thread's
 #pragma unroll 4
   for (int idx = threadIdx.x; idx < nm; idx += blockDim.x) {
     int r, p;
@@ -965,9 +966,13 @@ __global__ void __launch_bounds__(AXIS == 0 ? 256 : 512,
     }
     const int gp = fold_node(p - 1, n, per);
     const size_t o = AXIS == 0 ? (size_t)(line0 + r) * nx + gp : (size_t)gp * nx + line0 + r;
-    MK[r * (n + 2) + p] = weno_all ? 1 : (AXIS == 0 ? __ldcg(&mask[o]) : mask[o]);
+    const uint8_t mv = weno_all ? 1 : (AXIS == 0 ? __ldcg(&mask[o]) : mask[o]);
+    MK[r * (n + 2) + p] = mv;
+    anyf |= mv;
   }
-  __syncthreads();
+  // lines without a flagged node (most of a low-Mach HIT solve's) skip the
+  // WENO phase and the face flags
+  const bool anyflag = __syncthreads_or(anyf) != 0;
   if (!active) {
     if constexpr (AXIS == 0) pdl_wait();  // keeps the chain of waits unbroken
     return;
@@ -983,7 +988,7 @@ __global__ void __launch_bounds__(AXIS == 0 ? 256 : 512,
   // flagged face among itself and its neighbours) are found by ballot and
   // their (face, component) pairs are spread over the warp's lanes.
   const int nch = (n + 3 + 31) >> 5;
-  for (int task = warp; task < R * nch; task += nwarp) {
+  for (int task = warp; anyflag && task < R * nch; task += nwarp) {
     int r = 0, ch = task;
     while (ch >= nch) {
       ch -= nch;
@@ -1029,7 +1034,7 @@ __global__ void __launch_bounds__(AXIS == 0 ? 256 : 512,
 #pragma unroll
     for (int j = 0; j <= MN; ++j) {
       const int f = i0 - 1 + j;  // face f + 1/2
-      fl[j] = len > 0 && f <= n - 1 && flagged(mk, f);
+      fl[j] = anyflag && len > 0 && f <= n - 1 && flagged(mk, f);
     }
   }
 #pragma unroll
