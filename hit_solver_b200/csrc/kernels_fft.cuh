@@ -18,7 +18,7 @@
 // Power-of-two lengths take a faster kernel (fft_p2_kernel, below): radix-8
 // passes on points held in registers, real rows packed two to a complex
 // line.  Measured on a B200, rfft2 of 256 fields of 512^2: 2.0 ms with the
-// mixed-radix kernel, 0.85 ms with the radix-8 one (cuFFT: 0.47 ms).
+// mixed-radix kernel, 0.655 ms with the radix-8 one (cuFFT: 0.47 ms).
 #pragma once
 
 #include "common.cuh"
@@ -249,61 +249,51 @@ __global__ void __launch_bounds__(kFftThreads, 4)
   static_assert(!(IN_REAL && COLS), "real input is packed along rows only");
   extern __shared__ __align__(16) double2 fbuf[];
   double2* buf = fbuf;                // [L][n] points, slots fpad(l n + e)
-  double2* w = fbuf + kFftP2Slots;    // the n roots
+  double2* w = fbuf + kFftP2Slots;    // the passes' twiddles (at most n)
   const int L = kFftP2Points >> logn;  // complex lines of the CTA
   const int logL = 3 + 8 - logn;       // log2 L (kFftThreads = 256)
   const int clines = IN_REAL ? (lines + 1) >> 1 : lines;  // complex lines of a field
   const int groups = (clines + L - 1) / L;
   const int f = blockIdx.x / groups, g = blockIdx.x - f * groups;
-  for (int m = threadIdx.x; m < n; m += blockDim.x) {
-    double2 v = W[m];
-    if (sign > 0) v.y = -v.y;
-    w[m] = v;
+  // Twiddles of the radix-8 passes, one table per pass (Ns = r0 8^i) laid
+  // out [r - 1][k] (r = 1..7, k < Ns): the lanes of a warp read consecutive
+  // k for each r, free of bank conflicts.  At most n entries in all.
+  const int r0 = logn % 3;  // a first radix-2 (1) or radix-4 (2) pass
+  {
+    int base = 0;
+    for (int ns = 1 << r0; ns < n; ns <<= 3) {
+      const int step = n / (8 * ns);
+      for (int e = threadIdx.x; e < 7 * ns; e += blockDim.x) {
+        const int r = e / ns + 1, k = e - (r - 1) * ns;
+        double2 v = W[r * k * step];  // r k step < n
+        if (sign > 0) v.y = -v.y;
+        w[base + e] = v;
+      }
+      base += 7 * ns;
+    }
   }
   // ---- load ----
   // The CTA's lines hold kFftP2Points complex points (2 kFftP2Points real
   // values): a fixed number per thread, all loads issued before their
   // shared-memory stores.
   if constexpr (IN_REAL) {
-    // real rows g 2L .. g 2L + 2L - 1; row 2l + h is the (h ? imaginary : real) part of line l
+    // real rows g 2L .. g 2L + 2L - 1: point e of line l is
+    // (row 2l, row 2l + 1)[e]; a thread loads both rows' values of its points
+    // and stores each point whole (16 bytes, no bank conflicts)
     const double* src = static_cast<const double*>(in) + f * li.field;
-    constexpr int K = 2 * kFftP2Points / kFftThreads;
-    double v[K];
-    if (li.elem == 1 && ((li.line | li.field) & 1) == 0 && (reinterpret_cast<uintptr_t>(in) & 15) == 0) {
-      // contiguous rows: two consecutive values a load (16 bytes)
+    constexpr int K = kFftP2Points / kFftThreads;
+    double va[K], vb[K];
 #pragma unroll
-      for (int i = 0; i < K / 2; ++i) {
-        const int idx = 2 * (threadIdx.x + i * kFftThreads);
-        const int rl = idx >> logn, e = idx & (n - 1);
-        const int row = g * 2 * L + rl;
-        const double2 t = row < lines ? *reinterpret_cast<const double2*>(src + (long long)row * li.line + e)
-                                      : make_double2(0.0, 0.0);
-        v[2 * i] = t.x;
-        v[2 * i + 1] = t.y;
-      }
-#pragma unroll
-      for (int i = 0; i < K / 2; ++i) {
-        const int idx = 2 * (threadIdx.x + i * kFftThreads);
-        const int rl = idx >> logn, e = idx & (n - 1);
-        double* d = reinterpret_cast<double*>(buf + fpad(((rl >> 1) << logn) + e)) + (rl & 1);
-        d[0] = v[2 * i];
-        reinterpret_cast<double*>(buf + fpad(((rl >> 1) << logn) + e + 1))[rl & 1] = v[2 * i + 1];
-      }
-    } else {
-#pragma unroll
-      for (int i = 0; i < K; ++i) {
-        const int idx = threadIdx.x + i * kFftThreads;
-        const int rl = idx >> logn, e = idx & (n - 1);
-        const int row = g * 2 * L + rl;
-        v[i] = row < lines ? src[(long long)row * li.line + (long long)e * li.elem] : 0.0;
-      }
-#pragma unroll
-      for (int i = 0; i < K; ++i) {
-        const int idx = threadIdx.x + i * kFftThreads;
-        const int rl = idx >> logn, e = idx & (n - 1);
-        reinterpret_cast<double*>(buf + fpad(((rl >> 1) << logn) + e))[rl & 1] = v[i];
-      }
+    for (int i = 0; i < K; ++i) {
+      const int idx = threadIdx.x + i * kFftThreads;
+      const int l = idx >> logn, e = idx & (n - 1);
+      const int row = g * 2 * L + 2 * l;
+      const long long o = (long long)row * li.line + (long long)e * li.elem;
+      va[i] = row < lines ? src[o] : 0.0;
+      vb[i] = row + 1 < lines ? src[o + li.line] : 0.0;
     }
+#pragma unroll
+    for (int i = 0; i < K; ++i) buf[fpad(threadIdx.x + i * kFftThreads)] = make_double2(va[i], vb[i]);
   } else {
     const double2* src = static_cast<const double2*>(in) + f * li.field;
     constexpr int K = kFftP2Points / kFftThreads;
@@ -334,7 +324,6 @@ __global__ void __launch_bounds__(kFftThreads, 4)
   const int lt = threadIdx.x >> (logn - 3), j = threadIdx.x & (T - 1);
   const int a0 = lt << logn;  // the line's first point
   int Ns = 1;
-  const int r0 = logn % 3;  // a first radix-2 (1) or radix-4 (2) pass
   if (r0 != 0) {
     const int R = 1 << r0;
     double2 x[8];
@@ -366,14 +355,14 @@ __global__ void __launch_bounds__(kFftThreads, 4)
     Ns = R;
     __syncthreads();
   }
-  for (; Ns < n; Ns <<= 3) {
+  for (int wb = 0; Ns < n; wb += 7 * Ns, Ns <<= 3) {
     double2 x[8];
 #pragma unroll
     for (int r = 0; r < 8; ++r) x[r] = buf[fpad(a0 + j + r * T)];
     const int k = j & (Ns - 1);
-    const int tk = k * (n / (8 * Ns));  // r tk < n
+    const double2* wp = w + wb + k;  // this pass's table, column k
 #pragma unroll
-    for (int r = 1; r < 8; ++r) x[r] = cmul(x[r], w[r * tk]);
+    for (int r = 1; r < 8; ++r) x[r] = cmul(x[r], wp[(r - 1) * Ns]);
     dft8(x, sign);
     __syncthreads();
     const int o = (j - k) * 8 + k;
@@ -383,16 +372,18 @@ __global__ void __launch_bounds__(kFftThreads, 4)
   }
   // ---- store ----
   if constexpr (IN_REAL) {
+    // both rows of line l from the same two points Z[k], Z[n - k]
     double2* dst = static_cast<double2*>(out) + f * lo.field;
-    for (int idx = threadIdx.x; idx < 2 * L * out_count; idx += blockDim.x) {
-      const int rl = idx / out_count, k = idx - rl * out_count;
-      const int row = g * 2 * L + rl;
+    for (int idx = threadIdx.x; idx < L * out_count; idx += blockDim.x) {
+      const int l = idx / out_count, k = idx - l * out_count;
+      const int row = g * 2 * L + 2 * l;
       if (row >= lines) continue;
-      const int z0 = (rl >> 1) << logn;
+      const int z0 = l << logn;
       const double2 zk = buf[fpad(z0 + (k & (n - 1)))], zm = buf[fpad(z0 + ((n - k) & (n - 1)))];
-      const double2 v = (rl & 1) ? make_double2(0.5 * (zk.y + zm.y), -0.5 * (zk.x - zm.x))
-                                 : make_double2(0.5 * (zk.x + zm.x), 0.5 * (zk.y - zm.y));
-      dst[(long long)row * lo.line + (long long)k * lo.elem] = make_double2(v.x * scale, v.y * scale);
+      const long long o = (long long)row * lo.line + (long long)k * lo.elem;
+      dst[o] = make_double2(0.5 * (zk.x + zm.x) * scale, 0.5 * (zk.y - zm.y) * scale);
+      if (row + 1 < lines)
+        dst[o + lo.line] = make_double2(0.5 * (zk.y + zm.y) * scale, -0.5 * (zk.x - zm.x) * scale);
     }
   } else if constexpr (COLS) {
     for (int idx = threadIdx.x; idx < L * out_count; idx += blockDim.x) {
