@@ -18,7 +18,7 @@
 // Power-of-two lengths take a faster kernel (fft_p2_kernel, below): radix-8
 // passes on points held in registers, real rows packed two to a complex
 // line.  Measured on a B200, rfft2 of 256 fields of 512^2: 2.0 ms with the
-// mixed-radix kernel, 0.655 ms with the radix-8 one (cuFFT: 0.47 ms).
+// mixed-radix kernel, 0.594 ms with the radix-8 one (cuFFT: 0.47 ms).
 #pragma once
 
 #include "common.cuh"
@@ -191,13 +191,17 @@ inline size_t fft_smem_bytes(int n, int C) { return (size_t)(2 * C + 1) * n * si
 // z = x_a + i x_b and are separated after the transform,
 // X_a[k] = (Z[k] + conj Z[n-k]) / 2, X_b[k] = -i (Z[k] - conj Z[n-k]) / 2.
 constexpr int kFftP2Points = 8 * kFftThreads;  // points of a CTA's lines
-// Shared-memory slot of point i: one pad slot after every 8 points, so that
-// the first pass's stride-8 stores fall on different banks.
-__device__ __forceinline__ int fpad(int i) { return i + (i >> 3); }
-constexpr int kFftP2Slots = kFftP2Points + kFftP2Points / 8;
+// Shared-memory slot of point e of the CTA's line l: one pad slot after
+// every 8 points (the first pass's stride-8 stores fall on different banks)
+// and 2 more per line (the 8 lanes of a quarter-warp that take 4 columns'
+// points of 2 rows fall on different banks).
+__device__ __forceinline__ int fslot(int l, int e, int lstr) { return l * lstr + e + (e >> 3); }
+__host__ __device__ inline int fft_p2_lstr(int n) { return n + n / 8 + 2; }
 
 __host__ __device__ inline bool fft_pow2_ok(int n) { return n >= 8 && n <= kFftMaxN && (n & (n - 1)) == 0; }
-inline size_t fft_p2_smem_bytes(int n) { return (size_t)(kFftP2Slots + n) * sizeof(double2); }
+inline size_t fft_p2_smem_bytes(int n) {
+  return (size_t)((kFftP2Points / n) * fft_p2_lstr(n) + n) * sizeof(double2);
+}
 
 __device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
 __device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
@@ -248,9 +252,10 @@ __global__ void __launch_bounds__(kFftThreads, 4)
                   double scale) {
   static_assert(!(IN_REAL && COLS), "real input is packed along rows only");
   extern __shared__ __align__(16) double2 fbuf[];
-  double2* buf = fbuf;                // [L][n] points, slots fpad(l n + e)
-  double2* w = fbuf + kFftP2Slots;    // the passes' twiddles (at most n)
   const int L = kFftP2Points >> logn;  // complex lines of the CTA
+  const int lstr = fft_p2_lstr(n);
+  double2* buf = fbuf;                 // the CTA's lines, point (l, e) at fslot(l, e, lstr)
+  double2* w = fbuf + L * lstr;        // the passes' twiddles (at most n)
   const int logL = 3 + 8 - logn;       // log2 L (kFftThreads = 256)
   const int clines = IN_REAL ? (lines + 1) >> 1 : lines;  // complex lines of a field
   const int groups = (clines + L - 1) / L;
@@ -293,7 +298,10 @@ __global__ void __launch_bounds__(kFftThreads, 4)
       vb[i] = row + 1 < lines ? src[o + li.line] : 0.0;
     }
 #pragma unroll
-    for (int i = 0; i < K; ++i) buf[fpad(threadIdx.x + i * kFftThreads)] = make_double2(va[i], vb[i]);
+    for (int i = 0; i < K; ++i) {
+      const int idx = threadIdx.x + i * kFftThreads;
+      buf[fslot(idx >> logn, idx & (n - 1), lstr)] = make_double2(va[i], vb[i]);
+    }
   } else {
     const double2* src = static_cast<const double2*>(in) + f * li.field;
     constexpr int K = kFftP2Points / kFftThreads;
@@ -314,29 +322,28 @@ __global__ void __launch_bounds__(kFftThreads, 4)
 #pragma unroll
     for (int i = 0; i < K; ++i) {
       const int idx = threadIdx.x + i * kFftThreads;
-      if constexpr (COLS) buf[fpad(((idx & (L - 1)) << logn) + (idx >> logL))] = v[i];
-      else buf[fpad(idx)] = v[i];
+      if constexpr (COLS) buf[fslot(idx & (L - 1), idx >> logL, lstr)] = v[i];
+      else buf[fslot(idx >> logn, idx & (n - 1), lstr)] = v[i];
     }
   }
   __syncthreads();
   // ---- passes ----
   const int T = n >> 3;  // threads of a line
   const int lt = threadIdx.x >> (logn - 3), j = threadIdx.x & (T - 1);
-  const int a0 = lt << logn;  // the line's first point
   int Ns = 1;
   if (r0 != 0) {
     const int R = 1 << r0;
     double2 x[8];
 #pragma unroll
-    for (int i = 0; i < 8; ++i) x[i] = buf[fpad(a0 + j + i * T)];  // the 8 / R butterflies of this thread
+    for (int i = 0; i < 8; ++i) x[i] = buf[fslot(lt, j + i * T, lstr)];  // the 8 / R butterflies of this thread
     __syncthreads();
     if (R == 2) {
       // butterflies b = j + s T (s < 4): inputs b, b + n / 2 = x[s], x[s + 4]
 #pragma unroll
       for (int s = 0; s < 4; ++s) {
         const int b = j + s * T;
-        buf[fpad(a0 + 2 * b)] = cadd(x[s], x[s + 4]);
-        buf[fpad(a0 + 2 * b + 1)] = csub(x[s], x[s + 4]);
+        buf[fslot(lt, 2 * b, lstr)] = cadd(x[s], x[s + 4]);
+        buf[fslot(lt, 2 * b + 1, lstr)] = csub(x[s], x[s + 4]);
       }
     } else {
       // butterflies b = j + s T (s < 2): inputs b + r n / 4 = x[s + 2 r]
@@ -346,10 +353,10 @@ __global__ void __launch_bounds__(kFftThreads, 4)
         const double2 s0 = cadd(x[s], x[s + 4]), s1 = csub(x[s], x[s + 4]);
         const double2 s2 = cadd(x[s + 2], x[s + 6]);
         const double2 s3 = cmul_mi(csub(x[s + 2], x[s + 6]), sign);
-        buf[fpad(a0 + 4 * b)] = cadd(s0, s2);
-        buf[fpad(a0 + 4 * b + 1)] = cadd(s1, s3);
-        buf[fpad(a0 + 4 * b + 2)] = csub(s0, s2);
-        buf[fpad(a0 + 4 * b + 3)] = csub(s1, s3);
+        buf[fslot(lt, 4 * b, lstr)] = cadd(s0, s2);
+        buf[fslot(lt, 4 * b + 1, lstr)] = cadd(s1, s3);
+        buf[fslot(lt, 4 * b + 2, lstr)] = csub(s0, s2);
+        buf[fslot(lt, 4 * b + 3, lstr)] = csub(s1, s3);
       }
     }
     Ns = R;
@@ -358,7 +365,7 @@ __global__ void __launch_bounds__(kFftThreads, 4)
   for (int wb = 0; Ns < n; wb += 7 * Ns, Ns <<= 3) {
     double2 x[8];
 #pragma unroll
-    for (int r = 0; r < 8; ++r) x[r] = buf[fpad(a0 + j + r * T)];
+    for (int r = 0; r < 8; ++r) x[r] = buf[fslot(lt, j + r * T, lstr)];
     const int k = j & (Ns - 1);
     const double2* wp = w + wb + k;  // this pass's table, column k
 #pragma unroll
@@ -367,7 +374,7 @@ __global__ void __launch_bounds__(kFftThreads, 4)
     __syncthreads();
     const int o = (j - k) * 8 + k;
 #pragma unroll
-    for (int t = 0; t < 8; ++t) buf[fpad(a0 + o + t * Ns)] = x[t];
+    for (int t = 0; t < 8; ++t) buf[fslot(lt, o + t * Ns, lstr)] = x[t];
     __syncthreads();
   }
   // ---- store ----
@@ -378,8 +385,7 @@ __global__ void __launch_bounds__(kFftThreads, 4)
       const int l = idx / out_count, k = idx - l * out_count;
       const int row = g * 2 * L + 2 * l;
       if (row >= lines) continue;
-      const int z0 = l << logn;
-      const double2 zk = buf[fpad(z0 + (k & (n - 1)))], zm = buf[fpad(z0 + ((n - k) & (n - 1)))];
+      const double2 zk = buf[fslot(l, k & (n - 1), lstr)], zm = buf[fslot(l, (n - k) & (n - 1), lstr)];
       const long long o = (long long)row * lo.line + (long long)k * lo.elem;
       dst[o] = make_double2(0.5 * (zk.x + zm.x) * scale, 0.5 * (zk.y - zm.y) * scale);
       if (row + 1 < lines)
@@ -390,7 +396,7 @@ __global__ void __launch_bounds__(kFftThreads, 4)
       const int e = idx >> logL, c = idx & (L - 1);
       const int col = g * L + c;
       if (col >= lines) continue;
-      const double2 v = buf[fpad((c << logn) + e)];
+      const double2 v = buf[fslot(c, e, lstr)];
       const long long o = f * lo.field + (long long)col * lo.line + (long long)e * lo.elem;
       if constexpr (OUT_REAL) static_cast<double*>(out)[o] = v.x * scale;
       else static_cast<double2*>(out)[o] = make_double2(v.x * scale, v.y * scale);
@@ -400,7 +406,7 @@ __global__ void __launch_bounds__(kFftThreads, 4)
       const int l = idx / out_count, e = idx - l * out_count;
       const int row = g * L + l;
       if (row >= lines) continue;
-      const double2 v = buf[fpad((l << logn) + e)];
+      const double2 v = buf[fslot(l, e, lstr)];
       const long long o = f * lo.field + (long long)row * lo.line + (long long)e * lo.elem;
       if constexpr (OUT_REAL) static_cast<double*>(out)[o] = v.x * scale;
       else static_cast<double2*>(out)[o] = make_double2(v.x * scale, v.y * scale);
