@@ -606,13 +606,16 @@ constexpr unsigned long long kBulkWaitNs = 2000000000ull;  // bound of a copy wa
 //   MK  [R][n + 2]  sensor mask of nodes -1 .. n
 template <typename T>
 struct SweepLayout {
-  int n, LS, LW, R;
+  int n, LS, LW, R, LQ;
   __host__ __device__ SweepLayout(int n_, int R_) : n(n_), R(R_) {
     LS = (kSweepHalo + n + 16 + 7) & ~7;
+    // a line's 8 staged rows, plus 8 elements: the lines of a y panel, which
+    // a warp's lanes stage at the same node, start on different banks
+    LQ = 8 * LS + 8;
     LW = (n + 3 + 3) & ~3;
   }
   // byte offsets of the regions; the kernel and the host use the same ones
-  __host__ __device__ size_t off_wb() const { return (size_t)R * 8 * LS * sizeof(T); }
+  __host__ __device__ size_t off_wb() const { return (size_t)R * LQ * sizeof(T); }
   __host__ __device__ size_t off_mk() const { return off_wb() + (size_t)R * 4 * LW * sizeof(T); }
   __host__ __device__ size_t bytes() const {
     return (off_mk() + (size_t)R * (n + 2) + 15) & ~(size_t)15;
@@ -685,6 +688,30 @@ struct Affine {
 
 // Loads v[j] = row[base + j], j < N, from shared memory; 16-byte vector loads
 // when the start is aligned (always, for the thread layout of the sweep).
+// A thread's `len` consecutive values (len <= N) stored from index 0 of dst:
+// 16-byte stores when the run is whole and dst is aligned to 16 bytes (the
+// sweeps' derivative rows: every thread starts at a multiple of N of an
+// aligned row), so that the lanes' stores fall on different banks.
+template <typename T, int N>
+__device__ __forceinline__ void store_run(T* dst, const T (&v)[N], int len) {
+  constexpr int PER = 16 / sizeof(T);  // values per 16-byte store
+  if constexpr (N % PER == 0) {
+    if (len == N) {
+#pragma unroll
+      for (int k = 0; k < N; k += PER) {
+        if constexpr (sizeof(T) == 4)
+          *reinterpret_cast<float4*>(dst + k) = make_float4(v[k], v[k + 1], v[k + 2], v[k + 3]);
+        else
+          *reinterpret_cast<double2*>(dst + k) = make_double2(v[k], v[k + 1]);
+      }
+      return;
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < N; ++k)
+    if (k < len) dst[k] = v[k];
+}
+
 template <typename T, int N>
 __device__ __forceinline__ void load_run(const T* row, int base, T (&v)[N]) {
   constexpr int VEC = 16 / sizeof(T);
@@ -804,7 +831,7 @@ __global__ void __launch_bounds__(AXIS == 0 ? 256 : 512,
   const int rsh = R > 2 ? 2 : (R > 1 ? 1 : 0);  // R is 1 or 2 (x lines), up to 4 (y lines)
   const int RL = 1 << rsh;
   const SweepLayout<T> L(n, RL);
-  const int LS = L.LS, LW = L.LW;
+  const int LS = L.LS, LW = L.LW, LQ = L.LQ;
   const T g = T(S.gamma);
   const double h = AXIS == 0 ? S.dx : S.dy;
   const double* qin = bind.use ? bind.qin : stage_in(S, stage);
@@ -839,7 +866,7 @@ __global__ void __launch_bounds__(AXIS == 0 ? 256 : 512,
     pr = (g - T(1)) * (a3 - T(0.5) * rho * (u * u + v * v));
     pr = pr > T(kPFloor) ? pr : T(kPFloor);
     const T un = AXIS == 0 ? u : v;
-    T* f = FQ + r * 8 * LS + p;
+    T* f = FQ + r * LQ + p;
     f[0 * LS] = AXIS == 0 ? a1 : a2;
     f[1 * LS] = a1 * un + (AXIS == 0 ? pr : T(0));
     f[2 * LS] = a2 * un + (AXIS == 0 ? T(0) : pr);
@@ -1011,8 +1038,8 @@ __global__ void __launch_bounds__(AXIS == 0 ? 256 : 512,
     const int items = 4 * __popc(bal);
     for (int k = lane; k < items; k += 32) {
       const int c = k & 3, f = il0 + nth_set_bit(bal, k >> 2);
-      const T* F = FQ + (size_t)(r * 8 + c) * LS + kSweepHalo;
-      const T* Q = FQ + (size_t)(r * 8 + 4 + c) * LS + kSweepHalo;
+      const T* F = FQ + r * LQ + c * LS + kSweepHalo;
+      const T* Q = FQ + r * LQ + (4 + c) * LS + kSweepHalo;
       const int fe = per ? f : min(max(f, -1), n - 1);
       WB[(size_t)(r * 4 + c) * LW + f + 2] = weno_face<T>(F, Q, fe, alpha);
     }
@@ -1042,7 +1069,7 @@ __global__ void __launch_bounds__(AXIS == 0 ? 256 : 512,
     T H[MN + 1];
     if (len > 0) {
       T fv[MN + 8];  // F_c of nodes i0 - 4 .. i0 + MN + 3
-      load_run<T, MN + 8>(FQ + (size_t)(r * 8 + c) * LS, kSweepHalo + i0 - 4, fv);
+      load_run<T, MN + 8>(FQ + r * LQ + c * LS, kSweepHalo + i0 - 4, fv);
       const T* Wc = WB + (size_t)(r * 4 + c) * LW + 2;
 #pragma unroll
       for (int j = 0; j <= MN; ++j) {
@@ -1271,11 +1298,7 @@ __global__ void __launch_bounds__(AXIS == 0 ? 256 : 512,
     // R columns of a row, then the next row
     T* XS = WB;  // [R][4][LW]
 #pragma unroll
-    for (int k = 0; k < MN; ++k)
-      if (k < len) {
-#pragma unroll
-        for (int c = 0; c < 4; ++c) XS[(r * 4 + c) * LW + i0 + k] = x[c][k];
-      }
+    for (int c = 0; c < 4; ++c) store_run<T, MN>(XS + (r * 4 + c) * LW + i0, x[c], len);
     __syncthreads();
     T* rx = reinterpret_cast<T*>(S.rx);
     for (int idx = threadIdx.x; idx < (n << rsh); idx += blockDim.x) {
@@ -1352,11 +1375,7 @@ __global__ void __launch_bounds__(AXIS == 0 ? 256 : 512,
   // threads on consecutive nodes, so that every global access is coalesced.
   T* XS = WB;  // [R][4][LW]
 #pragma unroll
-  for (int k = 0; k < MN; ++k)
-    if (k < len) {
-#pragma unroll
-      for (int c = 0; c < 4; ++c) XS[(r * 4 + c) * LW + i0 + k] = x[c][k];
-    }
+  for (int c = 0; c < 4; ++c) store_run<T, MN>(XS + (r * 4 + c) * LW + i0, x[c], len);
   __syncthreads();  // derivatives and drag table ready; FQ free for the guard staging
   double* ST = reinterpret_cast<double*>(smem);  // new rows (guard staging), reuses FQ
   // Solve fields in registers and read-only inputs behind restrict-qualified
