@@ -499,7 +499,8 @@ def run_b200(args, world, rank, local):
                               "batched_gbs": STEP_BYTES_PER_CELL * B * cells * kb / tb / 1e9,
                               "batched_frac": STEP_BYTES_PER_CELL * B * cells * kb / tb / 1e9 / peak}},
         "tuning": {"knobs": "sweep_x, sweep_y, prepass: 0 latency / 1 throughput variant; "
-                            "fused prepass + sensor; y panel: 0 default / 1 other width "
+                            "fused prepass + sensor; y panel: 0 default / 1 other width; "
+                            "persistent stage launches (batches) "
                             "(hit_solver_b200.autotune)", **tuning},
         "gpu_launches": K * launches_per_step,
         "clocks": clk.summary(),

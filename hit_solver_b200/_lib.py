@@ -30,7 +30,8 @@ S_ALPHA_X, S_ALPHA_Y, S_DIV_RMS, S_VORT_RMS, S_DT, S_TIME, S_STEP, S_ACTIVE, S_M
 S_COUNT = 32
 # bits of the S_STATUS slot (HITB200_ST_*)
 ST_NONFINITE, ST_NONPOS_RHO, ST_NONPOS_P, ST_BARRIER, ST_NOISE = 1, 2, 4, 8, 16
-TUNE_SWEEP_X, TUNE_SWEEP_Y, TUNE_PREPASS, TUNE_FUSED_SENSOR, TUNE_Y_PANEL, TUNE_COUNT = 0, 1, 2, 3, 4, 5
+(TUNE_SWEEP_X, TUNE_SWEEP_Y, TUNE_PREPASS, TUNE_FUSED_SENSOR, TUNE_Y_PANEL, TUNE_PERSISTENT,
+ TUNE_COUNT) = range(7)
 
 NAN = float("nan")
 
@@ -213,7 +214,8 @@ def check_step_status(bits: int, label: str) -> None:
     raise).  The validation bits are left to the Riemann validation."""
     bits = int(bits)
     if bits & ST_BARRIER:
-        raise RuntimeError(f"{label}: a grid barrier of the fused prepass/sensor timed out")
+        raise RuntimeError(f"{label}: a bounded device wait (the fused prepass/sensor's grid barrier "
+                           "or a persistent stage's queue) timed out")
     if bits & ST_NOISE:
         raise RuntimeError(f"{label}: the device forcing-noise stream ran short of draws")
     if bits & ST_NONFINITE:

@@ -2,8 +2,11 @@
 
 Three kernel families have two compiled variants each: the x sweep, the y
 sweep and the prepass; a fourth knob fuses each prepass into the following
-sensor launch (single solves whose tiles all fit on the GPU at once), and a
-fifth picks the y sweep's tile shape (panels of 2 or 4 columns per CTA).
+sensor launch (single solves whose tiles all fit on the GPU at once), a
+fifth picks the y sweep's tile shape (panels of 2 or 4 columns per CTA), and
+a sixth runs each stage of a batch as one persistent launch (its members'
+prepass, sensor and sweep work from one queue) instead of one launch per
+phase.
 The latency variant keeps more registers per thread
 and suits launches that cannot fill the GPU (one 512^2 solve); the
 throughput variant fits more CTAs per SM and suits launches over many solves.
@@ -163,13 +166,15 @@ def _choose(profile_fn, set_fn, trials: int, run_fn=None) -> list[int]:
     (launch gaps matter there)."""
     ms = {}
     for variant in (0, 1):
-        set_fn([variant, variant, variant, 0, 0])
+        set_fn([variant] * len(_VARIANT_KNOBS) + [0] * (_lib.TUNE_COUNT - len(_VARIANT_KNOBS)))
         profile_fn()  # warm-up step of this variant
         ms[variant] = _profile_ms(profile_fn, trials)[0]
-    best = [0 if ms[0][k] <= ms[1][k] else 1 for k in _VARIANT_KNOBS] + [0, 0]
+    best = [0 if ms[0][k] <= ms[1][k] else 1 for k in _VARIANT_KNOBS]
+    best += [0] * (_lib.TUNE_COUNT - len(best))
     ym = {}
     for panel in (0, 1):
-        set_fn(best[:4] + [panel])
+        best[_lib.TUNE_Y_PANEL] = panel
+        set_fn(best)
         profile_fn()
         ym[panel] = _profile_ms(profile_fn, trials)[0][_lib.TUNE_SWEEP_Y]
     best[_lib.TUNE_Y_PANEL] = 0 if ym[0] <= ym[1] else 1
@@ -181,6 +186,26 @@ def _choose(profile_fn, set_fn, trials: int, run_fn=None) -> list[int]:
             step[fused] = _graph_ms(run_fn, max(4, 2 * trials))
         best[_lib.TUNE_FUSED_SENSOR] = 0 if step[0] <= step[1] else 1
     set_fn(best)
+    return best
+
+
+def _choose_persistent(batch, best: list[int], trials: int) -> list[int]:
+    """Persistent stage launches or one launch per phase, whichever gives the
+    shorter graph-replayed step (batches that cannot persist read the knob
+    back as 0 and keep it off)."""
+    trial = list(best)
+    trial[_lib.TUNE_PERSISTENT] = 1
+    batch.set_tuning(trial)
+    if batch.tuning[_lib.TUNE_PERSISTENT] != 1:
+        return best
+    step = {}
+    for persist in (0, 1):
+        trial[_lib.TUNE_PERSISTENT] = persist
+        batch.set_tuning(trial)
+        step[persist] = _graph_ms(batch.run, max(4, 2 * trials))
+    best = list(best)
+    best[_lib.TUNE_PERSISTENT] = 0 if step[0] <= step[1] else 1
+    batch.set_tuning(best)
     return best
 
 
@@ -199,6 +224,7 @@ def tune_batch(batch, trials: int = 3, use_cache: bool = True) -> list[int]:
                 sc = src.scalars()
                 m.set_time(sc[_lib.S_TIME], int(sc[_lib.S_STEP]), sc[_lib.S_DT], -1)
             best = _choose(scratch.step_profile, scratch.set_tuning, trials)
+            best = _choose_persistent(scratch, best, trials)
         finally:
             scratch.close()
             del scratch, plans, states

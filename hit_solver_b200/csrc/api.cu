@@ -25,6 +25,7 @@
 #include "kernels_spectra.cuh"
 #include "kernels_stencil.cuh"
 #include "sensor_step.cuh"
+#include "stage_persist.cuh"
 
 using namespace hitb200;
 
@@ -304,6 +305,7 @@ void default_tuning(int n_x, int n_y, int n_tiles32, int* t) {
   t[HITB200_TUNE_PREPASS] = n_tiles32 >= 4 * sms;
   t[HITB200_TUNE_FUSED_SENSOR] = 0;  // measured slower at 512^2; the autotuner decides
   t[HITB200_TUNE_Y_PANEL] = 0;
+  t[HITB200_TUNE_PERSISTENT] = 0;  // the autotuner decides (batches only)
 }
 
 }  // namespace
@@ -368,6 +370,19 @@ struct hitb200_batch {
   std::vector<int> off_yl2;
   int sensor_w = -1;  // shared width of the members' step sensor (-1: generic sensor)
   size_t smem_sensor_step = 0;
+  // Persistent stage launches (tuning knob HITB200_TUNE_PERSISTENT).  Launch
+  // groups: 0 all members (hitb200_batch_step), 1 and 2 the two halves of
+  // hitb200_batch_run's graph branches ([0, cut) and [cut, n)).
+  bool can_persist = false;
+  int cut = 1;
+  Work *d_xl4 = nullptr, *d_yl4 = nullptr;  // 4-row x groups and 4-column y panels
+  QItem* d_qitems = nullptr;
+  QCtl* d_qctl = nullptr;     // one queue per group
+  unsigned* d_qdep = nullptr;  // [members][4] phase counters
+  int q_off[4] = {};           // items of group g: [q_off[g], q_off[g + 1])
+  int q_npre[3] = {};          // prepass items at the start of group g
+  size_t smem_stage = 0, stage_sh_off = 0, stage_xstride = 0;  // dynamic shared memory layout
+  int stage_grid = 0;          // CTAs of a stage launch (all resident at once)
   int any_outflow = 0, any_forcing = 0, any_hv = 0, any_noise_upload = 0;
   cudaGraphExec_t graph = nullptr;
   cudaStream_t graph_stream = nullptr;
@@ -395,6 +410,14 @@ struct LaunchSet {
   double cells = 0, cells_visc = 0, cells_force = 0;
   int pdl = 0;  // launch the step's kernels with programmatic dependent launch
   int solve0 = 0;  // first member of a part of a batch (noise_rng's member 0)
+  // persistent stage launches (batches): the launch group's items and queue
+  int persist = 0;
+  const QItem* qitems = nullptr;
+  int nq = 0, nq_pre = 0, stage_grid = 0;
+  QCtl* qctl = nullptr;
+  unsigned* qdep = nullptr;
+  const Work *qtiles = nullptr, *xl4 = nullptr, *yl4 = nullptr;  // whole-batch lists
+  size_t smem_stage = 0, stage_sh_off = 0, stage_xstride = 0;
 };
 
 // A kernel launch on L's stream; with L.pdl the launch allows programmatic
@@ -502,6 +525,19 @@ void set_step_sensor_attr(size_t bytes) {
   }
 }
 
+// The persistent stage kernel's opt-in (per instantiation, by nodes per sweep
+// thread, and device).
+void set_stage_attr(const void* fn, int mch, size_t bytes) {
+  static size_t done[3][kMaxAttrDevices] = {};
+  const int dev = attr_device();
+  std::lock_guard<std::mutex> lock(g_attr_mu);
+  size_t& d = done[mch == 1 ? 0 : mch == 2 ? 1 : 2][dev];
+  if (bytes > d) {
+    cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    d = bytes;
+  }
+}
+
 template <typename T, int AXIS>
 void launch_sweep_t(const LaunchSet& L, int stage, int mode, const Bind& b) {
   const int mch = AXIS == 0 ? L.mch_x : L.mch_y;
@@ -581,6 +617,30 @@ void launch_presensor(const LaunchSet& L, int sel) {
   else launch_presensor_t<double>(L, sel);
 }
 
+// One SSP-RK3 stage of a batch's launch group in one persistent launch
+// (stage_persist.cuh); the first stage's list skips the prepass items.
+void launch_stage(const LaunchSet& L, int stage) {
+  const int skip = stage == 0 ? L.nq_pre : 0;
+  const int n = L.nq - skip;
+  const int grid = std::max(1, std::min(L.stage_grid, n));
+  const QItem* it = L.qitems + skip;
+  const int s0 = L.solve0, s1 = L.solve0 + L.nsolves;
+  // the sweeps' nodes per thread are the batch's (the line solves' order of
+  // operations depends on them)
+  void (*k)(const SolveDev*, const Work*, const Work*, const Work*, const QItem*, int, QCtl*, unsigned*, int,
+            int, int, unsigned, unsigned) = L.mch_x == 1   ? stage_kernel<float, 4, 1>
+                                  : L.mch_x == 2 ? stage_kernel<float, 4, 2>
+                                                 : stage_kernel<float, 4, 4>;
+  k<<<grid, kStageThreads, L.smem_stage, L.st>>>(L.solves, L.qtiles, L.yl4, L.xl4, it, n, L.qctl, L.qdep, s0,
+                                                  s1, stage, (unsigned)L.stage_sh_off, (unsigned)L.stage_xstride);
+}
+
+// The stage kernel of a batch (nodes per sweep thread mch on both axes).
+const void* stage_fn(int mch) {
+  return mch == 1 ? (const void*)stage_kernel<float, 4, 1>
+                  : mch == 2 ? (const void*)stage_kernel<float, 4, 2> : (const void*)stage_kernel<float, 4, 4>;
+}
+
 void launch_hv(const LaunchSet& L, const Bind& b) {
   if (L.elem == 4) launch_k(hv_kernel<float>, L.n_tiles, kStencilThreads, 0, L, L.solves, L.tiles, b);
   else launch_k(hv_kernel<double>, L.n_tiles, kStencilThreads, 0, L, L.solves, L.tiles, b);
@@ -641,6 +701,12 @@ int launch_step_sequence(const LaunchSet& L, int any_forcing, int noise_upload, 
     force_synth_kernel<<<L.n_srows, kRedThreads, 0, L.st>>>(L.solves, L.srows, nb);
   }
   for (int stage = 0; stage < 3; ++stage) {
+    if (L.persist) {
+      PMARK("stage", (stage == 0 ? 0 : 32 * N) + 33 * N + 3 * e * L.cells_visc + 33 * N + 4 * e * N +
+                         (stage == 0 ? 65 : 97) * N + 4 * e * N + 3 * e * L.cells_visc + 16 * L.cells_force);
+      launch_stage(L, stage);
+      continue;
+    }
     if (L.fused) {
       if (stage > 0) {
         PMARK("presensor", 65 * N + 3 * e * L.cells_visc);
@@ -1753,6 +1819,71 @@ static int batch_build(hitb200_batch* b) {
   }
   mark();
   b->off_yl2.push_back((int)yl2.size());
+  // The members in two groups (contiguous, balanced by cells) for the two
+  // branches of hitb200_batch_run's graph.
+  b->cut = n;
+  if (n > 1) {
+    double tot = 0.0, acc = 0.0;
+    for (hitb200_plan* p : b->plans) tot += (double)p->desc.nx * p->desc.ny;
+    for (b->cut = 1; b->cut < n - 1; ++b->cut) {
+      acc += (double)b->plans[b->cut - 1]->desc.nx * b->plans[b->cut - 1]->desc.ny;
+      if (acc >= 0.5 * tot) break;
+    }
+  }
+  // Persistent stage launches: FP32-bulk members with a shared step-sensor
+  // width and lines of at most 512 nodes (4 nodes per sweep thread).  Their
+  // sweep items are 4-row x groups and 4-column y panels of 512 threads;
+  // each launch group's queue holds its members' prepass tile pairs, sensor
+  // tiles, y panels and x groups, phase after phase.
+  std::vector<Work> xl4, yl4;
+  std::vector<QItem> qi;
+  {
+    int maxn = 0;
+    for (hitb200_plan* p : b->plans) maxn = std::max(maxn, std::max(p->desc.nx, p->desc.ny));
+    b->can_persist = b->elem == 4 && b->sensor_w == 4 && maxn <= 512 && b->mch_x == b->mch_y;
+  }
+  if (b->can_persist) {
+    std::vector<int> ox{0}, oy{0};
+    size_t sm = std::max(stage_pre_smem_bytes<float>(), (size_t)(kPreThreads + R_FIXED + 4 * kMaxDrag) * 8);
+    size_t xs = 0;
+    for (int i = 0; i < n; ++i) {
+      const hitb200_desc& d = b->plans[i]->desc;
+      for (int r0 = 0; r0 < d.ny; r0 += kStageLines) xl4.push_back({i, r0, std::min(kStageLines, d.ny - r0), 0});
+      for (int c0 = 0; c0 < d.nx; c0 += kStageLines) yl4.push_back({i, c0, std::min(kStageLines, d.nx - c0), 0});
+      ox.push_back((int)xl4.size());
+      oy.push_back((int)yl4.size());
+      xs = std::max(xs, SweepLayout<float>(d.nx, 1).bytes());
+      sm = std::max(sm, SweepLayout<float>(d.ny, kStageLines).bytes());
+    }
+    b->stage_xstride = (xs + 15) & ~(size_t)15;
+    sm = std::max(sm, kStageLines * b->stage_xstride);
+    b->stage_sh_off = (std::max(sm, b->smem_sensor_step) + 15) & ~(size_t)15;
+    b->smem_stage = b->stage_sh_off + kStageLines * sizeof(StageSweepShared<float>);
+    auto group = [&](int g, int g0, int g1) {
+      b->q_off[g] = (int)qi.size();
+      for (int i = g0; i < g1; ++i) {
+        const int t0 = b->off_tiles32[i], nt = b->off_tiles32[i + 1] - t0;
+        for (int k = 0; k < nt; k += 2) qi.push_back({Q_PRE, t0 + k, std::min(2, nt - k), 0, 0});
+      }
+      b->q_npre[g] = (int)qi.size() - b->q_off[g];
+      for (int i = g0; i < g1; ++i) {
+        const int t0 = b->off_tiles32[i], nt = b->off_tiles32[i + 1] - t0;
+        for (int k = 0; k < nt; ++k) qi.push_back({Q_SEN, t0 + k, 1, 1, 0});
+      }
+      for (int i = g0; i < g1; ++i) {
+        const int nt = b->off_tiles32[i + 1] - b->off_tiles32[i];
+        for (int k = oy[i]; k < oy[i + 1]; ++k) qi.push_back({Q_SWY, k, 1, nt, 0});
+      }
+      for (int i = g0; i < g1; ++i) {
+        const int nt = b->off_tiles32[i + 1] - b->off_tiles32[i];
+        for (int k = ox[i]; k < ox[i + 1]; ++k) qi.push_back({Q_SWX, k, 1, oy[i + 1] - oy[i], nt});
+      }
+    };
+    group(0, 0, n);
+    group(1, 0, b->cut);
+    group(2, b->cut, n);
+    b->q_off[3] = (int)qi.size();
+  }
   b->has_y2 = has_y2;
   b->n_y2 = (int)yl2.size();
   if (b->any_noise_upload) return invalid("batched solves draw forcing noise with the device RNG (noise_mode 1)");
@@ -1762,9 +1893,13 @@ static int batch_build(hitb200_batch* b) {
   b->n_y = (int)yl.size();
   b->n_srows = (int)sr.size();
   default_tuning(b->n_x, b->n_y, b->n_tiles32, b->tuning);
+  const std::vector<QCtl> qctl0(3, QCtl{0u, 0u, 0u, 0u});
+  const std::vector<unsigned> qdep0(b->can_persist ? 4 * (size_t)n : 0, 0u);
   size_t bytes = hs.size() * sizeof(SolveDev) +
-                 (tiles.size() + tiles32.size() + xl.size() + yl.size() + yl2.size() + sr.size()) * sizeof(Work) +
-                 partner.size() * sizeof(int) + 1024 + 8 * 256;
+                 (tiles.size() + tiles32.size() + xl.size() + yl.size() + yl2.size() + sr.size() + xl4.size() +
+                  yl4.size()) * sizeof(Work) +
+                 partner.size() * sizeof(int) + qi.size() * sizeof(QItem) + qctl0.size() * sizeof(QCtl) +
+                 qdep0.size() * sizeof(unsigned) + 1024 + 13 * 256;
   cudaError_t e = block_alloc(bytes, &b->tables);
   if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(batch tables)");
   unsigned char* buf = static_cast<unsigned char*>(b->tables.ptr);
@@ -1784,10 +1919,30 @@ static int batch_build(hitb200_batch* b) {
   b->d_ylines2 = yl2.empty() ? nullptr : reinterpret_cast<Work*>(put(yl2.data(), yl2.size() * sizeof(Work)));
   b->d_srows = reinterpret_cast<Work*>(put(sr.data(), sr.size() * sizeof(Work)));
   b->d_partner = reinterpret_cast<int*>(put(partner.data(), partner.size() * sizeof(int)));
+  if (b->can_persist) {
+    b->d_xl4 = reinterpret_cast<Work*>(put(xl4.data(), xl4.size() * sizeof(Work)));
+    b->d_yl4 = reinterpret_cast<Work*>(put(yl4.data(), yl4.size() * sizeof(Work)));
+    b->d_qitems = reinterpret_cast<QItem*>(put(qi.data(), qi.size() * sizeof(QItem)));
+    b->d_qctl = reinterpret_cast<QCtl*>(put(qctl0.data(), qctl0.size() * sizeof(QCtl)));
+    b->d_qdep = reinterpret_cast<unsigned*>(put(qdep0.data(), qdep0.size() * sizeof(unsigned)));
+  }
   if (ce != cudaSuccess) return cuda_fail(ce, "cudaMemcpy(batch tables)");
   if (b->sensor_w < 0) b->smem_sensor_step = 0;
   prime_attributes(b->elem, b->mch_x, b->mch_y, b->smem_x, std::max(b->smem_y, b->smem_y2), b->smem_sensor, b->sensor_w,
                    b->smem_sensor_step);
+  if (b->can_persist) {
+    // CTAs of a stage launch: as many as are resident at once
+    int dev = 0, sms = 148, nb = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const void* fn = stage_fn(b->mch_x);
+    set_stage_attr(fn, b->mch_x, b->smem_stage);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, kStageThreads, b->smem_stage) != cudaSuccess || nb < 1) {
+      cudaGetLastError();
+      b->can_persist = false;
+    } else {
+      b->stage_grid = nb * sms;
+    }
+  }
   // member plans use the batch's copy of their descriptor while batched
   for (int i = 0; i < n; ++i) {
     b->plans[i]->d_solve = b->d_solves + i;
@@ -1962,6 +2117,21 @@ static LaunchSet batch_launch_set(hitb200_batch* b, cudaStream_t st) {
   L.sensor_w = b->sensor_w;
   L.smem_sensor_step = b->smem_sensor_step;
   L.st = st;
+  L.persist = b->tuning[HITB200_TUNE_PERSISTENT] && b->can_persist;
+  if (b->can_persist) {
+    L.qitems = b->d_qitems + b->q_off[0];
+    L.nq = b->q_off[1] - b->q_off[0];
+    L.nq_pre = b->q_npre[0];
+    L.qctl = b->d_qctl;
+    L.qdep = b->d_qdep;
+    L.qtiles = b->d_tiles32;
+    L.xl4 = b->d_xl4;
+    L.yl4 = b->d_yl4;
+    L.smem_stage = b->smem_stage;
+    L.stage_sh_off = b->stage_sh_off;
+    L.stage_xstride = b->stage_xstride;
+    L.stage_grid = b->stage_grid;
+  }
   for (hitb200_plan* p : b->plans) {
     const double n = (double)p->desc.nx * p->desc.ny;
     L.cells += n;
@@ -2002,6 +2172,13 @@ static LaunchSet batch_sub_set(hitb200_batch* b, cudaStream_t st, int s0, int s1
   // the whole table); noise_rng takes the members from solve0 by CTA
   L.solve0 = s0;
   L.nsolves = s1 - s0;
+  if (b->can_persist) {
+    const int g = (s0 == 0 && s1 == (int)b->plans.size()) ? 0 : (s0 == 0 ? 1 : 2);
+    L.qitems = b->d_qitems + b->q_off[g];
+    L.nq = b->q_off[g + 1] - b->q_off[g];
+    L.nq_pre = b->q_npre[g];
+    L.qctl = b->d_qctl + g;
+  }
   L.cells = L.cells_visc = L.cells_force = 0.0;
   for (int i = s0; i < s1; ++i) {
     const hitb200_desc& d = b->plans[i]->desc;
@@ -2027,17 +2204,11 @@ int hitb200_batch_run(hitb200_batch* b, int32_t nsteps, void* stream) {
     // (3, 4 and 8 groups measured no better).  Results do not depend on it:
     // every kernel works on one member at a time.
     const int n = (int)b->plans.size();
-    int cut = n;
-    if (n > 1) {
-      double tot = 0.0, acc = 0.0;
-      for (hitb200_plan* p : b->plans) tot += (double)p->desc.nx * p->desc.ny;
-      for (cut = 1; cut < n - 1; ++cut) {
-        acc += (double)b->plans[cut - 1]->desc.nx * b->plans[cut - 1]->desc.ny;
-        if (acc >= 0.5 * tot) break;
-      }
-    }
-    const int r = capture_graph(n > 1 ? 2 : 1, [&](cudaStream_t* cs) {
-      if (n == 1) {
+    const int cut = b->cut;
+    // persistent stage launches fill the GPU by themselves: one branch
+    const bool one = n == 1 || (b->tuning[HITB200_TUNE_PERSISTENT] && b->can_persist);
+    const int r = capture_graph(one ? 1 : 2, [&](cudaStream_t* cs) {
+      if (one) {
         LaunchSet L = batch_launch_set(b, cs[0]);
         return launch_step_sequence(L, b->any_forcing, 0, b->any_outflow, b->any_hv);
       }
@@ -2074,6 +2245,7 @@ extern "C" int hitb200_plan_set_tuning(hitb200_plan* p, const int32_t* knobs, in
   if (!p) return invalid("NULL argument");
   if (p->in_batch) return invalid("plan belongs to a batch; tune the batch");
   const int r = tuning_set(p->tuning, knobs, n, p->n_x, p->n_y, p->n_tiles32);
+  p->tuning[HITB200_TUNE_PERSISTENT] = 0;  // a batch form
   if (r == HITB200_OK && p->graph) {
     cudaGraphExecDestroy(p->graph);
     p->graph = nullptr;
@@ -2091,6 +2263,7 @@ extern "C" int hitb200_plan_get_tuning(const hitb200_plan* p, int32_t* knobs, in
 extern "C" int hitb200_batch_set_tuning(hitb200_batch* b, const int32_t* knobs, int32_t n) {
   if (!b) return invalid("NULL argument");
   const int r = tuning_set(b->tuning, knobs, n, b->n_x, b->n_y, b->n_tiles32);
+  if (!b->can_persist) b->tuning[HITB200_TUNE_PERSISTENT] = 0;
   if (r == HITB200_OK && b->graph) {
     cudaGraphExecDestroy(b->graph);
     b->graph = nullptr;

@@ -237,6 +237,41 @@ __device__ __forceinline__ void enforce_node_rcp(T& q0, T& q1, T& q2, T& q3, T g
 __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 __device__ __forceinline__ void pdl_release() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 
+// The wait of a work item for the phase before it, in the kernels launched
+// one per phase: the programmatic-launch wait on the previous kernel.
+// (early() is the wait for an earlier kernel's output read before that:
+// complete at launch here.)  The work item runs on the whole CTA: tid(),
+// nthreads() and sync() are the CTA's thread index, size and barrier.
+struct PdlDep {
+  static constexpr bool kQueued = false;
+  static constexpr int kXR = 2;  // most x lines of a sweep item
+  __device__ __forceinline__ void wait() const { pdl_wait(); }
+  __device__ __forceinline__ void early() const {}
+  __device__ __forceinline__ void release() const { pdl_release(); }
+  __device__ __forceinline__ int tid() const { return threadIdx.x; }
+  __device__ __forceinline__ int nthreads() const { return blockDim.x; }
+  __device__ __forceinline__ void sync() const { __syncthreads(); }
+  __device__ __forceinline__ bool sync_or(bool p) const { return __syncthreads_or(p) != 0; }
+};
+
+// Barrier of the `count` threads of group `id` (1..15; barrier 0 is the
+// CTA's), optionally with the OR of a predicate over them.
+__device__ __forceinline__ void group_sync(unsigned id, unsigned count) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
+}
+__device__ __forceinline__ bool group_sync_or(unsigned id, unsigned count, bool p) {
+  unsigned r;
+  asm volatile(
+      "{\n\t.reg .pred pi, po;\n\t"
+      "setp.ne.u32 pi, %1, 0;\n\t"
+      "bar.red.or.pred po, %2, %3, pi;\n\t"
+      "selp.u32 %0, 1, 0, po;\n\t}"
+      : "=r"(r)
+      : "r"((unsigned)p), "r"(id), "r"(count)
+      : "memory");
+  return r != 0u;
+}
+
 // Bulk asynchronous copies (the TMA unit, no tensor map, no multicast) from
 // this GPU's global memory into this CTA's shared memory, completed on a
 // shared-memory mbarrier.  Source, destination and size are multiples of 16

@@ -169,17 +169,32 @@ __device__ __forceinline__ EnfPrim<T> enforced_prim(double q0, double q1, double
   return r;
 }
 
+// Shared memory of one prepass tile.
+template <typename T>
+struct PreShared {
+  T su[kTileY + 2][kTileX + 2];
+  T sv[kTileY + 2][kTileX + 2];
+  double2 tw[kTileY][kMaxKyDrag + 1];          // e^{-i k y}, k = 0..ky_drag, of the tile's rows
+  double cbuf[kPreWarps][4][32];               // per-warp column partials of one k
+  double ctab[kMaxKyDrag + 1][4][32];          // C_k(x) = sum_y m(x, y) e^{-i k y}
+  double sm[kPreWarps * (R_FIXED + 4 * kMaxDrag)];
+};
+
 // One tile of the prepass: every quantity it reduces, for the tile's cells,
 // into this CTA's row of partials (S.part_pre[w.c][*]); returns the number of
-// slots.  Runs on the first kPreThreads threads of the CTA; every thread of
-// the CTA must call it (it synchronises the CTA).
+// slots.  The tile runs on the kPreThreads threads whose index minus `tofs`
+// lies in [0, kPreThreads), with P as its shared memory; every thread of the
+// CTA must call it (it synchronises the CTA), with the same solve, mode and
+// `active` (a CTA may run two tiles at once, each half of its threads with its
+// own tofs and P).
 // Returns the number of reduction slots, or -1 when `active` is false: an
 // inactive solve's tile stops after its loads (issued before the caller's flag
 // arrives, so that they do not wait for it) and writes nothing.
 template <typename T>
 __device__ int prepass_tile(const SolveDev& S, const Work& w, int buf, int mode, int enf,
-                            const Bind& bind, bool active = true) {
-  const bool act = threadIdx.x < kPreThreads;
+                            const Bind& bind, bool active, PreShared<T>& P, int tofs = 0) {
+  const int tid = (int)threadIdx.x - tofs;
+  const bool act = tid >= 0 && tid < kPreThreads;
   const double* q = bind.use ? bind.qin : stage_in(S, buf);
   const int nx = S.nx, ny = S.ny, per = S.periodic;
   const size_t plane = (size_t)nx * ny;
@@ -196,16 +211,16 @@ __device__ int prepass_tile(const SolveDev& S, const Work& w, int buf, int mode,
   const int nslots = (mode == PRE_STAGE || mode == PRE_STEP) ? S.nred : R_FIXED;
   const int ndrag = nslots > R_FIXED ? S.n_drag : 0;
 
-  __shared__ T su[kTileY + 2][kTileX + 2];
-  __shared__ T sv[kTileY + 2][kTileX + 2];
-  __shared__ double2 tw[kTileY][kMaxKyDrag + 1];  // e^{-i k y}, k = 0..ky_drag, of the tile's rows
-  __shared__ double cbuf[kPreWarps][4][32];          // per-warp column partials of one k
-  __shared__ double ctab[kMaxKyDrag + 1][4][32];     // C_k(x) = sum_y m(x, y) e^{-i k y}
-  __shared__ double sm[kPreWarps * (R_FIXED + 4 * kMaxDrag)];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  auto& su = P.su;
+  auto& sv = P.sv;
+  auto& tw = P.tw;
+  auto& cbuf = P.cbuf;
+  auto& ctab = P.ctab;
+  double* sm = P.sm;
+  const int lane = threadIdx.x & 31, warp = tid >> 5;
 
   const int KY = ndrag > 0 ? S.ky_drag : -1;
-  for (int t = threadIdx.x; act && t < kTileY * (KY + 1); t += kPreThreads) {
+  for (int t = tid; act && t < kTileY * (KY + 1); t += kPreThreads) {
     const int a = t / (KY + 1), k = t - a * (KY + 1);
     const int gj = min(y0 + a, ny - 1);
     tw[a][k] = S.twy[mode_index(k, gj, ny)];
@@ -219,11 +234,11 @@ __device__ int prepass_tile(const SolveDev& S, const Work& w, int buf, int mode,
   const int gi = x0 + lane;
   // one-node ring for the central differences (corners are not used), loaded
   // first so that its latency overlaps the tile's
-  const bool ring = grads && threadIdx.x < 4 * kTileX;  // within the first kPreThreads
+  const bool ring = grads && act && tid < 4 * kTileX;
   int ra = 0, rb = 0;  // smem coordinates
   double rq[4] = {0.0, 0.0, 0.0, 0.0};
   if (ring) {
-    const int side = threadIdx.x >> 5, t = threadIdx.x & 31;
+    const int side = tid >> 5, t = tid & 31;
     if (side == 0) { ra = 0; rb = t + 1; }
     else if (side == 1) { ra = kTileY + 1; rb = t + 1; }
     else if (side == 2) { ra = t + 1; rb = 0; }
@@ -342,10 +357,10 @@ __device__ int prepass_tile(const SolveDev& S, const Work& w, int buf, int mode,
   }
   const double ax = double(axT), ay = double(ayT), mr = double(mrT), mp = double(mpT), me = double(meT);
   if (act) {
-  warp_to_smem4<OP_MAX>(ax, ay, mr, mp, sm, make_int4(R_AX, R_AY, R_RHO, R_P), nslots);
-  warp_to_smem4<OP_MAX>(me, sr, 0.0, 0.0, sm, make_int4(R_E, R_SR, -1, -1), nslots);
-  warp_to_smem4<OP_SUM>(div2, vort2, ps, vel2, sm, make_int4(R_DIV2, R_VORT2, R_PSUM, R_VEL2), nslots);
-  warp_to_smem<OP_SUM>(cs, sm, R_CSUM, nslots);
+  warp_to_smem4<OP_MAX>(ax, ay, mr, mp, sm, make_int4(R_AX, R_AY, R_RHO, R_P), nslots, warp);
+  warp_to_smem4<OP_MAX>(me, sr, 0.0, 0.0, sm, make_int4(R_E, R_SR, -1, -1), nslots, warp);
+  warp_to_smem4<OP_SUM>(div2, vort2, ps, vel2, sm, make_int4(R_DIV2, R_VORT2, R_PSUM, R_VEL2), nslots, warp);
+  warp_to_smem<OP_SUM>(cs, sm, R_CSUM, nslots, warp);
   bad = __reduce_or_sync(kFullMask, bad);
   if (lane == 0) {
     sm[warp * nslots + R_NONFINITE] = (bad & 1) ? 1.0 : 0.0;
@@ -373,7 +388,7 @@ __device__ int prepass_tile(const SolveDev& S, const Work& w, int buf, int mode,
     for (int j = 0; j < 4; ++j)
       if (act) cbuf[warp][j][lane] = v[j];
     __syncthreads();
-    if (warp < 4) {
+    if (act && warp < 4) {
       double acc = cbuf[0][warp][lane];
 #pragma unroll
       for (int ww = 1; ww < kPreWarps; ++ww) acc += cbuf[ww][warp][lane];
@@ -398,12 +413,12 @@ __device__ int prepass_tile(const SolveDev& S, const Work& w, int buf, int mode,
     // warp total of the four sums into lanes 0, 8, 16, 24 of sm row `warp`,
     // then straight to this CTA's partials
     const int sl = R_FIXED + 4 * md;
-    warp_to_smem4<OP_SUM>(v[0], v[1], v[2], v[3], sm, make_int4(sl, sl + 1, sl + 2, sl + 3), nslots);
+    warp_to_smem4<OP_SUM>(v[0], v[1], v[2], v[3], sm, make_int4(sl, sl + 1, sl + 2, sl + 3), nslots, warp);
     __syncwarp();
     if (lane < 4) S.part_pre[(size_t)w.c * nslots + sl + lane] = sm[warp * nslots + sl + lane];
   }
   __syncthreads();
-  for (int t = threadIdx.x; t < R_FIXED; t += kPreThreads) {
+  for (int t = tid; t < R_FIXED; t += kPreThreads) {
     if (!act) break;
     const int op = pre_op(t);
     double acc = sm[t];
@@ -420,9 +435,9 @@ __device__ int prepass_tile(const SolveDev& S, const Work& w, int buf, int mode,
 // every thread takes one slot and every C-th block (C = kPreThreads / slots),
 // with many loads in flight, and the C partials of a slot are combined in a
 // fixed order.  Every thread of the CTA must call it; the first kPreThreads
-// work.  The result is the same whichever CTA computes it.
-__device__ void prepass_finalize(const SolveDev& S, int nslots, double* red) {
-  __shared__ double chunk[kPreThreads];
+// work.  The result is the same whichever CTA computes it.  chunk is shared
+// scratch of kPreThreads doubles.
+__device__ void prepass_finalize(const SolveDev& S, int nslots, double* red, double* chunk) {
   const int C = max(1, kPreThreads / nslots);
   const int t = threadIdx.x % nslots, j = threadIdx.x / nslots;
   const int op = pre_op(t);
@@ -506,13 +521,15 @@ __global__ void __launch_bounds__(kPreThreads, OCC ? HITB200_PRE_MIN_BLOCKS : 2)
   pdl_wait();  // below: the state and scalars of the previous kernels
   if (mode == PRE_SENSOR && !bind.use && sc[S_HV_STEP] == 0.0) return;  // no hyperviscosity this step
   const bool active = !(mode == PRE_STAGE && !bind.use && sc[S_ACTIVE] == 0.0);
-  const int nslots = prepass_tile<T>(S, w, buf, mode, enf, bind, active);
+  __shared__ PreShared<T> ps;
+  const int nslots = prepass_tile<T>(S, w, buf, mode, enf, bind, active, ps);
   if (nslots < 0) return;
   pdl_release();
   if (!last_block(&S.counters[0], S.nblk_pre)) return;
   // ---- last CTA of this solve: fixed-order final reduction + scalar logic ----
   __shared__ double red[R_FIXED + 4 * kMaxDrag];
-  prepass_finalize(S, nslots, red);
+  __shared__ double chunk[kPreThreads];
+  prepass_finalize(S, nslots, red, chunk);
   if (threadIdx.x == 0) {
     prepass_scalars(S, red, sc, mode, bind.use);
     // a bounded wait of an earlier kernel of this solve that ran out

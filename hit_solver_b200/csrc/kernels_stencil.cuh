@@ -191,7 +191,10 @@ __global__ void __launch_bounds__(kSensorThreads, sizeof(T) == 8 ? 1 : HITB200_S
   }
   const int pre_mode = sel == 0 ? PRE_STEP : (sel == 3 ? PRE_SENSOR : PRE_STAGE);
   int pre_slots = 0;
-  if constexpr (FUSED) pre_slots = prepass_tile<T>(S, wk, sel == 3 ? 1 : sel, pre_mode, sel == 3 ? 0 : 1, bind);
+  if constexpr (FUSED) {
+    __shared__ PreShared<T> pre_sh;
+    pre_slots = prepass_tile<T>(S, wk, sel == 3 ? 1 : sel, pre_mode, sel == 3 ? 0 : 1, bind, true, pre_sh);
+  }
   const double* q = bind.use ? bind.qin : (sel == 3 ? S.q1 : stage_in(S, sel));
   uint8_t* mask = bind.use ? mask_out : S.mask;
   const int nx = S.nx, ny = S.ny, per = S.periodic;
@@ -334,7 +337,8 @@ __global__ void __launch_bounds__(kSensorThreads, sizeof(T) == 8 ? 1 : HITB200_S
     // order in every CTA), thresholds exactly as prepass_scalars forms them
     grid_barrier(&S.counters[4], &S.counters[5], gridDim.x, &S.counters[6]);
     __shared__ double fred[R_FIXED + 4 * kMaxDrag];
-    prepass_finalize(S, pre_slots, fred);
+    __shared__ double fchunk[kPreThreads];
+    prepass_finalize(S, pre_slots, fred, fchunk);
     // The last CTA past the barrier writes the scalar block (every CTA holds
     // the same reductions) and reports a wait that ran out: by then every
     // CTA that gave up has set the flag.
@@ -813,15 +817,43 @@ __device__ __forceinline__ void vst(E* p, const E (&v)[V]) {
   }
 }
 
-template <typename T, int AXIS, int MN, int OCC>
-__global__ void __launch_bounds__(AXIS == 0 ? 256 : 512,
-                                  AXIS == 0 ? (OCC ? kSweepMinBlocksX : 2) : (OCC ? kSweepMinBlocksY : 1))
-    sweep_kernel(const SolveDev* __restrict__ solves, const Work* __restrict__ work, int stage,
-                 int mode, Bind bind) {
-  extern __shared__ __align__(16) unsigned char smem[];
-  __shared__ Affine<T> scan_f[4][4], scan_b[4][4];  // per line, per warp totals
-  __shared__ T ends[4][4][4];                          // raw_0, raw_n-1, p_0, p_n-1
-  const Work wk = work[blockIdx.x];
+// Line of a node index `idx` among consecutive runs of `len` (x lines of a
+// work item: at most 2, or 4 in the persistent stage kernel).
+template <int XR>
+__device__ __forceinline__ int xline_of(int idx, int len) {
+  if constexpr (XR <= 2) return idx >= len ? 1 : 0;
+  else return (idx >= len ? 1 : 0) + (idx >= 2 * len ? 1 : 0) + (idx >= 3 * len ? 1 : 0);
+}
+
+// Statically sized shared memory of a sweep work item; XR is the most x lines
+// an item holds (1 for the y sweep, which has no drag rows).
+template <typename T, int XR>
+struct SweepShared {
+  Affine<T> scan_f[4][4], scan_b[4][4];  // per line, per warp totals
+  T ends[4][4][4];                         // raw_0, raw_n-1, p_0, p_n-1
+  T rpow[kPowTab];                         // rho^k for the outflow end rows
+  double2 dpx[XR][kMaxKx + 1], dpy[XR][kMaxKx + 1];  // drag band rows (x sweep)
+  unsigned long long tbar;                 // bulk-copy barrier (x sweep)
+};
+
+// The work of one CTA of the sweep (work item wk), or of a group of its
+// threads.  Dep is the wait for the previous phase: PdlDep in the sweep
+// kernels (programmatic dependent launch), the persistent stage kernel's
+// counter wait otherwise (Dep::kQueued; then every value the same launch may
+// have written is read through L2).  Dep also names the item's threads
+// (tid, nthreads), their barrier (sync, sync_or) and the most x lines an
+// item holds (kXR).
+template <typename T, int AXIS, int MN, typename Dep, typename SH>
+__device__ __forceinline__ void sweep_body(const SolveDev* __restrict__ solves, const Work wk, int stage,
+                                           int mode, Bind bind, unsigned char* smem, SH& sh,
+                                           const Dep& dep) {
+  constexpr bool QD = Dep::kQueued;
+  constexpr int XR = Dep::kXR;
+  // the item's threads (the CTA, or a group of it) and their barrier
+  const int tid = dep.tid(), nthr = dep.nthreads();
+  auto& scan_f = sh.scan_f;
+  auto& scan_b = sh.scan_b;
+  auto& ends = sh.ends;
   const SolveDev& S = solves[wk.solve];
   const double* sc = S.scal;
   const int nx = S.nx, ny = S.ny, per = S.periodic;
@@ -839,10 +871,14 @@ __global__ void __launch_bounds__(AXIS == 0 ? 256 : 512,
   T* FQ = reinterpret_cast<T*>(smem);
   T* WB = reinterpret_cast<T*>(smem + L.off_wb());
   uint8_t* MK = smem + L.off_mk();
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
-  __shared__ T rpow[kPowTab];  // rho^k for the outflow end rows
+  const int lane = tid & 31, warp = tid >> 5, nwarp = nthr >> 5;
+  auto& rpow = sh.rpow;
+  auto ldsc = [&](int i) -> double {
+    if constexpr (QD) return __ldcg(sc + i);
+    else return sc[i];
+  };
   if (!per)
-    for (int t = threadIdx.x; t < kPowTab; t += blockDim.x) rpow[t] = T(__ldg(&g_rho_pow[t]));
+    for (int t = tid; t < kPowTab; t += nthr) rpow[t] = T(__ldg(&g_rho_pow[t]));
   auto rho_pow = [&](int k) -> T { return (k >= 0 && k < kPowTab) ? rpow[k] : T(0); };
 
   // ---- L: stage flux and enforced state of the lines ---------------------------
@@ -877,21 +913,21 @@ __global__ void __launch_bounds__(AXIS == 0 ? 256 : 512,
     f[7 * LS] = a3;
   };
   bool bulk = false;
-  if constexpr (AXIS == 0 && sizeof(T) == 4 && kSweepXBulk) {
+  if constexpr (AXIS == 0 && sizeof(T) == 4 && kSweepXBulk && !QD) {
     // x lines by bulk copies: the R rows' n interior nodes of each of the four
     // planes land as FP64 in shared memory through the copy engine; the
     // threads fetch the few halo nodes meanwhile
     bulk = !bind.use && (nx & 1) == 0 && (reinterpret_cast<uintptr_t>(qin) & 15) == 0;
   }
   if (bulk) {
-    __shared__ unsigned long long tbar;
+    auto& tbar = sh.tbar;
     // The FP64 landing rows [R][4][LS] take the place of FQ ([R][8][LS] of
     // T): each thread moves its nodes' values into registers before the
     // flux staging overwrites them.
     double* SQ = reinterpret_cast<double*>(smem);
-    if (threadIdx.x == 0) mbar_init(&tbar, 1);
-    __syncthreads();
-    if (threadIdx.x == 0) {
+    if (tid == 0) mbar_init(&tbar, 1);
+    dep.sync();
+    if (tid == 0) {
       mbar_expect_tx(&tbar, (unsigned)(R * 4 * n * sizeof(double)));
       for (int rr = 0; rr < R; ++rr)
         for (int c = 0; c < 4; ++c)
@@ -899,7 +935,7 @@ __global__ void __launch_bounds__(AXIS == 0 ? 256 : 512,
                    (unsigned)(n * sizeof(double)), &tbar);
     }
     const int nh = LS - n;  // halo slots of a line: p < kSweepHalo or p >= kSweepHalo + n
-    for (int idx = threadIdx.x; idx < R * 4 * nh; idx += blockDim.x) {
+    for (int idx = tid; idx < R * 4 * nh; idx += nthr) {
       const int rc = idx / nh, h = idx - rc * nh;
       const int pp = h < kSweepHalo ? h : h + n;
       const int gp = fold_node(pp - kSweepHalo, n, per);
@@ -914,8 +950,8 @@ __global__ void __launch_bounds__(AXIS == 0 ? 256 : 512,
       if ((++it & 63) == 0 && global_ns() - t0 > kBulkWaitNs) break;
       done = mbar_try_wait(&tbar, 0);
     }
-    if (__syncthreads_or(!done)) {
-      if (threadIdx.x == 0) atomicOr(&S.counters[6], 1u);
+    if (dep.sync_or(!done)) {
+      if (tid == 0) atomicOr(&S.counters[6], 1u);
       const unsigned long long t1 = global_ns();
       while (!mbar_try_wait(&tbar, 0) && global_ns() - t1 < kBulkWaitNs) {
       }
@@ -925,7 +961,7 @@ __global__ void __launch_bounds__(AXIS == 0 ? 256 : 512,
     T held[4][MN + 1];
 #pragma unroll
     for (int j = 0; j <= MN; ++j) {
-      const int idx = threadIdx.x + j * blockDim.x;
+      const int idx = tid + j * nthr;
       if (idx < nl) {
         const int r = idx >= LS ? 1 : 0, pp = idx - r * LS;
         const double* sq = SQ + r * 4 * LS + pp;
@@ -933,10 +969,10 @@ __global__ void __launch_bounds__(AXIS == 0 ? 256 : 512,
         for (int c = 0; c < 4; ++c) held[c][j] = T(sq[c * LS]);
       }
     }
-    __syncthreads();
+    dep.sync();
 #pragma unroll
     for (int j = 0; j <= MN; ++j) {
-      const int idx = threadIdx.x + j * blockDim.x;
+      const int idx = tid + j * nthr;
       if (idx < nl) {
         const int r = idx >= LS ? 1 : 0, pp = idx - r * LS;
         stage_node(r, pp, held[0][j], held[1][j], held[2][j], held[3][j]);
@@ -944,10 +980,10 @@ __global__ void __launch_bounds__(AXIS == 0 ? 256 : 512,
     }
   } else {
 #pragma unroll 4
-    for (int idx = threadIdx.x; idx < nl; idx += blockDim.x) {
+    for (int idx = tid; idx < nl; idx += nthr) {
       int r, p;
       if (AXIS == 0) {
-        r = idx >= LS ? 1 : 0;
+        r = xline_of<XR>(idx, LS);
         p = idx - r * LS;
       } else {
         r = idx & (RL - 1);
@@ -970,21 +1006,23 @@ __global__ void __launch_bounds__(AXIS == 0 ? 256 : 512,
   // sweep reads before its wait (mask, Lax-Friedrichs speed, flags) was
   // written two or more kernels earlier and is read from L2.
   if constexpr (AXIS == 1) {
-    pdl_wait();
-    pdl_release();
+    dep.wait();
+    dep.release();
+  } else {
+    dep.early();  // below: the mask and the Lax-Friedrichs speed
   }
   // a finished solve's launch is a no-op; its flag is tested once the staging
   // loads are in flight, so that they do not wait for the scalar block
-  const bool active = bind.use || (AXIS == 0 ? __ldcg(&sc[S_ACTIVE]) : sc[S_ACTIVE]) != 0.0;
-  const T alpha = T(AXIS == 0 ? __ldcg(&sc[S_ALPHA_X]) : sc[S_ALPHA_Y]);
+  const bool active = bind.use || ((AXIS == 0 || QD) ? __ldcg(&sc[S_ACTIVE]) : sc[S_ACTIVE]) != 0.0;
+  const T alpha = T(AXIS == 0 ? __ldcg(&sc[S_ALPHA_X]) : ldsc(S_ALPHA_Y));
   const int weno_all = S.scheme == 1;
   const int nm = AXIS == 0 ? R * (n + 2) : ((n + 2) << rsh);
   unsigned anyf = 0;  // a flagged node among this thread's
 #pragma unroll 4
-  for (int idx = threadIdx.x; idx < nm; idx += blockDim.x) {
+  for (int idx = tid; idx < nm; idx += nthr) {
     int r, p;
     if (AXIS == 0) {
-      r = idx >= n + 2 ? 1 : 0;
+      r = xline_of<XR>(idx, n + 2);
       p = idx - r * (n + 2);
     } else {
       r = idx & (RL - 1);
@@ -993,15 +1031,15 @@ __global__ void __launch_bounds__(AXIS == 0 ? 256 : 512,
     }
     const int gp = fold_node(p - 1, n, per);
     const size_t o = AXIS == 0 ? (size_t)(line0 + r) * nx + gp : (size_t)gp * nx + line0 + r;
-    const uint8_t mv = weno_all ? 1 : (AXIS == 0 ? __ldcg(&mask[o]) : mask[o]);
+    const uint8_t mv = weno_all ? 1 : ((AXIS == 0 || QD) ? __ldcg(&mask[o]) : mask[o]);
     MK[r * (n + 2) + p] = mv;
     anyf |= mv;
   }
   // lines without a flagged node (most of a low-Mach HIT solve's) skip the
   // WENO phase and the face flags
-  const bool anyflag = __syncthreads_or(anyf) != 0;
+  const bool anyflag = dep.sync_or(anyf) != 0;
   if (!active) {
-    if constexpr (AXIS == 0) pdl_wait();  // keeps the chain of waits unbroken
+    if constexpr (AXIS == 0) dep.wait();  // keeps the chain of waits unbroken
     return;
   }
 
@@ -1044,11 +1082,11 @@ __global__ void __launch_bounds__(AXIS == 0 ? 256 : 512,
       WB[(size_t)(r * 4 + c) * LW + f + 2] = weno_face<T>(F, Q, fe, alpha);
     }
   }
-  __syncthreads();
+  dep.sync();
 
   // ---- H: this thread's faces and raw differences, in registers ------------------
-  const int r = threadIdx.x >> 7;         // line of the CTA
-  const int tl = threadIdx.x & 127;       // thread within the line
+  const int r = tid >> 7;         // line of the CTA
+  const int tl = tid & 127;       // thread within the line
   const int lw = tl >> 5;                 // warp within the line
   const int i0 = tl * MN;                 // first node
   const int len = r < R ? max(0, min(MN, n - i0)) : 0;
@@ -1137,7 +1175,7 @@ __global__ void __launch_bounds__(AXIS == 0 ? 256 : 512,
 #pragma unroll
     for (int c = 0; c < 4; ++c) fe.a[c] = T(0);
   }
-  __syncthreads();
+  dep.sync();
   {
     const int rr = min(r, 3);
     Affine<T> pre, tot;  // maps of the warps before this one, and of the whole line
@@ -1209,7 +1247,7 @@ __global__ void __launch_bounds__(AXIS == 0 ? 256 : 512,
 #pragma unroll
     for (int c = 0; c < 4; ++c) be.a[c] = T(0);
   }
-  __syncthreads();
+  dep.sync();
   {
     const int rr = min(r, 3);
     Affine<T> post, tot;  // maps of the warps after this one (innermost last), whole line
@@ -1263,7 +1301,7 @@ __global__ void __launch_bounds__(AXIS == 0 ? 256 : 512,
         ends[r][c][3] = pl;
       }
     }
-    __syncthreads();
+    dep.sync();
     // the homogeneous terms are below roundoff beyond ~80 nodes from an end
     if (len > 0 && (i0 < 96 || i0 + len > n - 96)) {
       if (n == 1) {
@@ -1288,8 +1326,8 @@ __global__ void __launch_bounds__(AXIS == 0 ? 256 : 512,
 
   // ---- E: epilogue ----------------------------------------------------------------------
   if constexpr (AXIS == 0) {
-    pdl_wait();  // below: the y sweep's partial rhs
-    pdl_release();
+    dep.wait();  // below: the y sweep's partial rhs
+    dep.release();
   }
   const int terms = bind.use ? bind.terms : fused_terms(S);
   if (AXIS == 1) {
@@ -1299,9 +1337,9 @@ __global__ void __launch_bounds__(AXIS == 0 ? 256 : 512,
     T* XS = WB;  // [R][4][LW]
 #pragma unroll
     for (int c = 0; c < 4; ++c) store_run<T, MN>(XS + (r * 4 + c) * LW + i0, x[c], len);
-    __syncthreads();
+    dep.sync();
     T* rx = reinterpret_cast<T*>(S.rx);
-    for (int idx = threadIdx.x; idx < (n << rsh); idx += blockDim.x) {
+    for (int idx = tid; idx < (n << rsh); idx += nthr) {
       const int rr = idx & (RL - 1), p = idx >> rsh;
       if (rr >= R) continue;
       const size_t o = (size_t)p * nx + line0 + rr;
@@ -1332,8 +1370,8 @@ __global__ void __launch_bounds__(AXIS == 0 ? 256 : 512,
     return;
   }
   // x sweep: full rhs, then the stage combine and the clean filter
-  const double fs = sc[S_F_SCALE];
-  const double dt = sc[S_DT];
+  const double fs = ldsc(S_F_SCALE);
+  const double dt = ldsc(S_DT);
   const double* q0 = bind.use ? bind.q0 : S.q;
   double* qo = bind.use ? bind.qout : stage_out(S, stage);
   const T* ry = reinterpret_cast<const T*>(S.rx);
@@ -1341,11 +1379,12 @@ __global__ void __launch_bounds__(AXIS == 0 ? 256 : 512,
   // drag band S = -c lowpass(m) (OOP/hit2d.py:352-399) of the CTA's rows:
   // P_k(y) = sum over modes with |kx| = k of C_m e^{i ky y} (conjugated for
   // kx < 0), C_m the mode's scaled transform from the prepass
-  __shared__ double2 dpx[2][kMaxKx + 1], dpy[2][kMaxKx + 1];
+  auto& dpx = sh.dpx;
+  auto& dpy = sh.dpy;
   const bool drag = (terms & 8) && S.drag_on;
   if (drag) {
     const int K = S.kx_drag;
-    for (int t = threadIdx.x; t < R * (K + 1); t += blockDim.x) {
+    for (int t = tid; t < R * (K + 1); t += nthr) {
       const int rr = t / (K + 1), k = t - rr * (K + 1);
       const int row = line0 + rr;
       double2 sx = make_double2(0.0, 0.0), sy = make_double2(0.0, 0.0);
@@ -1355,8 +1394,19 @@ __global__ void __launch_bounds__(AXIS == 0 ? 256 : 512,
         const double2 e = S.twy[mode_index(km.y, row, ny)];
         const double er = e.x, ei = -e.y;  // e^{+i ky y}
         const double* cf = sc + S_DRAG + 4 * md;
-        double ar = cf[0] * er - cf[1] * ei, ai = cf[0] * ei + cf[1] * er;
-        double br = cf[2] * er - cf[3] * ei, bi = cf[2] * ei + cf[3] * er;
+        double ar, ai, br, bi;
+        if constexpr (QD) {
+          const double c0 = __ldcg(cf), c1 = __ldcg(cf + 1), c2 = __ldcg(cf + 2), c3 = __ldcg(cf + 3);
+          ar = c0 * er - c1 * ei;
+          ai = c0 * ei + c1 * er;
+          br = c2 * er - c3 * ei;
+          bi = c2 * ei + c3 * er;
+        } else {
+          ar = cf[0] * er - cf[1] * ei;
+          ai = cf[0] * ei + cf[1] * er;
+          br = cf[2] * er - cf[3] * ei;
+          bi = cf[2] * ei + cf[3] * er;
+        }
         if (km.x < 0) {
           ai = -ai;
           bi = -bi;
@@ -1376,11 +1426,11 @@ __global__ void __launch_bounds__(AXIS == 0 ? 256 : 512,
   T* XS = WB;  // [R][4][LW]
 #pragma unroll
   for (int c = 0; c < 4; ++c) store_run<T, MN>(XS + (r * 4 + c) * LW + i0, x[c], len);
-  __syncthreads();  // derivatives and drag table ready; FQ free for the guard staging
+  dep.sync();  // derivatives and drag table ready; FQ free for the guard staging
   double* ST = reinterpret_cast<double*>(smem);  // new rows (guard staging), reuses FQ
   // Solve fields in registers and read-only inputs behind restrict-qualified
   // pointers: the stores to the stage output below cannot force reloads.
-  const double gam = S.gamma, cool = (terms & 16) ? sc[S_COOL] : 0.0;
+  const double gam = S.gamma, cool = (terms & 16) ? ldsc(S_COOL) : 0.0;
   const bool visc = (terms & 2) && S.mu > 0.0;
   const int kxd = S.kx_drag;
   const T* __restrict__ visp = reinterpret_cast<const T*>(S.vis);
@@ -1408,8 +1458,8 @@ __global__ void __launch_bounds__(AXIS == 0 ? 256 : 512,
     // pass 1: the full rhs of every node in T, back into XS (the same thread
     // reads it in pass 2); the FP64 stage combine runs as a separate pass so
     // that neither pass holds the other's inputs in registers
-    for (int idx = threadIdx.x * V; idx < R * n; idx += blockDim.x * V) {
-      const int rr = idx >= n ? 1 : 0, col = idx - rr * n;
+    for (int idx = tid * V; idx < R * n; idx += nthr * V) {
+      const int rr = xline_of<XR>(idx, n), col = idx - rr * n;
       const int o = (line0 + rr) * nx + col;
       T acc[4][V];
 #pragma unroll
@@ -1518,8 +1568,8 @@ __global__ void __launch_bounds__(AXIS == 0 ? 256 : 512,
     }
     if (mode == SW_RHS) return;
     // pass 2: stage combine in FP64 and the clean filter
-    for (int idx = threadIdx.x * V; idx < R * n; idx += blockDim.x * V) {
-      const int rr = idx >= n ? 1 : 0, col = idx - rr * n;
+    for (int idx = tid * V; idx < R * n; idx += nthr * V) {
+      const int rr = xline_of<XR>(idx, n), col = idx - rr * n;
       const int o = (line0 + rr) * nx + col;
       double sv[4][V];
 #pragma unroll
@@ -1563,13 +1613,13 @@ __global__ void __launch_bounds__(AXIS == 0 ? 256 : 512,
   if (gc == 0 || mode != SW_STAGE) return;
   // Outflow guard fused: every row j takes row J(j) = clamp(j, g, ny-g-1) and
   // every column i column I(i); the CTA owning row J(j) writes row j.
-  __syncthreads();
+  dep.sync();
   for (int rr = 0; rr < R; ++rr) {
     const int j0 = line0 + rr;
     if (j0 != guard_src(j0, ny, gc)) continue;  // a guard row: written by its source
     const int jlo = j0 == gc ? 0 : j0, jhi = j0 == ny - gc - 1 ? ny - 1 : j0;
     const int cnt = (jhi - jlo + 1) * nx;
-    for (int idx = threadIdx.x; idx < cnt; idx += blockDim.x) {
+    for (int idx = tid; idx < cnt; idx += nthr) {
       const int jj = idx / nx, i = idx - jj * nx;
       const size_t o = (size_t)(jlo + jj) * nx + i;
       const int si = guard_src(i, nx, gc);
@@ -1577,6 +1627,16 @@ __global__ void __launch_bounds__(AXIS == 0 ? 256 : 512,
       for (int c = 0; c < 4; ++c) qo[c * plane + o] = ST[(size_t)(rr * 4 + c) * n + si];
     }
   }
+}
+
+template <typename T, int AXIS, int MN, int OCC>
+__global__ void __launch_bounds__(AXIS == 0 ? 256 : 512,
+                                  AXIS == 0 ? (OCC ? kSweepMinBlocksX : 2) : (OCC ? kSweepMinBlocksY : 1))
+    sweep_kernel(const SolveDev* __restrict__ solves, const Work* __restrict__ work, int stage,
+                 int mode, Bind bind) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ SweepShared<T, AXIS == 0 ? 2 : 1> sh;
+  sweep_body<T, AXIS, MN>(solves, work[blockIdx.x], stage, mode, bind, smem, sh, PdlDep{});
 }
 
 // =============================================================================

@@ -21,21 +21,22 @@ constexpr int kCellsPerThread = kTileY / kRedWarps;  // rows of the tile per thr
 
 enum RedOp : int { OP_SUM = 0, OP_MAX = 1 };
 
-// Reduce `v` over the CTA into sm[warp][slot] (call from all threads).
+// Reduce `v` over the CTA into sm[row][slot] (call from all threads); row is
+// the warp's index in the CTA unless the caller names it.
 template <int OP>
-__device__ __forceinline__ void warp_to_smem(double v, double* sm, int slot, int nslots) {
+__device__ __forceinline__ void warp_to_smem(double v, double* sm, int slot, int nslots, int row = -1) {
   v = OP == OP_SUM ? warp_sum(v) : warp_max(v);
-  if ((threadIdx.x & 31) == 0) sm[(threadIdx.x >> 5) * nslots + slot] = v;
+  if ((threadIdx.x & 31) == 0) sm[(row < 0 ? (int)(threadIdx.x >> 5) : row) * nslots + slot] = v;
 }
 
 // Reduce four values over the warp with 6 exchanges instead of 20: after two
 // halving steps each lane carries one of the four partial sums, then a
 // butterfly over the low three lane bits completes it.  Lanes 0, 8, 16 and 24
-// hold the totals of v0, v1, v2 and v3 and store them in sm[warp][slot_j]
-// (slot_j < 0: not stored).
+// hold the totals of v0, v1, v2 and v3 and store them in sm[row][slot_j]
+// (slot_j < 0: not stored; row as in warp_to_smem).
 template <int OP>
 __device__ __forceinline__ void warp_to_smem4(double v0, double v1, double v2, double v3, double* sm,
-                                              int4 slot, int nslots) {
+                                              int4 slot, int nslots, int row = -1) {
   const unsigned full = 0xffffffffu;
   const int lane = threadIdx.x & 31;
   auto op = [](double a, double b) { return OP == OP_SUM ? a + b : fmax(a, b); };
@@ -53,7 +54,7 @@ __device__ __forceinline__ void warp_to_smem4(double v0, double v1, double v2, d
   if ((lane & 7) == 0) {
     const int j = lane >> 3;
     const int sl = j == 0 ? slot.x : j == 1 ? slot.y : j == 2 ? slot.z : slot.w;
-    if (sl >= 0) sm[(threadIdx.x >> 5) * nslots + sl] = b;
+    if (sl >= 0) sm[(row < 0 ? (int)(threadIdx.x >> 5) : row) * nslots + sl] = b;
   }
 }
 

@@ -54,20 +54,25 @@ __host__ __device__ inline size_t step_sensor_smem_bytes(int elem, bool viscous)
   return step_sensor_visc_off<W>(elem) + (viscous ? 5 * (size_t)kVisX * kVisY * elem : 0);
 }
 
+// One tile (work item wk) of the step sensor, with dynamic shared memory smem.
 // sel: 0 q, 1 q1, 2 q2 (stage inputs, enforced first, viscous terms written
 // when the solve is viscous), 3 the hyperviscosity input (q1 on hyperviscosity
-// steps, not enforced, no viscous terms).
-template <typename T, int W>
-__global__ void __launch_bounds__(kSensorThreads, sizeof(T) == 8 ? 1 : HITB200_SENSOR_MIN_BLOCKS)
-    sensor_step_kernel(const SolveDev* __restrict__ solves, const Work* __restrict__ work, int sel,
-                       int enf, int want_visc) {
+// steps, not enforced, no viscous terms).  Dep is the wait for the prepass
+// (PdlDep in sensor_step_kernel; the persistent stage kernel's counter wait,
+// after which the scalars are read through L2).
+template <typename T, int W, typename Dep>
+__device__ __forceinline__ void sensor_step_body(const SolveDev* __restrict__ solves, const Work wk, int sel,
+                                                 int enf, int want_visc, unsigned char* smem,
+                                                 const Dep& dep) {
   using Sh = StepSensorShape<W>;
   constexpr int HW = Sh::HW, SX = Sh::SX, SY = Sh::SY, RX = Sh::RX, RY = Sh::RY;
   constexpr int OFF = Sh::OFF, NTASK = Sh::NTASK;
-  extern __shared__ __align__(16) unsigned char smem[];
-  const Work wk = work[blockIdx.x];
   const SolveDev& S = solves[wk.solve];
   const double* sc = S.scal;
+  auto ldsc = [&](int i) -> double {
+    if constexpr (Dep::kQueued) return __ldcg(sc + i);
+    else return sc[i];
+  };
   // the hyperviscosity flag is written by the step's first kernel
   if (sel == 3 && sc[S_HV_STEP] == 0.0) return;
   const double* __restrict__ q = sel == 3 ? S.q1 : stage_in(S, sel);
@@ -276,12 +281,12 @@ __global__ void __launch_bounds__(kSensorThreads, sizeof(T) == 8 ? 1 : HITB200_S
     }
   }
 
-  pdl_wait();  // below: the prepass's thresholds and the solve's flags
+  dep.wait();  // below: the prepass's thresholds and the solve's flags
   // a finished solve's launch is a no-op
-  if (sel != 3 && sc[S_ACTIVE] == 0.0) return;
-  pdl_release();
-  const double l_comp = sc[S_COMP_LIM], l_shear = sc[S_SHEAR_LIM];
-  const T eps_q[3] = {T(sc[S_EPS_RHO]), T(sc[S_EPS_P]), T(sc[S_EPS_E])};
+  if (sel != 3 && ldsc(S_ACTIVE) == 0.0) return;
+  dep.release();
+  const double l_comp = ldsc(S_COMP_LIM), l_shear = ldsc(S_SHEAR_LIM);
+  const T eps_q[3] = {T(ldsc(S_EPS_RHO)), T(ldsc(S_EPS_P)), T(ldsc(S_EPS_E))};
   const T comp_lim = T(l_comp), shear_lim = T(l_shear);
   const bool comp_on = isfinite(comp_lim), shear_on = isfinite(shear_lim);
 
@@ -386,6 +391,14 @@ __global__ void __launch_bounds__(kSensorThreads, sizeof(T) == 8 ? 1 : HITB200_S
       }
     }
   }
+}
+
+template <typename T, int W>
+__global__ void __launch_bounds__(kSensorThreads, sizeof(T) == 8 ? 1 : HITB200_SENSOR_MIN_BLOCKS)
+    sensor_step_kernel(const SolveDev* __restrict__ solves, const Work* __restrict__ work, int sel,
+                       int enf, int want_visc) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  sensor_step_body<T, W>(solves, work[blockIdx.x], sel, enf, want_visc, smem, PdlDep{});
 }
 
 }  // namespace hitb200

@@ -133,7 +133,7 @@ def member_error(kind: str, bits: int) -> tuple[str, str] | None:
     barrier that timed out.  None while the solve is sound."""
     bits = int(bits)
     if bits & _lib.ST_BARRIER:
-        return "RuntimeError", "a grid barrier of the fused prepass/sensor timed out"
+        return "RuntimeError", "a bounded device wait (grid barrier or persistent stage queue) timed out"
     if bits & _lib.ST_NONFINITE:
         return "FloatingPointError", "NaN or infinite value detected in the state"
     if kind != "hit" and bits & _lib.ST_NONPOS_RHO:

@@ -436,7 +436,17 @@ int hitb200_batch_run(hitb200_batch* batch, int32_t nsteps, void* stream);
  * (4 or 2) where every member's panel fits in shared memory; ignored
  * otherwise.  Results are bit-identical either way. */
 #define HITB200_TUNE_Y_PANEL 4
-#define HITB200_TUNE_COUNT 5
+/* 1: a batch advances each SSP-RK3 stage in one persistent launch: the
+ * stage's prepass, sensor, y-sweep and x-sweep work of every member taken
+ * from one queue, each item waiting (bounded) only for its own solve's
+ * previous phase.  Applies to FP32-bulk batches whose members all have
+ * sensor width 4, grid lines of at most 512 nodes, and longest x and y lines
+ * in the same class (up to 128, 256 or 512 nodes); elsewhere (and for single
+ * plans) it reads back 0.  Off by default; the
+ * autotuner keeps it where it measures faster.  Results are bit-identical
+ * either way. */
+#define HITB200_TUNE_PERSISTENT 5
+#define HITB200_TUNE_COUNT 6
 int hitb200_plan_set_tuning(hitb200_plan* plan, const int32_t* knobs, int32_t n);
 int hitb200_plan_get_tuning(const hitb200_plan* plan, int32_t* knobs, int32_t n);
 int hitb200_batch_set_tuning(hitb200_batch* batch, const int32_t* knobs, int32_t n);

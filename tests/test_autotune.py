@@ -23,12 +23,16 @@ def _mixed(n_hit=48, n_riem=40):
 @pytest.mark.parametrize("precision", ["fp32-bulk", "fp64"])
 def test_variants_give_identical_states(precision):
     finals = []
-    for knobs in ([0, 0, 0, 0, 0], [1, 1, 1, 0, 1], [1, 0, 1, 0, 0], [0, 1, 0, 0, 1]):
+    for knobs in ([0, 0, 0, 0, 0, 0], [1, 1, 1, 0, 1, 0], [1, 0, 1, 0, 0, 1], [0, 1, 0, 0, 1, 1]):
         sv = [serving.make_solver(serving.Request(0, "hit", 48, seed=3, mach=0.3, steps=10 ** 6), precision),
               serving.make_solver(serving.Request(1, "riemann3", 40, split=0.45), precision)]
         b = Batch.from_plans([s.plan for s in sv], [s.q for s in sv])
         b.set_tuning(knobs)
-        assert b.tuning == knobs
+        # the persistent stage form is an FP32-bulk batch form
+        want = list(knobs)
+        if precision == "fp64":
+            want[_lib.TUNE_PERSISTENT] = 0
+        assert b.tuning == want
         b.run(7)
         torch.cuda.synchronize()
         finals.append([s.q.clone() for s in sv])
@@ -45,7 +49,8 @@ def test_single_plan_variants_identical(kind, n):
     # must reproduce the two-kernel path bit for bit, and the y sweep's other
     # panel width (knob 4)
     out = []
-    for knobs in ([0, 0, 0, 0, 0], [1, 1, 1, 0, 0], [0, 0, 0, 1, 1], [1, 1, 1, 1, 1], [0, 1, 0, 0, 1]):
+    for knobs in ([0, 0, 0, 0, 0, 0], [1, 1, 1, 0, 0, 0], [0, 0, 0, 1, 1, 0], [1, 1, 1, 1, 1, 0],
+                  [0, 1, 0, 0, 1, 0]):
         s = serving.make_solver(serving.Request(0, kind, n, split=0.5, seed=4, steps=10 ** 6),
                                 "fp32-bulk")
         s.plan.set_tuning(knobs)
@@ -107,3 +112,78 @@ def test_tuning_knob_validation():
         s.plan.set_tuning([0] * (_lib.TUNE_COUNT + 1))
     s.plan.set_tuning([-1] * _lib.TUNE_COUNT)  # back to the launch-size default
     assert set(s.plan.tuning) <= {0, 1}
+
+
+def _uneven_members():
+    """FP32-bulk solves of uneven, non-square grids, some with line lengths
+    that are not multiples of 4 (the last x group / y panel of a member holds
+    fewer than 4 lines): production HIT (viscous, forced, drag, cooling,
+    hyperviscosity every 5 steps) and Riemann configurations 3 and 6
+    (outflow edges, guard cells, hyperviscosity every step)."""
+    from hit_solver_b200.hit2d import HITSolver
+    from hit_solver_b200.problems.riemann import RiemannConfig3, RiemannConfig6, RiemannSolver
+
+    import dataclasses
+
+    out = []
+    for i, (nx, ny) in enumerate([(64, 48), (96, 80), (37, 61), (128, 128)]):
+        cfg = serving.hit_request_config(64, 10 + i, 0.15 + 0.05 * i, 10 ** 6, "fp32-bulk")
+        out.append(HITSolver(dataclasses.replace(cfg, nx=nx, ny=ny)))
+    out.append(RiemannSolver(RiemannConfig3(nx=37, ny=29, x_split=0.45, y_split=0.55, precision="fp32-bulk")))
+    out.append(RiemannSolver(RiemannConfig6(nx=50, ny=66, precision="fp32-bulk")))
+    out.append(RiemannSolver(RiemannConfig3(nx=160, ny=144, precision="fp32-bulk")))
+    return out
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("steps", [1, 6])
+def test_persistent_stage_matches_per_phase_launches(steps):
+    """One persistent launch per RK3 stage (knob 5) against one launch per
+    phase: the same states bit for bit after every member's first step
+    (whose first stage has no prepass items) and after several steps,
+    replayed from the two-branch graph and stepped plainly."""
+    finals = {}
+    for persist in (0, 1):
+        for mode in ("run", "step"):
+            sv = _uneven_members()
+            b = Batch.from_plans([s.plan for s in sv], [s.q for s in sv])
+            knobs = [1, 1, 1, 0, 0, persist]
+            b.set_tuning(knobs)
+            assert b.tuning == knobs
+            if mode == "run":
+                b.run(steps)
+            else:
+                for _ in range(steps):
+                    b.step()
+            torch.cuda.synchronize()
+            for s in sv:
+                assert int(s.plan.scalars()[_lib.S_STATUS]) == 0
+            finals[persist, mode] = [s.q.clone() for s in sv]
+            b.close()
+    ref = finals[0, "run"]
+    for key, got in finals.items():
+        for a, c in zip(ref, got):
+            assert torch.equal(a, c), key
+
+
+@pytest.mark.gpu
+def test_persistent_stage_not_available_reads_back_zero():
+    """The persistent form needs FP32-bulk members of sensor width 4, lines
+    of at most 512 nodes and longest x and y lines in the same class (the
+    sweeps' nodes per thread); elsewhere the knob reads 0."""
+    from hit_solver_b200.problems.riemann import RiemannConfig3, RiemannSolver
+
+    cases = [
+        [serving.make_solver(serving.Request(0, "riemann3", 40), "fp64")],
+        [serving.make_solver(serving.Request(0, "riemann3", 640), "fp32-bulk")],
+        [RiemannSolver(RiemannConfig3(nx=200, ny=64, precision="fp32-bulk"))],
+        [RiemannSolver(RiemannConfig3(nx=64, ny=64, sensor_width=3, precision="fp32-bulk"))],
+    ]
+    for sv in cases:
+        b = Batch.from_plans([s.plan for s in sv], [s.q for s in sv])
+        b.set_tuning([0, 0, 0, 0, 0, 1])
+        assert b.tuning[_lib.TUNE_PERSISTENT] == 0
+        b.close()
+    s = serving.make_solver(serving.Request(0, "riemann3", 40), "fp32-bulk")
+    s.plan.set_tuning([0, 0, 0, 0, 0, 1])
+    assert s.plan.tuning[_lib.TUNE_PERSISTENT] == 0
