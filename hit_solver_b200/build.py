@@ -21,7 +21,7 @@ LIB = PKG / "libhitb200.so"
 SOURCES = ["api.cu"]
 HEADERS = ["common.cuh", "reduce.cuh", "weno.cuh", "kernels_reduce.cuh", "kernels_stencil.cuh",
            "kernels_spectra.cuh", "kernels_init.cuh", "sensor_step.cuh",
-           "kernels_fft.cuh", "kernels_npnoise.cuh", "ziggurat_table.inc"]
+           "kernels_fft.cuh", "kernels_npnoise.cuh", "ziggurat_table.inc", "stage_persist.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
