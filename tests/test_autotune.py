@@ -127,7 +127,10 @@ def _uneven_members():
 
     out = []
     for i, (nx, ny) in enumerate([(64, 48), (96, 80), (37, 61), (128, 128)]):
-        cfg = serving.hit_request_config(64, 10 + i, 0.15 + 0.05 * i, 10 ** 6, "fp32-bulk")
+        # the 37 x 61 solve stops after 3 steps: a finished member's items
+        # must still count for its phase counters
+        steps = 3 if i == 2 else 10 ** 6
+        cfg = serving.hit_request_config(64, 10 + i, 0.15 + 0.05 * i, steps, "fp32-bulk")
         out.append(HITSolver(dataclasses.replace(cfg, nx=nx, ny=ny)))
     out.append(RiemannSolver(RiemannConfig3(nx=37, ny=29, x_split=0.45, y_split=0.55, precision="fp32-bulk")))
     out.append(RiemannSolver(RiemannConfig6(nx=50, ny=66, precision="fp32-bulk")))
@@ -158,6 +161,7 @@ def test_persistent_stage_matches_per_phase_launches(steps):
             torch.cuda.synchronize()
             for s in sv:
                 assert int(s.plan.scalars()[_lib.S_STATUS]) == 0
+            assert int(sv[2].plan.scalars()[_lib.S_STEP]) == min(steps, 3)
             finals[persist, mode] = [s.q.clone() for s in sv]
             b.close()
     ref = finals[0, "run"]
