@@ -845,12 +845,14 @@ struct SweepShared {
 // item holds (kXR).
 template <typename T, int AXIS, int MN, typename Dep, typename SH>
 __device__ __forceinline__ void sweep_body(const SolveDev* __restrict__ solves, const Work wk, int stage,
-                                           int mode, Bind bind, unsigned char* smem, SH& sh,
+                                           int mode, const Bind& bind, unsigned char* smem, SH& sh,
                                            const Dep& dep) {
   constexpr bool QD = Dep::kQueued;
   constexpr int XR = Dep::kXR;
-  // the item's threads (the CTA, or a group of it) and their barrier
-  const int tid = dep.tid(), nthr = dep.nthreads();
+  // the item's threads (the CTA, or a group of it): read where used, as the
+  // special registers they are for the CTA
+  const auto tid = [&]() { return dep.tid(); };
+  const auto nthr = [&]() { return dep.nthreads(); };
   auto& scan_f = sh.scan_f;
   auto& scan_b = sh.scan_b;
   auto& ends = sh.ends;
@@ -871,14 +873,14 @@ __device__ __forceinline__ void sweep_body(const SolveDev* __restrict__ solves, 
   T* FQ = reinterpret_cast<T*>(smem);
   T* WB = reinterpret_cast<T*>(smem + L.off_wb());
   uint8_t* MK = smem + L.off_mk();
-  const int lane = tid & 31, warp = tid >> 5, nwarp = nthr >> 5;
+  const int lane = tid() & 31, warp = tid() >> 5, nwarp = nthr() >> 5;
   auto& rpow = sh.rpow;
   auto ldsc = [&](int i) -> double {
     if constexpr (QD) return __ldcg(sc + i);
     else return sc[i];
   };
   if (!per)
-    for (int t = tid; t < kPowTab; t += nthr) rpow[t] = T(__ldg(&g_rho_pow[t]));
+    for (int t = tid(); t < kPowTab; t += nthr()) rpow[t] = T(__ldg(&g_rho_pow[t]));
   auto rho_pow = [&](int k) -> T { return (k >= 0 && k < kPowTab) ? rpow[k] : T(0); };
 
   // ---- L: stage flux and enforced state of the lines ---------------------------
@@ -925,9 +927,9 @@ __device__ __forceinline__ void sweep_body(const SolveDev* __restrict__ solves, 
     // T): each thread moves its nodes' values into registers before the
     // flux staging overwrites them.
     double* SQ = reinterpret_cast<double*>(smem);
-    if (tid == 0) mbar_init(&tbar, 1);
+    if (tid() == 0) mbar_init(&tbar, 1);
     dep.sync();
-    if (tid == 0) {
+    if (tid() == 0) {
       mbar_expect_tx(&tbar, (unsigned)(R * 4 * n * sizeof(double)));
       for (int rr = 0; rr < R; ++rr)
         for (int c = 0; c < 4; ++c)
@@ -935,7 +937,7 @@ __device__ __forceinline__ void sweep_body(const SolveDev* __restrict__ solves, 
                    (unsigned)(n * sizeof(double)), &tbar);
     }
     const int nh = LS - n;  // halo slots of a line: p < kSweepHalo or p >= kSweepHalo + n
-    for (int idx = tid; idx < R * 4 * nh; idx += nthr) {
+    for (int idx = tid(); idx < R * 4 * nh; idx += nthr()) {
       const int rc = idx / nh, h = idx - rc * nh;
       const int pp = h < kSweepHalo ? h : h + n;
       const int gp = fold_node(pp - kSweepHalo, n, per);
@@ -951,7 +953,7 @@ __device__ __forceinline__ void sweep_body(const SolveDev* __restrict__ solves, 
       done = mbar_try_wait(&tbar, 0);
     }
     if (dep.sync_or(!done)) {
-      if (tid == 0) atomicOr(&S.counters[6], 1u);
+      if (tid() == 0) atomicOr(&S.counters[6], 1u);
       const unsigned long long t1 = global_ns();
       while (!mbar_try_wait(&tbar, 0) && global_ns() - t1 < kBulkWaitNs) {
       }
@@ -961,7 +963,7 @@ __device__ __forceinline__ void sweep_body(const SolveDev* __restrict__ solves, 
     T held[4][MN + 1];
 #pragma unroll
     for (int j = 0; j <= MN; ++j) {
-      const int idx = tid + j * nthr;
+      const int idx = tid() + j * nthr();
       if (idx < nl) {
         const int r = idx >= LS ? 1 : 0, pp = idx - r * LS;
         const double* sq = SQ + r * 4 * LS + pp;
@@ -972,7 +974,7 @@ __device__ __forceinline__ void sweep_body(const SolveDev* __restrict__ solves, 
     dep.sync();
 #pragma unroll
     for (int j = 0; j <= MN; ++j) {
-      const int idx = tid + j * nthr;
+      const int idx = tid() + j * nthr();
       if (idx < nl) {
         const int r = idx >= LS ? 1 : 0, pp = idx - r * LS;
         stage_node(r, pp, held[0][j], held[1][j], held[2][j], held[3][j]);
@@ -980,7 +982,7 @@ __device__ __forceinline__ void sweep_body(const SolveDev* __restrict__ solves, 
     }
   } else {
 #pragma unroll 4
-    for (int idx = tid; idx < nl; idx += nthr) {
+    for (int idx = tid(); idx < nl; idx += nthr()) {
       int r, p;
       if (AXIS == 0) {
         r = xline_of<XR>(idx, LS);
@@ -1019,7 +1021,7 @@ __device__ __forceinline__ void sweep_body(const SolveDev* __restrict__ solves, 
   const int nm = AXIS == 0 ? R * (n + 2) : ((n + 2) << rsh);
   unsigned anyf = 0;  // a flagged node among this thread's
 #pragma unroll 4
-  for (int idx = tid; idx < nm; idx += nthr) {
+  for (int idx = tid(); idx < nm; idx += nthr()) {
     int r, p;
     if (AXIS == 0) {
       r = xline_of<XR>(idx, n + 2);
@@ -1085,8 +1087,8 @@ __device__ __forceinline__ void sweep_body(const SolveDev* __restrict__ solves, 
   dep.sync();
 
   // ---- H: this thread's faces and raw differences, in registers ------------------
-  const int r = tid >> 7;         // line of the CTA
-  const int tl = tid & 127;       // thread within the line
+  const int r = tid() >> 7;         // line of the CTA
+  const int tl = tid() & 127;       // thread within the line
   const int lw = tl >> 5;                 // warp within the line
   const int i0 = tl * MN;                 // first node
   const int len = r < R ? max(0, min(MN, n - i0)) : 0;
@@ -1339,7 +1341,7 @@ __device__ __forceinline__ void sweep_body(const SolveDev* __restrict__ solves, 
     for (int c = 0; c < 4; ++c) store_run<T, MN>(XS + (r * 4 + c) * LW + i0, x[c], len);
     dep.sync();
     T* rx = reinterpret_cast<T*>(S.rx);
-    for (int idx = tid; idx < (n << rsh); idx += nthr) {
+    for (int idx = tid(); idx < (n << rsh); idx += nthr()) {
       const int rr = idx & (RL - 1), p = idx >> rsh;
       if (rr >= R) continue;
       const size_t o = (size_t)p * nx + line0 + rr;
@@ -1384,7 +1386,7 @@ __device__ __forceinline__ void sweep_body(const SolveDev* __restrict__ solves, 
   const bool drag = (terms & 8) && S.drag_on;
   if (drag) {
     const int K = S.kx_drag;
-    for (int t = tid; t < R * (K + 1); t += nthr) {
+    for (int t = tid(); t < R * (K + 1); t += nthr()) {
       const int rr = t / (K + 1), k = t - rr * (K + 1);
       const int row = line0 + rr;
       double2 sx = make_double2(0.0, 0.0), sy = make_double2(0.0, 0.0);
@@ -1458,7 +1460,7 @@ __device__ __forceinline__ void sweep_body(const SolveDev* __restrict__ solves, 
     // pass 1: the full rhs of every node in T, back into XS (the same thread
     // reads it in pass 2); the FP64 stage combine runs as a separate pass so
     // that neither pass holds the other's inputs in registers
-    for (int idx = tid * V; idx < R * n; idx += nthr * V) {
+    for (int idx = tid() * V; idx < R * n; idx += nthr() * V) {
       const int rr = xline_of<XR>(idx, n), col = idx - rr * n;
       const int o = (line0 + rr) * nx + col;
       T acc[4][V];
@@ -1568,7 +1570,7 @@ __device__ __forceinline__ void sweep_body(const SolveDev* __restrict__ solves, 
     }
     if (mode == SW_RHS) return;
     // pass 2: stage combine in FP64 and the clean filter
-    for (int idx = tid * V; idx < R * n; idx += nthr * V) {
+    for (int idx = tid() * V; idx < R * n; idx += nthr() * V) {
       const int rr = xline_of<XR>(idx, n), col = idx - rr * n;
       const int o = (line0 + rr) * nx + col;
       double sv[4][V];
@@ -1619,7 +1621,7 @@ __device__ __forceinline__ void sweep_body(const SolveDev* __restrict__ solves, 
     if (j0 != guard_src(j0, ny, gc)) continue;  // a guard row: written by its source
     const int jlo = j0 == gc ? 0 : j0, jhi = j0 == ny - gc - 1 ? ny - 1 : j0;
     const int cnt = (jhi - jlo + 1) * nx;
-    for (int idx = tid; idx < cnt; idx += nthr) {
+    for (int idx = tid(); idx < cnt; idx += nthr()) {
       const int jj = idx / nx, i = idx - jj * nx;
       const size_t o = (size_t)(jlo + jj) * nx + i;
       const int si = guard_src(i, nx, gc);

@@ -89,8 +89,8 @@ struct QueueDepT {
       if (et > 0u) eseen = *(const volatile unsigned*)ec;
     }
   }
-  __device__ __forceinline__ int tid() const { return SUB ? (int)(threadIdx.x % kLineThreads) : (int)threadIdx.x; }
-  __device__ __forceinline__ int nthreads() const { return SUB ? kLineThreads : (int)blockDim.x; }
+  __device__ __forceinline__ unsigned tid() const { return SUB ? threadIdx.x % kLineThreads : threadIdx.x; }
+  __device__ __forceinline__ unsigned nthreads() const { return SUB ? (unsigned)kLineThreads : blockDim.x; }
   __device__ __forceinline__ unsigned group() const { return 1u + threadIdx.x / kLineThreads; }
   __device__ __forceinline__ void sync() const {
     if constexpr (SUB) group_sync(group(), kLineThreads);
