@@ -205,6 +205,9 @@ __device__ int prepass_tile(const SolveDev& S, const Work& w, int buf, int mode,
   const T hx = T(S.dx), hy = T(S.dy);
   const T ih2x = T(1.0 / (2.0 * S.dx)), ih2y = T(1.0 / (2.0 * S.dy));
   const int x0 = w.a, y0 = w.b;
+  // ranges the plans guarantee, stated for the index arithmetic
+  __builtin_assume(nx >= 1 && nx <= kMaxLine && ny >= 1 && ny <= kMaxLine);
+  __builtin_assume(x0 >= 0 && x0 < kMaxLine && y0 >= 0 && y0 < kMaxLine);
   const bool grads = mode != PRE_CHECK;
   const bool rawq = mode == PRE_STEP || mode == PRE_CHECK;  // time step, Mach, validation
   const bool psum = S.cooling_on && (mode == PRE_STAGE || mode == PRE_STEP);

@@ -862,6 +862,12 @@ __device__ __forceinline__ void sweep_body(const SolveDev* __restrict__ solves, 
   const int n = AXIS == 0 ? nx : ny;
   const size_t plane = (size_t)nx * ny;
   const int line0 = wk.a, R = wk.b;
+  // ranges the plans guarantee (lines of 1..kMaxLine nodes, items of 1..4
+  // lines starting inside the grid), stated for the index arithmetic
+  if constexpr (AXIS == 0) {
+    __builtin_assume(nx >= 1 && nx <= kMaxLine && ny >= 1 && ny <= kMaxLine);
+    __builtin_assume(R >= 1 && R <= 4 && line0 >= 0 && line0 < kMaxLine);
+  }
   const int rsh = R > 2 ? 2 : (R > 1 ? 1 : 0);  // R is 1 or 2 (x lines), up to 4 (y lines)
   const int RL = 1 << rsh;
   const SweepLayout<T> L(n, RL);

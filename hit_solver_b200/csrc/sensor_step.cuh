@@ -79,6 +79,9 @@ __device__ __forceinline__ void sensor_step_body(const SolveDev* __restrict__ so
   const int nx = S.nx, ny = S.ny, per = S.periodic;
   const size_t plane = (size_t)nx * ny;
   const int x0 = wk.a, y0 = wk.b;
+  // ranges the plans guarantee, stated for the index arithmetic
+  __builtin_assume(nx >= 1 && nx <= kMaxLine && ny >= 1 && ny <= kMaxLine);
+  __builtin_assume(x0 >= 0 && x0 < kMaxLine && y0 >= 0 && y0 < kMaxLine);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   constexpr int NWARP = kSensorThreads / 32;
   const bool visc = want_visc && S.mu != 0.0;
