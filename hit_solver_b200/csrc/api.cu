@@ -370,6 +370,18 @@ struct hitb200_batch {
   std::vector<int> off_yl2;
   int sensor_w = -1;  // shared width of the members' step sensor (-1: generic sensor)
   size_t smem_sensor_step = 0;
+  // Sweep work by launch group (0 all members, 1 and 2 the halves of
+  // hitb200_batch_run's graph branches), list (0 x lines, 1 y panels, 2 y
+  // panels of the other width) and nodes-per-thread class (1, 2, 4, 8 nodes
+  // per sweep thread): each member's lines run in a launch of its own class,
+  // as when it runs alone (the line solves' order of operations depends on
+  // the class).
+  struct SegRec {
+    int off = 0, n = 0;
+    size_t smem = 0;
+  };
+  Work* d_segs = nullptr;
+  SegRec segs[3][3][4];
   // Persistent stage launches (tuning knob HITB200_TUNE_PERSISTENT).  Launch
   // groups: 0 all members (hitb200_batch_step), 1 and 2 the two halves of
   // hitb200_batch_run's graph branches ([0, cut) and [cut, n)).
@@ -414,6 +426,15 @@ struct LaunchSet {
   int persist = 0;
   const QItem* qitems = nullptr;
   int nq = 0, nq_pre = 0, stage_grid = 0;
+  // sweep launches: one per nodes-per-thread class present (single plans
+  // have one; a batch runs each member with its own class, as alone)
+  struct SweepSeg {
+    const Work* w;
+    int n, mch;
+    size_t smem;
+  };
+  SweepSeg sx[4] = {}, sy[4] = {};
+  int nsx = 0, nsy = 0;
   QCtl* qctl = nullptr;
   unsigned* qdep = nullptr;
   const Work *qtiles = nullptr, *xl4 = nullptr, *yl4 = nullptr;  // whole-batch lists
@@ -539,11 +560,11 @@ void set_stage_attr(const void* fn, int mch, size_t bytes) {
 }
 
 template <typename T, int AXIS>
-void launch_sweep_t(const LaunchSet& L, int stage, int mode, const Bind& b) {
-  const int mch = AXIS == 0 ? L.mch_x : L.mch_y;
-  const int nb = AXIS == 0 ? L.n_x : L.n_y;
-  const size_t sm = AXIS == 0 ? L.smem_x : L.smem_y;
-  const Work* w = AXIS == 0 ? L.xl : L.yl;
+void launch_sweep_seg(const LaunchSet& L, const LaunchSet::SweepSeg& g, int stage, int mode, const Bind& b) {
+  const int mch = g.mch;
+  const int nb = g.n;
+  const size_t sm = g.smem;
+  const Work* w = g.w;
   const int thr = AXIS == 0 ? L.thr_x : L.thr_y;
   const int occ = AXIS == 0 ? L.occ_x : L.occ_y;
 #define HB_SWEEP(M)                                                                        \
@@ -563,6 +584,12 @@ void launch_sweep_t(const LaunchSet& L, int stage, int mode, const Bind& b) {
     HB_SWEEP(8)
   }
 #undef HB_SWEEP
+}
+
+template <typename T, int AXIS>
+void launch_sweep_t(const LaunchSet& L, int stage, int mode, const Bind& b) {
+  const int ns = AXIS == 0 ? L.nsx : L.nsy;
+  for (int i = 0; i < ns; ++i) launch_sweep_seg<T, AXIS>(L, AXIS == 0 ? L.sx[i] : L.sy[i], stage, mode, b);
 }
 
 void launch_sweep(const LaunchSet& L, int axis, int stage, int mode, const Bind& b) {
@@ -799,6 +826,9 @@ LaunchSet plan_launch_set(hitb200_plan* p, cudaStream_t st) {
   L.fused = p->tuning[HITB200_TUNE_FUSED_SENSOR] && p->fuse_ok;
   L.smem_x = p->smem_x;
   L.smem_y = p->tuning[HITB200_TUNE_Y_PANEL] && p->Ry2 != p->Ry ? p->smem_y2 : p->smem_y;
+  L.sx[0] = {L.xl, L.n_x, L.mch_x, L.smem_x};
+  L.sy[0] = {L.yl, L.n_y, L.mch_y, L.smem_y};
+  L.nsx = L.nsy = 1;
   L.smem_sensor = p->smem_sensor;
   L.gen = p->has_gen ? &p->gen : nullptr;
   L.gen_out = p->has_gen ? const_cast<double*>(p->hs.noise) : nullptr;
@@ -846,6 +876,26 @@ void prime_attributes(int elem, int mch_x, int mch_y, size_t smem_x, size_t smem
     if (sensor_w == 4) set_step_sensor_attr<double, 4>(smem_sensor_step);
     if (sensor_w == 3) set_step_sensor_attr<double, 3>(smem_sensor_step);
   }
+}
+
+// Shared-memory opt-in of one sweep instantiation family (both variants).
+void prime_sweep_attr(int elem, int axis, int mch, size_t bytes) {
+#define HB_ATTR1(TT, M)                          \
+  if (mch == M) {                                \
+    if (axis == 0) {                             \
+      set_sweep_attr<TT, 0, M, 0>(bytes);        \
+      set_sweep_attr<TT, 0, M, 1>(bytes);        \
+    } else {                                     \
+      set_sweep_attr<TT, 1, M, 0>(bytes);        \
+      set_sweep_attr<TT, 1, M, 1>(bytes);        \
+    }                                            \
+  }
+  if (elem == 4) {
+    HB_ATTR1(float, 1) HB_ATTR1(float, 2) HB_ATTR1(float, 4) HB_ATTR1(float, 8)
+  } else {
+    HB_ATTR1(double, 1) HB_ATTR1(double, 2) HB_ATTR1(double, 4) HB_ATTR1(double, 8)
+  }
+#undef HB_ATTR1
 }
 
 int validate_desc(const hitb200_desc* d) {
@@ -1841,6 +1891,9 @@ static int batch_build(hitb200_batch* b) {
     int maxn = 0;
     for (hitb200_plan* p : b->plans) maxn = std::max(maxn, std::max(p->desc.nx, p->desc.ny));
     b->can_persist = b->elem == 4 && b->sensor_w == 4 && maxn <= 512 && b->mch_x == b->mch_y;
+    // one nodes-per-thread class: the stage kernel's sweeps run with one
+    for (hitb200_plan* p : b->plans)
+      if (mch_for(p->desc.nx) != b->mch_x || mch_for(p->desc.ny) != b->mch_y) b->can_persist = false;
   }
   if (b->can_persist) {
     std::vector<int> ox{0}, oy{0};
@@ -1885,6 +1938,33 @@ static int batch_build(hitb200_batch* b) {
     b->q_off[3] = (int)qi.size();
   }
   b->has_y2 = has_y2;
+  std::vector<Work> sw;  // the sweep lists in segments
+  for (int g = 0; g < 3; ++g) {
+    const int g0 = g == 2 ? b->cut : 0, g1 = g == 1 ? b->cut : n;
+    for (int li = 0; li < 3; ++li) {
+      const std::vector<Work>& src = li == 0 ? xl : (li == 1 ? yl : yl2);
+      const std::vector<int>& off = li == 0 ? b->off_xl : (li == 1 ? b->off_yl : b->off_yl2);
+      for (int c = 0; c < 4; ++c) {
+        hitb200_batch::SegRec& r = b->segs[g][li][c];
+        r.off = (int)sw.size();
+        r.smem = 0;
+        if (li < 2 || has_y2)
+          for (int i = g0; i < g1; ++i) {
+            const hitb200_plan* p = b->plans[i];
+            if (mch_for(li == 0 ? p->desc.nx : p->desc.ny) != (1 << c)) continue;
+            sw.insert(sw.end(), src.begin() + off[i], src.begin() + off[i + 1]);
+            size_t by = p->smem_x;
+            if (li > 0) {
+              const int ry = li == 1 ? (ry4 ? 4 : p->Ry) : (ry4 ? p->Ry : 4);
+              by = p->elem == 4 ? SweepLayout<float>(p->desc.ny, ry).bytes()
+                                : SweepLayout<double>(p->desc.ny, ry).bytes();
+            }
+            r.smem = std::max(r.smem, by);
+          }
+        r.n = (int)sw.size() - r.off;
+      }
+    }
+  }
   b->n_y2 = (int)yl2.size();
   if (b->any_noise_upload) return invalid("batched solves draw forcing noise with the device RNG (noise_mode 1)");
   b->n_tiles = (int)tiles.size();
@@ -1899,7 +1979,7 @@ static int batch_build(hitb200_batch* b) {
                  (tiles.size() + tiles32.size() + xl.size() + yl.size() + yl2.size() + sr.size() + xl4.size() +
                   yl4.size()) * sizeof(Work) +
                  partner.size() * sizeof(int) + qi.size() * sizeof(QItem) + qctl0.size() * sizeof(QCtl) +
-                 qdep0.size() * sizeof(unsigned) + 1024 + 13 * 256;
+                 qdep0.size() * sizeof(unsigned) + sw.size() * sizeof(Work) + 1024 + 14 * 256;
   cudaError_t e = block_alloc(bytes, &b->tables);
   if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(batch tables)");
   unsigned char* buf = static_cast<unsigned char*>(b->tables.ptr);
@@ -1919,6 +1999,7 @@ static int batch_build(hitb200_batch* b) {
   b->d_ylines2 = yl2.empty() ? nullptr : reinterpret_cast<Work*>(put(yl2.data(), yl2.size() * sizeof(Work)));
   b->d_srows = reinterpret_cast<Work*>(put(sr.data(), sr.size() * sizeof(Work)));
   b->d_partner = reinterpret_cast<int*>(put(partner.data(), partner.size() * sizeof(int)));
+  b->d_segs = reinterpret_cast<Work*>(put(sw.data(), sw.size() * sizeof(Work)));
   if (b->can_persist) {
     b->d_xl4 = reinterpret_cast<Work*>(put(xl4.data(), xl4.size() * sizeof(Work)));
     b->d_yl4 = reinterpret_cast<Work*>(put(yl4.data(), yl4.size() * sizeof(Work)));
@@ -1930,6 +2011,9 @@ static int batch_build(hitb200_batch* b) {
   if (b->sensor_w < 0) b->smem_sensor_step = 0;
   prime_attributes(b->elem, b->mch_x, b->mch_y, b->smem_x, std::max(b->smem_y, b->smem_y2), b->smem_sensor, b->sensor_w,
                    b->smem_sensor_step);
+  for (int li = 0; li < 3; ++li)
+    for (int c = 0; c < 4; ++c)
+      if (b->segs[0][li][c].n > 0) prime_sweep_attr(b->elem, li == 0 ? 0 : 1, 1 << c, b->segs[0][li][c].smem);
   if (b->can_persist) {
     // CTAs of a stage launch: as many as are resident at once
     int dev = 0, sms = 148, nb = 0;
@@ -2078,6 +2162,18 @@ int hitb200_batch_step_profile(hitb200_batch* b, float* ms, double* bytes, int32
   return finish_profile(pr, ms, bytes, cap, count, names, names_size);
 }
 
+// The sweep segments of launch group g (see hitb200_batch::segs).
+static void batch_segs(LaunchSet& L, const hitb200_batch* b, int g) {
+  const bool y2 = b->tuning[HITB200_TUNE_Y_PANEL] && b->has_y2;
+  L.nsx = L.nsy = 0;
+  for (int c = 0; c < 4; ++c) {
+    const hitb200_batch::SegRec& rx = b->segs[g][0][c];
+    if (rx.n > 0) L.sx[L.nsx++] = {b->d_segs + rx.off, rx.n, 1 << c, rx.smem};
+    const hitb200_batch::SegRec& ry = b->segs[g][y2 ? 2 : 1][c];
+    if (ry.n > 0) L.sy[L.nsy++] = {b->d_segs + ry.off, ry.n, 1 << c, ry.smem};
+  }
+}
+
 static LaunchSet batch_launch_set(hitb200_batch* b, cudaStream_t st) {
   LaunchSet L;
   L.solves = b->d_solves;
@@ -2117,6 +2213,7 @@ static LaunchSet batch_launch_set(hitb200_batch* b, cudaStream_t st) {
   L.sensor_w = b->sensor_w;
   L.smem_sensor_step = b->smem_sensor_step;
   L.st = st;
+  batch_segs(L, b, 0);
   L.persist = b->tuning[HITB200_TUNE_PERSISTENT] && b->can_persist;
   if (b->can_persist) {
     L.qitems = b->d_qitems + b->q_off[0];
@@ -2172,6 +2269,7 @@ static LaunchSet batch_sub_set(hitb200_batch* b, cudaStream_t st, int s0, int s1
   // the whole table); noise_rng takes the members from solve0 by CTA
   L.solve0 = s0;
   L.nsolves = s1 - s0;
+  batch_segs(L, b, (s0 == 0 && s1 == (int)b->plans.size()) ? 0 : (s0 == 0 ? 1 : 2));
   if (b->can_persist) {
     const int g = (s0 == 0 && s1 == (int)b->plans.size()) ? 0 : (s0 == 0 ? 1 : 2);
     L.qitems = b->d_qitems + b->q_off[g];

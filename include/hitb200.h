@@ -408,6 +408,9 @@ int hitb200_batch_destroy(hitb200_batch* batch);
 hitb200_plan* hitb200_batch_plan(hitb200_batch* batch, int32_t i);
 /* Bind the state array of every solve (device pointers, kept until rebound). */
 int hitb200_batch_bind(hitb200_batch* batch, double* const* q);
+/* One step of every member.  Each member's sweeps run in a launch of its own
+ * nodes-per-thread class (the class its lines give it alone), so a member's
+ * results are bit for bit those of its solo run, in any mix. */
 int hitb200_batch_step(hitb200_batch* batch, void* stream);
 /* nsteps steps replayed from a graph captured at the first call on a stream:
  * the members in two halves (balanced by cells) on two branches of the graph,
@@ -440,9 +443,8 @@ int hitb200_batch_run(hitb200_batch* batch, int32_t nsteps, void* stream);
  * stage's prepass, sensor, y-sweep and x-sweep work of every member taken
  * from one queue, each item waiting (bounded) only for its own solve's
  * previous phase.  Applies to FP32-bulk batches whose members all have
- * sensor width 4, grid lines of at most 512 nodes, and longest x and y lines
- * in the same class (up to 128, 256 or 512 nodes); elsewhere (and for single
- * plans) it reads back 0.  Off by default; the
+ * sensor width 4 and whose x and y lines all fall in one class (up to 128,
+ * 256 or 512 nodes); elsewhere (and for single plans) it reads back 0.  Off by default; the
  * autotuner keeps it where it measures faster.  Results are bit-identical
  * either way. */
 #define HITB200_TUNE_PERSISTENT 5

@@ -119,7 +119,9 @@ def _uneven_members():
     that are not multiples of 4 (the last x group / y panel of a member holds
     fewer than 4 lines): production HIT (viscous, forced, drag, cooling,
     hyperviscosity every 5 steps) and Riemann configurations 3 and 6
-    (outflow edges, guard cells, hyperviscosity every step)."""
+    (outflow edges, guard cells, hyperviscosity every step); all lines of at
+    most 128 nodes (one nodes-per-thread class, as the persistent form
+    requires)."""
     from hit_solver_b200.hit2d import HITSolver
     from hit_solver_b200.problems.riemann import RiemannConfig3, RiemannConfig6, RiemannSolver
 
@@ -134,7 +136,7 @@ def _uneven_members():
         out.append(HITSolver(dataclasses.replace(cfg, nx=nx, ny=ny)))
     out.append(RiemannSolver(RiemannConfig3(nx=37, ny=29, x_split=0.45, y_split=0.55, precision="fp32-bulk")))
     out.append(RiemannSolver(RiemannConfig6(nx=50, ny=66, precision="fp32-bulk")))
-    out.append(RiemannSolver(RiemannConfig3(nx=160, ny=144, precision="fp32-bulk")))
+    out.append(RiemannSolver(RiemannConfig3(nx=120, ny=100, precision="fp32-bulk")))
     return out
 
 
@@ -173,8 +175,8 @@ def test_persistent_stage_matches_per_phase_launches(steps):
 @pytest.mark.gpu
 def test_persistent_stage_not_available_reads_back_zero():
     """The persistent form needs FP32-bulk members of sensor width 4, lines
-    of at most 512 nodes and longest x and y lines in the same class (the
-    sweeps' nodes per thread); elsewhere the knob reads 0."""
+    of at most 512 nodes and all lines in one nodes-per-thread class of the
+    sweeps; elsewhere the knob reads 0."""
     from hit_solver_b200.problems.riemann import RiemannConfig3, RiemannSolver
 
     cases = [
@@ -182,6 +184,8 @@ def test_persistent_stage_not_available_reads_back_zero():
         [serving.make_solver(serving.Request(0, "riemann3", 640), "fp32-bulk")],
         [RiemannSolver(RiemannConfig3(nx=200, ny=64, precision="fp32-bulk"))],
         [RiemannSolver(RiemannConfig3(nx=64, ny=64, sensor_width=3, precision="fp32-bulk"))],
+        [serving.make_solver(serving.Request(0, "riemann3", 64), "fp32-bulk"),
+         serving.make_solver(serving.Request(1, "riemann3", 200), "fp32-bulk")],
     ]
     for sv in cases:
         b = Batch.from_plans([s.plan for s in sv], [s.q for s in sv])

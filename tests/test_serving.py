@@ -127,3 +127,37 @@ def test_checkpoint_restore_resumes_bit_for_bit(kind):
     torch.cuda.synchronize()
     assert torch.equal(resumed.q, straight.q)
     assert resumed.plan.scalars() == straight.plan.scalars()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("mode", ["run", "step"])
+def test_mixed_line_classes_match_solo_runs(mode):
+    """Members whose grid lines fall in different nodes-per-thread classes of
+    the sweeps (up to 128, 256, 512 and 1024 nodes; one member with x and y
+    lines in different classes) keep the bits of their solo runs: a batch
+    launches each class's sweeps separately, with the class a member has
+    alone."""
+    from hit_solver_b200.batch import Batch
+    from hit_solver_b200.problems.riemann import RiemannConfig3, RiemannSolver
+
+    def members():
+        return [serving.make_solver(serving.Request(0, "hit", 64, seed=2, mach=0.25, steps=10 ** 6),
+                                    "fp32-bulk"),
+                serving.make_solver(serving.Request(1, "riemann3", 200, split=0.45), "fp32-bulk"),
+                RiemannSolver(RiemannConfig3(nx=320, ny=96, precision="fp32-bulk")),
+                serving.make_solver(serving.Request(3, "riemann6", 640, split=0.6), "fp32-bulk")]
+
+    sv = members()
+    b = Batch.from_plans([s.plan for s in sv], [s.q for s in sv])
+    if mode == "run":
+        b.run(5)
+    else:
+        for _ in range(5):
+            b.step()
+    torch.cuda.synchronize()
+    got = [s.q.clone() for s in sv]
+    b.close()
+    for i, ref in enumerate(members()):
+        ref.advance(5)
+        torch.cuda.synchronize()
+        assert torch.equal(got[i], ref.q), f"member {i} differs from its solo run"
