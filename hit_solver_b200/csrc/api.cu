@@ -1810,6 +1810,17 @@ static int batch_build(hitb200_batch* b) {
                                      : SweepLayout<double>(p->desc.ny, 4).bytes();
       if (by > 110 * 1024 || p->desc.nx < 4) has_y2 = false;
     }
+  // row chunks of the forcing synthesis per CTA: enough CTAs for about four
+  // per SM, at most 8 chunks each (a chunk alone is a short CTA whose fixed
+  // costs, barriers and the ticket, dominate)
+  int synth_group = 1;
+  {
+    int dev = 0, sms = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    long chunks = 0;
+    for (hitb200_plan* p : b->plans) chunks += (p->desc.ny + synth_rows(p->desc.nx) - 1) / synth_rows(p->desc.nx);
+    synth_group = (int)std::max(1L, std::min(8L, chunks / (4L * sms)));
+  }
   std::vector<Work> yl2;
   b->off_yl2.clear();
   b->ry_max2 = 1;
@@ -1846,8 +1857,12 @@ static int batch_build(hitb200_batch* b) {
       b->smem_y2 = std::max(b->smem_y2, p->elem == 4 ? SweepLayout<float>(p->desc.ny, ry2).bytes()
                                                        : SweepLayout<double>(p->desc.ny, ry2).bytes());
     }
+    // forcing synthesis: synth_group consecutive row chunks per CTA (each
+    // with its own partial row, so the grouping changes no result)
     const int srows = synth_rows(p->desc.nx);
-    for (int r0 = 0, ks = 0; r0 < p->desc.ny; r0 += srows) sr.push_back({i, 0, r0, ks++});
+    const int nchk = (p->desc.ny + srows - 1) / srows;
+    for (int k0 = 0; k0 < nchk; k0 += synth_group)
+      sr.push_back({i, std::min(synth_group, nchk - k0), k0 * srows, k0});
     ModeTables mt = build_modes(p->desc);
     partner.insert(partner.end(), mt.partner.begin(), mt.partner.end());
     b->elem = p->elem;

@@ -673,8 +673,11 @@ __global__ void noise_rng_kernel(const SolveDev* __restrict__ solves, int nsolve
 // Forcing synthesis: f_hat = (i ky phi, -i kx phi), fx = Re ifft2 (forcing.py:
 // 82-85) evaluated directly on the shell modes, plus the sums the rescaling
 // needs (forcing.py:87-118), then the scalar rescaling logic.  The synthesis
-// is separable: each CTA covers whole rows (about 1024 cells, synth_rows),
-// and for each of its rows y the modes are first folded into
+// is separable: each CTA covers whole rows, in chunks of about 1024 cells
+// (synth_rows; w.a chunks from row w.b, at least one), each with its own row
+// of partial sums (w.c, w.c + 1, ...), so that how chunks are grouped into
+// CTAs changes no result; for each of a chunk's rows y the modes are first
+// folded into
 // P_k(y) = sum over modes with |kx| = k of c_m e^{i ky y} (conjugated for
 // kx < 0), so that a cell needs only Re sum_k P_k(y) e^{i k x}, k = 0..max|kx|.
 __global__ void __launch_bounds__(kRedThreads)
@@ -709,8 +712,11 @@ __global__ void __launch_bounds__(kRedThreads)
   for (int k = threadIdx.x; k < K + 2; k += blockDim.x) kofs[k] = S.f_kofs[k];
   __syncthreads();
   const double2* __restrict__ twy = S.twy;
-  // this CTA: rows w.b .. w.b + rows - 1, every column
-  const int rows = min(synth_rows(nx), ny - w.b);
+  const int nch = w.a > 1 ? w.a : 1;
+  for (int ch = 0; ch < nch; ++ch) {
+  // this chunk: rows r0 .. r0 + rows - 1, every column
+  const int r0 = w.b + ch * synth_rows(nx);
+  const int rows = min(synth_rows(nx), ny - r0);
   // row tables in chunks of rows: one thread per (row, mode) term into shared
   // memory (the twiddle loads all in flight at once), then each (row, |kx|)
   // sum over its modes in mode order
@@ -721,7 +727,7 @@ __global__ void __launch_bounds__(kRedThreads)
     for (int t = threadIdx.x; t < na * nf; t += blockDim.x) {
       const int aa = t / nf, j = t - aa * nf;
       const int2 md = mk[j];
-      const double2 e = twy[mode_index(md.y, w.b + a0 + aa, ny)];  // e^{-i ky y}
+      const double2 e = twy[mode_index(md.y, r0 + a0 + aa, ny)];  // e^{-i ky y}
       const double er = e.x, ei = -e.y;                             // e^{+i ky y}
       double ar = ca[j].x * er - ca[j].y * ei, ai = ca[j].x * ei + ca[j].y * er;
       double br = cb[j].x * er - cb[j].y * ei, bi = cb[j].x * ei + cb[j].y * er;
@@ -750,7 +756,7 @@ __global__ void __launch_bounds__(kRedThreads)
   }
   double sxx = 0, syy = 0, sxy = 0, spow = 0;
   for (int idx = threadIdx.x; idx < rows * nx; idx += blockDim.x) {
-    const int a = idx / nx, gi = idx - a * nx, gj = w.b + a;
+    const int a = idx / nx, gi = idx - a * nx, gj = r0 + a;
     double fx = px[a][0].x, fy = py[a][0].x;
     int ix = 0;
     for (int k = 1; k <= K; ++k) {
@@ -780,9 +786,22 @@ __global__ void __launch_bounds__(kRedThreads)
   if (threadIdx.x < 4) {
     double acc = sm[threadIdx.x];
     for (int ww = 1; ww < kRedWarps; ++ww) acc += sm[ww * 4 + threadIdx.x];
-    S.part_synth[(size_t)w.c * 4 + threadIdx.x] = acc;
+    S.part_synth[(size_t)(w.c + ch) * 4 + threadIdx.x] = acc;
   }
-  if (!last_block(&S.counters[2], S.nblk_synth)) return;
+  __syncthreads();  // sm, px, py reused by the next chunk
+  }
+  // ticket over chunks: the CTA finishing the solve's last ones reduces them
+  __shared__ bool s_last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const unsigned t = atomicAdd(&S.counters[2], (unsigned)nch);
+    s_last = t + (unsigned)nch == (unsigned)S.nblk_synth;
+    if (s_last) S.counters[2] = 0u;
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
   {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     if (warp < 4) {
