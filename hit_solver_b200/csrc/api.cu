@@ -435,6 +435,9 @@ struct LaunchSet {
   };
   SweepSeg sx[4] = {}, sy[4] = {};
   int nsx = 0, nsy = 0;
+  // batches: the hyperviscosity chain as grid-stride loops over a few CTAs
+  // per SM (hv_sms: the SM count; 0 for single plans, one CTA per tile)
+  int hv_sms = 0;
   QCtl* qctl = nullptr;
   unsigned* qdep = nullptr;
   const Work *qtiles = nullptr, *xl4 = nullptr, *yl4 = nullptr;  // whole-batch lists
@@ -542,6 +545,7 @@ void set_step_sensor_attr(size_t bytes) {
   std::lock_guard<std::mutex> lock(g_attr_mu);
   if (bytes > done[dev]) {
     cudaFuncSetAttribute(sensor_step_kernel<T, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    cudaFuncSetAttribute(hv_sensor_loop_kernel<T, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
     done[dev] = bytes;
   }
 }
@@ -669,8 +673,28 @@ const void* stage_fn(int mch) {
 }
 
 void launch_hv(const LaunchSet& L, const Bind& b) {
-  if (L.elem == 4) launch_k(hv_kernel<float>, L.n_tiles, kStencilThreads, 0, L, L.solves, L.tiles, b);
-  else launch_k(hv_kernel<double>, L.n_tiles, kStencilThreads, 0, L, L.solves, L.tiles, b);
+  const int grid = L.hv_sms > 0 ? std::max(1, std::min(L.n_tiles, 4 * L.hv_sms)) : L.n_tiles;
+  if (L.elem == 4) launch_k(hv_kernel<float>, grid, kStencilThreads, 0, L, L.solves, L.tiles, L.n_tiles, b);
+  else launch_k(hv_kernel<double>, grid, kStencilThreads, 0, L, L.solves, L.tiles, L.n_tiles, b);
+}
+
+// The hyperviscosity prepass and sensor of a batch as grid-stride loops
+// (hv_prepass_loop_kernel, hv_sensor_loop_kernel).
+void launch_hv_prepass_loop(const LaunchSet& L) {
+  const int grid = std::max(1, std::min(L.n_tiles32, 4 * L.hv_sms));
+  if (L.elem == 4) hv_prepass_loop_kernel<float><<<grid, kPreThreads, 0, L.st>>>(L.solves, L.tiles32, L.n_tiles32);
+  else hv_prepass_loop_kernel<double><<<grid, kPreThreads, 0, L.st>>>(L.solves, L.tiles32, L.n_tiles32);
+}
+void launch_hv_sensor_loop(const LaunchSet& L) {
+  const int grid = std::max(1, std::min(L.n_tiles32, 2 * L.hv_sms));
+  const size_t sm = L.smem_sensor_step;
+  if (L.elem == 4) {
+    if (L.sensor_w == 4) hv_sensor_loop_kernel<float, 4><<<grid, kSensorThreads, sm, L.st>>>(L.solves, L.tiles32, L.n_tiles32);
+    else hv_sensor_loop_kernel<float, 3><<<grid, kSensorThreads, sm, L.st>>>(L.solves, L.tiles32, L.n_tiles32);
+  } else {
+    if (L.sensor_w == 4) hv_sensor_loop_kernel<double, 4><<<grid, kSensorThreads, sm, L.st>>>(L.solves, L.tiles32, L.n_tiles32);
+    else hv_sensor_loop_kernel<double, 3><<<grid, kSensorThreads, sm, L.st>>>(L.solves, L.tiles32, L.n_tiles32);
+  }
 }
 void launch_prepass(const LaunchSet& L, int buf, int mode, int enf, const Bind& b) {
 #define HB_PRE(TT, O) \
@@ -757,6 +781,11 @@ int launch_step_sequence(const LaunchSet& L, int any_forcing, int noise_upload, 
     if (L.fused) {
       PMARK("hv_presensor", 65 * N);
       launch_presensor(L, 3);
+    } else if (L.hv_sms > 0 && (L.sensor_w == 3 || L.sensor_w == 4)) {
+      PMARK("hv_prepass", 32 * N);
+      launch_hv_prepass_loop(L);
+      PMARK("hv_sensor", 33 * N);
+      launch_hv_sensor_loop(L);
     } else {
       PMARK("hv_prepass", 32 * N);
       launch_prepass(L, 1, PRE_SENSOR, 0, nb);
@@ -2229,6 +2258,11 @@ static LaunchSet batch_launch_set(hitb200_batch* b, cudaStream_t st) {
   L.smem_sensor_step = b->smem_sensor_step;
   L.st = st;
   batch_segs(L, b, 0);
+  {
+    int dev = 0, sms = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    L.hv_sms = sms;
+  }
   L.persist = b->tuning[HITB200_TUNE_PERSISTENT] && b->can_persist;
   if (b->can_persist) {
     L.qitems = b->d_qitems + b->q_off[0];

@@ -540,6 +540,35 @@ __global__ void __launch_bounds__(kPreThreads, OCC ? HITB200_PRE_MIN_BLOCKS : 2)
   }
 }
 
+// The hyperviscosity prepass of a batch (PRE_SENSOR on q1) as a grid-stride
+// loop over its tiles: on the steps without hyperviscosity every tile is a
+// no-op, and a grid of a few CTAs per SM costs a small fraction of one CTA
+// per tile.  Each tile runs prepass_kernel's code with its own partial row
+// and ticket, so the results are those of prepass_kernel.
+template <typename T>
+__global__ void __launch_bounds__(kPreThreads, HITB200_PRE_MIN_BLOCKS)
+    hv_prepass_loop_kernel(const SolveDev* __restrict__ solves, const Work* __restrict__ work, int nwork) {
+  __shared__ PreShared<T> ps;
+  __shared__ double red[R_FIXED + 4 * kMaxDrag];
+  __shared__ double chunk[kPreThreads];
+  const Bind nb{};
+  for (int item = blockIdx.x; item < nwork; item += gridDim.x) {
+    const Work w = work[item];
+    const SolveDev& S = solves[w.solve];
+    double* sc = S.scal;
+    if (sc[S_HV_STEP] == 0.0) continue;  // no hyperviscosity this step
+    const int nslots = prepass_tile<T>(S, w, 1, PRE_SENSOR, 0, nb, true, ps);
+    if (last_block(&S.counters[0], S.nblk_pre)) {
+      prepass_finalize(S, nslots, red, chunk);
+      if (threadIdx.x == 0) {
+        prepass_scalars(S, red, sc, PRE_SENSOR, false);
+        if (atomicExch(&S.counters[6], 0u)) sc[S_STATUS] = (double)((int)sc[S_STATUS] | ST_BARRIER);
+      }
+    }
+    __syncthreads();  // shared memory reused by the next tile
+  }
+}
+
 // Forward transform of the caller's white-noise field restricted to the
 // forcing shell (the masked fft2 of OOP/forcing.py:77-79), then the OU update
 // of the potential (forcing.py:80).

@@ -1652,16 +1652,22 @@ __global__ void __launch_bounds__(AXIS == 0 ? 256 : 512,
 // (OOP/spatial_operator.py:394-435 periodic; riemann_config3.py:390-416 with
 // an edge-padded Laplacian, applied to the padded Laplacian again).
 // =============================================================================
+// The CTAs take the tiles work[0 .. nwork) in a grid-stride loop: single
+// plans launch one CTA per tile; batches launch a few CTAs per SM, so that
+// the steps without hyperviscosity, whose tiles are all no-ops, cost a small
+// fraction of one CTA per tile.
 template <typename T>
 __global__ void __launch_bounds__(kStencilThreads)
-    hv_kernel(const SolveDev* __restrict__ solves, const Work* __restrict__ work, Bind bind) {
+    hv_kernel(const SolveDev* __restrict__ solves, const Work* __restrict__ work, int nwork, Bind bind) {
   constexpr int QX = kHvTX + 4, QY = kHvTY + 4, LX = kHvTX + 2, LY = kHvTY + 2;
   __shared__ T Qs[4][QY][QX];
   __shared__ T Ls[4][LY][LX];
-  const Work wk = work[blockIdx.x];
+  for (int item = blockIdx.x; item < nwork; item += gridDim.x) {
+  if (item > (int)blockIdx.x) __syncthreads();  // shared memory of the previous tile
+  const Work wk = work[item];
   const SolveDev& S = solves[wk.solve];
   // the hyperviscosity flag is written by the step's first kernel
-  if (!bind.use && S.scal[S_HV_STEP] == 0.0) return;
+  if (!bind.use && S.scal[S_HV_STEP] == 0.0) continue;
   const double* q = bind.use ? bind.qin : S.q1;
   double* out = bind.use ? bind.qout : S.q;
   const uint8_t* mask = bind.use ? bind.mask : S.mask;
@@ -1746,6 +1752,7 @@ __global__ void __launch_bounds__(kStencilThreads)
 #pragma unroll
         for (int c = 0; c < 4; ++c) out[c * plane + od] = s[c];
       }
+  }
   }
 }
 

@@ -404,4 +404,17 @@ __global__ void __launch_bounds__(kSensorThreads, sizeof(T) == 8 ? 1 : HITB200_S
   sensor_step_body<T, W>(solves, work[blockIdx.x], sel, enf, want_visc, smem, PdlDep{});
 }
 
+// The hyperviscosity sensor of a batch (sel 3) as a grid-stride loop over its
+// tiles (see hv_prepass_loop_kernel): the same tiles and results as
+// sensor_step_kernel's.
+template <typename T, int W>
+__global__ void __launch_bounds__(kSensorThreads, sizeof(T) == 8 ? 1 : HITB200_SENSOR_MIN_BLOCKS)
+    hv_sensor_loop_kernel(const SolveDev* __restrict__ solves, const Work* __restrict__ work, int nwork) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  for (int item = blockIdx.x; item < nwork; item += gridDim.x) {
+    sensor_step_body<T, W>(solves, work[item], 3, 0, 0, smem, PdlDep{});
+    __syncthreads();  // shared memory reused by the next tile
+  }
+}
+
 }  // namespace hitb200
