@@ -40,6 +40,17 @@ def test_binding_covers_header():
     assert set(declared_symbols()) <= bound
 
 
+def test_tuning_knob_indices_match_header():
+    """The binding's tuning-knob indices (and their count, which bounds the
+    knob arrays passed to hitb200_*_set_tuning) are the header's."""
+    text = (ROOT / "include" / "hitb200.h").read_text()
+    defs = dict(re.findall(r"#define HITB200_TUNE_([A-Z_]+) (\d+)", text))
+    assert {k: int(v) for k, v in defs.items()} == {
+        "SWEEP_X": _lib.TUNE_SWEEP_X, "SWEEP_Y": _lib.TUNE_SWEEP_Y, "PREPASS": _lib.TUNE_PREPASS,
+        "FUSED_SENSOR": _lib.TUNE_FUSED_SENSOR, "Y_PANEL": _lib.TUNE_Y_PANEL,
+        "PERSISTENT": _lib.TUNE_PERSISTENT, "COUNT": _lib.TUNE_COUNT}
+
+
 def test_desc_layout_and_defaults(lib):
     assert lib.hitb200_desc_size() == ctypes.sizeof(_lib.Desc)
     d = _lib.default_desc()
